@@ -1,0 +1,327 @@
+"""Generate the golden fixtures in this folder by running the reference's own CPU path.
+
+The reference (ahnobari/EDGE-TO) is pure Python + Numba.  Its package root imports
+cupy, cupyx, scikit-sparse, matplotlib, vtk and k3d at import time
+(EDGETO/__init__.py:4-10), none of which exist in this image, so this script
+injects inert stand-in modules for those names before importing it.  Nothing in the
+reference is copied or modified; only its CPU classes are exercised:
+``StructuredMesh2D/3D`` (geom/_mesh.py:19-78), ``StructuredStiffnessKernel``
+(kernels/_processors.py:46-155), ``StructuredFilter2D/3D`` (geom/_filters.py:72-161),
+``MultiGrid`` (solvers/_multigrid.py:11-230), the MG transfer/Galerkin kernels
+(core/_mgm.py), ``SingleMaterial`` (MaterialModels.py:31-99) and ``TopOpt``
+(TopOpt/_solver.py:17-417).
+
+Run from the repository root with the reference checked out at REFERENCE_ROOT:
+
+    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py [--only NAME]
+
+Outputs (all small .npz files, committed):
+  kat_stiffness.npz   element stiffness matrices (Q4 / hex8, several nu and box sizes)
+  ops_2d.npz, ops_3d.npz   op-level cases: matvec (with/without BCs), diagonal, dk,
+                      filter / filter transpose, restriction / prolongation,
+                      Galerkin level-1 and level-2 operators, OC update
+  loop_mbb2d.npz      120x40 MBB half-beam, 100 SIMP iterations, MG-PCG rtol 1e-8
+  loop_cant3d.npz     64x32x32 cantilever, first SIMP iterations, 4-level MG rtol 1e-6
+  grad_cant3d.npz     32x16x16 cantilever, random rho, compliance and filtered dr
+"""
+import argparse
+import os
+import sys
+import time
+import types
+from unittest import mock
+
+import numpy as np
+
+REFERENCE_ROOT = os.environ.get("EDGETO_REFERENCE", "/root/reference")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _import_reference():
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache")
+    os.environ.setdefault("NUMBA_NUM_THREADS", str(os.cpu_count() or 1))
+    for name in ["cupy", "cupyx", "cupyx.scipy", "cupyx.scipy.sparse", "cupyx.scipy.sparse.linalg",
+                 "sksparse", "sksparse.cholmod", "matplotlib", "matplotlib.pyplot", "matplotlib.path",
+                 "matplotlib.collections", "matplotlib.colors", "matplotlib.cm", "vtk", "k3d", "pygmsh",
+                 "vtk.util", "vtk.util.numpy_support"]:
+        sys.modules.setdefault(name, mock.MagicMock(name=name))
+    sys.path.insert(0, REFERENCE_ROOT)
+    import EDGETO  # noqa: F401
+    from EDGETO.geom._mesh import StructuredMesh2D, StructuredMesh3D
+    from EDGETO.kernels._processors import StructuredStiffnessKernel
+    from EDGETO.geom._filters import StructuredFilter2D, StructuredFilter3D
+    from EDGETO.solvers._multigrid import MultiGrid
+    from EDGETO.MaterialModels import SingleMaterial
+    from EDGETO.TopOpt._solver import TopOpt
+    from EDGETO.physics._linelas import auto_stiffness
+    from EDGETO.core import _mgm
+    ns = types.SimpleNamespace(**locals())
+    return ns
+
+
+def _stiff(nu):
+    ref = _REF
+
+    def f(x0):
+        return ref.auto_stiffness(x0, 1.0, nu)
+    return f
+
+
+def make_kat():
+    ref = _REF
+    out = {}
+    q = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], dtype=np.float64)
+    for nu in (0.3, 0.33):
+        K, D, B, A = ref.auto_stiffness(q, 1.0, nu)
+        out[f"q4_nu{nu}"] = K
+        out[f"q4_nu{nu}_area"] = np.array(A)
+    q2 = np.array([[0, 0], [0.5, 0], [0.5, 0.25], [0, 0.25]], dtype=np.float64)
+    out["q4_box_0.5x0.25_nu0.3"] = ref.auto_stiffness(q2, 1.0, 0.3)[0]
+    h = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                  [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=np.float64)
+    for nu in (0.3, 0.33):
+        K, D, B, A = ref.auto_stiffness(h, 1.0, nu)
+        out[f"hex8_nu{nu}"] = K
+        out[f"hex8_nu{nu}_volume"] = np.array(A)
+    hb = h * np.array([0.5, 0.25, 1.0])
+    out["hex8_box_0.5x0.25x1_nu0.3"] = ref.auto_stiffness(hb, 1.0, 0.3)[0]
+    np.savez_compressed(os.path.join(HERE, "kat_stiffness.npz"), **out)
+
+
+def _random_constraints(rng, n_nodes, dof, frac=0.15):
+    cons = np.zeros(n_nodes * dof, dtype=bool)
+    full = rng.choice(n_nodes, size=max(1, int(frac * n_nodes)), replace=False)
+    for d in range(dof):
+        cons[full * dof + d] = True
+    single = rng.choice(n_nodes * dof, size=max(1, int(frac * n_nodes)), replace=False)
+    cons[single] = True
+    return np.where(cons)[0]
+
+
+def _ops_case(out, tag, mesh, rng, rmins, with_galerkin=True):
+    ref = _REF
+    dof = mesh.dof
+    nel = mesh.elements.shape[0]
+    n_nodes = mesh.nodes.shape[0]
+    E = rng.uniform(1e-3, 1.0, nel)
+    E[rng.choice(nel, size=max(1, nel // 5), replace=False)] = 1e-9
+    u = rng.standard_normal(n_nodes * dof)
+    out[f"{tag}_E"] = E
+    out[f"{tag}_u"] = u
+    out[f"{tag}_nel"] = mesh.nel.copy()
+    k = ref.StructuredStiffnessKernel(mesh)
+    k.set_rho(E)
+    out[f"{tag}_matvec_nocon"] = k.dot(u).copy()
+    cons = _random_constraints(rng, n_nodes, dof)
+    k.add_constraints(cons)
+    out[f"{tag}_cons"] = cons
+    out[f"{tag}_matvec"] = k.dot(u).copy()
+    out[f"{tag}_diag"] = k.diagonal().copy()
+    out[f"{tag}_dk"] = k.process_grad(u).copy()
+    for r in rmins:
+        filt = (ref.StructuredFilter3D(mesh, r) if dof == 3 else ref.StructuredFilter2D(mesh, r))
+        rho = rng.uniform(0.0, 1.0, nel)
+        out[f"{tag}_filt{r}_in"] = rho
+        out[f"{tag}_filt{r}_H"] = filt.dot(rho)
+        out[f"{tag}_filt{r}_HT"] = filt._rmatvec(rho)
+        out[f"{tag}_filt{r}_ntaps"] = np.array(len(filt.weights))
+    v = rng.standard_normal(n_nodes * dof)
+    out[f"{tag}_restrict_in"] = v
+    out[f"{tag}_restrict"] = ref._mgm.apply_restriction(v, mesh.nel.astype(np.int32), dof)
+    nel_c = mesh.nel // 2
+    n_coarse = int(np.prod(nel_c + 1))
+    vc = rng.standard_normal(n_coarse * dof)
+    out[f"{tag}_prolong_in"] = vc
+    out[f"{tag}_prolong"] = ref._mgm.apply_prolongation(vc, mesh.nel.astype(np.int32), dof)
+    if with_galerkin:
+        solver = ref.MultiGrid(mesh, k, n_level=2, tol=1e-8)
+        solver._setup()
+        A1 = solver.levels[1][0]
+        A2 = solver.levels[2][0]
+        out[f"{tag}_A1"] = A1.toarray()
+        out[f"{tag}_A2"] = A2.toarray()
+        out[f"{tag}_D1inv"] = np.asarray(solver.levels[1][1])
+        out[f"{tag}_D0inv"] = np.asarray(solver.levels[0][1])
+        del solver.levels
+
+
+def _oc_case(out, tag, mesh, rng):
+    ref = _REF
+    mat = ref.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=0.4)
+    k = ref.StructuredStiffnessKernel(mesh)
+    solver = ref.MultiGrid(mesh, k, n_level=1, tol=1e-8)
+    filt = ref.StructuredFilter3D(mesh, 1.5) if mesh.dof == 3 else ref.StructuredFilter2D(mesh, 1.5)
+    opt = ref.TopOpt(mesh, mat, k, solver, filt, max_iter=1, move=0.2, verbose=False)
+    nel = mesh.elements.shape[0]
+    rho = rng.uniform(0.05, 0.95, nel)
+    df = -rng.uniform(0.0, 10.0, nel) ** 2
+    df[rng.choice(nel, size=nel // 10, replace=False)] = 0.0
+    out[f"{tag}_oc_rho"] = rho
+    out[f"{tag}_oc_df"] = df
+    out[f"{tag}_oc_vf"] = np.array(0.4)
+    out[f"{tag}_oc_out"] = opt.update_design(rho.copy(), df.reshape(-1, 1).copy())
+
+
+def make_ops():
+    ref = _REF
+    rng = np.random.default_rng(20240601)
+    out = {}
+    m = ref.StructuredMesh2D(8, 4, 8.0, 4.0, stiffness=_stiff(0.3))
+    _ops_case(out, "even", m, rng, (1.5, 2.0, 3.0))
+    _oc_case(out, "even", m, rng)
+    m = ref.StructuredMesh2D(7, 5, 7.0, 5.0, stiffness=_stiff(0.3))
+    _ops_case(out, "odd", m, rng, (1.5, 2.5), with_galerkin=False)
+    m = ref.StructuredMesh2D(6, 4, 3.0, 1.0, stiffness=_stiff(0.3))
+    _ops_case(out, "aniso", m, rng, (1.5,), with_galerkin=False)
+    np.savez_compressed(os.path.join(HERE, "ops_2d.npz"), **out)
+
+    out = {}
+    m = ref.StructuredMesh3D(4, 4, 4, 4.0, 4.0, 4.0, stiffness=_stiff(0.3))
+    _ops_case(out, "even", m, rng, (1.5, 2.0))
+    _oc_case(out, "even", m, rng)
+    m = ref.StructuredMesh3D(5, 3, 3, 5.0, 3.0, 3.0, stiffness=_stiff(0.3))
+    _ops_case(out, "odd", m, rng, (1.5,), with_galerkin=False)
+    m = ref.StructuredMesh3D(4, 2, 2, 2.0, 0.5, 1.0, stiffness=_stiff(0.3))
+    _ops_case(out, "aniso", m, rng, (1.5,), with_galerkin=False)
+    np.savez_compressed(os.path.join(HERE, "ops_3d.npz"), **out)
+
+
+class _Recorder:
+    """Wraps solver.solve to record the residual and the number of fine matvecs per solve."""
+
+    def __init__(self, solver, kernel):
+        self.solver = solver
+        self.kernel = kernel
+        self.residuals = []
+        self.matvecs = []
+        self._count = 0
+        orig_dot = kernel.dot
+
+        def counting_dot(rhs):
+            self._count += 1
+            return orig_dot(rhs)
+        kernel.dot = counting_dot
+        orig_solve = solver.solve
+
+        def recording_solve(*a, **kw):
+            self._count = 0
+            x, res = orig_solve(*a, **kw)
+            self.residuals.append(float(res))
+            self.matvecs.append(self._count)
+            return x, res
+        solver.solve = recording_solve
+
+
+def _run_loop(mesh, vf, rmin, rho0, n_iter, mg_kwargs, bc_fn, f_fn):
+    ref = _REF
+    mat = ref.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=vf)
+    mat.init_desvars = lambda nel, **kw: np.full(nel, rho0, dtype=np.float64)
+    k = ref.StructuredStiffnessKernel(mesh)
+    filt = ref.StructuredFilter3D(mesh, rmin) if mesh.dof == 3 else ref.StructuredFilter2D(mesh, rmin)
+    solver = ref.MultiGrid(mesh, k, **mg_kwargs)
+    rec = _Recorder(solver, k)
+    opt = ref.TopOpt(mesh, mat, k, solver, filt, max_iter=n_iter, move=0.2, ch_tol=0.0, fun_tol=0.0,
+                     verbose=False)
+    bc_nodes, bc_vals = bc_fn(mesh)
+    opt.add_BC_nodal(bc_nodes, bc_vals)
+    f_nodes, f_vals = f_fn(mesh)
+    opt.add_F_nodal(f_nodes, f_vals)
+    t0 = time.time()
+    rho, flag, hist = opt.optimize(save_comp_history=True, save_change_history=True, save_rho_history=True)
+    dt = time.time() - t0
+    out = {
+        "rho_final": rho,
+        "comp_history": np.array(hist["comp_history"]),
+        "change_history": np.array(hist["change_history"]),
+        "residuals": np.array(rec.residuals),
+        "matvecs_per_solve": np.array(rec.matvecs),
+        "rho_1": hist["rho_history"][0],
+        "f_idx": np.nonzero(opt.f)[0],
+        "f_val": opt.f[np.nonzero(opt.f)[0]],
+        "constraints": np.where(k.constraints)[0],
+        "wall_s": np.array(dt),
+    }
+    return out
+
+
+def make_loop_mbb():
+    ref = _REF
+    mesh = ref.StructuredMesh2D(120, 40, 120.0, 40.0, stiffness=_stiff(0.3))
+
+    def bc(mesh):
+        nodes = mesh.nodes
+        left = np.where(np.isclose(nodes[:, 0], 0.0))[0]
+        br = np.where(np.isclose(nodes[:, 0], 120.0) & np.isclose(nodes[:, 1], 0.0))[0]
+        ids = np.concatenate([left, br])
+        vals = np.zeros((ids.shape[0], 2), dtype=bool)
+        vals[: left.shape[0], 0] = True
+        vals[left.shape[0]:, 1] = True
+        return ids, vals
+
+    def force(mesh):
+        nodes = mesh.nodes
+        tl = np.where(np.isclose(nodes[:, 0], 0.0) & np.isclose(nodes[:, 1], 40.0))[0]
+        return tl, np.array([[0.0, -1.0]])
+
+    out = _run_loop(mesh, 0.5, 1.5, 0.5, 100, dict(tol=1e-8, n_level=3, maxiter=1000), bc, force)
+    np.savez_compressed(os.path.join(HERE, "loop_mbb2d.npz"), **out)
+    print("mbb2d: comp", out["comp_history"][0], "->", out["comp_history"][-1], "wall", out["wall_s"])
+
+
+def _cant_bc_force(L):
+    def bc(mesh):
+        nodes = mesh.nodes
+        ids = np.where(np.isclose(nodes[:, 0], 0.0))[0]
+        return ids, np.array([[True, True, True]])
+
+    def force(mesh):
+        nodes = mesh.nodes
+        ids = np.where(np.isclose(nodes[:, 0], L) & np.isclose(nodes[:, 1], 0.0))[0]
+        return ids, np.array([[0.0, -1.0, 0.0]]) / ids.shape[0]
+    return bc, force
+
+
+def make_loop_cant3d():
+    ref = _REF
+    mesh = ref.StructuredMesh3D(64, 32, 32, 64.0, 32.0, 32.0, stiffness=_stiff(0.3))
+    bc, force = _cant_bc_force(64.0)
+    out = _run_loop(mesh, 0.12, 1.5, 0.12, 4, dict(tol=1e-6, n_level=4, maxiter=1000), bc, force)
+    np.savez_compressed(os.path.join(HERE, "loop_cant3d.npz"), **out)
+    print("cant3d: comp", out["comp_history"], "wall", out["wall_s"])
+
+
+def make_grad():
+    ref = _REF
+    mesh = ref.StructuredMesh3D(32, 16, 16, 32.0, 16.0, 16.0, stiffness=_stiff(0.3))
+    bc, force = _cant_bc_force(32.0)
+    rng = np.random.default_rng(7)
+    rho = rng.uniform(0.2, 1.0, mesh.elements.shape[0])
+    mat = ref.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=0.3)
+    k = ref.StructuredStiffnessKernel(mesh)
+    filt = ref.StructuredFilter3D(mesh, 2.0)
+    solver = ref.MultiGrid(mesh, k, tol=1e-10, n_level=3, maxiter=2000)
+    opt = ref.TopOpt(mesh, mat, k, solver, filt, max_iter=1, verbose=False)
+    ids, vals = bc(mesh)
+    opt.add_BC_nodal(ids, vals)
+    ids, vals = force(mesh)
+    opt.add_F_nodal(ids, vals)
+    comp, dr, res = opt.solve_and_process(rho, 0)
+    np.savez_compressed(os.path.join(HERE, "grad_cant3d.npz"), rho=rho, compliance=np.array(comp),
+                        dr=dr.reshape(-1), residual=np.array(res), f=opt.f.copy())
+    print("grad: comp", comp, "res", res)
+
+
+_REF = None
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    _REF = _import_reference()
+    jobs = {"kat": make_kat, "ops": make_ops, "mbb": make_loop_mbb, "cant": make_loop_cant3d, "grad": make_grad}
+    for name, fn in jobs.items():
+        if args.only and name not in args.only.split(","):
+            continue
+        t0 = time.time()
+        fn()
+        print(f"[{name}] done in {time.time() - t0:.1f}s", flush=True)

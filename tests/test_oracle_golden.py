@@ -1,0 +1,147 @@
+"""Pin the CPU oracle against fixtures produced by the reference's own CPU code.
+
+The reference has no tests or golden files; tests/golden/make_golden.py ran its CPU
+classes (kernels/_processors.py, geom/_filters.py, core/_mgm.py, solvers/_multigrid.py,
+TopOpt/_solver.py) to produce them.  Everything here runs on the CPU.
+"""
+import numpy as np
+import pytest
+
+from oracle import elements, ops, topopt
+from oracle.grid import Grid
+
+H_OF = {2: {"even": None, "odd": None, "aniso": (0.5, 0.25)},
+        3: {"even": None, "odd": None, "aniso": (0.5, 0.25, 0.5)}}
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300))
+
+
+def test_element_stiffness_kat(golden):
+    kat = golden("kat_stiffness.npz")
+    for nu in (0.3, 0.33):
+        assert rel(elements.q4_stiffness(1, 1, 1, nu), kat[f"q4_nu{nu}"]) < 1e-14
+        assert rel(elements.hex8_stiffness(1, 1, 1, 1, nu), kat[f"hex8_nu{nu}"]) < 1e-14
+    assert rel(elements.q4_stiffness(0.5, 0.25, 1, 0.3), kat["q4_box_0.5x0.25_nu0.3"]) < 1e-14
+    assert rel(elements.hex8_stiffness(0.5, 0.25, 1, 1, 0.3), kat["hex8_box_0.5x0.25x1_nu0.3"]) < 1e-14
+    # hex8 K0[0,0] at nu=0.3 and symmetry / rigid-body null space
+    K = elements.hex8_stiffness(1, 1, 1, 1, 0.3)
+    assert abs(K[0, 0] - 0.23504273504273504) < 1e-15
+    assert np.abs(K - K.T).max() < 1e-15
+    assert np.abs(K.sum(axis=1)).max() < 1e-14
+
+
+def _cases(golden):
+    for dim, fn in ((2, "ops_2d.npz"), (3, "ops_3d.npz")):
+        z = golden(fn)
+        for tag in ("even", "odd", "aniso"):
+            g = Grid(tuple(z[f"{tag}_nel"]), H_OF[dim][tag])
+            K0 = elements.q4_stiffness(*g.h, 1, 0.3) if dim == 2 else elements.hex8_stiffness(*g.h, 1, 0.3)
+            yield dim, tag, z, g, K0
+
+
+def test_stiffness_ops(golden):
+    for dim, tag, z, g, K0 in _cases(golden):
+        E, u, cons = z[f"{tag}_E"], z[f"{tag}_u"], z[f"{tag}_cons"]
+        Kc = ops.assemble(g, K0, E, cons)
+        assert rel(ops.assemble(g, K0, E) @ u, z[f"{tag}_matvec_nocon"]) < 1e-13, (dim, tag)
+        assert rel(Kc @ u, z[f"{tag}_matvec"]) < 1e-13, (dim, tag)
+        assert rel(ops.diagonal(Kc), z[f"{tag}_diag"]) < 1e-13, (dim, tag)
+        assert rel(ops.dk(g, K0, u), z[f"{tag}_dk"]) < 1e-13, (dim, tag)
+        cm = np.zeros(g.n_dof, dtype=bool)
+        cm[cons] = True
+        assert rel(ops.matvec_free(g, K0, E, u, cm), z[f"{tag}_matvec"]) < 1e-13, (dim, tag)
+
+
+def test_filter(golden):
+    n = 0
+    for dim, tag, z, g, K0 in _cases(golden):
+        for k in z.files:
+            if k.startswith(f"{tag}_filt") and k.endswith("_in"):
+                r = float(k[len(tag) + 5:-3])
+                H, N = ops.filter_matrix(g, r)
+                x = z[k]
+                assert rel(H @ x, z[f"{tag}_filt{r}_H"]) < 1e-13
+                assert rel(H.T @ x, z[f"{tag}_filt{r}_HT"]) < 1e-13
+                assert len(ops.filter_stencil(g, r)[1]) == int(z[f"{tag}_filt{r}_ntaps"])
+                n += 1
+    assert n >= 8
+
+
+def test_transfer_and_galerkin(golden):
+    for dim, tag, z, g, K0 in _cases(golden):
+        R = ops.restriction_matrix(g, "cpu")
+        assert rel(R @ z[f"{tag}_restrict_in"], z[f"{tag}_restrict"]) < 1e-13
+        assert rel(ops.prolongation_matrix(g) @ z[f"{tag}_prolong_in"], z[f"{tag}_prolong"]) < 1e-13
+        if dim == 3:  # CPU and GPU restriction agree in 3-D
+            assert rel(ops.restriction_matrix(g, "gpu") @ z[f"{tag}_restrict_in"], z[f"{tag}_restrict"]) < 1e-13
+        if f"{tag}_A1" in z.files:
+            Kc = ops.assemble(g, K0, z[f"{tag}_E"], z[f"{tag}_cons"])
+            A1 = ops.galerkin(Kc, g)
+            A2 = ops.galerkin(A1, g.coarse())
+            assert rel(A1.toarray(), z[f"{tag}_A1"]) < 1e-13
+            assert rel(A2.toarray(), z[f"{tag}_A2"]) < 1e-13
+            assert rel(1.0 / A1.diagonal(), z[f"{tag}_D1inv"]) < 1e-13
+
+
+def test_gpu_restriction_is_twice_cpu_in_2d_interior(golden):
+    g = Grid((8, 4))
+    Rg = ops.restriction_matrix(g, "gpu").toarray()
+    Rc = ops.restriction_matrix(g, "cpu").toarray()
+    assert np.allclose(Rg, 2 * Rc)
+
+
+def test_oc_update(golden):
+    for dim, fn in ((2, "ops_2d.npz"), (3, "ops_3d.npz")):
+        z = golden(fn)
+        g = Grid(tuple(z["even_nel"]))
+        A = elements.element_measure(g.h)
+        rn, lam, steps = topopt.oc_update(z["even_oc_rho"], z["even_oc_df"], A, A * g.n_el, 0.4, 0.2)
+        assert np.array_equal(rn, z["even_oc_out"].reshape(-1))
+        assert 30 <= steps <= 60
+
+
+@pytest.mark.slow
+def test_mbb_trajectory_cpu_semantics(golden):
+    """The oracle in the reference CPU solver's semantics retraces its 100 iterations."""
+    z = golden("loop_mbb2d.npz")
+    p = topopt.mbb_problem(mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=1000, variant="cpu"), vf=0.5, rmin=1.5)
+    assert np.array_equal(np.nonzero(p.f)[0], z["f_idx"])
+    assert np.array_equal(p.cons, z["constraints"])
+    rho, h = p.optimize(0.5, 100)
+    c = np.array(h["comp"])
+    assert np.abs(c - z["comp_history"]).max() / c.min() < 1e-8
+    assert np.abs(rho - z["rho_final"]).max() < 1e-6
+    # fine matvecs per solve: 8 per PCG iteration + 1 initial residual
+    assert list(8 * np.array(p.solver.pcg_iters[:5]) + 1) == list(z["matvecs_per_solve"][:5])
+
+
+def test_mbb_trajectory_gpu_semantics(golden):
+    """GPU-solver semantics (omega reset, GPU restriction) reach the same designs."""
+    z = golden("loop_mbb2d.npz")
+    p = topopt.mbb_problem(mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=1000, variant="gpu"), vf=0.5, rmin=1.5)
+    rho, h = p.optimize(0.5, 100)
+    c = np.array(h["comp"])
+    assert np.abs(c - z["comp_history"]).max() / c.min() < 1e-6
+    assert np.abs(rho - z["rho_final"]).max() < 1e-5
+
+
+def test_cantilever_first_iterations(golden):
+    z = golden("loop_cant3d.npz")
+    p = topopt.cantilever_problem(64, 32, 32, vf=0.12, rmin=1.5,
+                                  mg_kwargs=dict(tol=1e-6, n_level=4, maxiter=1000, variant="cpu"))
+    assert np.array_equal(p.cons, z["constraints"])
+    assert np.array_equal(np.nonzero(p.f)[0], z["f_idx"])
+    rho, h = p.optimize(0.12, len(z["comp_history"]))
+    c = np.array(h["comp"])
+    assert np.abs(c - z["comp_history"]).max() / c.min() < 1e-6
+
+
+def test_gradient_random_rho(golden):
+    z = golden("grad_cant3d.npz")
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, rmin=2.0,
+                                  mg_kwargs=dict(tol=1e-10, n_level=3, maxiter=2000, variant="gpu"))
+    comp, dr, res, U = p.solve_and_process(z["rho"])
+    assert abs(comp - float(z["compliance"])) / comp < 1e-8
+    assert rel(dr, z["dr"]) < 1e-7
