@@ -1,0 +1,714 @@
+// Coarse levels of the geometric multigrid.
+//
+// Level l >= 1 operators are stored as compact stencils: for every coarse node the
+// 3^d neighbour blocks of dof x dof coefficients, coefficient-major
+// (S[(nb*dof*dof + c*dof + d)*n + slot]) so that one thread per node reads them
+// coalesced.  nb = (dz+1) + 3(dx+1) + 9(dy+1) in 3-D and (dx+1) + 3(dy+1) in 2-D.
+// This replaces the reference's fixed-81/18-nnz CSR (core/_mgm_cuda.py:69-221) with the
+// same values and no index arrays.
+//
+// Transfers restate restriction_{2d,3d}_kernel / prolongation_{2d,3d}_kernel
+// (core/_templated_cuda.cu:232-475): full weighting 1, 1/2, 1/4, 1/8 by Manhattan
+// distance, divided by the coarse node's boundary total (8, 6, 4.5, 3.375 in 3-D;
+// 4, 3, 2.25 in 2-D); prolongation divides each parent's value by its total and
+// averages over the in-range parents.
+//
+// Galerkin operators restate get_restricted_{3d,2d}_l0_nnz_based and _l1p_nnz_based
+// (core/_mgm_cuda.cu:1-649): A_{l+1} = R A_l R^T with R as above on both sides; level 1
+// is formed from E, K0 and the BC mask with constrained fine DOFs contributing the
+// identity.  Here level 1 is gathered per (coarse node, neighbour) from the fine
+// elements whose coarse cube holds both nodes: an element with lower corner 2m+s
+// (per axis) maps its corners onto the coarse cube {m, m+1} with weights
+// P_s = [[1,0],[1/2,1/2]] (s=0) or [[1/2,1/2],[0,1]] (s=1), so its contribution is
+// E_e * (P_s^T K0 P_s), eight 24x24 tables computed once on the host; elements that
+// touch a constrained DOF are projected with their masked K0 directly.
+#pragma once
+#include "common.cuh"
+#include "fine_apply.cuh"
+
+namespace edge {
+
+EDGE_HD double bnd_total3(int nb) { return nb == 3 ? 3.375 : nb == 2 ? 4.5 : nb == 1 ? 6.0 : 8.0; }
+EDGE_HD double bnd_total2(int nb) { return nb == 2 ? 2.25 : nb == 1 ? 3.0 : 4.0; }
+EDGE_HD double dist_w(int d) { return d == 0 ? 1.0 : d == 1 ? 0.5 : d == 2 ? 0.25 : 0.125; }
+EDGE_D int is_bnd(int i, int n) { return (i == 0 || i == n - 1) ? 1 : 0; }
+
+// ------------------------------------------------------------------ stencil apply (levels >= 1)
+template <typename T, typename TS, class Epi>
+__global__ void __launch_bounds__(128)
+k_st3_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
+            double* dot_dst) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y, j = blockIdx.z;
+  const long long n = g.n;
+  epi.init();
+  double dacc = 0.0;
+  if (k < g.nz) {
+    const long long s = g.slot3(i, j, k);
+    T Au[3] = {T(0), T(0), T(0)};
+#pragma unroll 1
+    for (int dy = -1; dy <= 1; ++dy) {
+      if (j + dy < 0 || j + dy >= g.ny) continue;
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        if (i + dx < 0 || i + dx >= g.nx) continue;
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz) {
+          if (k + dz < 0 || k + dz >= g.nz) continue;
+          const int nb = (dz + 1) + 3 * (dx + 1) + 9 * (dy + 1);
+          const long long sn = s + dy * g.plane + dx * g.pz + dz;
+          const T u0 = __ldg(u + sn), u1 = __ldg(u + n + sn), u2 = __ldg(u + 2 * n + sn);
+          const TS* Sb = S + (long long)nb * 9 * n + s;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            Au[c] += Conv<T>::from(__ldg(Sb + (c * 3 + 0) * n)) * u0 + Conv<T>::from(__ldg(Sb + (c * 3 + 1) * n)) * u1 +
+                     Conv<T>::from(__ldg(Sb + (c * 3 + 2) * n)) * u2;
+          }
+        }
+      }
+    }
+    T own[3] = {__ldg(u + s), __ldg(u + n + s), __ldg(u + 2 * n + s)};
+    epi(s, 3, own, Au, dacc);
+  }
+  finish_dot(epi, dacc, part, ticket, dot_dst);
+}
+
+template <typename T, typename TS, class Epi>
+__global__ void __launch_bounds__(128)
+k_st2_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
+            double* dot_dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const long long n = g.n;
+  epi.init();
+  double dacc = 0.0;
+  if (i < g.nx) {
+    const long long s = g.slot2(i, j);
+    T Au[2] = {T(0), T(0)};
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      if (j + dy < 0 || j + dy >= g.ny) continue;
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        if (i + dx < 0 || i + dx >= g.nx) continue;
+        const int nb = (dx + 1) + 3 * (dy + 1);
+        const long long sn = s + dy * g.pz + dx;
+        const T u0 = __ldg(u + sn), u1 = __ldg(u + n + sn);
+        const TS* Sb = S + (long long)nb * 4 * n + s;
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+          Au[c] += Conv<T>::from(__ldg(Sb + (c * 2 + 0) * n)) * u0 + Conv<T>::from(__ldg(Sb + (c * 2 + 1) * n)) * u1;
+      }
+    }
+    T own[2] = {__ldg(u + s), __ldg(u + n + s)};
+    epi(s, 2, own, Au, dacc);
+  }
+  finish_dot(epi, dacc, part, ticket, dot_dst);
+}
+
+// Dinv of a stencil level: 1 / centre-block diagonal.
+template <typename TS, typename TD>
+__global__ void k_st_dinv(const Geo g, const TS* __restrict__ S, TD* __restrict__ dinv) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  const int dof = g.dof;
+  const int centre = g.dim == 3 ? 13 : 4;
+  for (int c = 0; c < dof; ++c) {
+    const double v = (double)Conv<double>::from(S[((long long)centre * dof * dof + c * dof + c) * g.n + s]);
+    dinv[c * g.n + s] = Conv<TD>::from(v != 0.0 ? 1.0 / v : 0.0);
+  }
+}
+
+// ------------------------------------------------------------------ transfers
+template <typename TI, typename TO>
+__global__ void k_restrict3(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  const int K = blockIdx.x * blockDim.x + threadIdx.x;
+  const int I = blockIdx.y, J = blockIdx.z;
+  if (K >= gc.nz) return;
+  const int nb = is_bnd(I, gc.nx) + is_bnd(J, gc.ny) + is_bnd(K, gc.nz);
+  const double W = bnd_total3(nb);
+  double v[3] = {0, 0, 0};
+  for (int di = -1; di <= 1; ++di) {
+    const int fi = 2 * I + di;
+    if (fi < 0 || fi >= gf.nx) continue;
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int fj = 2 * J + dj;
+      if (fj < 0 || fj >= gf.ny) continue;
+      for (int dk = -1; dk <= 1; ++dk) {
+        const int fk = 2 * K + dk;
+        if (fk < 0 || fk >= gf.nz) continue;
+        const double w = dist_w(abs(di) + abs(dj) + abs(dk));
+        const long long sf = gf.slot3(fi, fj, fk);
+        for (int c = 0; c < 3; ++c) v[c] += w * (double)Conv<double>::from(in[c * gf.n + sf]);
+      }
+    }
+  }
+  const long long sc = gc.slot3(I, J, K);
+  for (int c = 0; c < 3; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] / W);
+}
+
+template <typename TI, typename TO>
+__global__ void k_restrict2(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  const int J = blockIdx.y;
+  if (I >= gc.nx) return;
+  const double W = bnd_total2(is_bnd(I, gc.nx) + is_bnd(J, gc.ny));
+  double v[2] = {0, 0};
+  for (int di = -1; di <= 1; ++di) {
+    const int fi = 2 * I + di;
+    if (fi < 0 || fi >= gf.nx) continue;
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int fj = 2 * J + dj;
+      if (fj < 0 || fj >= gf.ny) continue;
+      const double w = dist_w(abs(di) + abs(dj));
+      const long long sf = gf.slot2(fi, fj);
+      for (int c = 0; c < 2; ++c) v[c] += w * (double)Conv<double>::from(in[c * gf.n + sf]);
+    }
+  }
+  const long long sc = gc.slot2(I, J);
+  for (int c = 0; c < 2; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] / W);
+}
+
+template <typename TI, typename TO>
+__global__ void k_prolong3(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y, j = blockIdx.z;
+  if (k >= gf.nz) return;
+  double v[3] = {0, 0, 0};
+  int cnt = 0;
+  for (int ci = i / 2; ci <= i / 2 + (i & 1); ++ci) {
+    if (ci >= gc.nx) continue;
+    for (int cj = j / 2; cj <= j / 2 + (j & 1); ++cj) {
+      if (cj >= gc.ny) continue;
+      for (int ck = k / 2; ck <= k / 2 + (k & 1); ++ck) {
+        if (ck >= gc.nz) continue;
+        const double W = bnd_total3(is_bnd(ci, gc.nx) + is_bnd(cj, gc.ny) + is_bnd(ck, gc.nz));
+        const long long sc = gc.slot3(ci, cj, ck);
+        for (int c = 0; c < 3; ++c) v[c] += (double)Conv<double>::from(in[c * gc.n + sc]) / W;
+        ++cnt;
+      }
+    }
+  }
+  const long long sf = gf.slot3(i, j, k);
+  for (int c = 0; c < 3; ++c) out[c * gf.n + sf] = Conv<TO>::from(cnt ? v[c] / cnt : 0.0);
+}
+
+template <typename TI, typename TO>
+__global__ void k_prolong2(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= gf.nx) return;
+  double v[2] = {0, 0};
+  int cnt = 0;
+  for (int ci = i / 2; ci <= i / 2 + (i & 1); ++ci) {
+    if (ci >= gc.nx) continue;
+    for (int cj = j / 2; cj <= j / 2 + (j & 1); ++cj) {
+      if (cj >= gc.ny) continue;
+      const double W = bnd_total2(is_bnd(ci, gc.nx) + is_bnd(cj, gc.ny));
+      const long long sc = gc.slot2(ci, cj);
+      for (int c = 0; c < 2; ++c) v[c] += (double)Conv<double>::from(in[c * gc.n + sc]) / W;
+      ++cnt;
+    }
+  }
+  const long long sf = gf.slot2(i, j);
+  for (int c = 0; c < 2; ++c) out[c * gf.n + sf] = Conv<TO>::from(cnt ? v[c] / cnt : 0.0);
+}
+
+// ------------------------------------------------------------------ Galerkin, level 0 -> 1
+// Element constraint flags: flag[slot(e)] = 1 if any corner DOF of element e is constrained.
+__global__ void k_elem_flags(const Geo g, const uint8_t* __restrict__ mask, uint8_t* __restrict__ flag) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  uint8_t f = 0;
+  if (g.dim == 3) {
+    const int k = (int)(s % g.pz), i = (int)((s / g.pz) % g.nx), j = (int)(s / g.plane);
+    if (k < g.nz - 1 && i < g.nx - 1 && j < g.ny - 1)
+      for (int b = 0; b < 8; ++b) f |= mask[g.slot3(i + (b & 1), j + ((b >> 1) & 1), k + ((b >> 2) & 1))];
+  } else {
+    const int i = (int)(s % g.pz), j = (int)(s / g.pz);
+    if (i < g.nx - 1 && j < g.ny - 1)
+      for (int b = 0; b < 4; ++b) f |= mask[g.slot2(i + (b & 1), j + ((b >> 1) & 1))];
+  }
+  flag[s] = f ? 1 : 0;
+}
+
+EDGE_D double pw(int s, int a, int c) {  // 1-D corner weight P_s[a][c]
+  return s == 0 ? (a == 0 ? (c == 0 ? 1.0 : 0.0) : 0.5) : (a == 0 ? 0.5 : (c == 1 ? 1.0 : 0.0));
+}
+
+// One thread per (coarse node, neighbour nb = blockIdx.y).  Q: 8 parity tables [s][24][24]
+// (bit-order corners), K0b: dense element matrix in bit order.
+template <typename TE, typename TS>
+__global__ void __launch_bounds__(128)
+k_galerkin3_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
+               const uint8_t* __restrict__ eflag, const double* __restrict__ Q, const double* __restrict__ K0b,
+               TS* __restrict__ S) {
+  const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nb = blockIdx.y;
+  if (sc >= gc.n) return;
+  const int Kz = (int)(sc % gc.pz), Ix = (int)((sc / gc.pz) % gc.nx), Jy = (int)(sc / gc.plane);
+  const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
+  double V[9];
+  for (int q = 0; q < 9; ++q) V[q] = 0.0;
+  const int I[3] = {Ix, Jy, Kz};
+  const int Jn[3] = {Ix + dx, Jy + dy, Kz + dz};
+  const int ncn[3] = {gc.nx, gc.ny, gc.nz};
+  const int nfn[3] = {gf.nx, gf.ny, gf.nz};
+  bool valid = Kz < gc.nz;
+  for (int d = 0; d < 3; ++d) valid = valid && Jn[d] >= 0 && Jn[d] < ncn[d];
+  if (valid) {
+    // elements: per axis m in [max(I,J)-1, min(I,J)], parity s in {0,1}
+    int mlo[3], mhi[3];
+    for (int d = 0; d < 3; ++d) {
+      mlo[d] = max(I[d], Jn[d]) - 1;
+      mhi[d] = min(I[d], Jn[d]);
+    }
+    for (int my = mlo[1]; my <= mhi[1]; ++my)
+      for (int sy = 0; sy < 2; ++sy) {
+        const int ly = 2 * my + sy;
+        if (ly < 0 || ly >= nfn[1] - 1) continue;
+        for (int mx = mlo[0]; mx <= mhi[0]; ++mx)
+          for (int sx = 0; sx < 2; ++sx) {
+            const int lx = 2 * mx + sx;
+            if (lx < 0 || lx >= nfn[0] - 1) continue;
+            for (int mz = mlo[2]; mz <= mhi[2]; ++mz)
+              for (int sz = 0; sz < 2; ++sz) {
+                const int lz = 2 * mz + sz;
+                if (lz < 0 || lz >= nfn[2] - 1) continue;
+                const long long se = gf.slot3(lx, ly, lz);
+                const double Ee = (double)Conv<double>::from(E[se]);
+                const int cI = (I[0] - mx) | ((I[1] - my) << 1) | ((I[2] - mz) << 2);
+                const int cJ = (Jn[0] - mx) | ((Jn[1] - my) << 1) | ((Jn[2] - mz) << 2);
+                const int par = sx | (sy << 1) | (sz << 2);
+                if (!eflag[se]) {
+                  const double* Qs = Q + par * 576;
+                  for (int c = 0; c < 3; ++c)
+                    for (int d = 0; d < 3; ++d) V[c * 3 + d] += Ee * Qs[(cI * 3 + c) * 24 + cJ * 3 + d];
+                } else {
+                  const int sv[3] = {sx, sy, sz};
+                  for (int a = 0; a < 8; ++a) {
+                    double wa = 1.0;
+                    for (int d = 0; d < 3; ++d) wa *= pw(sv[d], (a >> d) & 1, (cI >> d) & 1);
+                    if (wa == 0.0) continue;
+                    const uint8_t ma = mask[gf.slot3(lx + (a & 1), ly + ((a >> 1) & 1), lz + ((a >> 2) & 1))];
+                    for (int b = 0; b < 8; ++b) {
+                      double wb = 1.0;
+                      for (int d = 0; d < 3; ++d) wb *= pw(sv[d], (b >> d) & 1, (cJ >> d) & 1);
+                      if (wb == 0.0) continue;
+                      const uint8_t mb = mask[gf.slot3(lx + (b & 1), ly + ((b >> 1) & 1), lz + ((b >> 2) & 1))];
+                      for (int c = 0; c < 3; ++c) {
+                        if ((ma >> c) & 1) continue;
+                        for (int d = 0; d < 3; ++d) {
+                          if ((mb >> d) & 1) continue;
+                          V[c * 3 + d] += Ee * wa * wb * K0b[(a * 3 + c) * 24 + b * 3 + d];
+                        }
+                      }
+                    }
+                  }
+                }
+              }
+          }
+      }
+    // identity rows/columns of constrained fine DOFs
+    int flo[3], fhi[3];
+    for (int d = 0; d < 3; ++d) {
+      flo[d] = max(max(2 * I[d], 2 * Jn[d]) - 1, 0);
+      fhi[d] = min(min(2 * I[d], 2 * Jn[d]) + 1, nfn[d] - 1);
+    }
+    for (int fy = flo[1]; fy <= fhi[1]; ++fy)
+      for (int fx = flo[0]; fx <= fhi[0]; ++fx)
+        for (int fz = flo[2]; fz <= fhi[2]; ++fz) {
+          const uint8_t m = mask[gf.slot3(fx, fy, fz)];
+          if (!m) continue;
+          const int f3[3] = {fx, fy, fz};
+          double w = 1.0;
+          for (int d = 0; d < 3; ++d) w *= (f3[d] == 2 * I[d] ? 1.0 : 0.5) * (f3[d] == 2 * Jn[d] ? 1.0 : 0.5);
+          for (int c = 0; c < 3; ++c)
+            if ((m >> c) & 1) V[c * 3 + c] += w;
+        }
+    const double WI = bnd_total3(is_bnd(I[0], ncn[0]) + is_bnd(I[1], ncn[1]) + is_bnd(I[2], ncn[2]));
+    const double WJ = bnd_total3(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]) + is_bnd(Jn[2], ncn[2]));
+    for (int q = 0; q < 9; ++q) V[q] = V[q] / WI / WJ;
+  }
+  for (int q = 0; q < 9; ++q) S[((long long)nb * 9 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+}
+
+template <typename TE, typename TS>
+__global__ void __launch_bounds__(128)
+k_galerkin2_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
+               const uint8_t* __restrict__ eflag, const double* __restrict__ Q, const double* __restrict__ K0b,
+               TS* __restrict__ S) {
+  const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nb = blockIdx.y;
+  if (sc >= gc.n) return;
+  const int Ix = (int)(sc % gc.pz), Jy = (int)(sc / gc.pz);
+  const int dx = nb % 3 - 1, dy = nb / 3 - 1;
+  double V[4] = {0, 0, 0, 0};
+  const int I[2] = {Ix, Jy};
+  const int Jn[2] = {Ix + dx, Jy + dy};
+  const int ncn[2] = {gc.nx, gc.ny};
+  const int nfn[2] = {gf.nx, gf.ny};
+  bool valid = Ix < gc.nx;
+  for (int d = 0; d < 2; ++d) valid = valid && Jn[d] >= 0 && Jn[d] < ncn[d];
+  if (valid) {
+    int mlo[2], mhi[2];
+    for (int d = 0; d < 2; ++d) {
+      mlo[d] = max(I[d], Jn[d]) - 1;
+      mhi[d] = min(I[d], Jn[d]);
+    }
+    for (int my = mlo[1]; my <= mhi[1]; ++my)
+      for (int sy = 0; sy < 2; ++sy) {
+        const int ly = 2 * my + sy;
+        if (ly < 0 || ly >= nfn[1] - 1) continue;
+        for (int mx = mlo[0]; mx <= mhi[0]; ++mx)
+          for (int sx = 0; sx < 2; ++sx) {
+            const int lx = 2 * mx + sx;
+            if (lx < 0 || lx >= nfn[0] - 1) continue;
+            const long long se = gf.slot2(lx, ly);
+            const double Ee = (double)Conv<double>::from(E[se]);
+            const int cI = (I[0] - mx) | ((I[1] - my) << 1);
+            const int cJ = (Jn[0] - mx) | ((Jn[1] - my) << 1);
+            const int par = sx | (sy << 1);
+            if (!eflag[se]) {
+              const double* Qs = Q + par * 64;
+              for (int c = 0; c < 2; ++c)
+                for (int d = 0; d < 2; ++d) V[c * 2 + d] += Ee * Qs[(cI * 2 + c) * 8 + cJ * 2 + d];
+            } else {
+              const int sv[2] = {sx, sy};
+              for (int a = 0; a < 4; ++a) {
+                double wa = 1.0;
+                for (int d = 0; d < 2; ++d) wa *= pw(sv[d], (a >> d) & 1, (cI >> d) & 1);
+                if (wa == 0.0) continue;
+                const uint8_t ma = mask[gf.slot2(lx + (a & 1), ly + ((a >> 1) & 1))];
+                for (int b = 0; b < 4; ++b) {
+                  double wb = 1.0;
+                  for (int d = 0; d < 2; ++d) wb *= pw(sv[d], (b >> d) & 1, (cJ >> d) & 1);
+                  if (wb == 0.0) continue;
+                  const uint8_t mb = mask[gf.slot2(lx + (b & 1), ly + ((b >> 1) & 1))];
+                  for (int c = 0; c < 2; ++c) {
+                    if ((ma >> c) & 1) continue;
+                    for (int d = 0; d < 2; ++d) {
+                      if ((mb >> d) & 1) continue;
+                      V[c * 2 + d] += Ee * wa * wb * K0b[(a * 2 + c) * 8 + b * 2 + d];
+                    }
+                  }
+                }
+              }
+            }
+          }
+      }
+    int flo[2], fhi[2];
+    for (int d = 0; d < 2; ++d) {
+      flo[d] = max(max(2 * I[d], 2 * Jn[d]) - 1, 0);
+      fhi[d] = min(min(2 * I[d], 2 * Jn[d]) + 1, nfn[d] - 1);
+    }
+    for (int fy = flo[1]; fy <= fhi[1]; ++fy)
+      for (int fx = flo[0]; fx <= fhi[0]; ++fx) {
+        const uint8_t m = mask[gf.slot2(fx, fy)];
+        if (!m) continue;
+        const int f2[2] = {fx, fy};
+        double w = 1.0;
+        for (int d = 0; d < 2; ++d) w *= (f2[d] == 2 * I[d] ? 1.0 : 0.5) * (f2[d] == 2 * Jn[d] ? 1.0 : 0.5);
+        for (int c = 0; c < 2; ++c)
+          if ((m >> c) & 1) V[c * 2 + c] += w;
+      }
+    const double WI = bnd_total2(is_bnd(I[0], ncn[0]) + is_bnd(I[1], ncn[1]));
+    const double WJ = bnd_total2(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]));
+    for (int q = 0; q < 4; ++q) V[q] = V[q] / WI / WJ;
+  }
+  for (int q = 0; q < 4; ++q) S[((long long)nb * 4 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+}
+
+// ------------------------------------------------------------------ Galerkin, stencil level l -> l+1
+template <typename TS>
+__global__ void __launch_bounds__(128)
+k_galerkin3_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __restrict__ Sc) {
+  const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nb = blockIdx.y;
+  if (sc >= gc.n) return;
+  const int Kz = (int)(sc % gc.pz), Ix = (int)((sc / gc.pz) % gc.nx), Jy = (int)(sc / gc.plane);
+  const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
+  const int I[3] = {Ix, Jy, Kz};
+  const int Jn[3] = {Ix + dx, Jy + dy, Kz + dz};
+  const int ncn[3] = {gc.nx, gc.ny, gc.nz};
+  const int nfn[3] = {gf.nx, gf.ny, gf.nz};
+  bool valid = Kz < gc.nz;
+  for (int d = 0; d < 3; ++d) valid = valid && Jn[d] >= 0 && Jn[d] < ncn[d];
+  double V[9];
+  for (int q = 0; q < 9; ++q) V[q] = 0.0;
+  if (valid) {
+    for (int iy = max(2 * I[1] - 1, 0); iy <= min(2 * I[1] + 1, nfn[1] - 1); ++iy)
+      for (int ix = max(2 * I[0] - 1, 0); ix <= min(2 * I[0] + 1, nfn[0] - 1); ++ix)
+        for (int iz = max(2 * I[2] - 1, 0); iz <= min(2 * I[2] + 1, nfn[2] - 1); ++iz) {
+          const double wi = dist_w(abs(ix - 2 * I[0]) + abs(iy - 2 * I[1]) + abs(iz - 2 * I[2]));
+          const long long si = gf.slot3(ix, iy, iz);
+          const int fi[3] = {ix, iy, iz};
+          int jlo[3], jhi[3];
+          for (int d = 0; d < 3; ++d) {
+            jlo[d] = max(max(2 * Jn[d] - 1, fi[d] - 1), 0);
+            jhi[d] = min(min(2 * Jn[d] + 1, fi[d] + 1), nfn[d] - 1);
+          }
+          for (int jy = jlo[1]; jy <= jhi[1]; ++jy)
+            for (int jx = jlo[0]; jx <= jhi[0]; ++jx)
+              for (int jz = jlo[2]; jz <= jhi[2]; ++jz) {
+                const double wj = dist_w(abs(jx - 2 * Jn[0]) + abs(jy - 2 * Jn[1]) + abs(jz - 2 * Jn[2]));
+                const int fnb = (jz - iz + 1) + 3 * (jx - ix + 1) + 9 * (jy - iy + 1);
+                const TS* A = Sf + (long long)fnb * 9 * gf.n + si;
+                const double w = wi * wj;
+                for (int q = 0; q < 9; ++q) V[q] += w * (double)Conv<double>::from(A[q * gf.n]);
+              }
+        }
+    const double WI = bnd_total3(is_bnd(I[0], ncn[0]) + is_bnd(I[1], ncn[1]) + is_bnd(I[2], ncn[2]));
+    const double WJ = bnd_total3(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]) + is_bnd(Jn[2], ncn[2]));
+    for (int q = 0; q < 9; ++q) V[q] = V[q] / WI / WJ;
+  }
+  for (int q = 0; q < 9; ++q) Sc[((long long)nb * 9 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+}
+
+template <typename TS>
+__global__ void __launch_bounds__(128)
+k_galerkin2_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __restrict__ Sc) {
+  const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nb = blockIdx.y;
+  if (sc >= gc.n) return;
+  const int Ix = (int)(sc % gc.pz), Jy = (int)(sc / gc.pz);
+  const int dx = nb % 3 - 1, dy = nb / 3 - 1;
+  const int I[2] = {Ix, Jy};
+  const int Jn[2] = {Ix + dx, Jy + dy};
+  const int ncn[2] = {gc.nx, gc.ny};
+  const int nfn[2] = {gf.nx, gf.ny};
+  bool valid = Ix < gc.nx;
+  for (int d = 0; d < 2; ++d) valid = valid && Jn[d] >= 0 && Jn[d] < ncn[d];
+  double V[4] = {0, 0, 0, 0};
+  if (valid) {
+    for (int iy = max(2 * I[1] - 1, 0); iy <= min(2 * I[1] + 1, nfn[1] - 1); ++iy)
+      for (int ix = max(2 * I[0] - 1, 0); ix <= min(2 * I[0] + 1, nfn[0] - 1); ++ix) {
+        const double wi = dist_w(abs(ix - 2 * I[0]) + abs(iy - 2 * I[1]));
+        const long long si = gf.slot2(ix, iy);
+        const int fi[2] = {ix, iy};
+        int jlo[2], jhi[2];
+        for (int d = 0; d < 2; ++d) {
+          jlo[d] = max(max(2 * Jn[d] - 1, fi[d] - 1), 0);
+          jhi[d] = min(min(2 * Jn[d] + 1, fi[d] + 1), nfn[d] - 1);
+        }
+        for (int jy = jlo[1]; jy <= jhi[1]; ++jy)
+          for (int jx = jlo[0]; jx <= jhi[0]; ++jx) {
+            const double wj = dist_w(abs(jx - 2 * Jn[0]) + abs(jy - 2 * Jn[1]));
+            const int fnb = (jx - ix + 1) + 3 * (jy - iy + 1);
+            const TS* A = Sf + (long long)fnb * 4 * gf.n + si;
+            const double w = wi * wj;
+            for (int q = 0; q < 4; ++q) V[q] += w * (double)Conv<double>::from(A[q * gf.n]);
+          }
+      }
+    const double WI = bnd_total2(is_bnd(I[0], ncn[0]) + is_bnd(I[1], ncn[1]));
+    const double WJ = bnd_total2(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]));
+    for (int q = 0; q < 4; ++q) V[q] = V[q] / WI / WJ;
+  }
+  for (int q = 0; q < 4; ++q) Sc[((long long)nb * 4 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+}
+
+// ------------------------------------------------------------------ coarsest level: dense FP64
+// Dense row-major A (nd x nd) from a stencil level; dense DOF index = node_index*dof + c with
+// node_index the unpadded lexicographic index (j, i, k) of the reference.
+template <typename TS>
+__global__ void k_st_to_dense(const Geo g, const TS* __restrict__ S, double* __restrict__ A, int nd) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  const int dof = g.dof;
+  int i, j, k = 0;
+  if (g.dim == 3) {
+    k = (int)(s % g.pz);
+    i = (int)((s / g.pz) % g.nx);
+    j = (int)(s / g.plane);
+    if (k >= g.nz) return;
+  } else {
+    i = (int)(s % g.pz);
+    j = (int)(s / g.pz);
+    if (i >= g.nx) return;
+  }
+  auto didx = [&](int ii, int jj, int kk) -> long long {
+    return g.dim == 3 ? ((long long)jj * g.nx * g.nz + (long long)ii * g.nz + kk) : ((long long)jj * g.nx + ii);
+  };
+  const long long row_node = didx(i, j, k);
+  const int nnb = g.dim == 3 ? 27 : 9;
+  for (int nb = 0; nb < nnb; ++nb) {
+    int di, dj, dk = 0;
+    if (g.dim == 3) {
+      dk = nb % 3 - 1;
+      di = (nb / 3) % 3 - 1;
+      dj = nb / 9 - 1;
+      if (k + dk < 0 || k + dk >= g.nz) continue;
+    } else {
+      di = nb % 3 - 1;
+      dj = nb / 3 - 1;
+    }
+    if (i + di < 0 || i + di >= g.nx || j + dj < 0 || j + dj >= g.ny) continue;
+    const long long col_node = didx(i + di, j + dj, k + dk);
+    for (int c = 0; c < dof; ++c)
+      for (int d = 0; d < dof; ++d)
+        A[(row_node * dof + c) * nd + col_node * dof + d] =
+            (double)Conv<double>::from(S[((long long)nb * dof * dof + c * dof + d) * g.n + s]);
+  }
+}
+
+// Blocked right-looking Cholesky (lower) of an SPD nd x nd row-major FP64 matrix, tile
+// size CB.  Per tile column K: k_chol_diag factors the diagonal tile in shared memory,
+// k_chol_panel solves the tiles below it, k_chol_update applies the symmetric rank-CB
+// update to the trailing lower triangle.  `status` is set to 1 on a non-positive pivot
+// (the pivot is then replaced by 1 so the factor stays finite).
+constexpr int CB = 32;
+
+__global__ void __launch_bounds__(CB * CB / 4) k_chol_diag(double* A, int nd, int K, int* status) {
+  __shared__ double t[CB][CB + 1];
+  const int k0 = K * CB;
+  const int m = min(CB, nd - k0);
+  for (int q = threadIdx.x; q < CB * CB; q += blockDim.x) {
+    const int r = q / CB, c = q % CB;
+    t[r][c] = (r < m && c < m) ? A[(long long)(k0 + r) * nd + k0 + c] : (r == c ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  for (int k = 0; k < CB; ++k) {
+    if (threadIdx.x == 0) {
+      double d = t[k][k];
+      if (!(d > 0.0)) {
+        if (k < m) *status = 1;
+        d = 1.0;
+      }
+      t[k][k] = sqrt(d);
+    }
+    __syncthreads();
+    const double p = t[k][k];
+    for (int i = k + 1 + threadIdx.x; i < CB; i += blockDim.x) t[i][k] /= p;
+    __syncthreads();
+    for (int q = threadIdx.x; q < CB * CB; q += blockDim.x) {
+      const int i = q / CB, j = q % CB;
+      if (i > k && j > k && j <= i) t[i][j] -= t[i][k] * t[j][k];
+    }
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < CB * CB; q += blockDim.x) {
+    const int r = q / CB, c = q % CB;
+    if (r < m && c < m) A[(long long)(k0 + r) * nd + k0 + c] = (c <= r) ? t[r][c] : 0.0;
+  }
+}
+
+// Tile row I = K+1+blockIdx.x: X L_KK^T = A_IK  (X overwrites A_IK)
+__global__ void __launch_bounds__(CB * CB / 4) k_chol_panel(double* A, int nd, int K) {
+  __shared__ double L[CB][CB + 1];
+  __shared__ double X[CB][CB + 1];
+  const int k0 = K * CB;
+  const int i0 = (K + 1 + blockIdx.x) * CB;
+  const int mk = min(CB, nd - k0), mi = min(CB, nd - i0);
+  for (int q = threadIdx.x; q < CB * CB; q += blockDim.x) {
+    const int r = q / CB, c = q % CB;
+    L[r][c] = (r < mk && c < mk) ? A[(long long)(k0 + r) * nd + k0 + c] : (r == c ? 1.0 : 0.0);
+    X[r][c] = (r < mi && c < mk) ? A[(long long)(i0 + r) * nd + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  // row r of X: x_r[c] = (a_r[c] - sum_{j<c} x_r[j] L[c][j]) / L[c][c], one thread per row
+  for (int r = threadIdx.x; r < CB; r += blockDim.x) {
+    for (int c = 0; c < CB; ++c) {
+      double v = X[r][c];
+      for (int j = 0; j < c; ++j) v -= X[r][j] * L[c][j];
+      X[r][c] = v / L[c][c];
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < CB * CB; q += blockDim.x) {
+    const int r = q / CB, c = q % CB;
+    if (r < mi && c < mk) A[(long long)(i0 + r) * nd + k0 + c] = X[r][c];
+  }
+}
+
+// Trailing update A_IJ -= A_IK A_JK^T for K < J <= I; blockIdx.x enumerates (I, J).
+__global__ void __launch_bounds__(CB * CB / 4) k_chol_update(double* A, int nd, int K, int nt) {
+  __shared__ double P[CB][CB + 1];
+  __shared__ double Q[CB][CB + 1];
+  const int m = nt - K - 1;  // tiles below K
+  int q = blockIdx.x, I = 0;
+  while (q >= I + 1) {  // triangular enumeration: (I, J) with 0 <= J <= I < m
+    q -= I + 1;
+    ++I;
+  }
+  const int J = q;
+  if (I >= m) return;
+  const int k0 = K * CB, i0 = (K + 1 + I) * CB, j0 = (K + 1 + J) * CB;
+  const int mk = min(CB, nd - k0), mi = min(CB, nd - i0), mj = min(CB, nd - j0);
+  for (int t = threadIdx.x; t < CB * CB; t += blockDim.x) {
+    const int r = t / CB, c = t % CB;
+    P[r][c] = (r < mi && c < mk) ? A[(long long)(i0 + r) * nd + k0 + c] : 0.0;
+    Q[r][c] = (r < mj && c < mk) ? A[(long long)(j0 + r) * nd + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < CB * CB; t += blockDim.x) {
+    const int r = t / CB, c = t % CB;
+    if (r >= mi || c >= mj) continue;
+    if (I == J && c > r) continue;
+    double v = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < CB; ++k) v += P[r][k] * Q[c][k];
+    A[(long long)(i0 + r) * nd + j0 + c] -= v;
+  }
+}
+
+// U = L^T (row-major), so that both substitutions below read rows.
+__global__ void k_transpose_lower(const double* __restrict__ L, double* __restrict__ U, int nd) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= (long long)nd * nd) return;
+  const int r = (int)(q / nd), c = (int)(q % nd);
+  U[(long long)c * nd + r] = (c <= r) ? L[q] : 0.0;
+}
+
+// Column `col` of A^-1 = L^-T L^-1 e_col, one block per column.  U = L^T row-major.
+__global__ void __launch_bounds__(256) k_chol_inverse(const double* __restrict__ L, const double* __restrict__ U,
+                                                      double* __restrict__ X, int nd) {
+  extern __shared__ double y[];
+  const int col = blockIdx.x;
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int i = t; i < nd; i += nt) y[i] = (i == col) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int k = col; k < nd; ++k) {  // L y = e_col (y_i = 0 for i < col)
+    const double yk = y[k] / U[(long long)k * nd + k];
+    __syncthreads();
+    if (t == 0) y[k] = yk;
+    for (int i = k + 1 + t; i < nd; i += nt) y[i] -= U[(long long)k * nd + i] * yk;
+    __syncthreads();
+  }
+  for (int k = nd - 1; k >= 0; --k) {  // L^T x = y
+    const double xk = y[k] / L[(long long)k * nd + k];
+    __syncthreads();
+    if (t == 0) y[k] = xk;
+    for (int i = t; i < k; i += nt) y[i] -= L[(long long)k * nd + i] * xk;
+    __syncthreads();
+  }
+  for (int i = t; i < nd; i += nt) X[(long long)i * nd + col] = y[i];
+}
+
+// x = Ainv b on the coarsest level: b and x in slot layout (types TB/TX), Ainv dense FP64.
+// One warp per dense row.
+template <typename TB, typename TX>
+__global__ void k_coarse_solve(const Geo g, const double* __restrict__ Ainv, int nd, const TB* __restrict__ b,
+                               TX* __restrict__ x) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= nd) return;
+  const int dof = g.dof;
+  auto slot_of = [&](int dn) -> long long {
+    const int node = dn / dof;
+    if (g.dim == 3) {
+      const int k = node % g.nz, i = (node / g.nz) % g.nx, j = node / (g.nz * g.nx);
+      return g.slot3(i, j, k);
+    }
+    const int i = node % g.nx, j = node / g.nx;
+    return g.slot2(i, j);
+  };
+  double acc = 0.0;
+  for (int cidx = lane; cidx < nd; cidx += 32) {
+    const double bv = (double)Conv<double>::from(b[(cidx % dof) * g.n + slot_of(cidx)]);
+    acc += Ainv[(long long)row * nd + cidx] * bv;
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) x[(row % dof) * g.n + slot_of(row)] = Conv<TX>::from(acc);
+}
+
+}  // namespace edge

@@ -1,0 +1,503 @@
+// Element-wise and reduction kernels of the SIMP loop: layout conversion, density
+// filter and its transpose, SIMP material law, element sensitivities, compliance,
+// OC bisection, PCG vector updates.
+#pragma once
+#include "common.cuh"
+#include "element_op.cuh"
+
+namespace edge {
+
+// ------------------------------------------------------------------ layout conversion
+// User vectors are the reference's interleaved node-major arrays: v[node*dof + c] with
+// node = j*nx*nz + i*nz + k (3-D) or j*nx + i (2-D).
+EDGE_D bool node_of_slot(const Geo& g, long long s, int& i, int& j, int& k, long long& node) {
+  if (g.dim == 3) {
+    k = (int)(s % g.pz);
+    i = (int)((s / g.pz) % g.nx);
+    j = (int)(s / g.plane);
+    if (k >= g.nz) return false;
+    node = ((long long)j * g.nx + i) * g.nz + k;
+  } else {
+    k = 0;
+    i = (int)(s % g.pz);
+    j = (int)(s / g.pz);
+    if (i >= g.nx) return false;
+    node = (long long)j * g.nx + i;
+  }
+  return true;
+}
+
+template <typename TO>
+__global__ void k_user_to_slots(const Geo g, const double* __restrict__ user, TO* __restrict__ v) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  const bool ok = node_of_slot(g, s, i, j, k, node);
+  for (int c = 0; c < g.dof; ++c) v[c * g.n + s] = Conv<TO>::from(ok ? user[node * g.dof + c] : 0.0);
+}
+
+template <typename TI>
+__global__ void k_slots_to_user(const Geo g, const TI* __restrict__ v, double* __restrict__ user) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  if (!node_of_slot(g, s, i, j, k, node)) return;
+  for (int c = 0; c < g.dof; ++c) user[node * g.dof + c] = (double)Conv<double>::from(v[c * g.n + s]);
+}
+
+// Per-node constraint bits from the reference's per-DOF boolean array.
+__global__ void k_mask_from_user(const Geo g, const uint8_t* __restrict__ cons, uint8_t* __restrict__ mask) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  uint8_t m = 0;
+  if (node_of_slot(g, s, i, j, k, node))
+    for (int c = 0; c < g.dof; ++c) m |= (cons[node * g.dof + c] ? 1 : 0) << c;
+  mask[s] = m;
+}
+
+// Element arrays: user order e = i*nely*nelz + j*nelz + k (3-D), i*nely + j (2-D)
+// (core/_geom.py:17-18, 43-46) <-> node-aligned slots.
+EDGE_D long long user_elem(const Geo& g, int i, int j, int k) {
+  const int nely = g.ny - 1;
+  if (g.dim == 3) return ((long long)i * nely + j) * (g.nz - 1) + k;
+  return (long long)i * nely + j;
+}
+
+template <typename TO>
+__global__ void k_elem_user_to_slots(const Geo g, const double* __restrict__ user, TO* __restrict__ v) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  double val = 0.0;
+  if (node_of_slot(g, s, i, j, k, node) && i < g.nx - 1 && j < g.ny - 1 && (g.dim == 2 || k < g.nz - 1))
+    val = user[user_elem(g, i, j, k)];
+  v[s] = Conv<TO>::from(val);
+}
+
+// ------------------------------------------------------------------ density filter
+// Cone filter (geom/_filters.py:72-161, core/_filter.py:78-124): taps o_k with global
+// weights w_k; (H rho)_e = sum_k w_k rho_{e+o_k} / sum_{in-bounds k} w_k.
+constexpr int MAX_TAPS = 128;
+struct Taps {
+  int n;
+  int off[MAX_TAPS][3];  // (dx, dy, dz) in element units
+  double w[MAX_TAPS];
+};
+
+// Forward filter fused with the SIMP law (MaterialModels.py:47-60):
+//   rho_f = H rho (user order), E = clip(rho_f^p, void, 1) written in slot layout
+//   (types TE1 and optional TE2 for a second precision).
+template <typename TE1, typename TE2>
+__global__ void k_filter_material(const Geo g, const Taps taps, const double* __restrict__ rho,
+                                  double* __restrict__ rho_f, TE1* __restrict__ E1, TE2* __restrict__ E2,
+                                  double penalty, double vmin, int plain) {
+  const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nel = (long long)nelx * nely * nelz;
+  if (e >= nel) return;
+  int i, j, k;
+  if (g.dim == 3) {
+    k = (int)(e % nelz);
+    j = (int)((e / nelz) % nely);
+    i = (int)(e / ((long long)nelz * nely));
+  } else {
+    k = 0;
+    j = (int)(e % nely);
+    i = (int)(e / nely);
+  }
+  double sv = 0.0, sw = 0.0;
+  for (int t = 0; t < taps.n; ++t) {
+    const int ii = i + taps.off[t][0], jj = j + taps.off[t][1], kk = k + taps.off[t][2];
+    if (ii < 0 || ii >= nelx || jj < 0 || jj >= nely || kk < 0 || kk >= nelz) continue;
+    const double w = taps.w[t];
+    sv += w * __ldg(rho + user_elem(g, ii, jj, kk));
+    sw += w;
+  }
+  const double rf = sw > 0.0 ? sv / sw : 0.0;
+  rho_f[e] = rf;
+  double Ev;
+  if (plain) {
+    Ev = fmin(fmax(rf, vmin), 1.0);
+  } else {
+    Ev = fmin(fmax(pow(rf, penalty), vmin), 1.0);
+  }
+  const long long s = g.dim == 3 ? g.slot3(i, j, k) : g.slot2(i, j);
+  E1[s] = Conv<TE1>::from(Ev);
+  if (E2) E2[s] = Conv<TE2>::from(Ev);
+}
+
+// Filter only (H rho), user order in and out.
+__global__ void k_filter(const Geo g, const Taps taps, const double* __restrict__ in, double* __restrict__ out) {
+  const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nel = (long long)nelx * nely * nelz;
+  if (e >= nel) return;
+  int i, j, k;
+  if (g.dim == 3) {
+    k = (int)(e % nelz);
+    j = (int)((e / nelz) % nely);
+    i = (int)(e / ((long long)nelz * nely));
+  } else {
+    k = 0;
+    j = (int)(e % nely);
+    i = (int)(e / nely);
+  }
+  double sv = 0.0, sw = 0.0;
+  for (int t = 0; t < taps.n; ++t) {
+    const int ii = i + taps.off[t][0], jj = j + taps.off[t][1], kk = k + taps.off[t][2];
+    if (ii < 0 || ii >= nelx || jj < 0 || jj >= nely || kk < 0 || kk >= nelz) continue;
+    sv += taps.w[t] * __ldg(in + user_elem(g, ii, jj, kk));
+    sw += taps.w[t];
+  }
+  out[e] = sw > 0.0 ? sv / sw : 0.0;
+}
+
+// Normaliser N_e = sum of in-bounds weights (core/_filter.py:6-40).
+__global__ void k_filter_norm(const Geo g, const Taps taps, double* __restrict__ N) {
+  const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nel = (long long)nelx * nely * nelz;
+  if (e >= nel) return;
+  int i, j, k;
+  if (g.dim == 3) {
+    k = (int)(e % nelz);
+    j = (int)((e / nelz) % nely);
+    i = (int)(e / ((long long)nelz * nely));
+  } else {
+    k = 0;
+    j = (int)(e % nely);
+    i = (int)(e / nely);
+  }
+  double sw = 0.0;
+  for (int t = 0; t < taps.n; ++t) {
+    const int ii = i + taps.off[t][0], jj = j + taps.off[t][1], kk = k + taps.off[t][2];
+    if (ii < 0 || ii >= nelx || jj < 0 || jj >= nely || kk < 0 || kk >= nelz) continue;
+    sw += taps.w[t];
+  }
+  N[e] = sw;
+}
+
+// Transpose: (H^T v)_e = sum_k (w_k / N_{e+o_k}) v_{e+o_k} (core/_filter.py:42-76).
+__global__ void k_filter_T(const Geo g, const Taps taps, const double* __restrict__ N, const double* __restrict__ in,
+                           double* __restrict__ out) {
+  const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nel = (long long)nelx * nely * nelz;
+  if (e >= nel) return;
+  int i, j, k;
+  if (g.dim == 3) {
+    k = (int)(e % nelz);
+    j = (int)((e / nelz) % nely);
+    i = (int)(e / ((long long)nelz * nely));
+  } else {
+    k = 0;
+    j = (int)(e % nely);
+    i = (int)(e / nely);
+  }
+  double sv = 0.0;
+  for (int t = 0; t < taps.n; ++t) {
+    const int ii = i + taps.off[t][0], jj = j + taps.off[t][1], kk = k + taps.off[t][2];
+    if (ii < 0 || ii >= nelx || jj < 0 || jj >= nely || kk < 0 || kk >= nelz) continue;
+    const long long q = user_elem(g, ii, jj, kk);
+    sv += (taps.w[t] / __ldg(N + q)) * __ldg(in + q);
+  }
+  out[e] = sv;
+}
+
+// ------------------------------------------------------------------ sensitivities
+// dk_e = -u_e^T K0 u_e (core/_ops.py:5-13) from the solution in slot layout, and
+// optionally g_e = p clip(rho_f, void, 1)^(p-1) dk_e (MaterialModels.py:62-73).
+// `wht` selects the transform form; otherwise K0b (bit-order dense) is used.
+template <typename TU>
+__global__ void k_dk(const Geo g, const TU* __restrict__ U, KHat3<double> K3, KHat2<double> K2,
+                     const double* __restrict__ K0b, int wht, double* __restrict__ dk, const double* __restrict__ rho_f,
+                     double* __restrict__ gout, double penalty, double vmin) {
+  const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nel = (long long)nelx * nely * nelz;
+  if (e >= nel) return;
+  double val;
+  if (g.dim == 3) {
+    const int k = (int)(e % nelz), j = (int)((e / nelz) % nely), i = (int)(e / ((long long)nelz * nely));
+    double u[8][3];
+    for (int b = 0; b < 8; ++b) {
+      const long long s = g.slot3(i + (b & 1), j + ((b >> 1) & 1), k + ((b >> 2) & 1));
+      for (int c = 0; c < 3; ++c) u[b][c] = (double)Conv<double>::from(U[c * g.n + s]);
+    }
+    if (wht) {
+      val = -elem3_energy(K3, u);
+    } else {
+      double acc = 0.0;
+      for (int r = 0; r < 24; ++r) {
+        double t = 0.0;
+        for (int q = 0; q < 24; ++q) t += K0b[r * 24 + q] * u[q / 3][q % 3];
+        acc += u[r / 3][r % 3] * t;
+      }
+      val = -acc;
+    }
+  } else {
+    const int j = (int)(e % nely), i = (int)(e / nely);
+    double u[4][2];
+    for (int b = 0; b < 4; ++b) {
+      const long long s = g.slot2(i + (b & 1), j + ((b >> 1) & 1));
+      for (int c = 0; c < 2; ++c) u[b][c] = (double)Conv<double>::from(U[c * g.n + s]);
+    }
+    if (wht) {
+      val = -elem2_energy(K2, u);
+    } else {
+      double acc = 0.0;
+      for (int r = 0; r < 8; ++r) {
+        double t = 0.0;
+        for (int q = 0; q < 8; ++q) t += K0b[r * 8 + q] * u[q / 2][q % 2];
+        acc += u[r / 2][r % 2] * t;
+      }
+      val = -acc;
+    }
+  }
+  if (dk) dk[e] = val;
+  if (gout) gout[e] = penalty * pow(fmin(fmax(rho_f[e], vmin), 1.0), penalty - 1.0) * val;
+}
+
+// Fine diagonal of K(E) with BCs (core/_ops.py:45-76): sum over the node's elements of
+// E_e K0[(a,c),(a,c)], 1 on constrained DOFs; writes Dinv = 1/diag in type TD.
+template <typename TE, typename TD>
+__global__ void k_fine_dinv(const Geo g, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
+                            const double* __restrict__ K0diag /* [corner][c] bit order */, TD* __restrict__ dinv,
+                            double* __restrict__ diag_out) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  const bool ok = node_of_slot(g, s, i, j, k, node);
+  const int dof = g.dof;
+  double d[3] = {0, 0, 0};
+  if (ok) {
+    const int nc = g.dim == 3 ? 8 : 4;
+    for (int a = 0; a < nc; ++a) {
+      const int li = i - (a & 1), lj = j - ((a >> 1) & 1), lk = k - ((a >> 2) & 1);
+      if (li < 0 || lj < 0 || li >= g.nx - 1 || lj >= g.ny - 1) continue;
+      if (g.dim == 3 && (lk < 0 || lk >= g.nz - 1)) continue;
+      const double Ee = (double)Conv<double>::from(E[g.dim == 3 ? g.slot3(li, lj, lk) : g.slot2(li, lj)]);
+      for (int c = 0; c < dof; ++c) d[c] += Ee * K0diag[a * dof + c];
+    }
+    const uint8_t m = mask[s];
+    for (int c = 0; c < dof; ++c)
+      if ((m >> c) & 1) d[c] = 1.0;
+  }
+  for (int c = 0; c < dof; ++c) {
+    dinv[c * g.n + s] = Conv<TD>::from(ok ? 1.0 / d[c] : 0.0);
+    if (diag_out && ok) diag_out[node * dof + c] = d[c];
+  }
+}
+
+// ------------------------------------------------------------------ reductions
+template <typename TA, typename TB>
+__global__ void k_dot(long long n, const TA* __restrict__ a, const TB* __restrict__ b, double* part, unsigned* ticket,
+                      double* dst) {
+  double acc = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    acc += (double)Conv<double>::from(a[q]) * (double)Conv<double>::from(b[q]);
+  __shared__ double sh[32];
+  double bt = block_sum(acc, sh);
+  grid_reduce_finish(bt, part, ticket, DotSink{dst});
+}
+
+// ------------------------------------------------------------------ PCG device scalars
+struct PcgState {
+  double rz;      // r.z used by the current iteration's alpha / beta
+  double rz_new;  // r.z of the latest V-cycle
+  double pq;      // p.(A p)
+  double rr;      // r.r
+  double bb;      // f.f
+  double alpha, beta;
+  double res;     // ||r|| / ||f||
+  double omega;   // smoother weight for the next V-cycle
+  double tol, min_omega, d_omega;
+  int iter, maxiter, done;  // done: 1 converged, 2 maxiter
+};
+
+// x += alpha p ; r -= alpha q ; rr = r.r with alpha = rz_new / pq.  The finisher
+// updates res / omega / done as solvers/_multigrid_cuda.py:219-227 and moves rz_new to rz.
+template <typename TX, typename TP>
+__global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__ p, TX* __restrict__ r,
+                         const TP* __restrict__ q, PcgState* st, double* part, unsigned* ticket) {
+  const double alpha = st->rz_new / st->pq;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double pi = (double)Conv<double>::from(p[i]);
+    const double qi = (double)Conv<double>::from(q[i]);
+    x[i] = Conv<TX>::from((double)Conv<double>::from(x[i]) + alpha * pi);
+    const double ri = (double)Conv<double>::from(r[i]) - alpha * qi;
+    r[i] = Conv<TX>::from(ri);
+    acc += ri * ri;
+  }
+  __shared__ double sh[32];
+  double bt = block_sum(acc, sh);
+  struct Fin {
+    PcgState* st;
+    double alpha;
+    EDGE_D void operator()(double t) const {
+      st->alpha = alpha;
+      st->rz = st->rz_new;
+      st->rr = t;
+      const double R = sqrt(t) / sqrt(st->bb);
+      st->res = R;
+      st->iter += 1;
+      if (R < st->tol) {
+        st->done = 1;
+      } else {
+        const double Rc = fmin(fmax(R, st->tol), 1e-1);
+        st->omega = st->min_omega + st->d_omega / 2.0 * exp((-Rc + st->tol) * 500.0);
+        if (st->iter >= st->maxiter) st->done = 2;
+      }
+    }
+  };
+  grid_reduce_finish(bt, part, ticket, Fin{st, alpha});
+}
+
+// p = z + beta p
+template <typename TP>
+__global__ void k_pcg_p(long long n, TP* __restrict__ p, const TP* __restrict__ z, const PcgState* st) {
+  const double beta = st->rz_new / st->rz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = Conv<TP>::from((double)Conv<double>::from(z[i]) + beta * (double)Conv<double>::from(p[i]));
+}
+
+// ------------------------------------------------------------------ OC bisection (TopOpt/_cuda.py:242-280)
+// ocP = max(1e-12, rho * sqrt(max(-dr/A, 0))) with NaN -> 0; the all-zero fallback of
+// MaterialModels.py:87-88 is applied by k_oc_fallback when sum(ocP_raw) == 0.
+__global__ void k_oc_prep(long long n, const double* __restrict__ rho, const double* __restrict__ dr, double A,
+                          double* __restrict__ ocp, double* part, unsigned* ticket, double* sum_dst) {
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double v = rho[i] * sqrt(fmax(-dr[i] / A, 0.0));
+    if (isnan(v)) v = 0.0;
+    acc += fabs(v);
+    ocp[i] = v;
+  }
+  __shared__ double sh[32];
+  double bt = block_sum(acc, sh);
+  grid_reduce_finish(bt, part, ticket, DotSink{sum_dst});
+}
+
+__global__ void k_oc_floor(long long n, double* __restrict__ ocp, const double* __restrict__ sum) {
+  const bool allzero = (*sum == 0.0);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double v = allzero ? 1e-3 : ocp[i];
+    ocp[i] = fmax(1e-12, v);
+  }
+}
+
+constexpr int OC_DEPTH = 4;                  // bisection levels resolved per pass
+constexpr int OC_NODES = (1 << OC_DEPTH) - 1;
+struct OcState {
+  double l1, l2, last;
+  double vf, vol;
+  int steps, done;
+  double sums[OC_NODES];
+};
+
+EDGE_D double oc_rho(double r, double o, double lam, double move) {
+  const double xU = fmin(fmax(r + move, 0.0), 1.0);
+  const double xL = fmin(fmax(r - move, 0.0), 1.0);
+  return fmax(0.0, fmax(xL, fmin(1.0, fmin(xU, o / lam))));
+}
+
+// Evaluate sum(rho_new(lambda) * A) at every node of the next OC_DEPTH levels of the
+// bisection tree.  Tree node t (heap order): children 2t+1 (volume ok -> l2 = mid)
+// and 2t+2 (l1 = mid).
+__global__ void __launch_bounds__(256) k_oc_pass(long long n, const double* __restrict__ rho, const double* __restrict__ ocp,
+                                                 double A, double move, OcState* st, double* part, unsigned* ticket) {
+  if (st->done) return;
+  double lam[OC_NODES];
+  {
+    double L1[OC_NODES], L2[OC_NODES];
+    L1[0] = st->l1;
+    L2[0] = st->l2;
+    for (int t = 0; t < OC_NODES; ++t) {
+      lam[t] = 0.5 * (L1[t] + L2[t]);
+      if (2 * t + 2 < OC_NODES) {
+        L1[2 * t + 1] = L1[t];
+        L2[2 * t + 1] = lam[t];
+        L1[2 * t + 2] = lam[t];
+        L2[2 * t + 2] = L2[t];
+      }
+    }
+  }
+  double acc[OC_NODES];
+  for (int t = 0; t < OC_NODES; ++t) acc[t] = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double r = rho[i], o = ocp[i];
+    for (int t = 0; t < OC_NODES; ++t) acc[t] += oc_rho(r, o, lam[t], move) * A;
+  }
+  __shared__ double sh[32];
+  __shared__ double bsum[OC_NODES];
+  for (int t = 0; t < OC_NODES; ++t) {
+    double v = block_sum(acc[t], sh);
+    if (threadIdx.x == 0) bsum[t] = v;
+  }
+  __syncthreads();
+  // grid-wide: partials laid out [block][t]
+  __shared__ bool am_last;
+  const unsigned nblk = gridDim.x;
+  if (threadIdx.x == 0) {
+    for (int t = 0; t < OC_NODES; ++t) part[(long long)blockIdx.x * OC_NODES + t] = bsum[t];
+    __threadfence();
+    am_last = (atomicAdd(ticket, 1u) == nblk - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  for (int t = 0; t < OC_NODES; ++t) {
+    double a = 0.0;
+    for (unsigned b = threadIdx.x; b < nblk; b += blockDim.x) a += ((volatile double*)part)[(long long)b * OC_NODES + t];
+    double tot = block_sum(a, sh);
+    if (threadIdx.x == 0) st->sums[t] = tot;
+  }
+  if (threadIdx.x == 0) {
+    // walk the tree exactly as the sequential bisection would
+    int t = 0;
+    double l1 = st->l1, l2 = st->l2;
+    for (int d = 0; d < OC_DEPTH; ++d) {
+      if (!((l2 - l1) / (l2 + l1) > 1e-4)) {
+        st->done = 1;
+        break;
+      }
+      const double mid = 0.5 * (l1 + l2);
+      const bool valid = (st->sums[t] / st->vol <= st->vf);
+      if (valid) l2 = mid;
+      else l1 = mid;
+      st->last = mid;
+      st->steps += 1;
+      t = 2 * t + (valid ? 1 : 2);
+    }
+    st->l1 = l1;
+    st->l2 = l2;
+    if (!((l2 - l1) / (l2 + l1) > 1e-4)) st->done = 1;
+    *ticket = 0u;
+  }
+}
+
+// rho_new at the last lambda tried; also sum((rho_new - rho)^2) for the RMS change.
+__global__ void k_oc_final(long long n, const double* __restrict__ rho, const double* __restrict__ ocp, double move,
+                           const OcState* st, double* __restrict__ rho_new, double* part, unsigned* ticket,
+                           double* chg_dst) {
+  const double lam = st->last;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double r = rho[i];
+    const double v = oc_rho(r, ocp[i], lam, move);
+    rho_new[i] = v;
+    acc += (v - r) * (v - r);
+  }
+  __shared__ double sh[32];
+  double bt = block_sum(acc, sh);
+  grid_reduce_finish(bt, part, ticket, DotSink{chg_dst});
+}
+
+}  // namespace edge

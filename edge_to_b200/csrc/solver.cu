@@ -1,0 +1,1113 @@
+// Host orchestration and the C ABI (include/edge_b200.h).
+//
+// Problem = one structured Q4/hex8 mesh with its stiffness operator, BC mask, density,
+// multigrid hierarchy and PCG workspace, all allocated at create/config time.
+// The solve path (edge_mg_solve / edge_simp_solve_and_process) only launches kernels on
+// the problem's stream; the host reads back the PCG state once per iteration to decide
+// convergence, exactly where the reference syncs (solvers/_multigrid_cuda.py:223-226).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/edge_b200.h"
+#include "coarse.cuh"
+#include "common.cuh"
+#include "element_op.cuh"
+#include "fine_apply.cuh"
+#include "misc.cuh"
+
+namespace edge {
+
+static thread_local std::string g_err;
+
+struct EdgeError {
+  int code;
+  std::string msg;
+};
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) throw EdgeError{EDGE_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+#define KCHECK() CK(cudaGetLastError())
+
+static void fail(int code, const std::string& m) { throw EdgeError{code, m}; }
+
+static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+// ------------------------------------------------------------------ element matrix analysis
+struct ElemInfo {
+  int dim = 0, nc = 0, nk = 0;  // corners, matrix size
+  double K0b[576];              // bit-order corners
+  double kdiag[24];
+  bool wht = false;
+  KHat3<double> k3{};
+  KHat2<double> k2{};
+  std::vector<double> Q;  // Galerkin parity tables
+};
+
+static const int REF_CORNER3[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                      {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+static const int REF_CORNER2[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
+
+static double pw_h(int s, int a, int c) {
+  return s == 0 ? (a == 0 ? (c == 0 ? 1.0 : 0.0) : 0.5) : (a == 0 ? 0.5 : (c == 1 ? 1.0 : 0.0));
+}
+
+static void analyse_element(int dim, const double* K0ref, ElemInfo& ei) {
+  ei.dim = dim;
+  ei.nc = 1 << dim;
+  ei.nk = ei.nc * dim;
+  const int nc = ei.nc, nk = ei.nk, d = dim;
+  std::vector<int> bit(nc);
+  for (int L = 0; L < nc; ++L)
+    bit[L] = dim == 3 ? (REF_CORNER3[L][0] | (REF_CORNER3[L][1] << 1) | (REF_CORNER3[L][2] << 2))
+                      : (REF_CORNER2[L][0] | (REF_CORNER2[L][1] << 1));
+  for (int L1 = 0; L1 < nc; ++L1)
+    for (int c1 = 0; c1 < d; ++c1)
+      for (int L2 = 0; L2 < nc; ++L2)
+        for (int c2 = 0; c2 < d; ++c2)
+          ei.K0b[(bit[L1] * d + c1) * nk + bit[L2] * d + c2] = K0ref[(L1 * d + c1) * nk + L2 * d + c2];
+  for (int b = 0; b < nc; ++b)
+    for (int c = 0; c < d; ++c) ei.kdiag[b * d + c] = ei.K0b[(b * d + c) * nk + b * d + c];
+  // transform: Ks = T K0b T / 4^d with T[(h,c),(b,c)] = (-1)^popcount(h&b)
+  std::vector<double> tmp(nk * nk, 0.0), Ks(nk * nk, 0.0);
+  auto sgn = [](int h, int b) { return (__builtin_popcount(h & b) & 1) ? -1.0 : 1.0; };
+  for (int h = 0; h < nc; ++h)
+    for (int c = 0; c < d; ++c)
+      for (int col = 0; col < nk; ++col) {
+        double s = 0;
+        for (int b = 0; b < nc; ++b) s += sgn(h, b) * ei.K0b[(b * d + c) * nk + col];
+        tmp[(h * d + c) * nk + col] = s;
+      }
+  const double scale = 1.0 / double(nc * nc);
+  double mx = 0.0;
+  for (int row = 0; row < nk; ++row)
+    for (int h = 0; h < nc; ++h)
+      for (int c = 0; c < d; ++c) {
+        double s = 0;
+        for (int b = 0; b < nc; ++b) s += tmp[row * nk + b * d + c] * sgn(h, b);
+        Ks[row * nk + h * d + c] = s * scale;
+        mx = std::max(mx, std::fabs(s * scale));
+      }
+  // pattern check
+  bool ok = mx > 0.0;
+  double outside = 0.0;
+  for (int h = 0; h < nc; ++h)
+    for (int c = 0; c < d; ++c)
+      for (int h2 = 0; h2 < nc; ++h2)
+        for (int c2 = 0; c2 < d; ++c2) {
+          bool in = false;
+          if (h != 0 && h2 == h && c2 == c) in = true;
+          if (h != 0 && c2 != c && (((h >> c) & 1) != ((h >> c2) & 1)) && h2 == (h ^ (1 << c) ^ (1 << c2))) in = true;
+          if (!in) outside = std::max(outside, std::fabs(Ks[(h * d + c) * nk + h2 * d + c2]));
+        }
+  if (outside > 1e-12 * mx) ok = false;
+  ei.wht = ok;
+  if (dim == 3) {
+    for (int c = 0; c < 3; ++c)
+      for (int h = 0; h < 8; ++h) {
+        ei.k3.dg[c][h] = Ks[(h * 3 + c) * 24 + h * 3 + c];
+        for (int c2 = 0; c2 < 3; ++c2) {
+          const int h2 = h ^ (1 << c) ^ (1 << c2);
+          ei.k3.of[c][c2][h] = (c2 != c) ? Ks[(h * 3 + c) * 24 + h2 * 3 + c2] : 0.0;
+        }
+      }
+  } else {
+    for (int c = 0; c < 2; ++c)
+      for (int h = 0; h < 4; ++h) {
+        ei.k2.dg[c][h] = Ks[(h * 2 + c) * 8 + h * 2 + c];
+        for (int c2 = 0; c2 < 2; ++c2) {
+          const int h2 = h ^ 3;
+          ei.k2.of[c][c2][h] = (c2 != c) ? Ks[(h * 2 + c) * 8 + h2 * 2 + c2] : 0.0;
+        }
+      }
+  }
+  // Galerkin parity tables Q_s = P_s^T K0b P_s
+  const int npar = nc;
+  ei.Q.assign((size_t)npar * nk * nk, 0.0);
+  for (int s = 0; s < npar; ++s) {
+    std::vector<double> P(nc * nc);
+    for (int a = 0; a < nc; ++a)
+      for (int cI = 0; cI < nc; ++cI) {
+        double w = 1.0;
+        for (int q = 0; q < d; ++q) w *= pw_h((s >> q) & 1, (a >> q) & 1, (cI >> q) & 1);
+        P[a * nc + cI] = w;
+      }
+    for (int cI = 0; cI < nc; ++cI)
+      for (int c = 0; c < d; ++c)
+        for (int cJ = 0; cJ < nc; ++cJ)
+          for (int e = 0; e < d; ++e) {
+            double v = 0.0;
+            for (int a = 0; a < nc; ++a) {
+              if (P[a * nc + cI] == 0.0) continue;
+              for (int b = 0; b < nc; ++b) {
+                if (P[b * nc + cJ] == 0.0) continue;
+                v += P[a * nc + cI] * ei.K0b[(a * d + c) * nk + b * d + e] * P[b * nc + cJ];
+              }
+            }
+            ei.Q[(size_t)s * nk * nk + (cI * d + c) * nk + cJ * d + e] = v;
+          }
+  }
+}
+
+template <typename T> static KHat3<T> cast3(const KHat3<double>& k) {
+  KHat3<T> o;
+  for (int c = 0; c < 3; ++c)
+    for (int h = 0; h < 8; ++h) {
+      o.dg[c][h] = (T)k.dg[c][h];
+      for (int d = 0; d < 3; ++d) o.of[c][d][h] = (T)k.of[c][d][h];
+    }
+  return o;
+}
+template <typename T> static KHat2<T> cast2(const KHat2<double>& k) {
+  KHat2<T> o;
+  for (int c = 0; c < 2; ++c)
+    for (int h = 0; h < 4; ++h) {
+      o.dg[c][h] = (T)k.dg[c][h];
+      for (int d = 0; d < 2; ++d) o.of[c][d][h] = (T)k.of[c][d][h];
+    }
+  return o;
+}
+
+// ------------------------------------------------------------------ problem
+struct Level {
+  Geo g;
+  void *b = nullptr, *xa = nullptr, *xb = nullptr, *r = nullptr, *ea = nullptr, *eb = nullptr, *res = nullptr;
+  void* S = nullptr;     // stencil (l >= 1)
+  void* dinv = nullptr;  // Jacobi inverse diagonal
+};
+
+struct Prob {
+  int dim = 0, nel[3] = {1, 1, 1}, prec = EDGE_FP64;
+  Geo g0;
+  long long n_el = 0, n_dof = 0;
+  ElemInfo ei;
+  cudaStream_t stream = 0;
+  std::vector<void*> allocs;
+  // element / operator data
+  double* dK0b = nullptr;
+  float* dK0bf = nullptr;
+  double* dK0diag = nullptr;
+  double* dQ = nullptr;
+  uint8_t* mask = nullptr;
+  uint8_t* eflag = nullptr;
+  double* E64 = nullptr;
+  float* E32 = nullptr;
+  bool has_rho = false, has_cons = false;
+  // MG configuration
+  int n_level = -1, n_smooth = 3;
+  double omega = 0.5, min_omega = 0.4;
+  bool cycle_w = false;
+  std::vector<int> w_levels;
+  std::vector<Level> lv;
+  int nd = 0;
+  double *Adense = nullptr, *Ainv = nullptr, *Ut = nullptr;
+  int* chol_status = nullptr;
+  // PCG (level 0) vectors, FP64 slots
+  double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr;
+  void *p = nullptr, *q = nullptr;  // type T of the precision mode
+  float* r32 = nullptr;
+  // user-layout scratch for the fused SIMP step
+  double *rho_f = nullptr, *gsens = nullptr;
+  // reductions
+  double* part = nullptr;
+  unsigned* ticket = nullptr;
+  PcgState* st = nullptr;
+  PcgState* st_h = nullptr;  // pinned
+  OcState* oc = nullptr;
+  OcState* oc_h = nullptr;
+  double* ocp = nullptr;
+  double* scal = nullptr;    // device scalars
+  double* scal_h = nullptr;  // pinned
+  int* zero_int = nullptr;
+  // stats
+  cudaEvent_t ev[4];
+  double last_setup_ms = 0, last_solve_ms = 0;
+  int last_iters = 0, last_true_res = 0;
+  size_t part_cap = 0;
+
+  template <typename T> T* alloc(size_t n) {
+    void* ptr = nullptr;
+    CK(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)));
+    CK(cudaMemset(ptr, 0, std::max<size_t>(n, 1) * sizeof(T)));
+    allocs.push_back(ptr);
+    return (T*)ptr;
+  }
+  ~Prob() {
+    for (void* a : allocs) cudaFree(a);
+    if (st_h) cudaFreeHost(st_h);
+    if (oc_h) cudaFreeHost(oc_h);
+    if (scal_h) cudaFreeHost(scal_h);
+    for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+  }
+};
+
+static Geo level_geo(const Prob& P, int l) {
+  int ne[3] = {P.nel[0], P.nel[1], P.nel[2]};
+  for (int i = 0; i < l; ++i)
+    for (int d = 0; d < 3; ++d) ne[d] /= 2;
+  return make_geo(P.dim, ne[0], ne[1], P.dim == 3 ? ne[2] : 0);
+}
+
+static size_t vbytes(int prec) { return prec == EDGE_FP64 ? sizeof(double) : sizeof(float); }
+
+// ------------------------------------------------------------------ launch helpers
+static const int FINE_BX = 8;
+static const int FINE2_NW = 4;
+
+static dim3 fine3_grid(const Geo& g, int& ly) {
+  const unsigned tz = cdiv(g.nz, 31), tx = cdiv(g.nx, FINE_BX - 1);
+  const long long want = 148LL * 4;
+  long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
+  chunks = std::min<long long>(chunks, g.ny);
+  ly = (int)cdiv(g.ny, chunks);
+  return dim3(tz, tx, cdiv(g.ny, ly));
+}
+static dim3 fine2_grid(const Geo& g, int& ly) {
+  const unsigned tx = cdiv(g.nx, 32 * FINE2_NW - 1);
+  const long long want = 148LL * 8;
+  long long chunks = std::max<long long>(1, (want + tx - 1) / tx);
+  chunks = std::min<long long>(chunks, g.ny);
+  ly = (int)cdiv(g.ny, chunks);
+  return dim3(tx, cdiv(g.ny, ly));
+}
+
+template <typename T> struct TypeOps;
+template <> struct TypeOps<double> {
+  static const double* E(const Prob& P) { return P.E64; }
+  static const double* K0b(const Prob& P) { return P.dK0b; }
+};
+template <> struct TypeOps<float> {
+  static const float* E(const Prob& P) { return P.E32; }
+  static const float* K0b(const Prob& P) { return P.dK0bf; }
+};
+
+// Fine-level operator with epilogue.  u, E in type T.
+template <typename T, class Epi>
+static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
+  const Geo& g = P.g0;
+  const T* E = TypeOps<T>::E(P);
+  if (P.ei.wht) {
+    if (P.dim == 3) {
+      int ly;
+      dim3 grid = fine3_grid(g, ly);
+      k_fine3_wht<T, T, Epi, FINE_BX><<<grid, dim3(32, FINE_BX), 0, P.stream>>>(
+          g, u, E, P.mask, cast3<T>(P.ei.k3), ly, epi, P.part, P.ticket, dot_dst);
+    } else {
+      int ly;
+      dim3 grid = fine2_grid(g, ly);
+      k_fine2_wht<T, T, Epi, FINE2_NW><<<grid, 32 * FINE2_NW, 0, P.stream>>>(
+          g, u, E, P.mask, cast2<T>(P.ei.k2), ly, epi, P.part, P.ticket, dot_dst);
+    }
+  } else {
+    if (P.dim == 3) {
+      k_fine3_dense<T, T, Epi><<<dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, P.stream>>>(
+          g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
+    } else {
+      k_fine2_dense<T, T, Epi><<<dim3(cdiv(g.nx, 128), g.ny), 128, 0, P.stream>>>(
+          g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
+    }
+  }
+  KCHECK();
+}
+
+// Same operator, forcing the dense path (cross-checks).
+template <typename T, class Epi>
+static void fine_apply_dense(Prob& P, const T* u, Epi epi, double* dot_dst) {
+  const Geo& g = P.g0;
+  const T* E = TypeOps<T>::E(P);
+  if (P.dim == 3)
+    k_fine3_dense<T, T, Epi><<<dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, P.stream>>>(
+        g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
+  else
+    k_fine2_dense<T, T, Epi><<<dim3(cdiv(g.nx, 128), g.ny), 128, 0, P.stream>>>(
+        g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
+  KCHECK();
+}
+
+template <typename T, class Epi>
+static void st_apply(Prob& P, const Geo& g, const T* u, const T* S, Epi epi, double* dot_dst) {
+  if (g.dim == 3)
+    k_st3_apply<T, T, Epi><<<dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, P.stream>>>(g, u, S, epi, P.part, P.ticket,
+                                                                                    dot_dst);
+  else
+    k_st2_apply<T, T, Epi><<<dim3(cdiv(g.nx, 128), g.ny), 128, 0, P.stream>>>(g, u, S, epi, P.part, P.ticket, dot_dst);
+  KCHECK();
+}
+
+template <typename T, class Epi>
+static void level_apply(Prob& P, int l, const T* u, Epi epi, double* dot_dst = nullptr) {
+  if (l == 0)
+    fine_apply<T>(P, u, epi, dot_dst);
+  else
+    st_apply<T>(P, P.lv[l].g, u, (const T*)P.lv[l].S, epi, dot_dst);
+}
+
+static unsigned ew_blocks(long long n) { return (unsigned)std::min<long long>(cdiv(n, 256), 148LL * 16); }
+
+// ------------------------------------------------------------------ small kernels
+template <typename TB, typename TD, typename TO>
+__global__ void k_jacobi0(long long n, const TB* __restrict__ b, const TD* __restrict__ dinv, TO* __restrict__ x,
+                          const double* omega, double wscale) {
+  const double w = (*omega) * wscale;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    using Tc = TO;
+    const Tc wt = Conv<Tc>::from(w);
+    x[i] = wt * Conv<Tc>::from(dinv[i]) * Conv<Tc>::from(b[i]);
+  }
+}
+template <typename TA, typename TB, typename TO>
+__global__ void k_add(long long n, const TA* __restrict__ a, const TB* __restrict__ b, TO* __restrict__ o) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    o[i] = Conv<TO>::from((double)Conv<double>::from(a[i]) + (double)Conv<double>::from(b[i]));
+}
+template <typename TI, typename TO>
+__global__ void k_copy(long long n, const TI* __restrict__ a, TO* __restrict__ o) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    o[i] = Conv<TO>::from(a[i]);
+}
+__global__ void k_pcg_init(PcgState* st, double tol, int maxiter, double min_omega, double d_omega) {
+  st->tol = tol;
+  st->maxiter = maxiter;
+  st->min_omega = min_omega;
+  st->d_omega = d_omega;
+  st->omega = min_omega;
+  st->iter = 0;
+  st->done = 0;
+  st->rz = st->rz_new = st->pq = st->rr = st->alpha = st->beta = 0.0;
+  st->res = 0.0;
+}
+__global__ void k_pcg_check_bb(PcgState* st) {
+  // ||f|| == 0: nothing to solve, report residual 0 like a converged solve
+  if (st->bb == 0.0) {
+    st->done = 1;
+    st->res = 0.0;
+  }
+}
+
+// ------------------------------------------------------------------ multigrid setup
+template <typename T, typename TD0>
+static void mg_setup(Prob& P) {
+  const int L = P.n_level;
+  const Geo& g0 = P.g0;
+  const T* E = TypeOps<T>::E(P);
+  // fine Jacobi diagonal
+  k_fine_dinv<T, TD0><<<cdiv(g0.n, 256), 256, 0, P.stream>>>(g0, E, P.mask, P.dK0diag, (TD0*)P.lv[0].dinv, nullptr);
+  KCHECK();
+  if (L == 0) return;
+  // level 1 from the fine operator
+  {
+    const Geo& gc = P.lv[1].g;
+    const int nnb = P.dim == 3 ? 27 : 9;
+    dim3 grid(cdiv(gc.n, 128), nnb);
+    if (P.dim == 3)
+      k_galerkin3_l0<T, T><<<grid, 128, 0, P.stream>>>(g0, gc, E, P.mask, P.eflag, P.dQ, P.dK0b, (T*)P.lv[1].S);
+    else
+      k_galerkin2_l0<T, T><<<grid, 128, 0, P.stream>>>(g0, gc, E, P.mask, P.eflag, P.dQ, P.dK0b, (T*)P.lv[1].S);
+    KCHECK();
+  }
+  for (int l = 1; l < L; ++l) {
+    const Geo& gf = P.lv[l].g;
+    const Geo& gc = P.lv[l + 1].g;
+    const int nnb = P.dim == 3 ? 27 : 9;
+    dim3 grid(cdiv(gc.n, 128), nnb);
+    if (P.dim == 3)
+      k_galerkin3_st<T><<<grid, 128, 0, P.stream>>>(gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
+    else
+      k_galerkin2_st<T><<<grid, 128, 0, P.stream>>>(gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
+    KCHECK();
+  }
+  for (int l = 1; l < L; ++l) {
+    const Geo& g = P.lv[l].g;
+    k_st_dinv<T, T><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, (const T*)P.lv[l].S, (T*)P.lv[l].dinv);
+    KCHECK();
+  }
+  // coarsest: dense FP64 Cholesky and explicit inverse
+  const Geo& gL = P.lv[L].g;
+  const int nd = P.nd;
+  CK(cudaMemsetAsync(P.Adense, 0, (size_t)nd * nd * sizeof(double), P.stream));
+  k_st_to_dense<T><<<cdiv(gL.n, 256), 256, 0, P.stream>>>(gL, (const T*)P.lv[L].S, P.Adense, nd);
+  KCHECK();
+  CK(cudaMemsetAsync(P.chol_status, 0, sizeof(int), P.stream));
+  const int nt = (nd + CB - 1) / CB;
+  for (int K = 0; K < nt; ++K) {
+    k_chol_diag<<<1, CB * CB / 4, 0, P.stream>>>(P.Adense, nd, K, P.chol_status);
+    if (K + 1 < nt) {
+      k_chol_panel<<<nt - K - 1, CB * CB / 4, 0, P.stream>>>(P.Adense, nd, K);
+      const int m = nt - K - 1;
+      k_chol_update<<<m * (m + 1) / 2, CB * CB / 4, 0, P.stream>>>(P.Adense, nd, K, nt);
+    }
+  }
+  KCHECK();
+  k_transpose_lower<<<cdiv((long long)nd * nd, 256), 256, 0, P.stream>>>(P.Adense, P.Ut, nd);
+  if (nd * sizeof(double) > 48 * 1024)
+    CK(cudaFuncSetAttribute(k_chol_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(nd * sizeof(double))));
+  k_chol_inverse<<<nd, 256, nd * sizeof(double), P.stream>>>(P.Adense, P.Ut, P.Ainv, nd);
+  KCHECK();
+}
+
+// ------------------------------------------------------------------ V-cycle
+// Result in `out`; b and out have type T.  With dot_dst, the last fine sweep also
+// computes dotv . out (FP64 accumulation).
+template <typename T, typename TD0, typename TV>
+static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* dot_dst) {
+  Level& Lv = P.lv[l];
+  const Geo& g = Lv.g;
+  const long long nv = (long long)g.dof * g.n;
+  if (l == P.n_level) {
+    k_coarse_solve<T, T><<<cdiv((long long)P.nd * 32, 256), 256, 0, P.stream>>>(g, P.Ainv, P.nd, b, out);
+    KCHECK();
+    return;
+  }
+  const double ws = std::pow(1.06, l);
+  const double* om = &P.st->omega;
+  T* x = (T*)Lv.xa;
+  T* y = (T*)Lv.xb;
+  T* r = (T*)Lv.r;
+  auto sweep = [&](const T* bb, T* in, T* outv) {
+    if (l == 0) {
+      EpiJacobi<T, T, TD0> e{bb, (const TD0*)Lv.dinv, outv, om, ws, g.n};
+      level_apply<T>(P, l, in, e);
+    } else {
+      EpiJacobi<T, T, T> e{bb, (const T*)Lv.dinv, outv, om, ws, g.n};
+      level_apply<T>(P, l, in, e);
+    }
+  };
+  // pre-smoothing from x = 0
+  if (P.n_smooth >= 1) {
+    if (l == 0)
+      k_jacobi0<T, TD0, T><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, b, (const TD0*)Lv.dinv, x, om, ws);
+    else
+      k_jacobi0<T, T, T><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, b, (const T*)Lv.dinv, x, om, ws);
+    KCHECK();
+    for (int s = 1; s < P.n_smooth; ++s) {
+      sweep(b, x, y);
+      std::swap(x, y);
+    }
+  } else {
+    CK(cudaMemsetAsync(x, 0, nv * sizeof(T), P.stream));
+  }
+  bool first = true;
+  const int visits = (P.cycle_w && std::find(P.w_levels.begin(), P.w_levels.end(), l) != P.w_levels.end()) ? 2 : 1;
+  for (int vis = 0; vis < visits; ++vis) {
+    // residual on this level
+    {
+      EpiResid<T, T, T> e{b, r, g.n};
+      level_apply<T>(P, l, first ? x : out, e);
+    }
+    const T* xcur = first ? x : out;
+    Level& Lc = P.lv[l + 1];
+    if (P.dim == 3)
+      k_restrict3<T, T><<<dim3(cdiv(Lc.g.nz, 64), Lc.g.nx, Lc.g.ny), 64, 0, P.stream>>>(g, Lc.g, r, (T*)Lc.b);
+    else
+      k_restrict2<T, T><<<dim3(cdiv(Lc.g.nx, 64), Lc.g.ny), 64, 0, P.stream>>>(g, Lc.g, r, (T*)Lc.b);
+    KCHECK();
+    vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr);
+    T* e1 = (T*)Lv.ea;
+    T* e2 = (T*)Lv.eb;
+    if (P.dim == 3)
+      k_prolong3<T, T><<<dim3(cdiv(g.nz, 64), g.nx, g.ny), 64, 0, P.stream>>>(g, Lc.g, (const T*)Lc.res, e1);
+    else
+      k_prolong2<T, T><<<dim3(cdiv(g.nx, 64), g.ny), 64, 0, P.stream>>>(g, Lc.g, (const T*)Lc.res, e1);
+    KCHECK();
+    const bool last_visit = (vis == visits - 1);
+    if (P.n_smooth >= 1) {
+      for (int s = 0; s < P.n_smooth - 1; ++s) {
+        sweep(r, e1, e2);
+        std::swap(e1, e2);
+      }
+      const bool dot = last_visit && dot_dst != nullptr;
+      if (l == 0) {
+        if (dot) {
+          EpiJacobiAdd<T, T, TD0, T, true> e{r, (const TD0*)Lv.dinv, xcur, out, (const T*)dotv, om, ws, g.n};
+          level_apply<T>(P, l, e1, e, dot_dst);
+        } else {
+          EpiJacobiAdd<T, T, TD0, T, false> e{r, (const TD0*)Lv.dinv, xcur, out, (const T*)nullptr, om, ws, g.n};
+          level_apply<T>(P, l, e1, e);
+        }
+      } else {
+        EpiJacobiAdd<T, T, T, T, false> e{r, (const T*)Lv.dinv, xcur, out, (const T*)nullptr, om, ws, g.n};
+        level_apply<T>(P, l, e1, e);
+      }
+    } else {
+      k_add<T, T, T><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, xcur, e1, out);
+      KCHECK();
+      if (last_visit && dot_dst) {
+        k_dot<TV, T><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, dotv, out, P.part, P.ticket,
+                                                                                   dot_dst);
+        KCHECK();
+      }
+    }
+    first = false;
+  }
+}
+
+// ------------------------------------------------------------------ allocation of the hierarchy
+static void mg_allocate(Prob& P) {
+  const int L = P.n_level;
+  const size_t vb = vbytes(P.prec);
+  P.lv.clear();
+  P.lv.resize(L + 1);
+  for (int l = 0; l <= L; ++l) {
+    Level& Lv = P.lv[l];
+    Lv.g = level_geo(P, l);
+    const size_t nv = (size_t)Lv.g.dof * Lv.g.n;
+    auto vec = [&]() -> void* { return vb == 8 ? (void*)P.alloc<double>(nv) : (void*)P.alloc<float>(nv); };
+    if (l > 0) Lv.b = vec();
+    Lv.res = vec();
+    if (l < L) {
+      Lv.xa = vec();
+      Lv.xb = vec();
+      Lv.r = vec();
+      Lv.ea = vec();
+      Lv.eb = vec();
+      if (l == 0)
+        Lv.dinv = (P.prec == EDGE_FP64) ? (void*)P.alloc<double>(nv) : (void*)P.alloc<__nv_bfloat16>(nv);
+      else
+        Lv.dinv = vec();
+    }
+    if (l > 0) {
+      const size_t ns = (size_t)(P.dim == 3 ? 243 : 36) * Lv.g.n;
+      Lv.S = vb == 8 ? (void*)P.alloc<double>(ns) : (void*)P.alloc<float>(ns);
+    }
+  }
+  const Geo& gL = P.lv[L].g;
+  P.nd = gL.nx * gL.ny * gL.nz * gL.dof;
+  if (P.nd > 8192) fail(EDGE_EINVAL, "coarsest level has " + std::to_string(P.nd) + " DOFs; use more levels (<= 8192)");
+  P.Adense = P.alloc<double>((size_t)P.nd * P.nd);
+  P.Ainv = P.alloc<double>((size_t)P.nd * P.nd);
+  P.Ut = P.alloc<double>((size_t)P.nd * P.nd);
+}
+
+// ------------------------------------------------------------------ PCG
+template <typename T, typename TD0>
+static void pcg_fp64(Prob& P, double tol, int maxiter) {
+  // b64, x64 are set; T == double
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  double* r = P.r64;
+  double* x = P.x64;
+  double* p = (double*)P.p;
+  double* q = (double*)P.q;
+  double* z = (double*)P.lv[0].res;
+  k_pcg_init<<<1, 1, 0, P.stream>>>(P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
+  KCHECK();
+  // r = b - A x ; bb = b.b
+  {
+    EpiResid<double, double, double> e{P.b64, r, g.n};
+    fine_apply<double>(P, x, e, nullptr);
+  }
+  k_dot<double, double><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, P.b64, P.b64, P.part,
+                                                                                       P.ticket, &P.st->bb);
+  KCHECK();
+  k_pcg_check_bb<<<1, 1, 0, P.stream>>>(P.st);
+  vcycle<double, TD0, double>(P, 0, r, z, r, &P.st->rz_new);
+  k_copy<double, double><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, z, p);
+  KCHECK();
+  int it = 0;
+  for (;;) {
+    {
+      EpiStoreDot<double> e{q, g.n};
+      fine_apply<double>(P, p, e, &P.st->pq);
+    }
+    k_pcg_xr<double, double><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, x, p, r, q, P.st,
+                                                                                           P.part, P.ticket);
+    KCHECK();
+    CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
+    CK(cudaStreamSynchronize(P.stream));
+    ++it;
+    if (P.st_h->done) break;
+    vcycle<double, TD0, double>(P, 0, r, z, r, &P.st->rz_new);
+    k_pcg_p<double><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, p, z, P.st);
+    KCHECK();
+  }
+  P.last_iters = P.st_h->iter;
+}
+
+static void ensure_mg(Prob& P) {
+  if (P.n_level < 0) fail(EDGE_ESTATE, "multigrid not configured (edge_mg_config)");
+}
+
+static void solve_internal(Prob& P, double tol, int maxiter) {
+  ensure_mg(P);
+  if (!P.has_rho) fail(EDGE_ESTATE, "Solver requires a density vector to be passed or set on the kernel.");
+  CK(cudaEventRecord(P.ev[0], P.stream));
+  if (P.prec == EDGE_FP64) {
+    mg_setup<double, double>(P);
+  } else {
+    fail(EDGE_EINVAL, "mixed precision solve not available in this build");
+  }
+  CK(cudaEventRecord(P.ev[1], P.stream));
+  // check the coarse factorisation
+  int status = 0;
+  CK(cudaMemcpyAsync(&status, P.chol_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaStreamSynchronize(P.stream));
+  if (status) fail(EDGE_ENOTPD, "coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
+  pcg_fp64<double, double>(P, tol, maxiter);
+  CK(cudaEventRecord(P.ev[2], P.stream));
+  CK(cudaEventSynchronize(P.ev[2]));
+  float a = 0, b = 0;
+  CK(cudaEventElapsedTime(&a, P.ev[0], P.ev[1]));
+  CK(cudaEventElapsedTime(&b, P.ev[1], P.ev[2]));
+  P.last_setup_ms = a;
+  P.last_solve_ms = b;
+}
+
+}  // namespace edge
+
+using namespace edge;
+
+struct edge_problem {
+  Prob P;
+};
+struct edge_filter {
+  Geo g;
+  Taps taps;
+  double* N = nullptr;
+  long long n_el = 0;
+  ~edge_filter() {
+    if (N) cudaFree(N);
+  }
+};
+
+#define API_BEGIN try {
+#define API_END                 \
+  }                             \
+  catch (const EdgeError& e) {  \
+    g_err = e.msg;              \
+    return e.code;              \
+  }                             \
+  catch (const std::exception& e) { \
+    g_err = e.what();           \
+    return EDGE_ECUDA;          \
+  }                             \
+  return EDGE_OK;
+
+extern "C" {
+
+const char* edge_last_error(void) { return g_err.c_str(); }
+int edge_version(void) { return 1; }
+
+int edge_problem_create(int dim, const int* nel, const double* K0, int precision, edge_problem** out) {
+  API_BEGIN
+  if (!out || !nel || !K0) fail(EDGE_EINVAL, "null argument");
+  if (dim != 2 && dim != 3) fail(EDGE_EINVAL, "dim must be 2 or 3");
+  if (precision != EDGE_FP64 && precision != EDGE_MIXED) fail(EDGE_EINVAL, "unknown precision");
+  for (int d = 0; d < dim; ++d)
+    if (nel[d] < 1) fail(EDGE_EINVAL, "element counts must be >= 1");
+  auto* h = new edge_problem();
+  Prob& P = h->P;
+  try {
+    P.dim = dim;
+    P.prec = precision;
+    for (int d = 0; d < dim; ++d) P.nel[d] = nel[d];
+    P.g0 = make_geo(dim, nel[0], nel[1], dim == 3 ? nel[2] : 0);
+    P.n_el = (long long)nel[0] * nel[1] * (dim == 3 ? nel[2] : 1);
+    P.n_dof = (long long)P.g0.nx * P.g0.ny * P.g0.nz * dim;
+    analyse_element(dim, K0, P.ei);
+    const int nk = P.ei.nk;
+    P.dK0b = P.alloc<double>(nk * nk);
+    CK(cudaMemcpy(P.dK0b, P.ei.K0b, nk * nk * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<float> kf(nk * nk);
+    for (int i = 0; i < nk * nk; ++i) kf[i] = (float)P.ei.K0b[i];
+    P.dK0bf = P.alloc<float>(nk * nk);
+    CK(cudaMemcpy(P.dK0bf, kf.data(), nk * nk * sizeof(float), cudaMemcpyHostToDevice));
+    P.dK0diag = P.alloc<double>(nk);
+    CK(cudaMemcpy(P.dK0diag, P.ei.kdiag, nk * sizeof(double), cudaMemcpyHostToDevice));
+    P.dQ = P.alloc<double>(P.ei.Q.size());
+    CK(cudaMemcpy(P.dQ, P.ei.Q.data(), P.ei.Q.size() * sizeof(double), cudaMemcpyHostToDevice));
+    const Geo& g = P.g0;
+    P.mask = P.alloc<uint8_t>(g.n);
+    P.eflag = P.alloc<uint8_t>(g.n);
+    P.E64 = P.alloc<double>(g.n);
+    if (precision == EDGE_MIXED) P.E32 = P.alloc<float>(g.n);
+    const size_t nv = (size_t)g.dof * g.n;
+    P.b64 = P.alloc<double>(nv);
+    P.x64 = P.alloc<double>(nv);
+    P.r64 = P.alloc<double>(nv);
+    if (precision == EDGE_FP64) {
+      P.p = P.alloc<double>(nv);
+      P.q = P.alloc<double>(nv);
+    } else {
+      P.p = P.alloc<float>(nv);
+      P.q = P.alloc<float>(nv);
+      P.r32 = P.alloc<float>(nv);
+    }
+    P.rho_f = P.alloc<double>(P.n_el);
+    P.gsens = P.alloc<double>(P.n_el);
+    P.ocp = P.alloc<double>(P.n_el);
+    P.part_cap = 1 << 20;
+    P.part = P.alloc<double>(P.part_cap);
+    P.ticket = P.alloc<unsigned>(1);
+    P.st = P.alloc<PcgState>(1);
+    P.oc = P.alloc<OcState>(1);
+    P.scal = P.alloc<double>(16);
+    P.zero_int = P.alloc<int>(1);
+    P.chol_status = P.alloc<int>(1);
+    CK(cudaMallocHost(&P.st_h, sizeof(PcgState)));
+    CK(cudaMallocHost(&P.oc_h, sizeof(OcState)));
+    CK(cudaMallocHost(&P.scal_h, 16 * sizeof(double)));
+    for (int i = 0; i < 4; ++i) CK(cudaEventCreate(&P.ev[i]));
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  *out = h;
+  API_END
+}
+
+int edge_problem_destroy(edge_problem* p) {
+  API_BEGIN
+  if (p) {
+    cudaStreamSynchronize(p->P.stream);
+    delete p;
+  }
+  API_END
+}
+
+int edge_set_stream(edge_problem* p, void* stream) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.stream = (cudaStream_t)stream;
+  API_END
+}
+
+int edge_uses_transform(const edge_problem* p) { return p && p->P.ei.wht ? 1 : 0; }
+
+int edge_set_constraints(edge_problem* p, const uint8_t* cons_dev) {
+  API_BEGIN
+  if (!p || !cons_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  k_mask_from_user<<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, cons_dev, P.mask);
+  k_elem_flags<<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, P.mask, P.eflag);
+  KCHECK();
+  P.has_cons = true;
+  API_END
+}
+
+int edge_set_rho(edge_problem* p, const double* E_dev) {
+  API_BEGIN
+  if (!p || !E_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  k_elem_user_to_slots<double><<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, E_dev, P.E64);
+  if (P.E32) k_elem_user_to_slots<float><<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, E_dev, P.E32);
+  KCHECK();
+  P.has_rho = true;
+  API_END
+}
+
+int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev) {
+  API_BEGIN
+  if (!p || !u_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. dot works only after setting rho.");
+  const Geo& g = P.g0;
+  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, u_dev, P.b64);
+  EpiStore<double, double> e{P.r64, g.n};
+  fine_apply<double>(P, P.b64, e, nullptr);
+  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.r64, out_dev);
+  KCHECK();
+  API_END
+}
+
+// Same product through the dense kernel (used by tests as an independent path).
+int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev) {
+  API_BEGIN
+  if (!p || !u_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. dot works only after setting rho.");
+  const Geo& g = P.g0;
+  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, u_dev, P.b64);
+  EpiStore<double, double> e{P.r64, g.n};
+  fine_apply_dense<double>(P, P.b64, e, nullptr);
+  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.r64, out_dev);
+  KCHECK();
+  API_END
+}
+
+int edge_diagonal(edge_problem* p, double* diag_dev) {
+  API_BEGIN
+  if (!p || !diag_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. diagonal works only after setting rho or if rho is provided.");
+  const Geo& g = P.g0;
+  k_fine_dinv<double, double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.E64, P.mask, P.dK0diag, P.r64, diag_dev);
+  KCHECK();
+  API_END
+}
+
+int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev) {
+  API_BEGIN
+  if (!p || !U_dev || !dk_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  const Geo& g = P.g0;
+  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, U_dev, P.b64);
+  k_dk<double><<<cdiv(P.n_el, 256), 256, 0, P.stream>>>(g, P.b64, P.ei.k3, P.ei.k2, P.dK0b, P.ei.wht ? 1 : 0, dk_dev,
+                                                         nullptr, nullptr, 0.0, 0.0);
+  KCHECK();
+  API_END
+}
+
+int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, double min_omega, int cycle_w,
+                   const int* w_levels, int n_w) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  Prob& P = p->P;
+  if (n_level < 1 || n_smooth < 0) fail(EDGE_EINVAL, "n_level must be >= 1 and n_smooth >= 0");
+  for (int l = 1; l <= n_level; ++l) {
+    Geo g = level_geo(P, l);
+    if (g.nx < 2 || g.ny < 2 || (P.dim == 3 && g.nz < 2))
+      fail(EDGE_EINVAL, "n_level too large for this mesh: level " + std::to_string(l) + " has no elements");
+  }
+  cudaStreamSynchronize(P.stream);
+  const bool realloc = (n_level != P.n_level);
+  P.n_smooth = n_smooth;
+  P.omega = omega;
+  P.min_omega = std::max(omega / 2, min_omega);
+  P.cycle_w = cycle_w != 0;
+  P.w_levels.assign(w_levels, w_levels + (w_levels ? n_w : 0));
+  if (realloc) {
+    // free the old hierarchy
+    for (auto& Lv : P.lv) {
+      for (void* q : {Lv.b, Lv.xa, Lv.xb, Lv.r, Lv.ea, Lv.eb, Lv.res, Lv.S, Lv.dinv}) {
+        if (!q) continue;
+        auto it = std::find(P.allocs.begin(), P.allocs.end(), q);
+        if (it != P.allocs.end()) {
+          cudaFree(q);
+          P.allocs.erase(it);
+        }
+      }
+    }
+    for (void* q : {(void*)P.Adense, (void*)P.Ainv, (void*)P.Ut}) {
+      if (!q) continue;
+      auto it = std::find(P.allocs.begin(), P.allocs.end(), q);
+      if (it != P.allocs.end()) {
+        cudaFree(q);
+        P.allocs.erase(it);
+      }
+    }
+    P.n_level = n_level;
+    mg_allocate(P);
+  }
+  API_END
+}
+
+int edge_mg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
+                  double* residual_out, int* iters_out) {
+  API_BEGIN
+  if (!p || !f_dev || !x_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  const Geo& g = P.g0;
+  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, f_dev, P.b64);
+  if (use_last)
+    k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, x_dev, P.x64);
+  else
+    CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
+  KCHECK();
+  solve_internal(P, tol, maxiter);
+  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.x64, x_dev);
+  KCHECK();
+  CK(cudaStreamSynchronize(P.stream));
+  if (residual_out) *residual_out = P.st_h->res;
+  if (iters_out) *iters_out = P.st_h->iter;
+  API_END
+}
+
+int edge_last_solve_stats(const edge_problem* p, double* setup_ms, double* solve_ms, int* pcg_iters,
+                          int* true_residuals) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  const Prob& P = p->P;
+  if (setup_ms) *setup_ms = P.last_setup_ms;
+  if (solve_ms) *solve_ms = P.last_solve_ms;
+  if (pcg_iters) *pcg_iters = P.last_iters;
+  if (true_residuals) *true_residuals = P.last_true_res;
+  API_END
+}
+
+static void transfer(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream, bool restrict_) {
+  if (dim != 2 && dim != 3) fail(EDGE_EINVAL, "dim must be 2 or 3");
+  Geo gf = make_geo(dim, nel[0], nel[1], dim == 3 ? nel[2] : 0);
+  Geo gc = make_geo(dim, nel[0] / 2, nel[1] / 2, dim == 3 ? nel[2] / 2 : 0);
+  cudaStream_t s = (cudaStream_t)stream;
+  double *vf = nullptr, *vc = nullptr;
+  CK(cudaMallocAsync((void**)&vf, (size_t)gf.dof * gf.n * sizeof(double), s));
+  CK(cudaMallocAsync((void**)&vc, (size_t)gc.dof * gc.n * sizeof(double), s));
+  if (restrict_) {
+    k_user_to_slots<double><<<cdiv(gf.n, 256), 256, 0, s>>>(gf, in_dev, vf);
+    if (dim == 3)
+      k_restrict3<double, double><<<dim3(cdiv(gc.nz, 64), gc.nx, gc.ny), 64, 0, s>>>(gf, gc, vf, vc);
+    else
+      k_restrict2<double, double><<<dim3(cdiv(gc.nx, 64), gc.ny), 64, 0, s>>>(gf, gc, vf, vc);
+    k_slots_to_user<double><<<cdiv(gc.n, 256), 256, 0, s>>>(gc, vc, out_dev);
+  } else {
+    CK(cudaMemsetAsync(vc, 0, (size_t)gc.dof * gc.n * sizeof(double), s));
+    k_user_to_slots<double><<<cdiv(gc.n, 256), 256, 0, s>>>(gc, in_dev, vc);
+    if (dim == 3)
+      k_prolong3<double, double><<<dim3(cdiv(gf.nz, 64), gf.nx, gf.ny), 64, 0, s>>>(gf, gc, vc, vf);
+    else
+      k_prolong2<double, double><<<dim3(cdiv(gf.nx, 64), gf.ny), 64, 0, s>>>(gf, gc, vc, vf);
+    k_slots_to_user<double><<<cdiv(gf.n, 256), 256, 0, s>>>(gf, vf, out_dev);
+  }
+  KCHECK();
+  CK(cudaFreeAsync(vf, s));
+  CK(cudaFreeAsync(vc, s));
+}
+
+int edge_restrict(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream) {
+  API_BEGIN
+  if (!nel || !in_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  transfer(dim, nel, in_dev, out_dev, stream, true);
+  API_END
+}
+
+int edge_prolong(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream) {
+  API_BEGIN
+  if (!nel || !in_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  transfer(dim, nel, in_dev, out_dev, stream, false);
+  API_END
+}
+
+int edge_filter_create(int dim, const int* nel, int n_taps, const int* offsets, const double* weights,
+                       edge_filter** out) {
+  API_BEGIN
+  if (!nel || !offsets || !weights || !out) fail(EDGE_EINVAL, "null argument");
+  if (dim != 2 && dim != 3) fail(EDGE_EINVAL, "dim must be 2 or 3");
+  if (n_taps < 1 || n_taps > MAX_TAPS) fail(EDGE_EINVAL, "filter radius gives " + std::to_string(n_taps) + " taps (max " + std::to_string(MAX_TAPS) + ")");
+  auto* f = new edge_filter();
+  f->g = make_geo(dim, nel[0], nel[1], dim == 3 ? nel[2] : 0);
+  f->n_el = (long long)nel[0] * nel[1] * (dim == 3 ? nel[2] : 1);
+  f->taps.n = n_taps;
+  for (int t = 0; t < n_taps; ++t) {
+    for (int d = 0; d < 3; ++d) f->taps.off[t][d] = offsets[t * 3 + d];
+    f->taps.w[t] = weights[t];
+  }
+  cudaError_t e = cudaMalloc(&f->N, f->n_el * sizeof(double));
+  if (e != cudaSuccess) {
+    delete f;
+    fail(EDGE_ECUDA, cudaGetErrorString(e));
+  }
+  k_filter_norm<<<cdiv(f->n_el, 256), 256>>>(f->g, f->taps, f->N);
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    delete f;
+    fail(EDGE_ECUDA, cudaGetErrorString(e));
+  }
+  *out = f;
+  API_END
+}
+
+int edge_filter_destroy(edge_filter* f) {
+  API_BEGIN
+  delete f;
+  API_END
+}
+
+int edge_filter_apply(edge_filter* f, const double* in_dev, double* out_dev, void* stream) {
+  API_BEGIN
+  if (!f || !in_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  k_filter<<<cdiv(f->n_el, 256), 256, 0, (cudaStream_t)stream>>>(f->g, f->taps, in_dev, out_dev);
+  KCHECK();
+  API_END
+}
+
+int edge_filter_apply_T(edge_filter* f, const double* in_dev, double* out_dev, void* stream) {
+  API_BEGIN
+  if (!f || !in_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  k_filter_T<<<cdiv(f->n_el, 256), 256, 0, (cudaStream_t)stream>>>(f->g, f->taps, f->N, in_dev, out_dev);
+  KCHECK();
+  API_END
+}
+
+static void oc_run(Prob& P, long long n, const double* rho, const double* dr, double A, double vol, double vf,
+                   double move, double* rho_new) {
+  if (n != P.n_el) fail(EDGE_EINVAL, "OC vector length does not match the number of elements");
+  const unsigned nb = std::min<unsigned>(ew_blocks(n), 1024);
+  k_oc_prep<<<nb, 256, 0, P.stream>>>(n, rho, dr, A, P.ocp, P.part, P.ticket, P.scal);
+  k_oc_floor<<<nb, 256, 0, P.stream>>>(n, P.ocp, P.scal);
+  OcState init{};
+  init.l1 = 1e-9;
+  init.l2 = 1e9;
+  init.last = 0.5 * (init.l1 + init.l2);
+  init.vf = vf;
+  init.vol = vol;
+  *P.oc_h = init;
+  CK(cudaMemcpyAsync(P.oc, P.oc_h, sizeof(OcState), cudaMemcpyHostToDevice, P.stream));
+  const unsigned nbp = std::min<unsigned>(nb, (unsigned)(P.part_cap / OC_NODES));
+  const int max_pass = (200 + OC_DEPTH - 1) / OC_DEPTH;
+  for (int pass = 0; pass < max_pass; ++pass) {
+    k_oc_pass<<<nbp, 256, 0, P.stream>>>(n, rho, P.ocp, A, move, P.oc, P.part, P.ticket);
+    if ((pass & 3) == 3) {
+      CK(cudaMemcpyAsync(P.oc_h, P.oc, sizeof(OcState), cudaMemcpyDeviceToHost, P.stream));
+      CK(cudaStreamSynchronize(P.stream));
+      if (P.oc_h->done) break;
+    }
+  }
+  KCHECK();
+  k_oc_final<<<nb, 256, 0, P.stream>>>(n, rho, P.ocp, move, P.oc, rho_new, P.part, P.ticket, P.scal + 1);
+  KCHECK();
+  CK(cudaMemcpyAsync(P.oc_h, P.oc, sizeof(OcState), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaMemcpyAsync(P.scal_h, P.scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaStreamSynchronize(P.stream));
+}
+
+int edge_oc_update(edge_problem* p, const double* rho_dev, const double* dr_dev, double A, double vol, double vf,
+                   double move, double* rho_new_dev, double* lambda_out, int* steps_out, double* sqchange_out) {
+  API_BEGIN
+  if (!p || !rho_dev || !dr_dev || !rho_new_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  oc_run(P, P.n_el, rho_dev, dr_dev, A, vol, vf, move, rho_new_dev);
+  if (lambda_out) *lambda_out = P.oc_h->last;
+  if (steps_out) *steps_out = P.oc_h->steps;
+  if (sqchange_out) *sqchange_out = P.scal_h[1];
+  API_END
+}
+
+int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* rho_dev, double penalty, double void_,
+                                const double* f_dev, double* U_dev, int use_last, double tol, int maxiter,
+                                double* compliance_out, double* dr_dev, double* rho_f_dev, double* residual_out,
+                                int* iters_out) {
+  API_BEGIN
+  if (!p || !f || !rho_dev || !f_dev || !U_dev || !dr_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  const Geo& g = P.g0;
+  if (f->n_el != P.n_el) fail(EDGE_EINVAL, "filter and mesh sizes differ");
+  double* rf = rho_f_dev ? rho_f_dev : P.rho_f;
+  const unsigned nbe = cdiv(P.n_el, 256);
+  // rho_f = H rho ; E = clip(rho_f^p, void, 1)
+  k_filter_material<double, float><<<nbe, 256, 0, P.stream>>>(g, f->taps, rho_dev, rf, P.E64, P.E32, penalty, void_, 0);
+  KCHECK();
+  P.has_rho = true;
+  // U = K(E)^-1 f (warm start from U_dev)
+  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, f_dev, P.b64);
+  if (use_last)
+    k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, U_dev, P.x64);
+  else
+    CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
+  KCHECK();
+  solve_internal(P, tol, maxiter);
+  const long long nv = (long long)g.dof * g.n;
+  // compliance c = f . U
+  k_dot<double, double><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, P.b64, P.x64, P.part,
+                                                                                       P.ticket, P.scal + 2);
+  // dr = H^T (p clip(rho_f)^(p-1) dk)
+  k_dk<double><<<nbe, 256, 0, P.stream>>>(g, P.x64, P.ei.k3, P.ei.k2, P.dK0b, P.ei.wht ? 1 : 0, nullptr, rf, P.gsens,
+                                          penalty, void_);
+  k_filter_T<<<nbe, 256, 0, P.stream>>>(f->g, f->taps, f->N, P.gsens, dr_dev);
+  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.x64, U_dev);
+  KCHECK();
+  CK(cudaMemcpyAsync(P.scal_h + 2, P.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaStreamSynchronize(P.stream));
+  if (compliance_out) *compliance_out = P.scal_h[2];
+  if (residual_out) *residual_out = P.st_h->res;
+  if (iters_out) *iters_out = P.st_h->iter;
+  API_END
+}
+
+}  // extern "C"

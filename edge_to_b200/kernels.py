@@ -1,0 +1,178 @@
+"""Matrix-free structured stiffness kernel K(rho), drop-in for StructuredStiffnessKernel
+(kernels/_cuda.py:62-302) on CuStructuredMesh2D/3D.
+
+Vectors are torch CUDA tensors in the reference layout (FP64, v[node*dof + c]); the
+operator itself runs in libedge_b200.so (hand-written sm_100a kernels).  As in the
+reference, ``dot`` returns a buffer that the next call overwrites
+(kernels/_cuda.py:175-204), and constrained DOFs act as identity rows/columns.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def _as_dev_f64(x, name="array"):
+    if isinstance(x, np.ndarray):
+        x = torch.from_numpy(x)
+    if not isinstance(x, torch.Tensor):
+        raise NotImplementedError("Only torch tensors (or numpy arrays) are supported as vectors.")
+    if x.dtype != torch.float64 or not x.is_cuda or not x.is_contiguous():
+        x = x.to(device="cuda", dtype=torch.float64).contiguous()
+    return x
+
+
+class StiffnessKernel:
+    def __init__(self):
+        self.has_rho = False
+        self.rho = None
+        self.shape = None
+        self.matvec = self.dot
+        self.rmatvec = self.dot
+
+    def __matmul__(self, rhs):
+        return self.dot(rhs)
+
+
+class CuStructuredStiffnessKernel(StiffnessKernel):
+    def __init__(self, mesh):
+        super().__init__()
+        self.mesh = mesh
+        self.dof = mesh.dof
+        self.K_single = mesh.K_single
+        self.dtype = mesh.dtype
+        self.elements_size = mesh.elements_size
+        self.n_nodes = mesh.n_nodes
+        self.n_elements = mesh.n_elements
+        self.dim = len(mesh.nel)
+        self.shape = (self.n_nodes * self.dof, self.n_nodes * self.dof)
+        self.constraints = torch.zeros(self.n_nodes * self.dof, dtype=torch.bool, device="cuda")
+        self.has_con = False
+        self.mat_vec = None
+        self.diag = None
+        self.dk = None
+        h = ctypes.c_void_p()
+        nel = _lib.int_array(list(mesh.nel) + [1] * (3 - self.dim))
+        K0 = np.ascontiguousarray(np.asarray(mesh.K_single, dtype=np.float64))
+        _lib.call("edge_problem_create", self.dim, nel, K0.ctypes.data_as(_lib.c_double_p), _lib.EDGE_FP64,
+                  ctypes.byref(h))
+        self._h = h
+        self._bind_stream()
+
+    # --------------------------------------------------------------- plumbing
+    @property
+    def handle(self):
+        return self._h
+
+    def _bind_stream(self):
+        _lib.call("edge_set_stream", self._h, _lib.stream_ptr())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().edge_problem_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def uses_transform(self):
+        return bool(_lib.lib().edge_uses_transform(self._h))
+
+    # --------------------------------------------------------------- reference API
+    def set_rho(self, rho):
+        rho = _as_dev_f64(rho)
+        if rho.numel() != self.n_elements:
+            raise ValueError("rho size does not match the number of elements.")
+        self.rho = rho
+        self._bind_stream()
+        _lib.call("edge_set_rho", self._h, _lib.ptr(rho))
+        self.has_rho = True
+
+    def _push_constraints(self):
+        self._bind_stream()
+        c = self.constraints.to(torch.uint8).contiguous()
+        _lib.call("edge_set_constraints", self._h, _lib.ptr(c))
+        torch.cuda.current_stream().synchronize()
+
+    def set_constraints(self, constraints):
+        self.constraints[:] = False
+        idx = torch.as_tensor(np.asarray(constraints, dtype=np.int64) if not isinstance(constraints, torch.Tensor)
+                              else constraints, device="cuda").long()
+        if idx.numel():
+            self.constraints[idx] = True
+        self.has_con = True
+        self._push_constraints()
+
+    def add_constraints(self, constraints):
+        idx = torch.as_tensor(np.asarray(constraints, dtype=np.int64) if not isinstance(constraints, torch.Tensor)
+                              else constraints, device="cuda").long()
+        if idx.numel():
+            self.constraints[idx] = True
+        self.has_con = True
+        self._push_constraints()
+
+    def reset(self):
+        self.has_rho = False
+        self.rho = None
+        self.constraints[:] = False
+        self.has_con = False
+        self._push_constraints()
+        self.mat_vec = None
+        self.diag = None
+        self.dk = None
+
+    def _matvec(self, rho, vec):
+        if rho is not self.rho:
+            self.set_rho(rho)
+        return self.dot(vec)
+
+    def _rmatvec(self, rho, vec):
+        return self._matvec(rho, vec)
+
+    def dot(self, rhs):
+        if not self.has_rho:
+            raise ValueError("Rho has not been set. dot works only after setting rho.")
+        if not isinstance(rhs, (torch.Tensor, np.ndarray)):
+            raise NotImplementedError("Only torch tensors as vectors are supported.")
+        if rhs.shape[0] != self.n_nodes * self.dof:
+            raise ValueError("Shape of the input vector does not match the number of nodes and dof.")
+        u = _as_dev_f64(rhs)
+        if self.mat_vec is None:
+            self.mat_vec = torch.empty(self.shape[0], dtype=torch.float64, device="cuda")
+        self._bind_stream()
+        _lib.call("edge_matvec", self._h, _lib.ptr(u), _lib.ptr(self.mat_vec))
+        return self.mat_vec
+
+    def dot_dense(self, rhs):
+        """The same product through the dense node-centric kernel (cross-check path)."""
+        u = _as_dev_f64(rhs)
+        out = torch.empty(self.shape[0], dtype=torch.float64, device="cuda")
+        self._bind_stream()
+        _lib.call("edge_matvec_dense", self._h, _lib.ptr(u), _lib.ptr(out))
+        return out
+
+    def diagonal(self, rho=None):
+        if rho is None and not self.has_rho:
+            raise ValueError("Rho has not been set. diagonal works only after setting rho or if rho is provided.")
+        if rho is not None:
+            self.set_rho(rho)
+        if self.diag is None:
+            self.diag = torch.empty(self.shape[0], dtype=torch.float64, device="cuda")
+        self._bind_stream()
+        _lib.call("edge_diagonal", self._h, _lib.ptr(self.diag))
+        return self.diag
+
+    def process_grad(self, U):
+        U = _as_dev_f64(U)
+        if self.dk is None:
+            self.dk = torch.empty(self.n_elements, dtype=torch.float64, device="cuda")
+        self._bind_stream()
+        _lib.call("edge_process_grad", self._h, _lib.ptr(U), _lib.ptr(self.dk))
+        return self.dk
+
+
+StructuredStiffnessKernel = CuStructuredStiffnessKernel

@@ -1,0 +1,109 @@
+"""Geometric-multigrid-preconditioned CG, drop-in for CuMultiGrid
+(solvers/_multigrid_cuda.py:15-242) on the structured stiffness kernel of this package.
+
+Same constructor keywords and the same algorithm: Galerkin hierarchy rebuilt on every
+solve, damped-Jacobi V-cycle with omega*1.06^level, exact coarsest solve, PCG with warm
+start from the last solution and the residual-driven omega schedule; omega is reset to
+min_omega at the start of each solve as the GPU reference does.  The coarsest level is
+factorised by a dense FP64 Cholesky on the GPU (exact, like the reference's splu), so
+coarse_solver only selects between equivalent exact solves.
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+from .kernels import CuStructuredStiffnessKernel, _as_dev_f64
+
+
+class Solver:
+    def __call__(self, *args, **kwargs):
+        return self.solve(*args, **kwargs)
+
+    def solve(self, *args, **kwargs):
+        pass
+
+    def reset(self):
+        pass
+
+
+class CuMultiGrid(Solver):
+    def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
+                 w_level=1, coarse_solver="splu", matrix_free=False, low_level_tol=1e-8, low_level_maxiter=5000,
+                 min_omega=0.4, omega_boost=1.06, precision="fp64"):
+        if not isinstance(kernel, CuStructuredStiffnessKernel):
+            raise TypeError("CuMultiGrid needs the package's CuStructuredStiffnessKernel")
+        self.kernel = kernel
+        self.mesh = mesh
+        self.last_x0 = None
+        self.tol = tol
+        self.maxiter = maxiter
+        self.n_smooth = n_smooth
+        self.omega = omega
+        self.max_omega = omega
+        self.min_omega = max(omega / 2, min_omega)
+        self.d_omega = self.max_omega - self.min_omega
+        self.omega_boost = omega_boost
+        self.n_level = n_level
+        self.cycle = cycle
+        self.w_level = [w_level] if isinstance(w_level, int) else list(w_level)
+        self.matrix_free = matrix_free
+        self.dof = mesh.dof
+        self.coarse_solver = coarse_solver
+        self.low_level_tol = low_level_tol
+        self.low_level_maxiter = low_level_maxiter
+        self.precision = precision
+        if coarse_solver in ("splu", "spsolve") and matrix_free:
+            raise ValueError("Matrix free is not supported with splu solver use cg instead.")
+        if coarse_solver not in ("cg", "gmres", "splu", "spsolve"):
+            raise ValueError("Coarse solver not recognized.")
+        if matrix_free:
+            raise NotImplementedError("Matrix free is not implemented yet.")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.last_iters = 0
+        self._configured = None
+
+    def reset(self):
+        self.last_x0 = None
+
+    def _configure(self):
+        key = (self.n_level, self.n_smooth, self.max_omega, self.min_omega, self.cycle, tuple(self.w_level))
+        if self._configured == key:
+            return
+        w = _lib.int_array(self.w_level) if self.w_level else None
+        _lib.call("edge_mg_config", self.kernel.handle, int(self.n_level), int(self.n_smooth), float(self.max_omega),
+                  float(self.min_omega), 1 if self.cycle == "w" else 0, w, len(self.w_level))
+        self._configured = key
+
+    def solve(self, rhs, rho=None, use_last=True):
+        if not (self.kernel.has_rho or rho is not None):
+            raise ValueError("Solver requires a density vector to be passed or set on the kernel.")
+        if rho is not None:
+            self.kernel.set_rho(rho)
+        self._configure()
+        f = _as_dev_f64(rhs)
+        if use_last and self.last_x0 is not None:
+            x = self.last_x0
+            warm = 1
+        else:
+            x = torch.zeros_like(f)
+            warm = 0
+        res = ctypes.c_double()
+        its = ctypes.c_int()
+        self.kernel._bind_stream()
+        _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
+                  int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
+        self.last_x0 = x
+        self.last_iters = its.value
+        return x, res.value
+
+    def stats(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        i, t = ctypes.c_int(), ctypes.c_int()
+        _lib.call("edge_last_solve_stats", self.kernel.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(i),
+                  ctypes.byref(t))
+        return {"setup_ms": a.value, "solve_ms": b.value, "pcg_iters": i.value, "true_residuals": t.value}
+
+
+MultiGrid = CuMultiGrid

@@ -1,0 +1,102 @@
+/* C ABI of the B200 SIMP / GMG-PCG library (libedge_b200.so).
+ *
+ * Every pointer argument named *_dev is a CUDA device pointer owned by the caller; the
+ * library owns only the workspaces it allocates in *_create / edge_mg_config and never
+ * allocates on the solve path.  Arrays use the reference's (ahnobari/EDGE-TO) layouts:
+ *   DOF vectors      v[node*dof + c], node = j*nx*nz + i*nz + k (3-D) or j*nx + i (2-D)
+ *   element arrays   e = i*nely*nelz + j*nelz + k (3-D) or i*nely + j (2-D)
+ *   constraint mask  one byte per DOF (nonzero = constrained)
+ * (core/_geom.py:4-59).  All calls return EDGE_OK or an error code; edge_last_error()
+ * gives the message of the last failing call on the calling thread.  A handle is not
+ * thread-safe; calls on one handle are ordered on the handle's stream.
+ */
+#ifndef EDGE_B200_H
+#define EDGE_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDGE_OK 0
+#define EDGE_EINVAL 1   /* bad argument or shape: Python ValueError             */
+#define EDGE_ECUDA 2    /* CUDA runtime error: Python RuntimeError              */
+#define EDGE_ENOTPD 3   /* coarsest Galerkin matrix not positive definite       */
+#define EDGE_ESTATE 4   /* call out of order (e.g. rho not set): ValueError     */
+
+#define EDGE_FP64 0     /* every level and vector in FP64 (the plain FP64 path) */
+#define EDGE_MIXED 1    /* FP32 operator/V-cycle, BF16 fine Jacobi diagonal,
+                           FP64 x, r, dot products, true residuals, coarse solve */
+
+typedef struct edge_problem edge_problem;
+typedef struct edge_filter edge_filter;
+
+const char* edge_last_error(void);
+int edge_version(void);
+
+/* ---- structured mesh + stiffness operator.
+ * Replaces StructuredStiffnessKernel (kernels/_cuda.py:62-302) built on
+ * CuStructuredMesh2D/3D (geom/_mesh.py:81-143).  K0 is the element stiffness of
+ * element 0 (host, row-major (2^dim*dim)^2, the reference's local node order). */
+int edge_problem_create(int dim, const int* nel, const double* K0, int precision, edge_problem** out);
+int edge_problem_destroy(edge_problem* p);
+int edge_set_stream(edge_problem* p, void* stream);
+/* kernels/_cuda.py:141-150 (set_constraints / add_constraints after the caller merged them) */
+int edge_set_constraints(edge_problem* p, const uint8_t* cons_dev);
+/* kernels/_cuda.py:36-38 : E is the penalised density per element (user order, FP64) */
+int edge_set_rho(edge_problem* p, const double* E_dev);
+/* kernels/_cuda.py:173-204, 278-302 : out = K(E) u with BC rows/cols -> identity */
+int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev);
+/* kernels/_cuda.py:105-139 : diag(K(E)), 1 on constrained DOFs */
+int edge_diagonal(edge_problem* p, double* diag_dev);
+/* kernels/_cuda.py:152-156 : dk_e = -u_e^T K0 u_e */
+int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev);
+/* Same product through the dense node-centric kernel (an independent path for tests). */
+int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
+/* 1 when the element matrix has the box structure used by the transform kernels */
+int edge_uses_transform(const edge_problem* p);
+
+/* ---- geometric multigrid PCG.  Replaces CuMultiGrid (solvers/_multigrid_cuda.py:15-242).
+ * cycle_w != 0 reproduces cycle == 'w' (second coarse visit on the levels in w_levels). */
+int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, double min_omega, int cycle_w,
+                   const int* w_levels, int n_w);
+/* Solves K(E) x = f to ||r||/||f|| < tol.  x_dev holds the warm start when use_last != 0
+ * and receives the solution.  Never fails on non-convergence: *residual_out reports it. */
+int edge_mg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
+                  double* residual_out, int* iters_out);
+
+/* ---- grid transfers.  Replace apply_restriction_cuda / apply_prolongation_cuda
+ * (core/_mgm_cuda.py:223-314); nel is the FINE grid. */
+int edge_restrict(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream);
+int edge_prolong(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream);
+
+/* ---- density filter.  Replaces CuStructuredFilter2D/3D (geom/_filters.py:164-254):
+ * offsets (n_taps x 3 ints, dz = 0 in 2-D) and globally normalised weights. */
+int edge_filter_create(int dim, const int* nel, int n_taps, const int* offsets, const double* weights,
+                       edge_filter** out);
+int edge_filter_destroy(edge_filter* f);
+int edge_filter_apply(edge_filter* f, const double* in_dev, double* out_dev, void* stream);
+int edge_filter_apply_T(edge_filter* f, const double* in_dev, double* out_dev, void* stream);
+
+/* ---- OC update.  Replaces TopOpt.update_design (TopOpt/_cuda.py:242-280) with
+ * SingleMaterial.ocP / evaluate_constraint (MaterialModels.py:75-90).  Also returns
+ * sum((rho_new - rho)^2) for the RMS design change. */
+int edge_oc_update(edge_problem* p, const double* rho_dev, const double* dr_dev, double A, double vol, double vf,
+                   double move, double* rho_new_dev, double* lambda_out, int* steps_out, double* sqchange_out);
+
+/* ---- one SIMP analysis, fused.  Replaces TopOpt.solve_and_process (TopOpt/_cuda.py:282-302)
+ * for SingleMaterial: rho_f = H rho, E = clip(rho_f^p, void, 1), solve, c = f.U,
+ * dr = H^T (p clip(rho_f, void, 1)^(p-1) dk). */
+int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* rho_dev, double penalty,
+                                double void_, const double* f_dev, double* U_dev, int use_last, double tol,
+                                int maxiter, double* compliance_out, double* dr_dev, double* rho_f_dev,
+                                double* residual_out, int* iters_out);
+
+/* Kernel timing of the last edge_mg_solve (ms), for the benchmarks. */
+int edge_last_solve_stats(const edge_problem* p, double* setup_ms, double* solve_ms, int* pcg_iters,
+                          int* true_residuals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,175 @@
+"""Op-level parity of the CUDA path against the reference-generated fixtures and the oracle.
+
+Tolerance: FP64 kernels must match to 1e-12 relative (max-norm), since only the order of
+floating-point additions differs from the reference.
+"""
+import numpy as np
+import pytest
+
+from oracle import elements, ops, topopt
+from oracle.grid import Grid
+
+pytestmark = pytest.mark.gpu
+
+H_OF = {2: {"even": None, "odd": None, "aniso": (0.5, 0.25)},
+        3: {"even": None, "odd": None, "aniso": (0.5, 0.25, 0.5)}}
+TOL = 1e-12
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _mesh(dim, nel, h, nu=0.3):
+    import edge_to_b200 as eb
+    st = lambda x: eb.auto_stiffness(x, 1.0, nu)  # noqa: E731
+    h = h or (1.0,) * dim
+    if dim == 2:
+        return eb.CuStructuredMesh2D(nel[0], nel[1], nel[0] * h[0], nel[1] * h[1], stiffness=st)
+    return eb.CuStructuredMesh3D(nel[0], nel[1], nel[2], nel[0] * h[0], nel[1] * h[1], nel[2] * h[2], stiffness=st)
+
+
+def _cases(golden):
+    for dim, fn in ((2, "ops_2d.npz"), (3, "ops_3d.npz")):
+        z = golden(fn)
+        for tag in ("even", "odd", "aniso"):
+            yield dim, tag, z, tuple(int(v) for v in z[f"{tag}_nel"]), H_OF[dim][tag]
+
+
+def test_matvec_diag_dk_against_reference(golden):
+    import torch
+    import edge_to_b200 as eb
+    for dim, tag, z, nel, h in _cases(golden):
+        mesh = _mesh(dim, nel, h)
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        assert k.uses_transform
+        E = torch.as_tensor(z[f"{tag}_E"], device="cuda")
+        u = torch.as_tensor(z[f"{tag}_u"], device="cuda")
+        k.set_rho(E)
+        assert rel(k.dot(u).cpu(), z[f"{tag}_matvec_nocon"]) < TOL, (dim, tag)
+        assert rel(k.dot_dense(u).cpu(), z[f"{tag}_matvec_nocon"]) < TOL, (dim, tag)
+        k.add_constraints(z[f"{tag}_cons"])
+        assert rel(k.dot(u).cpu(), z[f"{tag}_matvec"]) < TOL, (dim, tag)
+        assert rel(k.dot_dense(u).cpu(), z[f"{tag}_matvec"]) < TOL, (dim, tag)
+        assert rel(k.diagonal().cpu(), z[f"{tag}_diag"]) < TOL, (dim, tag)
+        assert rel(k.process_grad(u).cpu(), z[f"{tag}_dk"]) < TOL, (dim, tag)
+
+
+@pytest.mark.parametrize("nel", [(33, 17), (64, 31), (130, 3), (5, 70), (7, 5, 3), (40, 9, 33), (9, 33, 65), (3, 3, 130)])
+def test_matvec_ragged_sizes(nel):
+    """Tile edges: sizes that are not multiples of the 31-node / 7-column tiles."""
+    import torch
+    import edge_to_b200 as eb
+    dim = len(nel)
+    rng = np.random.default_rng(sum(nel))
+    mesh = _mesh(dim, nel, None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    g = Grid(nel)
+    E = rng.uniform(1e-3, 1, g.n_el)
+    E[rng.random(g.n_el) < 0.2] = 1e-9
+    u = rng.standard_normal(g.n_dof)
+    cons = np.where(rng.random(g.n_dof) < 0.1)[0]
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    k.add_constraints(cons)
+    K0 = elements.q4_stiffness(1, 1, 1, 0.3) if dim == 2 else elements.hex8_stiffness(1, 1, 1, 1, 0.3)
+    ref = ops.assemble(g, K0, E, cons) @ u
+    ut = torch.as_tensor(u, device="cuda")
+    assert rel(k.dot(ut).cpu(), ref) < TOL
+    assert rel(k.dot_dense(ut).cpu(), ref) < TOL
+
+
+def test_filter_against_reference(golden):
+    import torch
+    import edge_to_b200 as eb
+    n = 0
+    for dim, tag, z, nel, h in _cases(golden):
+        mesh = _mesh(dim, nel, h)
+        for key in z.files:
+            if key.startswith(f"{tag}_filt") and key.endswith("_in"):
+                r = float(key[len(tag) + 5:-3])
+                f = (eb.CuStructuredFilter2D if dim == 2 else eb.CuStructuredFilter3D)(mesh, r)
+                x = torch.as_tensor(z[key], device="cuda")
+                assert rel(f.dot(x).cpu(), z[f"{tag}_filt{r}_H"]) < TOL
+                assert rel(f.T.dot(x).cpu(), z[f"{tag}_filt{r}_HT"]) < TOL
+                n += 1
+    assert n >= 8
+
+
+def test_transfers_against_oracle(golden):
+    import torch
+    from edge_to_b200 import _lib
+    for dim, tag, z, nel, h in _cases(golden):
+        g = Grid(nel)
+        v = z[f"{tag}_restrict_in"]
+        out = torch.empty(g.coarse().n_dof, dtype=torch.float64, device="cuda")
+        _lib.call("edge_restrict", dim, _lib.int_array(list(nel) + [1] * (3 - dim)),
+                  _lib.ptr(torch.as_tensor(v, device="cuda")), _lib.ptr(out), _lib.stream_ptr())
+        assert rel(out.cpu(), ops.restriction_matrix(g, "gpu") @ v) < TOL
+        vc = z[f"{tag}_prolong_in"]
+        outf = torch.empty(g.n_dof, dtype=torch.float64, device="cuda")
+        _lib.call("edge_prolong", dim, _lib.int_array(list(nel) + [1] * (3 - dim)),
+                  _lib.ptr(torch.as_tensor(vc, device="cuda")), _lib.ptr(outf), _lib.stream_ptr())
+        assert rel(outf.cpu(), z[f"{tag}_prolong"]) < TOL
+
+
+def test_oc_update_against_reference(golden):
+    import torch
+    import edge_to_b200 as eb
+    for dim, fn in ((2, "ops_2d.npz"), (3, "ops_3d.npz")):
+        z = golden(fn)
+        nel = tuple(int(v) for v in z["even_nel"])
+        mesh = _mesh(dim, nel, None)
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        mat = eb.SingleMaterial(void=1e-9, penalty=3.0, volume_fraction=0.4)
+        opt = eb.CuTopOpt(mesh, mat, k, eb.CuMultiGrid(mesh, k, n_level=1), None, verbose=False)
+        out = opt.update_design(torch.as_tensor(z["even_oc_rho"], device="cuda"),
+                                torch.as_tensor(z["even_oc_df"], device="cuda"))
+        np.testing.assert_array_equal(out.cpu().numpy(), z["even_oc_out"].reshape(-1))
+
+
+def test_oc_update_edge_cases():
+    """All-zero sensitivities take the 1e-3 fallback; random large problems match the oracle."""
+    import torch
+    import edge_to_b200 as eb
+    mesh = _mesh(2, (50, 30), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    mat = eb.SingleMaterial(void=1e-9, volume_fraction=0.3)
+    opt = eb.CuTopOpt(mesh, mat, k, eb.CuMultiGrid(mesh, k, n_level=1), None, verbose=False)
+    rng = np.random.default_rng(3)
+    A = float(mesh.As[0])
+    for df in (np.zeros(1500), -rng.uniform(0, 5, 1500) ** 3, rng.standard_normal(1500)):
+        rho = rng.uniform(0, 1, 1500)
+        out = opt.update_design(torch.as_tensor(rho, device="cuda"), torch.as_tensor(df, device="cuda"))
+        ref, lam, steps = topopt.oc_update(rho, df, A, A * 1500, 0.3, 0.2)
+        np.testing.assert_array_equal(out.cpu().numpy(), ref)
+        assert opt.last_stats["oc_steps"] == steps
+
+
+def test_pcg_tracks_oracle_iterations():
+    """The GPU GMG-PCG follows the oracle's FP64 iteration (GPU semantics) step for step."""
+    import torch
+    import edge_to_b200 as eb
+    for nel, nl in (((32, 16), 3), ((16, 8, 8), 2)):
+        dim = len(nel)
+        p = (topopt.mbb_problem(*nel, vf=0.5, mg_kwargs=dict(tol=1e-10, n_level=nl, maxiter=500, variant="gpu"))
+             if dim == 2 else
+             topopt.cantilever_problem(*nel, vf=0.3, mg_kwargs=dict(tol=1e-10, n_level=nl, maxiter=500,
+                                                                     variant="gpu")))
+        rng = np.random.default_rng(1)
+        rho = rng.uniform(0.1, 1.0, p.grid.n_el)
+        E = np.clip(ops.filter_apply(p.H, rho) ** 3, 1e-9, 1)
+        K = ops.assemble(p.grid, p.K0, E, p.cons)
+        x_ref, res_ref = p.solver.solve(K, p.f, use_last=False)
+        mesh = _mesh(dim, nel, None)
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        cons = np.zeros(p.grid.n_dof, dtype=bool)
+        cons[p.cons] = True
+        k.add_constraints(np.where(cons)[0])
+        k.set_rho(torch.as_tensor(E, device="cuda"))
+        s = eb.CuMultiGrid(mesh, k, tol=1e-10, n_level=nl, maxiter=500)
+        x, res = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
+        assert s.last_iters == p.solver.pcg_iters[-1], (s.last_iters, p.solver.pcg_iters[-1])
+        assert rel(x.cpu(), x_ref) < 1e-9
+        assert res < 1e-10
