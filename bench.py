@@ -1,0 +1,360 @@
+"""Benchmark: SIMP iterations/s of the GMG-PCG minimum-compliance loop at 12.8M DOF.
+
+Workload (the reference's large 3-D demo size): hex8 cantilever 256x128x128
+(4,194,304 elements, 12,830,211 DOF), E0=1, Emin(void)=1e-9, nu=0.3, p=3, vf=0.1,
+r_min=2, x=0 face clamped, unit total downward load on the bottom edge at x=L,
+6-grid GMG (n_level=5, coarsest 675 DOF, FP64 Cholesky), PCG rtol 1e-6, move 0.2.
+A step = one SIMP iteration (OC update + filter + SIMP law + GMG-PCG solve + compliance
++ sensitivity + filter transpose), warm-started like the reference.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py --impl reference ...   (CPU reference arm: multi-threaded port of the
+                                           reference's matvec on the host cores)
+
+Prints one JSON line (rank 0).  `value` is device-timed with inputs resident in HBM;
+`e2e` runs the same steps through the public API with the design kept in pinned host
+memory (H2D of rho, D2H of rho_new and the compliance every step).  Every working array
+(12.8M-DOF vectors, 1 GB level-1 operator) is larger than the 126 MB L2, so no flush is
+needed between steps.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SIMP iter/s at 12.8M DOF: mixed-prec vs FP64 GMG-PCG, compl rel.err≤1e-6"
+CONFIGS = {
+    "cantilever_256x128x128": dict(nel=(256, 128, 128), vf=0.1, rmin=2.0, n_level=5, tol=1e-6),
+    "cantilever_128x64x64": dict(nel=(128, 64, 64), vf=0.1, rmin=2.0, n_level=4, tol=1e-6),
+    "cantilever_64x32x32": dict(nel=(64, 32, 32), vf=0.12, rmin=1.5, n_level=4, tol=1e-6),
+}
+# Mean PCG iterations per SIMP solve of the FP64 path on cantilever_256x128x128 (measured
+# by this benchmark on a B200, see profiles/); the CPU arms use it to turn a timed matvec
+# into SIMP iterations/s, since both run the same FP64 algorithm.
+PCG_ITERS_FP64_CFG5 = 40.0
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile(config):
+    """Per-launch DRAM bytes of the fine operator from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "fine_operator_traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        d = json.load(open(p))
+        return d.get(config)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"edge_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 8:
+                try:
+                    rows.append((float(f[0]), float(f[1]), f[4], f[5], f[6], f[7]))
+                except ValueError:
+                    pass
+        if not rows:
+            return None
+        import statistics
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        loaded = [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def build_problem(cfg, precision):
+    import numpy as np
+    import torch
+    import edge_to_b200 as eb
+    nel = cfg["nel"]
+    mesh = eb.CuStructuredMesh3D(*nel, *[float(v) for v in nel], stiffness=lambda x: eb.auto_stiffness(x, 1.0, 0.3))
+    mat = eb.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=cfg["vf"])
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    filt = eb.CuStructuredFilter3D(mesh, cfg["rmin"])
+    solver = eb.CuMultiGrid(mesh, k, tol=cfg["tol"], n_level=cfg["n_level"], maxiter=1000, precision=precision)
+    opt = eb.CuTopOpt(mesh, mat, k, solver, filt, max_iter=1, move=0.2, verbose=False)
+    nx, ny, nz = nel[0] + 1, nel[1] + 1, nel[2] + 1
+    j, k_ = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+    face = (j * nx * nz + k_).ravel()                    # i = 0
+    opt.add_BC_nodal(face, np.array([[True, True, True]]))
+    edge = (0 * nx * nz + nel[0] * nz + np.arange(nz))    # i = nelx, j = 0
+    opt.add_F_nodal(edge, np.array([[0.0, -1.0, 0.0]]) / edge.shape[0])
+    rho = torch.full((mesh.n_elements,), cfg["vf"], dtype=torch.float64, device="cuda")
+    return opt, rho
+
+
+def run_ours(args, cfg_name):
+    import numpy as np
+    import torch
+    from edge_to_b200 import _lib
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    cfg = CONFIGS[cfg_name]
+    opt, rho = build_problem(cfg, args.precision)
+    # initial analysis + warm-up steps (untimed)
+    c, dr, res = opt.solve_and_process(rho, 0)
+    it = 0
+    for _ in range(args.warmup):
+        rho = opt.update_design(rho, dr)
+        c, dr, res = opt.solve_and_process(rho, it)
+        it += 1
+    stream = torch.cuda.current_stream()
+    h = opt.kernel.handle
+    pcg = []
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # ---------------- device-timed region: inputs resident in HBM
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    _lib.call("edge_profile_begin", h, 200000)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rho = opt.update_design(rho, dr)
+        c, dr, res = opt.solve_and_process(rho, it)
+        pcg.append(opt.last_stats.get("pcg_iters", 0))
+        it += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    import ctypes
+    kms, kby, kl, tl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int(), ctypes.c_longlong()
+    _lib.call("edge_profile_end", h, ctypes.byref(kms), ctypes.byref(kby), ctypes.byref(kl), ctypes.byref(tl))
+    clk = clocks.stop()
+    t_ms = e0.elapsed_time(e1)
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    comp_last = float(c)
+
+    # ---------------- end-to-end: design on the host, copies inside the timed region
+    rho_h = torch.empty(rho.numel(), dtype=torch.float64, pin_memory=True)
+    rho_h.copy_(rho.cpu())
+    out_h = torch.empty_like(rho_h)
+    dr_e = dr
+    barrier()
+    torch.cuda.synchronize()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        rho_d = rho_h.to("cuda", non_blocking=True)
+        rho_n = opt.update_design(rho_d, dr_e)
+        c, dr_e, res = opt.solve_and_process(rho_n, it)
+        out_h.copy_(rho_n, non_blocking=True)
+        comp_host = float(c)  # D2H of the compliance (synchronising)
+        rho_h, out_h = out_h, rho_h
+        it += 1
+    s1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = s0.elapsed_time(s1)
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    n_el = int(np.prod(cfg["nel"]))
+    peak, peak_kind = peaks()
+    achieved = (kby.value / (kms.value / 1e3) / 1e9) if kms.value > 0 else None
+    traffic = traffic_from_profile(cfg_name)
+    line = {
+        "metric": METRIC,
+        "value": ws * args.steps / (t_ms / 1e3),
+        "unit": "iter/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+bf16/f64",
+        "data": "synthetic: reference cantilever BCs and load, rho0 = vf, random-free",
+        "config": {"workload": cfg_name, "dof": 3 * int(np.prod([n + 1 for n in cfg["nel"]])), "elements": n_el,
+                   "n_level": cfg["n_level"], "rtol": cfg["tol"], "precision": args.precision,
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                   "l2": "working set > 126 MB L2 (no flush needed)",
+                   "pcg_iters_per_step": pcg, "compliance_last": comp_last},
+        "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_wht + fused epilogues)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                     "traffic": traffic, "launches": kl.value, "kernel_ms": kms.value,
+                     "share_of_step": kms.value / t_ms if t_ms else None},
+        "e2e": {"value": args.steps / (e2e_ms / 1e3), "unit": "iter/s", "h2d_bytes_per_step": 8 * n_el,
+                "d2h_bytes_per_step": 8 * n_el + 8},
+        "gpu_launches": int(tl.value),
+        "clocks": clk,
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, pcg_iters=float(np.mean(pcg)) if pcg else PCG_ITERS_FP64_CFG5,
+                                            reps=2)
+    return line
+
+
+def cpu_baseline(cfg, pcg_iters, reps=2):
+    """Reference CPU algorithm (multi-threaded port of its matvec) timed on this host."""
+    import numpy as np
+    from oracle import cpu_matvec, elements
+    K0 = elements.hex8_stiffness(1, 1, 1, 1.0, 0.3)
+    t, _ = cpu_matvec.time_matvec(cfg["nel"], K0, reps=reps)
+    mv_per_iter = 8 * pcg_iters + 1
+    try:
+        import numba
+        threads = numba.get_num_threads()
+    except Exception:
+        threads = os.cpu_count()
+    return {"value": 1.0 / (t * mv_per_iter), "unit": "iter/s", "cores": threads, "kind": "port",
+            "sample": f"{reps} fine matvecs at full size ({t:.3f} s each, Numba prange on {threads} threads); "
+                      f"iter/s = 1/(t_matvec * (8*{pcg_iters:.1f} PCG iters + 1)), matvec-only lower bound "
+                      "on the reference CPU loop time"}
+
+
+def run_matvec(args, cfg_name):
+    """Profiling helper: K fine-operator applications (kernel.dot) on the workload's grid,
+    E = (0.1 + 0.9 * uniform)^3, x=0 face constrained.  Prints its own JSON line."""
+    import numpy as np
+    import torch
+    opt, rho = build_problem(CONFIGS[cfg_name], args.precision)
+    k = opt.kernel
+    g = torch.Generator(device="cuda").manual_seed(0)
+    E = (0.1 + 0.9 * torch.rand(k.n_elements, generator=g, device="cuda", dtype=torch.float64)) ** 3
+    k.set_rho(E)
+    u = torch.randn(k.shape[0], generator=g, device="cuda", dtype=torch.float64)
+    for _ in range(args.warmup):
+        k.dot(u)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        k.dot(u)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    n_dof, n_el = k.shape[0], k.n_elements
+    alg = 16 * n_dof + 8 * n_el
+    peak, kind = peaks()
+    return {"mode": "matvec", "workload": cfg_name, "ms_per_matvec": ms, "algorithmic_bytes": alg,
+            "GBps": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak, "peak_source": kind,
+            "note": "includes the user-layout <-> slot-layout conversions of edge_matvec"}
+
+
+def run_reference(args, cfg_name):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return None
+    import numpy as np
+    from oracle import cpu_matvec, elements
+    cfg = CONFIGS[cfg_name]
+    K0 = elements.hex8_stiffness(1, 1, 1, 1.0, 0.3)
+    # warm-up = JIT + cache warming; each timed step is one full-size matvec sample
+    cpu_matvec.time_matvec((4, 4, 4), K0, reps=max(1, args.warmup))
+    t, _ = cpu_matvec.time_matvec(cfg["nel"], K0, reps=max(1, args.steps))
+    mv_per_iter = 8 * PCG_ITERS_FP64_CFG5 + 1
+    v = 1.0 / (t * mv_per_iter)
+    try:
+        import numba
+        threads = numba.get_num_threads()
+    except Exception:
+        threads = os.cpu_count()
+    sample = (f"{args.steps} full-size fine matvecs, {t:.3f} s median; iter/s = 1/(t_matvec*(8*{PCG_ITERS_FP64_CFG5}"
+              f"+1)) with the FP64 PCG iteration count of this workload")
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * mv_per_iter * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg_name, "precision": "fp64", "parallelism": "host cores"},
+            "cpu_baseline": {"value": v, "unit": "iter/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--config", default="cantilever_256x128x128", choices=list(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="simp", choices=["simp", "matvec"])
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        line = run_reference(args, args.config)
+    elif args.mode == "matvec":
+        line = run_matvec(args, args.config)
+    else:
+        line = run_ours(args, args.config)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

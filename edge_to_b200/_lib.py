@@ -46,6 +46,8 @@ _SIGS = {
                                                    ctypes.c_double, ctypes.c_int, c_double_p, vp, vp, c_double_p,
                                                    c_int_p]),
     "edge_last_solve_stats": (ctypes.c_int, [vp, c_double_p, c_double_p, c_int_p, c_int_p]),
+    "edge_profile_begin": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_profile_end": (ctypes.c_int, [vp, c_double_p, c_double_p, c_int_p, ctypes.POINTER(ctypes.c_longlong)]),
 }
 
 

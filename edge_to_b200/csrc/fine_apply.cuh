@@ -26,10 +26,12 @@ namespace edge {
 // ------------------------------------------------------------------ epilogues
 // Each epilogue receives the node slot s, the node's input values `own` (raw on
 // constrained components) and the operator output Au (identity rows applied).
+// kIoBytes: algorithmic bytes per DOF the epilogue reads/writes besides the input vector.
 template <typename T, typename TO> struct EpiStore {
   TO* out;
   long long n;
   static constexpr bool kDot = false;
+  static constexpr int kIoBytes = sizeof(TO);
   EDGE_D void init() {}
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) out[c * n + s] = Conv<TO>::from(Au[c]);
@@ -41,6 +43,7 @@ template <typename T> struct EpiStoreDot {
   T* out;
   long long n;
   static constexpr bool kDot = true;
+  static constexpr int kIoBytes = sizeof(T);
   EDGE_D void init() {}
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) {
@@ -56,6 +59,7 @@ template <typename T, typename TB, typename TO> struct EpiResid {
   TO* r;
   long long n;
   static constexpr bool kDot = false;
+  static constexpr int kIoBytes = sizeof(TB) + sizeof(TO);
   EDGE_D void init() {}
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) r[c * n + s] = Conv<TO>::from(Conv<T>::from(b[c * n + s]) - Au[c]);
@@ -72,6 +76,7 @@ template <typename T, typename TB, typename TD> struct EpiJacobi {
   long long n;
   T w;
   static constexpr bool kDot = false;
+  static constexpr int kIoBytes = sizeof(TB) + sizeof(TD) + sizeof(T);
   EDGE_D void init() { w = Conv<T>::from(__ldg(omega) * wscale); }
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) {
@@ -94,6 +99,7 @@ template <typename T, typename TB, typename TD, typename TX, bool DOT> struct Ep
   long long n;
   T w;
   static constexpr bool kDot = DOT;
+  static constexpr int kIoBytes = sizeof(TB) + sizeof(TD) + 2 * sizeof(TX) + (DOT ? sizeof(TB) : 0);
   EDGE_D void init() { w = Conv<T>::from(__ldg(omega) * wscale); }
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) {

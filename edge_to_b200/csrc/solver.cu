@@ -231,6 +231,12 @@ struct Prob {
   double last_setup_ms = 0, last_solve_ms = 0;
   int last_iters = 0, last_true_res = 0;
   size_t part_cap = 0;
+  long long nlaunch = 0;
+  // fine-operator profiling (CUDA events around each launch + algorithmic bytes)
+  bool prof = false;
+  std::vector<cudaEvent_t> pev;
+  std::vector<double> pbytes;
+  size_t pev_used = 0;
 
   template <typename T> T* alloc(size_t n) {
     void* ptr = nullptr;
@@ -245,8 +251,19 @@ struct Prob {
     if (oc_h) cudaFreeHost(oc_h);
     if (scal_h) cudaFreeHost(scal_h);
     for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+    for (auto e : pev) cudaEventDestroy(e);
   }
 };
+
+
+// Every kernel launch of the solve path goes through here: counted for the benchmark's
+// launch tally and checked immediately.
+template <typename... KArgs, typename... Args>
+static void launch(Prob& P, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
+  kern<<<grid, block, smem, P.stream>>>(static_cast<KArgs>(args)...);
+  ++P.nlaunch;
+  KCHECK();
+}
 
 static Geo level_geo(const Prob& P, int l) {
   int ne[3] = {P.nel[0], P.nel[1], P.nel[2]};
@@ -288,33 +305,40 @@ template <> struct TypeOps<float> {
   static const float* K0b(const Prob& P) { return P.dK0bf; }
 };
 
-// Fine-level operator with epilogue.  u, E in type T.
+// Fine-level operator with epilogue.  u, E in type T.  When profiling is on, each launch is
+// bracketed by CUDA events on the problem's stream and its algorithmic bytes recorded:
+// input vector + E + the epilogue's per-DOF traffic (BC mask excluded).
 template <typename T, class Epi>
 static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
   const Geo& g = P.g0;
   const T* E = TypeOps<T>::E(P);
+  const bool rec = P.prof && P.pev_used + 2 <= P.pev.size();
+  if (rec) CK(cudaEventRecord(P.pev[P.pev_used], P.stream));
   if (P.ei.wht) {
     if (P.dim == 3) {
       int ly;
       dim3 grid = fine3_grid(g, ly);
-      k_fine3_wht<T, T, Epi, FINE_BX><<<grid, dim3(32, FINE_BX), 0, P.stream>>>(
-          g, u, E, P.mask, cast3<T>(P.ei.k3), ly, epi, P.part, P.ticket, dot_dst);
+      launch(P, k_fine3_wht<T, T, Epi, FINE_BX>, grid, dim3(32, FINE_BX), 0, g, u, E, (const uint8_t*)P.mask,
+             cast3<T>(P.ei.k3), ly, epi, P.part, P.ticket, dot_dst);
     } else {
       int ly;
       dim3 grid = fine2_grid(g, ly);
-      k_fine2_wht<T, T, Epi, FINE2_NW><<<grid, 32 * FINE2_NW, 0, P.stream>>>(
-          g, u, E, P.mask, cast2<T>(P.ei.k2), ly, epi, P.part, P.ticket, dot_dst);
+      launch(P, k_fine2_wht<T, T, Epi, FINE2_NW>, grid, dim3(32 * FINE2_NW), 0, g, u, E, (const uint8_t*)P.mask,
+             cast2<T>(P.ei.k2), ly, epi, P.part, P.ticket, dot_dst);
     }
   } else {
-    if (P.dim == 3) {
-      k_fine3_dense<T, T, Epi><<<dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, P.stream>>>(
-          g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
-    } else {
-      k_fine2_dense<T, T, Epi><<<dim3(cdiv(g.nx, 128), g.ny), 128, 0, P.stream>>>(
-          g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
-    }
+    if (P.dim == 3)
+      launch(P, k_fine3_dense<T, T, Epi>, dim3(cdiv(g.nz, 128), g.nx, g.ny), dim3(128), 0, g, u, E,
+             (const uint8_t*)P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
+    else
+      launch(P, k_fine2_dense<T, T, Epi>, dim3(cdiv(g.nx, 128), g.ny), dim3(128), 0, g, u, E, (const uint8_t*)P.mask,
+             TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
   }
-  KCHECK();
+  if (rec) {
+    CK(cudaEventRecord(P.pev[P.pev_used + 1], P.stream));
+    P.pev_used += 2;
+    P.pbytes.push_back((double)P.n_dof * (sizeof(T) + Epi::kIoBytes) + (double)P.n_el * sizeof(T));
+  }
 }
 
 // Same operator, forcing the dense path (cross-checks).
@@ -323,10 +347,10 @@ static void fine_apply_dense(Prob& P, const T* u, Epi epi, double* dot_dst) {
   const Geo& g = P.g0;
   const T* E = TypeOps<T>::E(P);
   if (P.dim == 3)
-    k_fine3_dense<T, T, Epi><<<dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, P.stream>>>(
+    launch(P, k_fine3_dense<T, T, Epi>, dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, 
         g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
   else
-    k_fine2_dense<T, T, Epi><<<dim3(cdiv(g.nx, 128), g.ny), 128, 0, P.stream>>>(
+    launch(P, k_fine2_dense<T, T, Epi>, dim3(cdiv(g.nx, 128), g.ny), 128, 0, 
         g, u, E, P.mask, TypeOps<T>::K0b(P), epi, P.part, P.ticket, dot_dst);
   KCHECK();
 }
@@ -334,10 +358,10 @@ static void fine_apply_dense(Prob& P, const T* u, Epi epi, double* dot_dst) {
 template <typename T, class Epi>
 static void st_apply(Prob& P, const Geo& g, const T* u, const T* S, Epi epi, double* dot_dst) {
   if (g.dim == 3)
-    k_st3_apply<T, T, Epi><<<dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, P.stream>>>(g, u, S, epi, P.part, P.ticket,
+    launch(P, k_st3_apply<T, T, Epi>, dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, g, u, S, epi, P.part, P.ticket,
                                                                                     dot_dst);
   else
-    k_st2_apply<T, T, Epi><<<dim3(cdiv(g.nx, 128), g.ny), 128, 0, P.stream>>>(g, u, S, epi, P.part, P.ticket, dot_dst);
+    launch(P, k_st2_apply<T, T, Epi>, dim3(cdiv(g.nx, 128), g.ny), 128, 0, g, u, S, epi, P.part, P.ticket, dot_dst);
   KCHECK();
 }
 
@@ -398,7 +422,7 @@ static void mg_setup(Prob& P) {
   const Geo& g0 = P.g0;
   const T* E = TypeOps<T>::E(P);
   // fine Jacobi diagonal
-  k_fine_dinv<T, TD0><<<cdiv(g0.n, 256), 256, 0, P.stream>>>(g0, E, P.mask, P.dK0diag, (TD0*)P.lv[0].dinv, nullptr);
+  launch(P, k_fine_dinv<T, TD0>, cdiv(g0.n, 256), 256, 0, g0, E, P.mask, P.dK0diag, (TD0*)P.lv[0].dinv, nullptr);
   KCHECK();
   if (L == 0) return;
   // level 1 from the fine operator
@@ -407,9 +431,9 @@ static void mg_setup(Prob& P) {
     const int nnb = P.dim == 3 ? 27 : 9;
     dim3 grid(cdiv(gc.n, 128), nnb);
     if (P.dim == 3)
-      k_galerkin3_l0<T, T><<<grid, 128, 0, P.stream>>>(g0, gc, E, P.mask, P.eflag, P.dQ, P.dK0b, (T*)P.lv[1].S);
+      launch(P, k_galerkin3_l0<T, T>, grid, 128, 0, g0, gc, E, P.mask, P.eflag, P.dQ, P.dK0b, (T*)P.lv[1].S);
     else
-      k_galerkin2_l0<T, T><<<grid, 128, 0, P.stream>>>(g0, gc, E, P.mask, P.eflag, P.dQ, P.dK0b, (T*)P.lv[1].S);
+      launch(P, k_galerkin2_l0<T, T>, grid, 128, 0, g0, gc, E, P.mask, P.eflag, P.dQ, P.dK0b, (T*)P.lv[1].S);
     KCHECK();
   }
   for (int l = 1; l < L; ++l) {
@@ -418,37 +442,37 @@ static void mg_setup(Prob& P) {
     const int nnb = P.dim == 3 ? 27 : 9;
     dim3 grid(cdiv(gc.n, 128), nnb);
     if (P.dim == 3)
-      k_galerkin3_st<T><<<grid, 128, 0, P.stream>>>(gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
+      launch(P, k_galerkin3_st<T>, grid, 128, 0, gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
     else
-      k_galerkin2_st<T><<<grid, 128, 0, P.stream>>>(gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
+      launch(P, k_galerkin2_st<T>, grid, 128, 0, gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
     KCHECK();
   }
   for (int l = 1; l < L; ++l) {
     const Geo& g = P.lv[l].g;
-    k_st_dinv<T, T><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, (const T*)P.lv[l].S, (T*)P.lv[l].dinv);
+    launch(P, k_st_dinv<T, T>, cdiv(g.n, 256), 256, 0, g, (const T*)P.lv[l].S, (T*)P.lv[l].dinv);
     KCHECK();
   }
   // coarsest: dense FP64 Cholesky and explicit inverse
   const Geo& gL = P.lv[L].g;
   const int nd = P.nd;
   CK(cudaMemsetAsync(P.Adense, 0, (size_t)nd * nd * sizeof(double), P.stream));
-  k_st_to_dense<T><<<cdiv(gL.n, 256), 256, 0, P.stream>>>(gL, (const T*)P.lv[L].S, P.Adense, nd);
+  launch(P, k_st_to_dense<T>, cdiv(gL.n, 256), 256, 0, gL, (const T*)P.lv[L].S, P.Adense, nd);
   KCHECK();
   CK(cudaMemsetAsync(P.chol_status, 0, sizeof(int), P.stream));
   const int nt = (nd + CB - 1) / CB;
   for (int K = 0; K < nt; ++K) {
-    k_chol_diag<<<1, CB * CB / 4, 0, P.stream>>>(P.Adense, nd, K, P.chol_status);
+    launch(P, k_chol_diag, 1, CB * CB / 4, 0, P.Adense, nd, K, P.chol_status);
     if (K + 1 < nt) {
-      k_chol_panel<<<nt - K - 1, CB * CB / 4, 0, P.stream>>>(P.Adense, nd, K);
+      launch(P, k_chol_panel, nt - K - 1, CB * CB / 4, 0, P.Adense, nd, K);
       const int m = nt - K - 1;
-      k_chol_update<<<m * (m + 1) / 2, CB * CB / 4, 0, P.stream>>>(P.Adense, nd, K, nt);
+      launch(P, k_chol_update, m * (m + 1) / 2, CB * CB / 4, 0, P.Adense, nd, K, nt);
     }
   }
   KCHECK();
-  k_transpose_lower<<<cdiv((long long)nd * nd, 256), 256, 0, P.stream>>>(P.Adense, P.Ut, nd);
+  launch(P, k_transpose_lower, cdiv((long long)nd * nd, 256), 256, 0, P.Adense, P.Ut, nd);
   if (nd * sizeof(double) > 48 * 1024)
     CK(cudaFuncSetAttribute(k_chol_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(nd * sizeof(double))));
-  k_chol_inverse<<<nd, 256, nd * sizeof(double), P.stream>>>(P.Adense, P.Ut, P.Ainv, nd);
+  launch(P, k_chol_inverse, nd, 256, nd * sizeof(double), P.Adense, P.Ut, P.Ainv, nd);
   KCHECK();
 }
 
@@ -461,7 +485,7 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
   const Geo& g = Lv.g;
   const long long nv = (long long)g.dof * g.n;
   if (l == P.n_level) {
-    k_coarse_solve<T, T><<<cdiv((long long)P.nd * 32, 256), 256, 0, P.stream>>>(g, P.Ainv, P.nd, b, out);
+    launch(P, k_coarse_solve<T, T>, cdiv((long long)P.nd * 32, 256), 256, 0, g, P.Ainv, P.nd, b, out);
     KCHECK();
     return;
   }
@@ -482,9 +506,9 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
   // pre-smoothing from x = 0
   if (P.n_smooth >= 1) {
     if (l == 0)
-      k_jacobi0<T, TD0, T><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, b, (const TD0*)Lv.dinv, x, om, ws);
+      launch(P, k_jacobi0<T, TD0, T>, ew_blocks(nv), 256, 0, nv, b, (const TD0*)Lv.dinv, x, om, ws);
     else
-      k_jacobi0<T, T, T><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, b, (const T*)Lv.dinv, x, om, ws);
+      launch(P, k_jacobi0<T, T, T>, ew_blocks(nv), 256, 0, nv, b, (const T*)Lv.dinv, x, om, ws);
     KCHECK();
     for (int s = 1; s < P.n_smooth; ++s) {
       sweep(b, x, y);
@@ -504,17 +528,17 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     const T* xcur = first ? x : out;
     Level& Lc = P.lv[l + 1];
     if (P.dim == 3)
-      k_restrict3<T, T><<<dim3(cdiv(Lc.g.nz, 64), Lc.g.nx, Lc.g.ny), 64, 0, P.stream>>>(g, Lc.g, r, (T*)Lc.b);
+      launch(P, k_restrict3<T, T>, dim3(cdiv(Lc.g.nz, 64), Lc.g.nx, Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
     else
-      k_restrict2<T, T><<<dim3(cdiv(Lc.g.nx, 64), Lc.g.ny), 64, 0, P.stream>>>(g, Lc.g, r, (T*)Lc.b);
+      launch(P, k_restrict2<T, T>, dim3(cdiv(Lc.g.nx, 64), Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
     KCHECK();
     vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr);
     T* e1 = (T*)Lv.ea;
     T* e2 = (T*)Lv.eb;
     if (P.dim == 3)
-      k_prolong3<T, T><<<dim3(cdiv(g.nz, 64), g.nx, g.ny), 64, 0, P.stream>>>(g, Lc.g, (const T*)Lc.res, e1);
+      launch(P, k_prolong3<T, T>, dim3(cdiv(g.nz, 64), g.nx, g.ny), 64, 0, g, Lc.g, (const T*)Lc.res, e1);
     else
-      k_prolong2<T, T><<<dim3(cdiv(g.nx, 64), g.ny), 64, 0, P.stream>>>(g, Lc.g, (const T*)Lc.res, e1);
+      launch(P, k_prolong2<T, T>, dim3(cdiv(g.nx, 64), g.ny), 64, 0, g, Lc.g, (const T*)Lc.res, e1);
     KCHECK();
     const bool last_visit = (vis == visits - 1);
     if (P.n_smooth >= 1) {
@@ -536,10 +560,10 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
         level_apply<T>(P, l, e1, e);
       }
     } else {
-      k_add<T, T, T><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, xcur, e1, out);
+      launch(P, k_add<T, T, T>, ew_blocks(nv), 256, 0, nv, xcur, e1, out);
       KCHECK();
       if (last_visit && dot_dst) {
-        k_dot<TV, T><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, dotv, out, P.part, P.ticket,
+        launch(P, k_dot<TV, T>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, dotv, out, P.part, P.ticket,
                                                                                    dot_dst);
         KCHECK();
       }
@@ -596,19 +620,19 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
   double* p = (double*)P.p;
   double* q = (double*)P.q;
   double* z = (double*)P.lv[0].res;
-  k_pcg_init<<<1, 1, 0, P.stream>>>(P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
+  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
   KCHECK();
   // r = b - A x ; bb = b.b
   {
     EpiResid<double, double, double> e{P.b64, r, g.n};
     fine_apply<double>(P, x, e, nullptr);
   }
-  k_dot<double, double><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, P.b64, P.b64, P.part,
+  launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, P.b64, P.b64, P.part,
                                                                                        P.ticket, &P.st->bb);
   KCHECK();
-  k_pcg_check_bb<<<1, 1, 0, P.stream>>>(P.st);
+  launch(P, k_pcg_check_bb, 1, 1, 0, P.st);
   vcycle<double, TD0, double>(P, 0, r, z, r, &P.st->rz_new);
-  k_copy<double, double><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, z, p);
+  launch(P, k_copy<double, double>, ew_blocks(nv), 256, 0, nv, z, p);
   KCHECK();
   int it = 0;
   for (;;) {
@@ -616,7 +640,7 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
       EpiStoreDot<double> e{q, g.n};
       fine_apply<double>(P, p, e, &P.st->pq);
     }
-    k_pcg_xr<double, double><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, x, p, r, q, P.st,
+    launch(P, k_pcg_xr<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, x, p, r, q, P.st,
                                                                                            P.part, P.ticket);
     KCHECK();
     CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
@@ -624,7 +648,7 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
     ++it;
     if (P.st_h->done) break;
     vcycle<double, TD0, double>(P, 0, r, z, r, &P.st->rz_new);
-    k_pcg_p<double><<<ew_blocks(nv), 256, 0, P.stream>>>(nv, p, z, P.st);
+    launch(P, k_pcg_p<double>, ew_blocks(nv), 256, 0, nv, p, z, P.st);
     KCHECK();
   }
   P.last_iters = P.st_h->iter;
@@ -784,8 +808,8 @@ int edge_set_constraints(edge_problem* p, const uint8_t* cons_dev) {
   API_BEGIN
   if (!p || !cons_dev) fail(EDGE_EINVAL, "null argument");
   Prob& P = p->P;
-  k_mask_from_user<<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, cons_dev, P.mask);
-  k_elem_flags<<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, P.mask, P.eflag);
+  launch(P, k_mask_from_user, cdiv(P.g0.n, 256), 256, 0, P.g0, cons_dev, P.mask);
+  launch(P, k_elem_flags, cdiv(P.g0.n, 256), 256, 0, P.g0, P.mask, P.eflag);
   KCHECK();
   P.has_cons = true;
   API_END
@@ -795,8 +819,8 @@ int edge_set_rho(edge_problem* p, const double* E_dev) {
   API_BEGIN
   if (!p || !E_dev) fail(EDGE_EINVAL, "null argument");
   Prob& P = p->P;
-  k_elem_user_to_slots<double><<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, E_dev, P.E64);
-  if (P.E32) k_elem_user_to_slots<float><<<cdiv(P.g0.n, 256), 256, 0, P.stream>>>(P.g0, E_dev, P.E32);
+  launch(P, k_elem_user_to_slots<double>, cdiv(P.g0.n, 256), 256, 0, P.g0, E_dev, P.E64);
+  if (P.E32) launch(P, k_elem_user_to_slots<float>, cdiv(P.g0.n, 256), 256, 0, P.g0, E_dev, P.E32);
   KCHECK();
   P.has_rho = true;
   API_END
@@ -808,10 +832,10 @@ int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev) {
   Prob& P = p->P;
   if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. dot works only after setting rho.");
   const Geo& g = P.g0;
-  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, u_dev, P.b64);
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, u_dev, P.b64);
   EpiStore<double, double> e{P.r64, g.n};
   fine_apply<double>(P, P.b64, e, nullptr);
-  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.r64, out_dev);
+  launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, P.r64, out_dev);
   KCHECK();
   API_END
 }
@@ -823,10 +847,10 @@ int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev) {
   Prob& P = p->P;
   if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. dot works only after setting rho.");
   const Geo& g = P.g0;
-  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, u_dev, P.b64);
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, u_dev, P.b64);
   EpiStore<double, double> e{P.r64, g.n};
   fine_apply_dense<double>(P, P.b64, e, nullptr);
-  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.r64, out_dev);
+  launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, P.r64, out_dev);
   KCHECK();
   API_END
 }
@@ -837,7 +861,7 @@ int edge_diagonal(edge_problem* p, double* diag_dev) {
   Prob& P = p->P;
   if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. diagonal works only after setting rho or if rho is provided.");
   const Geo& g = P.g0;
-  k_fine_dinv<double, double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.E64, P.mask, P.dK0diag, P.r64, diag_dev);
+  launch(P, k_fine_dinv<double, double>, cdiv(g.n, 256), 256, 0, g, P.E64, P.mask, P.dK0diag, P.r64, diag_dev);
   KCHECK();
   API_END
 }
@@ -847,8 +871,8 @@ int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev) {
   if (!p || !U_dev || !dk_dev) fail(EDGE_EINVAL, "null argument");
   Prob& P = p->P;
   const Geo& g = P.g0;
-  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, U_dev, P.b64);
-  k_dk<double><<<cdiv(P.n_el, 256), 256, 0, P.stream>>>(g, P.b64, P.ei.k3, P.ei.k2, P.dK0b, P.ei.wht ? 1 : 0, dk_dev,
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, U_dev, P.b64);
+  launch(P, k_dk<double>, cdiv(P.n_el, 256), 256, 0, g, P.b64, P.ei.k3, P.ei.k2, P.dK0b, P.ei.wht ? 1 : 0, dk_dev,
                                                          nullptr, nullptr, 0.0, 0.0);
   KCHECK();
   API_END
@@ -904,18 +928,56 @@ int edge_mg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_l
   if (!p || !f_dev || !x_dev) fail(EDGE_EINVAL, "null argument");
   Prob& P = p->P;
   const Geo& g = P.g0;
-  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, f_dev, P.b64);
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, f_dev, P.b64);
   if (use_last)
-    k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, x_dev, P.x64);
+    launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, x_dev, P.x64);
   else
     CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
   KCHECK();
   solve_internal(P, tol, maxiter);
-  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.x64, x_dev);
+  launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, P.x64, x_dev);
   KCHECK();
   CK(cudaStreamSynchronize(P.stream));
   if (residual_out) *residual_out = P.st_h->res;
   if (iters_out) *iters_out = P.st_h->iter;
+  API_END
+}
+
+int edge_profile_begin(edge_problem* p, int max_launches) {
+  API_BEGIN
+  if (!p || max_launches < 1) fail(EDGE_EINVAL, "bad argument");
+  Prob& P = p->P;
+  while ((int)P.pev.size() < 2 * max_launches) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    P.pev.push_back(e);
+  }
+  P.pev_used = 0;
+  P.pbytes.clear();
+  P.pbytes.reserve(max_launches);
+  P.prof = true;
+  P.nlaunch = 0;
+  API_END
+}
+
+int edge_profile_end(edge_problem* p, double* kernel_ms, double* kernel_bytes, int* kernel_launches,
+                     long long* total_launches) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  Prob& P = p->P;
+  CK(cudaStreamSynchronize(P.stream));
+  double ms = 0.0, by = 0.0;
+  for (size_t i = 0; i + 1 < P.pev_used; i += 2) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, P.pev[i], P.pev[i + 1]));
+    ms += t;
+    by += P.pbytes[i / 2];
+  }
+  if (kernel_ms) *kernel_ms = ms;
+  if (kernel_bytes) *kernel_bytes = by;
+  if (kernel_launches) *kernel_launches = (int)(P.pev_used / 2);
+  if (total_launches) *total_launches = P.nlaunch;
+  P.prof = false;
   API_END
 }
 
@@ -1029,8 +1091,8 @@ static void oc_run(Prob& P, long long n, const double* rho, const double* dr, do
                    double move, double* rho_new) {
   if (n != P.n_el) fail(EDGE_EINVAL, "OC vector length does not match the number of elements");
   const unsigned nb = std::min<unsigned>(ew_blocks(n), 1024);
-  k_oc_prep<<<nb, 256, 0, P.stream>>>(n, rho, dr, A, P.ocp, P.part, P.ticket, P.scal);
-  k_oc_floor<<<nb, 256, 0, P.stream>>>(n, P.ocp, P.scal);
+  launch(P, k_oc_prep, nb, 256, 0, n, rho, dr, A, P.ocp, P.part, P.ticket, P.scal);
+  launch(P, k_oc_floor, nb, 256, 0, n, P.ocp, P.scal);
   OcState init{};
   init.l1 = 1e-9;
   init.l2 = 1e9;
@@ -1042,7 +1104,7 @@ static void oc_run(Prob& P, long long n, const double* rho, const double* dr, do
   const unsigned nbp = std::min<unsigned>(nb, (unsigned)(P.part_cap / OC_NODES));
   const int max_pass = (200 + OC_DEPTH - 1) / OC_DEPTH;
   for (int pass = 0; pass < max_pass; ++pass) {
-    k_oc_pass<<<nbp, 256, 0, P.stream>>>(n, rho, P.ocp, A, move, P.oc, P.part, P.ticket);
+    launch(P, k_oc_pass, nbp, 256, 0, n, rho, P.ocp, A, move, P.oc, P.part, P.ticket);
     if ((pass & 3) == 3) {
       CK(cudaMemcpyAsync(P.oc_h, P.oc, sizeof(OcState), cudaMemcpyDeviceToHost, P.stream));
       CK(cudaStreamSynchronize(P.stream));
@@ -1050,7 +1112,7 @@ static void oc_run(Prob& P, long long n, const double* rho, const double* dr, do
     }
   }
   KCHECK();
-  k_oc_final<<<nb, 256, 0, P.stream>>>(n, rho, P.ocp, move, P.oc, rho_new, P.part, P.ticket, P.scal + 1);
+  launch(P, k_oc_final, nb, 256, 0, n, rho, P.ocp, move, P.oc, rho_new, P.part, P.ticket, P.scal + 1);
   KCHECK();
   CK(cudaMemcpyAsync(P.oc_h, P.oc, sizeof(OcState), cudaMemcpyDeviceToHost, P.stream));
   CK(cudaMemcpyAsync(P.scal_h, P.scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
@@ -1081,26 +1143,26 @@ int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* r
   double* rf = rho_f_dev ? rho_f_dev : P.rho_f;
   const unsigned nbe = cdiv(P.n_el, 256);
   // rho_f = H rho ; E = clip(rho_f^p, void, 1)
-  k_filter_material<double, float><<<nbe, 256, 0, P.stream>>>(g, f->taps, rho_dev, rf, P.E64, P.E32, penalty, void_, 0);
+  launch(P, k_filter_material<double, float>, nbe, 256, 0, g, f->taps, rho_dev, rf, P.E64, P.E32, penalty, void_, 0);
   KCHECK();
   P.has_rho = true;
   // U = K(E)^-1 f (warm start from U_dev)
-  k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, f_dev, P.b64);
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, f_dev, P.b64);
   if (use_last)
-    k_user_to_slots<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, U_dev, P.x64);
+    launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, U_dev, P.x64);
   else
     CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
   KCHECK();
   solve_internal(P, tol, maxiter);
   const long long nv = (long long)g.dof * g.n;
   // compliance c = f . U
-  k_dot<double, double><<<std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, P.stream>>>(nv, P.b64, P.x64, P.part,
+  launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, P.b64, P.x64, P.part,
                                                                                        P.ticket, P.scal + 2);
   // dr = H^T (p clip(rho_f)^(p-1) dk)
-  k_dk<double><<<nbe, 256, 0, P.stream>>>(g, P.x64, P.ei.k3, P.ei.k2, P.dK0b, P.ei.wht ? 1 : 0, nullptr, rf, P.gsens,
+  launch(P, k_dk<double>, nbe, 256, 0, g, P.x64, P.ei.k3, P.ei.k2, P.dK0b, P.ei.wht ? 1 : 0, nullptr, rf, P.gsens,
                                           penalty, void_);
-  k_filter_T<<<nbe, 256, 0, P.stream>>>(f->g, f->taps, f->N, P.gsens, dr_dev);
-  k_slots_to_user<double><<<cdiv(g.n, 256), 256, 0, P.stream>>>(g, P.x64, U_dev);
+  launch(P, k_filter_T, nbe, 256, 0, f->g, f->taps, f->N, P.gsens, dr_dev);
+  launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, P.x64, U_dev);
   KCHECK();
   CK(cudaMemcpyAsync(P.scal_h + 2, P.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, P.stream));
   CK(cudaStreamSynchronize(P.stream));

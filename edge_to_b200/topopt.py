@@ -189,7 +189,8 @@ class CuTopOpt:
         self.kernel.has_rho = True
         sv.last_iters = its.value
         self._U = U
-        self.last_stats.update(pcg_iters=its.value, residual=res.value, **sv.stats())
+        self.last_stats.update(sv.stats())
+        self.last_stats.update(pcg_iters=its.value, residual=res.value)
         return torch.tensor(c.value, dtype=torch.float64), dr.reshape(-1, 1), res.value
 
     # ----------------------------------------------------------------- loop (TopOpt/_cuda.py:304-382)

@@ -92,6 +92,13 @@ int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* r
                                 int maxiter, double* compliance_out, double* dr_dev, double* rho_f_dev,
                                 double* residual_out, int* iters_out);
 
+/* Benchmark instrumentation: between begin and end, every fine-level operator launch
+ * (the dominant kernel) is bracketed by CUDA events on the problem's stream and its
+ * algorithmic bytes recorded (input vector + E + epilogue traffic); end() returns their
+ * summed device time, bytes and count, and the number of library kernels launched. */
+int edge_profile_begin(edge_problem* p, int max_launches);
+int edge_profile_end(edge_problem* p, double* kernel_ms, double* kernel_bytes, int* kernel_launches,
+                     long long* total_launches);
 /* Kernel timing of the last edge_mg_solve (ms), for the benchmarks. */
 int edge_last_solve_stats(const edge_problem* p, double* setup_ms, double* solve_ms, int* pcg_iters,
                           int* true_residuals);
