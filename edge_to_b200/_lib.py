@@ -32,8 +32,10 @@ _SIGS = {
     "edge_process_grad": (ctypes.c_int, [vp, vp, vp]),
     "edge_uses_transform": (ctypes.c_int, [vp]),
     "edge_mg_config": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
-                                      c_int_p, ctypes.c_int]),
+                                      c_int_p, ctypes.c_int, ctypes.c_int]),
     "edge_mg_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_double_p, c_int_p]),
+    "edge_mg_setup": (ctypes.c_int, [vp]),
+    "edge_mg_level_dense": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_longlong]),
     "edge_restrict": (ctypes.c_int, [ctypes.c_int, c_int_p, vp, vp, vp]),
     "edge_prolong": (ctypes.c_int, [ctypes.c_int, c_int_p, vp, vp, vp]),
     "edge_filter_create": (ctypes.c_int, [ctypes.c_int, c_int_p, ctypes.c_int, c_int_p, c_double_p, ctypes.POINTER(vp)]),

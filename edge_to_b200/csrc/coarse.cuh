@@ -1,11 +1,15 @@
 // Coarse levels of the geometric multigrid.
 //
-// Level l >= 1 operators are stored as compact stencils: for every coarse node the
-// 3^d neighbour blocks of dof x dof coefficients, coefficient-major
-// (S[(nb*dof*dof + c*dof + d)*n + slot]) so that one thread per node reads them
-// coalesced.  nb = (dz+1) + 3(dx+1) + 9(dy+1) in 3-D and (dx+1) + 3(dy+1) in 2-D.
-// This replaces the reference's fixed-81/18-nnz CSR (core/_mgm_cuda.py:69-221) with the
-// same values and no index arrays.
+// Level l >= 1 operators are stored as compact symmetric stencils.  Neighbour
+// directions are numbered nb = (dz+1) + 3(dx+1) + 9(dy+1) in 3-D and (dx+1) + 3(dy+1)
+// in 2-D; the centre is nb = 13 / 4 and nb > centre are the "upper" directions.  Since
+// A_l is symmetric, only the upper triangle of the centre block and the blocks towards the
+// upper neighbours are stored, coefficient-major (one array of n slots per coefficient, so
+// one thread per node reads them coalesced):
+//   3-D: 6 centre (00 01 02 11 12 22) + 13 x 9 = 123 arrays, 2-D: 3 + 4 x 4 = 19 arrays.
+// The block towards a lower neighbour J = I - d is the transpose of J's stored block for +d.
+// This replaces the reference's fixed-81/18-nnz CSR (core/_mgm_cuda.py:69-221): same
+// values, no index arrays, half the coefficients.
 //
 // Transfers restate restriction_{2d,3d}_kernel / prolongation_{2d,3d}_kernel
 // (core/_templated_cuda.cu:232-475): full weighting 1, 1/2, 1/4, 1/8 by Manhattan
@@ -33,41 +37,91 @@ EDGE_HD double bnd_total2(int nb) { return nb == 2 ? 2.25 : nb == 1 ? 3.0 : 4.0;
 EDGE_HD double dist_w(int d) { return d == 0 ? 1.0 : d == 1 ? 0.5 : d == 2 ? 0.25 : 0.125; }
 EDGE_D int is_bnd(int i, int n) { return (i == 0 || i == n - 1) ? 1 : 0; }
 
+// ------------------------------------------------------------------ symmetric stencil access
+constexpr int NST3 = 123;
+constexpr int NST2 = 19;
+EDGE_HD int nst(int dim) { return dim == 3 ? NST3 : NST2; }
+EDGE_HD int centre_nb(int dim) { return dim == 3 ? 13 : 4; }
+// index of centre coefficient (c, d) in the symmetric 3x3 / 2x2 storage
+EDGE_HD int cidx(int dim, int c, int d) {
+  if (c > d) { int t = c; c = d; d = t; }
+  return dim == 3 ? (c == 0 ? d : (c == 1 ? 2 + d : 5)) : (c == 0 ? d : 2);
+}
+// array index of coefficient (c, d) of the block towards upper direction nb
+EDGE_HD int uidx(int dim, int nb, int c, int d) {
+  return dim == 3 ? 6 + (nb - 14) * 9 + c * 3 + d : 3 + (nb - 5) * 4 + c * 2 + d;
+}
+EDGE_HD void nb_dir(int dim, int nb, int& dx, int& dy, int& dz) {
+  if (dim == 3) {
+    dz = nb % 3 - 1;
+    dx = (nb / 3) % 3 - 1;
+    dy = nb / 9 - 1;
+  } else {
+    dx = nb % 3 - 1;
+    dy = nb / 3 - 1;
+    dz = 0;
+  }
+}
+EDGE_HD long long nb_off(const Geo& g, int nb) {
+  int dx, dy, dz;
+  nb_dir(g.dim, nb, dx, dy, dz);
+  return g.dim == 3 ? (long long)dy * g.plane + (long long)dx * g.pz + dz : (long long)dy * g.pz + dx;
+}
+// A[I, I+dir(nb)](c, d) with I at slot s; the caller guarantees I+dir(nb) is in the grid.
+template <typename TS>
+EDGE_D double st_get(const Geo& g, const TS* __restrict__ S, long long s, int nb, int c, int d) {
+  const int cn = centre_nb(g.dim);
+  if (nb == cn) return (double)Conv<double>::from(S[(long long)cidx(g.dim, c, d) * g.n + s]);
+  if (nb > cn) return (double)Conv<double>::from(S[(long long)uidx(g.dim, nb, c, d) * g.n + s]);
+  const long long sj = s + nb_off(g, nb);
+  return (double)Conv<double>::from(S[(long long)uidx(g.dim, 2 * cn - nb, d, c) * g.n + sj]);
+}
+
 // ------------------------------------------------------------------ stencil apply (levels >= 1)
+// One thread per slot (flat grid); padding slots exit.
 template <typename T, typename TS, class Epi>
 __global__ void __launch_bounds__(128)
 k_st3_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
             double* dot_dst) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y, j = blockIdx.z;
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long n = g.n;
   epi.init();
   double dacc = 0.0;
-  if (k < g.nz) {
-    const long long s = g.slot3(i, j, k);
-    T Au[3] = {T(0), T(0), T(0)};
+  const int k = (int)(s % g.pz), i = (int)((s / g.pz) % g.nx), j = (int)(s / g.plane);
+  if (s < n && k < g.nz) {
+    const T u0 = __ldg(u + s), u1 = __ldg(u + n + s), u2 = __ldg(u + 2 * n + s);
+    const T c00 = Conv<T>::from(__ldg(S + s)), c01 = Conv<T>::from(__ldg(S + n + s)),
+            c02 = Conv<T>::from(__ldg(S + 2 * n + s)), c11 = Conv<T>::from(__ldg(S + 3 * n + s)),
+            c12 = Conv<T>::from(__ldg(S + 4 * n + s)), c22 = Conv<T>::from(__ldg(S + 5 * n + s));
+    T Au[3];
+    Au[0] = c00 * u0 + c01 * u1 + c02 * u2;
+    Au[1] = c01 * u0 + c11 * u1 + c12 * u2;
+    Au[2] = c02 * u0 + c12 * u1 + c22 * u2;
 #pragma unroll 1
-    for (int dy = -1; dy <= 1; ++dy) {
-      if (j + dy < 0 || j + dy >= g.ny) continue;
+    for (int nb = 14; nb < 27; ++nb) {
+      const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
+      const long long off = (long long)dy * g.plane + (long long)dx * g.pz + dz;
+      const TS* Sb = S + (long long)(6 + (nb - 14) * 9) * n;
+      if (i + dx >= 0 && i + dx < g.nx && j + dy >= 0 && j + dy < g.ny && k + dz >= 0 && k + dz < g.nz) {
+        const long long sn = s + off;  // upper neighbour: block stored here
+        const T v0 = __ldg(u + sn), v1 = __ldg(u + n + sn), v2 = __ldg(u + 2 * n + sn);
 #pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        if (i + dx < 0 || i + dx >= g.nx) continue;
+        for (int c = 0; c < 3; ++c)
+          Au[c] += Conv<T>::from(__ldg(Sb + (c * 3 + 0) * n + s)) * v0 +
+                   Conv<T>::from(__ldg(Sb + (c * 3 + 1) * n + s)) * v1 +
+                   Conv<T>::from(__ldg(Sb + (c * 3 + 2) * n + s)) * v2;
+      }
+      if (i - dx >= 0 && i - dx < g.nx && j - dy >= 0 && j - dy < g.ny && k - dz >= 0 && k - dz < g.nz) {
+        const long long sm = s - off;  // lower neighbour: transpose of its block for +d
+        const T v0 = __ldg(u + sm), v1 = __ldg(u + n + sm), v2 = __ldg(u + 2 * n + sm);
 #pragma unroll
-        for (int dz = -1; dz <= 1; ++dz) {
-          if (k + dz < 0 || k + dz >= g.nz) continue;
-          const int nb = (dz + 1) + 3 * (dx + 1) + 9 * (dy + 1);
-          const long long sn = s + dy * g.plane + dx * g.pz + dz;
-          const T u0 = __ldg(u + sn), u1 = __ldg(u + n + sn), u2 = __ldg(u + 2 * n + sn);
-          const TS* Sb = S + (long long)nb * 9 * n + s;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            Au[c] += Conv<T>::from(__ldg(Sb + (c * 3 + 0) * n)) * u0 + Conv<T>::from(__ldg(Sb + (c * 3 + 1) * n)) * u1 +
-                     Conv<T>::from(__ldg(Sb + (c * 3 + 2) * n)) * u2;
-          }
-        }
+        for (int c = 0; c < 3; ++c)
+          Au[c] += Conv<T>::from(__ldg(Sb + (0 * 3 + c) * n + sm)) * v0 +
+                   Conv<T>::from(__ldg(Sb + (1 * 3 + c) * n + sm)) * v1 +
+                   Conv<T>::from(__ldg(Sb + (2 * 3 + c) * n + sm)) * v2;
       }
     }
-    T own[3] = {__ldg(u + s), __ldg(u + n + s), __ldg(u + 2 * n + s)};
+    T own[3] = {u0, u1, u2};
     epi(s, 3, own, Au, dacc);
   }
   finish_dot(epi, dacc, part, ticket, dot_dst);
@@ -77,44 +131,49 @@ template <typename T, typename TS, class Epi>
 __global__ void __launch_bounds__(128)
 k_st2_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
             double* dot_dst) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long n = g.n;
   epi.init();
   double dacc = 0.0;
-  if (i < g.nx) {
-    const long long s = g.slot2(i, j);
-    T Au[2] = {T(0), T(0)};
+  const int i = (int)(s % g.pz), j = (int)(s / g.pz);
+  if (s < n && i < g.nx) {
+    const T u0 = __ldg(u + s), u1 = __ldg(u + n + s);
+    const T c00 = Conv<T>::from(__ldg(S + s)), c01 = Conv<T>::from(__ldg(S + n + s)),
+            c11 = Conv<T>::from(__ldg(S + 2 * n + s));
+    T Au[2];
+    Au[0] = c00 * u0 + c01 * u1;
+    Au[1] = c01 * u0 + c11 * u1;
 #pragma unroll
-    for (int dy = -1; dy <= 1; ++dy) {
-      if (j + dy < 0 || j + dy >= g.ny) continue;
-#pragma unroll
-      for (int dx = -1; dx <= 1; ++dx) {
-        if (i + dx < 0 || i + dx >= g.nx) continue;
-        const int nb = (dx + 1) + 3 * (dy + 1);
-        const long long sn = s + dy * g.pz + dx;
-        const T u0 = __ldg(u + sn), u1 = __ldg(u + n + sn);
-        const TS* Sb = S + (long long)nb * 4 * n + s;
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-          Au[c] += Conv<T>::from(__ldg(Sb + (c * 2 + 0) * n)) * u0 + Conv<T>::from(__ldg(Sb + (c * 2 + 1) * n)) * u1;
+    for (int nb = 5; nb < 9; ++nb) {
+      const int dx = nb % 3 - 1, dy = nb / 3 - 1;
+      const long long off = (long long)dy * g.pz + dx;
+      const TS* Sb = S + (long long)(3 + (nb - 5) * 4) * n;
+      if (i + dx >= 0 && i + dx < g.nx && j + dy >= 0 && j + dy < g.ny) {
+        const long long sn = s + off;
+        const T v0 = __ldg(u + sn), v1 = __ldg(u + n + sn);
+        Au[0] += Conv<T>::from(__ldg(Sb + s)) * v0 + Conv<T>::from(__ldg(Sb + n + s)) * v1;
+        Au[1] += Conv<T>::from(__ldg(Sb + 2 * n + s)) * v0 + Conv<T>::from(__ldg(Sb + 3 * n + s)) * v1;
+      }
+      if (i - dx >= 0 && i - dx < g.nx && j - dy >= 0 && j - dy < g.ny) {
+        const long long sm = s - off;
+        const T v0 = __ldg(u + sm), v1 = __ldg(u + n + sm);
+        Au[0] += Conv<T>::from(__ldg(Sb + sm)) * v0 + Conv<T>::from(__ldg(Sb + 2 * n + sm)) * v1;
+        Au[1] += Conv<T>::from(__ldg(Sb + n + sm)) * v0 + Conv<T>::from(__ldg(Sb + 3 * n + sm)) * v1;
       }
     }
-    T own[2] = {__ldg(u + s), __ldg(u + n + s)};
+    T own[2] = {u0, u1};
     epi(s, 2, own, Au, dacc);
   }
   finish_dot(epi, dacc, part, ticket, dot_dst);
 }
 
-// Dinv of a stencil level: 1 / centre-block diagonal.
+// Dinv of a stencil level: 1 / centre diagonal.
 template <typename TS, typename TD>
 __global__ void k_st_dinv(const Geo g, const TS* __restrict__ S, TD* __restrict__ dinv) {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
-  const int dof = g.dof;
-  const int centre = g.dim == 3 ? 13 : 4;
-  for (int c = 0; c < dof; ++c) {
-    const double v = (double)Conv<double>::from(S[((long long)centre * dof * dof + c * dof + c) * g.n + s]);
+  for (int c = 0; c < g.dof; ++c) {
+    const double v = (double)Conv<double>::from(S[(long long)cidx(g.dim, c, c) * g.n + s]);
     dinv[c * g.n + s] = Conv<TD>::from(v != 0.0 ? 1.0 / v : 0.0);
   }
 }
@@ -232,6 +291,19 @@ __global__ void k_elem_flags(const Geo g, const uint8_t* __restrict__ mask, uint
   flag[s] = f ? 1 : 0;
 }
 
+// Store a computed block V (dof x dof, row-major) for centre/upper direction nb.
+template <typename TS>
+EDGE_D void store_block(const Geo& g, TS* S, long long s, int nb, const double* V, bool valid) {
+  const int d = g.dof;
+  if (nb == centre_nb(g.dim)) {
+    for (int a = 0; a < d; ++a)
+      for (int b = a; b < d; ++b) S[(long long)cidx(g.dim, a, b) * g.n + s] = Conv<TS>::from(valid ? V[a * d + b] : 0.0);
+  } else {
+    for (int a = 0; a < d; ++a)
+      for (int b = 0; b < d; ++b) S[(long long)uidx(g.dim, nb, a, b) * g.n + s] = Conv<TS>::from(valid ? V[a * d + b] : 0.0);
+  }
+}
+
 EDGE_D double pw(int s, int a, int c) {  // 1-D corner weight P_s[a][c]
   return s == 0 ? (a == 0 ? (c == 0 ? 1.0 : 0.0) : 0.5) : (a == 0 ? 0.5 : (c == 1 ? 1.0 : 0.0));
 }
@@ -244,7 +316,7 @@ k_galerkin3_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8
                const uint8_t* __restrict__ eflag, const double* __restrict__ Q, const double* __restrict__ K0b,
                TS* __restrict__ S) {
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int nb = blockIdx.y;
+  const int nb = 13 + blockIdx.y;  // centre and upper directions only
   if (sc >= gc.n) return;
   const int Kz = (int)(sc % gc.pz), Ix = (int)((sc / gc.pz) % gc.nx), Jy = (int)(sc / gc.plane);
   const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
@@ -330,7 +402,7 @@ k_galerkin3_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8
     const double WJ = bnd_total3(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]) + is_bnd(Jn[2], ncn[2]));
     for (int q = 0; q < 9; ++q) V[q] = V[q] / WI / WJ;
   }
-  for (int q = 0; q < 9; ++q) S[((long long)nb * 9 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+  store_block(gc, S, sc, nb, V, valid);
 }
 
 template <typename TE, typename TS>
@@ -339,7 +411,7 @@ k_galerkin2_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8
                const uint8_t* __restrict__ eflag, const double* __restrict__ Q, const double* __restrict__ K0b,
                TS* __restrict__ S) {
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int nb = blockIdx.y;
+  const int nb = 4 + blockIdx.y;  // centre and upper directions only
   if (sc >= gc.n) return;
   const int Ix = (int)(sc % gc.pz), Jy = (int)(sc / gc.pz);
   const int dx = nb % 3 - 1, dy = nb / 3 - 1;
@@ -416,7 +488,7 @@ k_galerkin2_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8
     const double WJ = bnd_total2(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]));
     for (int q = 0; q < 4; ++q) V[q] = V[q] / WI / WJ;
   }
-  for (int q = 0; q < 4; ++q) S[((long long)nb * 4 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+  store_block(gc, S, sc, nb, V, valid);
 }
 
 // ------------------------------------------------------------------ Galerkin, stencil level l -> l+1
@@ -424,7 +496,7 @@ template <typename TS>
 __global__ void __launch_bounds__(128)
 k_galerkin3_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __restrict__ Sc) {
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int nb = blockIdx.y;
+  const int nb = 13 + blockIdx.y;
   if (sc >= gc.n) return;
   const int Kz = (int)(sc % gc.pz), Ix = (int)((sc / gc.pz) % gc.nx), Jy = (int)(sc / gc.plane);
   const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
@@ -453,23 +525,23 @@ k_galerkin3_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __rest
               for (int jz = jlo[2]; jz <= jhi[2]; ++jz) {
                 const double wj = dist_w(abs(jx - 2 * Jn[0]) + abs(jy - 2 * Jn[1]) + abs(jz - 2 * Jn[2]));
                 const int fnb = (jz - iz + 1) + 3 * (jx - ix + 1) + 9 * (jy - iy + 1);
-                const TS* A = Sf + (long long)fnb * 9 * gf.n + si;
                 const double w = wi * wj;
-                for (int q = 0; q < 9; ++q) V[q] += w * (double)Conv<double>::from(A[q * gf.n]);
+                for (int c = 0; c < 3; ++c)
+                  for (int d = 0; d < 3; ++d) V[c * 3 + d] += w * st_get(gf, Sf, si, fnb, c, d);
               }
         }
     const double WI = bnd_total3(is_bnd(I[0], ncn[0]) + is_bnd(I[1], ncn[1]) + is_bnd(I[2], ncn[2]));
     const double WJ = bnd_total3(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]) + is_bnd(Jn[2], ncn[2]));
     for (int q = 0; q < 9; ++q) V[q] = V[q] / WI / WJ;
   }
-  for (int q = 0; q < 9; ++q) Sc[((long long)nb * 9 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+  store_block(gc, Sc, sc, nb, V, valid);
 }
 
 template <typename TS>
 __global__ void __launch_bounds__(128)
 k_galerkin2_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __restrict__ Sc) {
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int nb = blockIdx.y;
+  const int nb = 4 + blockIdx.y;
   if (sc >= gc.n) return;
   const int Ix = (int)(sc % gc.pz), Jy = (int)(sc / gc.pz);
   const int dx = nb % 3 - 1, dy = nb / 3 - 1;
@@ -495,16 +567,16 @@ k_galerkin2_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __rest
           for (int jx = jlo[0]; jx <= jhi[0]; ++jx) {
             const double wj = dist_w(abs(jx - 2 * Jn[0]) + abs(jy - 2 * Jn[1]));
             const int fnb = (jx - ix + 1) + 3 * (jy - iy + 1);
-            const TS* A = Sf + (long long)fnb * 4 * gf.n + si;
             const double w = wi * wj;
-            for (int q = 0; q < 4; ++q) V[q] += w * (double)Conv<double>::from(A[q * gf.n]);
+            for (int c = 0; c < 2; ++c)
+              for (int d = 0; d < 2; ++d) V[c * 2 + d] += w * st_get(gf, Sf, si, fnb, c, d);
           }
       }
     const double WI = bnd_total2(is_bnd(I[0], ncn[0]) + is_bnd(I[1], ncn[1]));
     const double WJ = bnd_total2(is_bnd(Jn[0], ncn[0]) + is_bnd(Jn[1], ncn[1]));
     for (int q = 0; q < 4; ++q) V[q] = V[q] / WI / WJ;
   }
-  for (int q = 0; q < 4; ++q) Sc[((long long)nb * 4 + q) * gc.n + sc] = Conv<TS>::from(valid ? V[q] : 0.0);
+  store_block(gc, Sc, sc, nb, V, valid);
 }
 
 // ------------------------------------------------------------------ coarsest level: dense FP64
@@ -532,22 +604,13 @@ __global__ void k_st_to_dense(const Geo g, const TS* __restrict__ S, double* __r
   const long long row_node = didx(i, j, k);
   const int nnb = g.dim == 3 ? 27 : 9;
   for (int nb = 0; nb < nnb; ++nb) {
-    int di, dj, dk = 0;
-    if (g.dim == 3) {
-      dk = nb % 3 - 1;
-      di = (nb / 3) % 3 - 1;
-      dj = nb / 9 - 1;
-      if (k + dk < 0 || k + dk >= g.nz) continue;
-    } else {
-      di = nb % 3 - 1;
-      dj = nb / 3 - 1;
-    }
+    int di, dj, dk;
+    nb_dir(g.dim, nb, di, dj, dk);
+    if (g.dim == 3 && (k + dk < 0 || k + dk >= g.nz)) continue;
     if (i + di < 0 || i + di >= g.nx || j + dj < 0 || j + dj >= g.ny) continue;
     const long long col_node = didx(i + di, j + dj, k + dk);
     for (int c = 0; c < dof; ++c)
-      for (int d = 0; d < dof; ++d)
-        A[(row_node * dof + c) * nd + col_node * dof + d] =
-            (double)Conv<double>::from(S[((long long)nb * dof * dof + c * dof + d) * g.n + s]);
+      for (int d = 0; d < dof; ++d) A[(row_node * dof + c) * nd + col_node * dof + d] = st_get(g, S, s, nb, c, d);
   }
 }
 

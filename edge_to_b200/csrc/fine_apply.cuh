@@ -88,18 +88,18 @@ template <typename T, typename TB, typename TD> struct EpiJacobi {
 
 // Last post-smoothing sweep fused with the correction: xo = xbase + e + w Dinv (b - A e),
 // with e = u.  With kDot, acc += dotv . xo (the PCG's r.z at level 0).
-template <typename T, typename TB, typename TD, typename TX, bool DOT> struct EpiJacobiAdd {
+template <typename T, typename TB, typename TD, typename TX, bool DOT, typename TV = TB> struct EpiJacobiAdd {
   const TB* b;
   const TD* dinv;
   const TX* xbase;
   TX* xo;
-  const TB* dotv;
+  const TV* dotv;
   const double* omega;
   double wscale;
   long long n;
   T w;
   static constexpr bool kDot = DOT;
-  static constexpr int kIoBytes = sizeof(TB) + sizeof(TD) + 2 * sizeof(TX) + (DOT ? sizeof(TB) : 0);
+  static constexpr int kIoBytes = sizeof(TB) + sizeof(TD) + 2 * sizeof(TX) + (DOT ? sizeof(TV) : 0);
   EDGE_D void init() { w = Conv<T>::from(__ldg(omega) * wscale); }
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) {

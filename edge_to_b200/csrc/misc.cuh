@@ -323,9 +323,12 @@ struct PcgState {
 
 // x += alpha p ; r -= alpha q ; rr = r.r with alpha = rz_new / pq.  The finisher
 // updates res / omega / done as solvers/_multigrid_cuda.py:219-227 and moves rz_new to rz.
+// With r32 != nullptr the updated residual is also written in FP32 (the V-cycle input of
+// the mixed-precision solver).
 template <typename TX, typename TP>
 __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__ p, TX* __restrict__ r,
-                         const TP* __restrict__ q, PcgState* st, double* part, unsigned* ticket) {
+                         const TP* __restrict__ q, PcgState* st, double* part, unsigned* ticket,
+                         float* __restrict__ r32) {
   const double alpha = st->rz_new / st->pq;
   double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -334,6 +337,7 @@ __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__
     x[i] = Conv<TX>::from((double)Conv<double>::from(x[i]) + alpha * pi);
     const double ri = (double)Conv<double>::from(r[i]) - alpha * qi;
     r[i] = Conv<TX>::from(ri);
+    if (r32) r32[i] = (float)ri;
     acc += ri * ri;
   }
   __shared__ double sh[32];
@@ -358,6 +362,20 @@ __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__
     }
   };
   grid_reduce_finish(bt, part, ticket, Fin{st, alpha});
+}
+
+// Residual replacement: st->rr holds the TRUE residual r.r (b - A x in FP64).  Decides
+// convergence on it; otherwise the iteration continues with the replaced residual.
+__global__ void k_pcg_true_res(PcgState* st) {
+  const double R = sqrt(st->rr) / sqrt(st->bb);
+  st->res = R;
+  if (R < st->tol) {
+    st->done = 1;
+  } else {
+    st->done = (st->iter >= st->maxiter) ? 2 : 0;
+    const double Rc = fmin(fmax(R, st->tol), 1e-1);
+    st->omega = st->min_omega + st->d_omega / 2.0 * exp((-Rc + st->tol) * 500.0);
+  }
 }
 
 // p = z + beta p

@@ -358,11 +358,9 @@ static void fine_apply_dense(Prob& P, const T* u, Epi epi, double* dot_dst) {
 template <typename T, class Epi>
 static void st_apply(Prob& P, const Geo& g, const T* u, const T* S, Epi epi, double* dot_dst) {
   if (g.dim == 3)
-    launch(P, k_st3_apply<T, T, Epi>, dim3(cdiv(g.nz, 128), g.nx, g.ny), 128, 0, g, u, S, epi, P.part, P.ticket,
-                                                                                    dot_dst);
+    launch(P, k_st3_apply<T, T, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
   else
-    launch(P, k_st2_apply<T, T, Epi>, dim3(cdiv(g.nx, 128), g.ny), 128, 0, g, u, S, epi, P.part, P.ticket, dot_dst);
-  KCHECK();
+    launch(P, k_st2_apply<T, T, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
 }
 
 template <typename T, class Epi>
@@ -428,7 +426,7 @@ static void mg_setup(Prob& P) {
   // level 1 from the fine operator
   {
     const Geo& gc = P.lv[1].g;
-    const int nnb = P.dim == 3 ? 27 : 9;
+    const int nnb = P.dim == 3 ? 14 : 5;  // centre + upper directions
     dim3 grid(cdiv(gc.n, 128), nnb);
     if (P.dim == 3)
       launch(P, k_galerkin3_l0<T, T>, grid, 128, 0, g0, gc, E, P.mask, P.eflag, P.dQ, P.dK0b, (T*)P.lv[1].S);
@@ -439,7 +437,7 @@ static void mg_setup(Prob& P) {
   for (int l = 1; l < L; ++l) {
     const Geo& gf = P.lv[l].g;
     const Geo& gc = P.lv[l + 1].g;
-    const int nnb = P.dim == 3 ? 27 : 9;
+    const int nnb = P.dim == 3 ? 14 : 5;
     dim3 grid(cdiv(gc.n, 128), nnb);
     if (P.dim == 3)
       launch(P, k_galerkin3_st<T>, grid, 128, 0, gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
@@ -549,7 +547,7 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
       const bool dot = last_visit && dot_dst != nullptr;
       if (l == 0) {
         if (dot) {
-          EpiJacobiAdd<T, T, TD0, T, true> e{r, (const TD0*)Lv.dinv, xcur, out, (const T*)dotv, om, ws, g.n};
+          EpiJacobiAdd<T, T, TD0, T, true, TV> e{r, (const TD0*)Lv.dinv, xcur, out, dotv, om, ws, g.n};
           level_apply<T>(P, l, e1, e, dot_dst);
         } else {
           EpiJacobiAdd<T, T, TD0, T, false> e{r, (const TD0*)Lv.dinv, xcur, out, (const T*)nullptr, om, ws, g.n};
@@ -597,7 +595,7 @@ static void mg_allocate(Prob& P) {
         Lv.dinv = vec();
     }
     if (l > 0) {
-      const size_t ns = (size_t)(P.dim == 3 ? 243 : 36) * Lv.g.n;
+      const size_t ns = (size_t)nst(P.dim) * Lv.g.n;
       Lv.S = vb == 8 ? (void*)P.alloc<double>(ns) : (void*)P.alloc<float>(ns);
     }
   }
@@ -641,7 +639,7 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
       fine_apply<double>(P, p, e, &P.st->pq);
     }
     launch(P, k_pcg_xr<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, x, p, r, q, P.st,
-                                                                                           P.part, P.ticket);
+                                                                                           P.part, P.ticket, (float*)nullptr);
     KCHECK();
     CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
     CK(cudaStreamSynchronize(P.stream));
@@ -654,6 +652,61 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
   P.last_iters = P.st_h->iter;
 }
 
+// Mixed precision: FP32 operator, V-cycle and search directions; FP64 solution, residual
+// recurrence, dot products, coarse solve, and true residuals r = b - A x (FP64 operator
+// with FP64 E) that replace the recurrence every time it has dropped by REPLACE_DROP and
+// before convergence is declared.
+static const double REPLACE_DROP = 1e-2;
+
+static void pcg_mixed(Prob& P, double tol, int maxiter) {
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  double* r = P.r64;
+  double* x = P.x64;
+  float* r32 = P.r32;
+  float* p = (float*)P.p;
+  float* q = (float*)P.q;
+  float* z = (float*)P.lv[0].res;
+  const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
+  auto true_residual = [&]() {
+    EpiResid<double, double, double> e{P.b64, r, g.n};
+    fine_apply<double>(P, x, e, nullptr);
+    launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)r, (const double*)r, P.part, P.ticket, &P.st->rr);
+    launch(P, k_copy<double, float>, ew_blocks(nv), 256, 0, nv, (const double*)r, r32);
+    ++P.last_true_res;
+  };
+  P.last_true_res = 0;
+  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
+  launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.b64, (const double*)P.b64, P.part, P.ticket,
+         &P.st->bb);
+  true_residual();
+  launch(P, k_pcg_check_bb, 1, 1, 0, P.st);
+  vcycle<float, __nv_bfloat16, double>(P, 0, r32, z, r, &P.st->rz_new);
+  launch(P, k_copy<float, float>, ew_blocks(nv), 256, 0, nv, (const float*)z, p);
+  double last_replace = 1.0;
+  for (;;) {
+    {
+      EpiStoreDot<float> e{q, g.n};
+      fine_apply<float>(P, p, e, &P.st->pq);
+    }
+    launch(P, k_pcg_xr<double, float>, nb, 256, 0, nv, x, (const float*)p, r, (const float*)q, P.st, P.part, P.ticket,
+           r32);
+    CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
+    CK(cudaStreamSynchronize(P.stream));
+    if (P.st_h->done == 1 || P.st_h->res < REPLACE_DROP * last_replace) {
+      true_residual();
+      launch(P, k_pcg_true_res, 1, 1, 0, P.st);
+      CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
+      CK(cudaStreamSynchronize(P.stream));
+      last_replace = P.st_h->res;
+    }
+    if (P.st_h->done) break;
+    vcycle<float, __nv_bfloat16, double>(P, 0, r32, z, r, &P.st->rz_new);
+    launch(P, k_pcg_p<float>, ew_blocks(nv), 256, 0, nv, p, (const float*)z, P.st);
+  }
+  P.last_iters = P.st_h->iter;
+}
+
 static void ensure_mg(Prob& P) {
   if (P.n_level < 0) fail(EDGE_ESTATE, "multigrid not configured (edge_mg_config)");
 }
@@ -662,18 +715,20 @@ static void solve_internal(Prob& P, double tol, int maxiter) {
   ensure_mg(P);
   if (!P.has_rho) fail(EDGE_ESTATE, "Solver requires a density vector to be passed or set on the kernel.");
   CK(cudaEventRecord(P.ev[0], P.stream));
-  if (P.prec == EDGE_FP64) {
+  if (P.prec == EDGE_FP64)
     mg_setup<double, double>(P);
-  } else {
-    fail(EDGE_EINVAL, "mixed precision solve not available in this build");
-  }
+  else
+    mg_setup<float, __nv_bfloat16>(P);
   CK(cudaEventRecord(P.ev[1], P.stream));
   // check the coarse factorisation
   int status = 0;
   CK(cudaMemcpyAsync(&status, P.chol_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
   CK(cudaStreamSynchronize(P.stream));
   if (status) fail(EDGE_ENOTPD, "coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
-  pcg_fp64<double, double>(P, tol, maxiter);
+  if (P.prec == EDGE_FP64)
+    pcg_fp64<double, double>(P, tol, maxiter);
+  else
+    pcg_mixed(P, tol, maxiter);
   CK(cudaEventRecord(P.ev[2], P.stream));
   CK(cudaEventSynchronize(P.ev[2]));
   float a = 0, b = 0;
@@ -750,19 +805,14 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     P.mask = P.alloc<uint8_t>(g.n);
     P.eflag = P.alloc<uint8_t>(g.n);
     P.E64 = P.alloc<double>(g.n);
-    if (precision == EDGE_MIXED) P.E32 = P.alloc<float>(g.n);
+    P.E32 = P.alloc<float>(g.n);
     const size_t nv = (size_t)g.dof * g.n;
     P.b64 = P.alloc<double>(nv);
     P.x64 = P.alloc<double>(nv);
     P.r64 = P.alloc<double>(nv);
-    if (precision == EDGE_FP64) {
-      P.p = P.alloc<double>(nv);
-      P.q = P.alloc<double>(nv);
-    } else {
-      P.p = P.alloc<float>(nv);
-      P.q = P.alloc<float>(nv);
-      P.r32 = P.alloc<float>(nv);
-    }
+    P.p = P.alloc<double>(nv);  // sized for FP64; the mixed path uses the first half as FP32
+    P.q = P.alloc<double>(nv);
+    P.r32 = P.alloc<float>(nv);
     P.rho_f = P.alloc<double>(P.n_el);
     P.gsens = P.alloc<double>(P.n_el);
     P.ocp = P.alloc<double>(P.n_el);
@@ -879,10 +929,11 @@ int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev) {
 }
 
 int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, double min_omega, int cycle_w,
-                   const int* w_levels, int n_w) {
+                   const int* w_levels, int n_w, int precision) {
   API_BEGIN
   if (!p) fail(EDGE_EINVAL, "null handle");
   Prob& P = p->P;
+  if (precision != EDGE_FP64 && precision != EDGE_MIXED) fail(EDGE_EINVAL, "unknown precision");
   if (n_level < 1 || n_smooth < 0) fail(EDGE_EINVAL, "n_level must be >= 1 and n_smooth >= 0");
   for (int l = 1; l <= n_level; ++l) {
     Geo g = level_geo(P, l);
@@ -890,7 +941,7 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
       fail(EDGE_EINVAL, "n_level too large for this mesh: level " + std::to_string(l) + " has no elements");
   }
   cudaStreamSynchronize(P.stream);
-  const bool realloc = (n_level != P.n_level);
+  const bool realloc = (n_level != P.n_level) || (precision != P.prec);
   P.n_smooth = n_smooth;
   P.omega = omega;
   P.min_omega = std::max(omega / 2, min_omega);
@@ -917,6 +968,7 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
       }
     }
     P.n_level = n_level;
+    P.prec = precision;
     mg_allocate(P);
   }
   API_END
@@ -978,6 +1030,38 @@ int edge_profile_end(edge_problem* p, double* kernel_ms, double* kernel_bytes, i
   if (kernel_launches) *kernel_launches = (int)(P.pev_used / 2);
   if (total_launches) *total_launches = P.nlaunch;
   P.prof = false;
+  API_END
+}
+
+int edge_mg_setup(edge_problem* p) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  Prob& P = p->P;
+  ensure_mg(P);
+  if (!P.has_rho) fail(EDGE_ESTATE, "rho not set");
+  if (P.prec == EDGE_FP64)
+    mg_setup<double, double>(P);
+  else
+    mg_setup<float, __nv_bfloat16>(P);
+  CK(cudaStreamSynchronize(P.stream));
+  API_END
+}
+
+int edge_mg_level_dense(edge_problem* p, int level, double* out_dev, long long n) {
+  API_BEGIN
+  if (!p || !out_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  ensure_mg(P);
+  if (level < 1 || level > P.n_level) fail(EDGE_EINVAL, "level must be in [1, n_level]");
+  const Geo& g = P.lv[level].g;
+  const long long nd = (long long)g.nx * g.ny * g.nz * g.dof;
+  if (n != nd) fail(EDGE_EINVAL, "dense size mismatch: level has " + std::to_string(nd) + " DOFs");
+  CK(cudaMemsetAsync(out_dev, 0, (size_t)nd * nd * sizeof(double), P.stream));
+  if (P.prec == EDGE_FP64)
+    launch(P, k_st_to_dense<double>, cdiv(g.n, 256), 256, 0, g, (const double*)P.lv[level].S, out_dev, (int)nd);
+  else
+    launch(P, k_st_to_dense<float>, cdiv(g.n, 256), 256, 0, g, (const float*)P.lv[level].S, out_dev, (int)nd);
+  CK(cudaStreamSynchronize(P.stream));
   API_END
 }
 

@@ -68,12 +68,14 @@ class CuMultiGrid(Solver):
         self.last_x0 = None
 
     def _configure(self):
-        key = (self.n_level, self.n_smooth, self.max_omega, self.min_omega, self.cycle, tuple(self.w_level))
+        key = (self.n_level, self.n_smooth, self.max_omega, self.min_omega, self.cycle, tuple(self.w_level),
+               self.precision)
         if self._configured == key:
             return
         w = _lib.int_array(self.w_level) if self.w_level else None
+        prec = _lib.EDGE_FP64 if self.precision == "fp64" else _lib.EDGE_MIXED
         _lib.call("edge_mg_config", self.kernel.handle, int(self.n_level), int(self.n_smooth), float(self.max_omega),
-                  float(self.min_omega), 1 if self.cycle == "w" else 0, w, len(self.w_level))
+                  float(self.min_omega), 1 if self.cycle == "w" else 0, w, len(self.w_level), prec)
         self._configured = key
 
     def solve(self, rhs, rho=None, use_last=True):

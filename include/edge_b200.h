@@ -37,7 +37,8 @@ int edge_version(void);
 /* ---- structured mesh + stiffness operator.
  * Replaces StructuredStiffnessKernel (kernels/_cuda.py:62-302) built on
  * CuStructuredMesh2D/3D (geom/_mesh.py:81-143).  K0 is the element stiffness of
- * element 0 (host, row-major (2^dim*dim)^2, the reference's local node order). */
+ * element 0 (host, row-major (2^dim*dim)^2, the reference's local node order).
+ * precision is the initial solver precision (edge_mg_config can change it). */
 int edge_problem_create(int dim, const int* nel, const double* K0, int precision, edge_problem** out);
 int edge_problem_destroy(edge_problem* p);
 int edge_set_stream(edge_problem* p, void* stream);
@@ -57,13 +58,20 @@ int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
 int edge_uses_transform(const edge_problem* p);
 
 /* ---- geometric multigrid PCG.  Replaces CuMultiGrid (solvers/_multigrid_cuda.py:15-242).
- * cycle_w != 0 reproduces cycle == 'w' (second coarse visit on the levels in w_levels). */
+ * cycle_w != 0 reproduces cycle == 'w' (second coarse visit on the levels in w_levels).
+ * precision: EDGE_FP64 or EDGE_MIXED (see above). */
 int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, double min_omega, int cycle_w,
-                   const int* w_levels, int n_w);
+                   const int* w_levels, int n_w, int precision);
 /* Solves K(E) x = f to ||r||/||f|| < tol.  x_dev holds the warm start when use_last != 0
  * and receives the solution.  Never fails on non-convergence: *residual_out reports it. */
 int edge_mg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
                   double* residual_out, int* iters_out);
+
+/* Builds the hierarchy for the current E / BCs without solving (CuMultiGrid._setup,
+ * solvers/_multigrid_cuda.py:64-118), and returns level l (1..n_level) as a dense
+ * row-major n x n FP64 matrix in the reference's coarse DOF order (test inspection). */
+int edge_mg_setup(edge_problem* p);
+int edge_mg_level_dense(edge_problem* p, int level, double* out_dev, long long n);
 
 /* ---- grid transfers.  Replace apply_restriction_cuda / apply_prolongation_cuda
  * (core/_mgm_cuda.py:223-314); nel is the FINE grid. */

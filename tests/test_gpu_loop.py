@@ -99,3 +99,32 @@ def test_fused_and_object_paths_agree():
         type(opt).fused = orig
     assert abs(float(c1) - float(c2)) / float(c2) < 1e-12
     assert (dr1.reshape(-1) - dr2.reshape(-1)).abs().max().item() / dr2.abs().max().item() < 1e-10
+
+
+def test_mixed_precision_mbb_against_reference(golden):
+    """Mixed precision (FP32 operator / V-cycle, BF16 Jacobi diagonal, FP64 residual
+    replacement): same 100-iteration trajectory within the parity bar."""
+    z = golden("loop_mbb2d.npz")
+    opt = _mbb("mixed")
+    opt.max_iter = 100
+    rho, flag, hist = opt.optimize(save_comp_history=True)
+    c = np.array(hist["comp_history"])
+    err_c = np.abs(c - z["comp_history"]) / z["comp_history"]
+    err_rho = np.abs(rho.cpu().numpy() - z["rho_final"]).max()
+    print(f"mixed mbb: max compliance rel err {err_c.max():.3e}, final rho max err {err_rho:.3e}")
+    assert err_c.max() <= 1e-6
+    assert err_rho <= 1e-5
+
+
+def test_mixed_vs_fp64_cantilever():
+    """3-D cantilever, 5 SIMP iterations at rtol 1e-6: mixed vs FP64 compliance within 1e-6."""
+    res = {}
+    for prec in ("fp64", "mixed"):
+        opt = _cant((64, 32, 32), 0.12, 1.5, dict(tol=1e-6, n_level=4, maxiter=1000), prec)
+        opt.max_iter = 5
+        rho, flag, hist = opt.optimize(save_comp_history=True)
+        res[prec] = (np.array(hist["comp_history"]), rho.cpu().numpy(), opt.solver.last_iters)
+    err = np.abs(res["mixed"][0] - res["fp64"][0]) / res["fp64"][0]
+    print("mixed vs fp64 compliance rel err", err, "pcg iters", res["fp64"][2], res["mixed"][2])
+    assert err.max() <= 1e-6
+    assert np.abs(res["mixed"][1] - res["fp64"][1]).max() <= 1e-5
