@@ -59,6 +59,16 @@ __global__ void k_mask_from_user(const Geo g, const uint8_t* __restrict__ cons, 
   mask[s] = m;
 }
 
+// Copy of the per-node mask with rows padded to 16 bytes (the TMA source of the fine kernel).
+__global__ void k_mask_pitch16(const Geo g, const uint8_t* __restrict__ mask, uint8_t* __restrict__ m16, int mpz) {
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  if (!node_of_slot(g, s, i, j, k, node)) return;
+  m16[((long long)j * g.nx + i) * mpz + k] = mask[s];
+}
+
 // Element arrays: user order e = i*nely*nelz + j*nelz + k (3-D), i*nely + j (2-D)
 // (core/_geom.py:17-18, 43-46) <-> node-aligned slots.
 EDGE_D long long user_elem(const Geo& g, int i, int j, int k) {

@@ -5,9 +5,12 @@
 // The solve path (edge_mg_solve / edge_simp_solve_and_process) only launches kernels on
 // the problem's stream; the host reads back the PCG state once per iteration to decide
 // convergence, exactly where the reference syncs (solvers/_multigrid_cuda.py:223-226).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -18,6 +21,7 @@
 #include "common.cuh"
 #include "element_op.cuh"
 #include "fine_apply.cuh"
+#include "fine_tma.cuh"
 #include "misc.cuh"
 
 namespace edge {
@@ -196,7 +200,12 @@ struct Prob {
   double* dK0diag = nullptr;
   double* dQ = nullptr;
   uint8_t* mask = nullptr;
+  uint8_t* mask16 = nullptr;  // same bits, rows padded to 16 bytes (TMA source)
+  int mpz = 0;
   uint8_t* eflag = nullptr;
+  int* err = nullptr;          // set by kernels whose bounded waits expired
+  bool use_tma = true;
+  std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
   double* E64 = nullptr;
   float* E32 = nullptr;
   bool has_rho = false, has_cons = false;
@@ -272,6 +281,69 @@ static Geo level_geo(const Prob& P, int l) {
   return make_geo(P.dim, ne[0], ne[1], P.dim == 3 ? ne[2] : 0);
 }
 
+// ------------------------------------------------------------------ TMA tensor maps
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static void get_encode() {
+  if (g_encode) return;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (q != cudaDriverEntryPointSuccess || !fn) fail(EDGE_ECUDA, "cuTensorMapEncodeTiled not available");
+  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+}
+
+static CUtensorMap encode_map(const void* base, CUtensorMapDataType dt, int rank, const uint64_t* dims,
+                              const uint64_t* strides, const uint32_t* box) {
+  get_encode();
+  CUtensorMap m;
+  uint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = g_encode(&m, dt, rank, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(EDGE_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return m;
+}
+
+template <typename T> static CUtensorMapDataType tma_dt() {
+  return sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+}
+
+// kind 0: 3-component fine vector (box 48 x (BX+1) x 1 x 3); 1: fine element array (48 x BX x 1)
+template <typename T, int BX>
+static const CUtensorMap& fine_map(Prob& P, const T* base, int kind) {
+  auto key = std::make_pair((const void*)base, kind * 16 + (int)sizeof(T) + 100 * BX);
+  auto it = P.tmaps.find(key);
+  if (it != P.tmaps.end()) return it->second;
+  const Geo& g = P.g0;
+  const uint64_t sz = sizeof(T);
+  CUtensorMap m;
+  if (kind == 0) {
+    uint64_t dims[4] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny, 3};
+    uint64_t str[3] = {g.pz * sz, g.plane * sz, g.n * sz};
+    uint32_t box[4] = {TMA_ZB, BX + 1, 1, 3};
+    m = encode_map(base, tma_dt<T>(), 4, dims, str, box);
+  } else {
+    uint64_t dims[3] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny};
+    uint64_t str[2] = {g.pz * sz, g.plane * sz};
+    uint32_t box[3] = {TMA_ZB, BX, 1};
+    m = encode_map(base, tma_dt<T>(), 3, dims, str, box);
+  }
+  return P.tmaps.emplace(key, m).first->second;
+}
+
+template <int BX>
+static const CUtensorMap& mask_map(Prob& P) {
+  auto key = std::make_pair((const void*)P.mask16, 1000 + BX);
+  auto it = P.tmaps.find(key);
+  if (it != P.tmaps.end()) return it->second;
+  const Geo& g = P.g0;
+  uint64_t dims[3] = {(uint64_t)P.mpz, (uint64_t)g.nx, (uint64_t)g.ny};
+  uint64_t str[2] = {(uint64_t)P.mpz, (uint64_t)P.mpz * g.nx};
+  uint32_t box[3] = {TMA_ZB, BX + 1, 1};
+  return P.tmaps.emplace(key, encode_map(P.mask16, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims, str, box)).first->second;
+}
+
 static size_t vbytes(int prec) { return prec == EDGE_FP64 ? sizeof(double) : sizeof(float); }
 
 // ------------------------------------------------------------------ launch helpers
@@ -315,7 +387,20 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
   const bool rec = P.prof && P.pev_used + 2 <= P.pev.size();
   if (rec) CK(cudaEventRecord(P.pev[P.pev_used], P.stream));
   if (P.ei.wht) {
-    if (P.dim == 3) {
+    if (P.dim == 3 && P.use_tma) {
+      constexpr int NS = 4;
+      constexpr int smem = tma_smem_bytes<T, FINE_BX, NS>();
+      static bool attr = false;
+      if (!attr) {
+        CK(cudaFuncSetAttribute(k_fine3_tma<T, Epi, FINE_BX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr = true;
+      }
+      int ly;
+      dim3 grid = fine3_grid(g, ly);
+      launch(P, k_fine3_tma<T, Epi, FINE_BX, NS>, grid, dim3(32, FINE_BX), smem, g, fine_map<T, FINE_BX>(P, u, 0),
+             mask_map<FINE_BX>(P), fine_map<T, FINE_BX>(P, E, 1), u, (const uint8_t*)P.mask, cast3<T>(P.ei.k3), ly,
+             epi, P.part, P.ticket, dot_dst, P.err);
+    } else if (P.dim == 3) {
       int ly;
       dim3 grid = fine3_grid(g, ly);
       launch(P, k_fine3_wht<T, T, Epi, FINE_BX>, grid, dim3(32, FINE_BX), 0, g, u, E, (const uint8_t*)P.mask,
@@ -707,6 +792,16 @@ static void pcg_mixed(Prob& P, double tol, int maxiter) {
   P.last_iters = P.st_h->iter;
 }
 
+static void check_err(Prob& P) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, P.err, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaStreamSynchronize(P.stream));
+  if (e) {
+    CK(cudaMemsetAsync(P.err, 0, sizeof(int), P.stream));
+    fail(EDGE_ECUDA, "a bounded wait for a TMA stage expired; results of this call are invalid");
+  }
+}
+
 static void ensure_mg(Prob& P) {
   if (P.n_level < 0) fail(EDGE_ESTATE, "multigrid not configured (edge_mg_config)");
 }
@@ -731,6 +826,7 @@ static void solve_internal(Prob& P, double tol, int maxiter) {
     pcg_mixed(P, tol, maxiter);
   CK(cudaEventRecord(P.ev[2], P.stream));
   CK(cudaEventSynchronize(P.ev[2]));
+  check_err(P);
   float a = 0, b = 0;
   CK(cudaEventElapsedTime(&a, P.ev[0], P.ev[1]));
   CK(cudaEventElapsedTime(&b, P.ev[1], P.ev[2]));
@@ -803,7 +899,12 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     CK(cudaMemcpy(P.dQ, P.ei.Q.data(), P.ei.Q.size() * sizeof(double), cudaMemcpyHostToDevice));
     const Geo& g = P.g0;
     P.mask = P.alloc<uint8_t>(g.n);
+    if (dim == 3) {
+      P.mpz = (g.nz + 15) & ~15;
+      P.mask16 = P.alloc<uint8_t>((size_t)g.ny * g.nx * P.mpz);
+    }
     P.eflag = P.alloc<uint8_t>(g.n);
+    P.err = P.alloc<int>(1);
     P.E64 = P.alloc<double>(g.n);
     P.E32 = P.alloc<float>(g.n);
     const size_t nv = (size_t)g.dof * g.n;
@@ -854,11 +955,19 @@ int edge_set_stream(edge_problem* p, void* stream) {
 
 int edge_uses_transform(const edge_problem* p) { return p && p->P.ei.wht ? 1 : 0; }
 
+int edge_set_tma(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.use_tma = enable != 0;
+  API_END
+}
+
 int edge_set_constraints(edge_problem* p, const uint8_t* cons_dev) {
   API_BEGIN
   if (!p || !cons_dev) fail(EDGE_EINVAL, "null argument");
   Prob& P = p->P;
   launch(P, k_mask_from_user, cdiv(P.g0.n, 256), 256, 0, P.g0, cons_dev, P.mask);
+  if (P.mask16) launch(P, k_mask_pitch16, cdiv(P.g0.n, 256), 256, 0, P.g0, (const uint8_t*)P.mask, P.mask16, P.mpz);
   launch(P, k_elem_flags, cdiv(P.g0.n, 256), 256, 0, P.g0, P.mask, P.eflag);
   KCHECK();
   P.has_cons = true;
@@ -969,6 +1078,7 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
     }
     P.n_level = n_level;
     P.prec = precision;
+    P.tmaps.clear();
     mg_allocate(P);
   }
   API_END

@@ -54,6 +54,9 @@ int edge_diagonal(edge_problem* p, double* diag_dev);
 int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev);
 /* Same product through the dense node-centric kernel (an independent path for tests). */
 int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
+/* Tuning/testing switch: 1 (default) stages 3-D fine-level tiles with TMA, 0 uses the
+ * cooperative-load version of the same kernel. */
+int edge_set_tma(edge_problem* p, int enable);
 /* 1 when the element matrix has the box structure used by the transform kernels */
 int edge_uses_transform(const edge_problem* p);
 
