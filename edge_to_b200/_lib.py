@@ -28,6 +28,7 @@ _SIGS = {
     "edge_set_rho": (ctypes.c_int, [vp, vp]),
     "edge_matvec": (ctypes.c_int, [vp, vp, vp]),
     "edge_matvec_dense": (ctypes.c_int, [vp, vp, vp]),
+    "edge_matvec_f32": (ctypes.c_int, [vp, vp, vp]),
     "edge_diagonal": (ctypes.c_int, [vp, vp]),
     "edge_process_grad": (ctypes.c_int, [vp, vp, vp]),
     "edge_uses_transform": (ctypes.c_int, [vp]),

@@ -999,6 +999,22 @@ int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev) {
   API_END
 }
 
+// The product through the FP32 operator of the mixed-precision solver (FP32 E and u).
+int edge_matvec_f32(edge_problem* p, const double* u_dev, double* out_dev) {
+  API_BEGIN
+  if (!p || !u_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. dot works only after setting rho.");
+  const Geo& g = P.g0;
+  float* u32 = (float*)P.p;
+  float* o32 = (float*)P.q;
+  launch(P, k_user_to_slots<float>, cdiv(g.n, 256), 256, 0, g, u_dev, u32);
+  EpiStore<float, float> e{o32, g.n};
+  fine_apply<float>(P, u32, e, nullptr);
+  launch(P, k_slots_to_user<float>, cdiv(g.n, 256), 256, 0, g, (const float*)o32, out_dev);
+  API_END
+}
+
 // Same product through the dense kernel (used by tests as an independent path).
 int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev) {
   API_BEGIN

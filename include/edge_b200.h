@@ -52,6 +52,8 @@ int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev);
 int edge_diagonal(edge_problem* p, double* diag_dev);
 /* kernels/_cuda.py:152-156 : dk_e = -u_e^T K0 u_e */
 int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev);
+/* The same product through the FP32 operator of the mixed-precision solver. */
+int edge_matvec_f32(edge_problem* p, const double* u_dev, double* out_dev);
 /* Same product through the dense node-centric kernel (an independent path for tests). */
 int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
 /* Tuning/testing switch: 1 (default) stages 3-D fine-level tiles with TMA, 0 uses the

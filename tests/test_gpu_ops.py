@@ -249,3 +249,23 @@ def test_fine_kernel_variants_agree(nel):
     b = k.dot(ut).cpu().clone()
     _lib.call("edge_set_tma", k.handle, 1)
     assert rel(a, ref) < TOL and rel(b, ref) < TOL
+
+
+def test_fp32_operator_accuracy():
+    """The mixed-precision solver's FP32 operator agrees with FP64 to single-precision accuracy."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    for nel in ((40, 9, 33), (64, 32)):
+        dim = len(nel)
+        rng = np.random.default_rng(5)
+        mesh = _mesh(dim, nel, None)
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        g = Grid(nel)
+        k.set_rho(torch.as_tensor(rng.uniform(1e-3, 1, g.n_el), device="cuda"))
+        k.add_constraints(np.where(rng.random(g.n_dof) < 0.05)[0])
+        u = torch.as_tensor(rng.standard_normal(g.n_dof), device="cuda")
+        a = k.dot(u).clone()
+        b = torch.empty_like(a)
+        _lib.call("edge_matvec_f32", k.handle, _lib.ptr(u), _lib.ptr(b))
+        assert rel(b.cpu(), a.cpu()) < 1e-5
