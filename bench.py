@@ -253,10 +253,30 @@ def run_ours(args, cfg_name):
         "gpu_launches": int(tl.value),
         "clocks": clk,
     }
+    if args.breakdown:
+        line["breakdown_ms_per_step"] = breakdown(opt, rho, dr, it)
     if ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, pcg_iters=float(np.mean(pcg)) if pcg else PCG_ITERS_FP64_CFG5,
                                             reps=2)
     return line
+
+
+CATS = ["other", "fine_operator", "coarse_stencils", "transfers", "vector_pcg", "setup_galerkin_chol",
+        "coarsest_solve", "oc_update", "filter_sensitivity"]
+
+
+def breakdown(opt, rho, dr, it):
+    """One more SIMP step (outside the timed region) with CUDA events around every launch."""
+    import ctypes
+    from edge_to_b200 import _lib
+    h = opt.kernel.handle
+    _lib.call("edge_breakdown_begin", h, 60000)
+    rho = opt.update_design(rho, dr)
+    opt.solve_and_process(rho, it)
+    ms = (ctypes.c_double * 16)()
+    nn = (ctypes.c_int * 16)()
+    _lib.call("edge_breakdown_end", h, ms, nn, 16)
+    return {CATS[i]: {"ms": round(ms[i], 3), "launches": nn[i]} for i in range(len(CATS))}
 
 
 def cpu_baseline(cfg, pcg_iters, reps=2):
@@ -353,6 +373,8 @@ def main():
     ap.add_argument("--config", default="cantilever_256x128x128", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec"])
+    ap.add_argument("--breakdown", action="store_true",
+                    help="extra untimed step with per-category launch timing (events on every launch)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -51,6 +51,8 @@ _SIGS = {
                                                    c_int_p]),
     "edge_last_solve_stats": (ctypes.c_int, [vp, c_double_p, c_double_p, c_int_p, c_int_p]),
     "edge_profile_begin": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_breakdown_begin": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_breakdown_end": (ctypes.c_int, [vp, c_double_p, c_int_p, ctypes.c_int]),
     "edge_profile_end": (ctypes.c_int, [vp, c_double_p, c_double_p, c_int_p, ctypes.POINTER(ctypes.c_longlong)]),
 }
 

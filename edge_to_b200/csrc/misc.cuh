@@ -59,14 +59,22 @@ __global__ void k_mask_from_user(const Geo g, const uint8_t* __restrict__ cons, 
   mask[s] = m;
 }
 
-// Copy of the per-node mask with rows padded to 16 bytes (the TMA source of the fine kernel).
-__global__ void k_mask_pitch16(const Geo g, const uint8_t* __restrict__ mask, uint8_t* __restrict__ m16, int mpz) {
+// Element constraint flags with rows padded to 16 bytes (the TMA source of the fine
+// kernel): f(i,j,k) = 1 if any existing corner (i+a, j+b, k+c), a,b,c in {0,1}, of the
+// element slot has a constrained DOF.  Slots past the last element (ghosts) are flagged
+// from their existing corners, so f(i,j,k) always covers node (i,j,k) itself.
+__global__ void k_flag_pitch16(const Geo g, const uint8_t* __restrict__ mask, uint8_t* __restrict__ f16, int mpz) {
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   int i, j, k;
   long long node;
   if (!node_of_slot(g, s, i, j, k, node)) return;
-  m16[((long long)j * g.nx + i) * mpz + k] = mask[s];
+  uint8_t f = 0;
+  for (int b = 0; b < 8; ++b) {
+    const int ii = i + (b & 1), jj = j + ((b >> 1) & 1), kk = k + ((b >> 2) & 1);
+    if (ii < g.nx && jj < g.ny && kk < g.nz) f |= mask[g.slot3(ii, jj, kk)];
+  }
+  f16[((long long)j * g.nx + i) * mpz + k] = f ? 1 : 0;
 }
 
 // Element arrays: user order e = i*nely*nelz + j*nelz + k (3-D), i*nely + j (2-D)

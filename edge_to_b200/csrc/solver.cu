@@ -200,7 +200,7 @@ struct Prob {
   double* dK0diag = nullptr;
   double* dQ = nullptr;
   uint8_t* mask = nullptr;
-  uint8_t* mask16 = nullptr;  // same bits, rows padded to 16 bytes (TMA source)
+  uint8_t* eflag16 = nullptr;  // element flags with rows padded to 16 bytes (TMA source)
   int mpz = 0;
   uint8_t* eflag = nullptr;
   int* err = nullptr;          // set by kernels whose bounded waits expired
@@ -246,6 +246,12 @@ struct Prob {
   std::vector<cudaEvent_t> pev;
   std::vector<double> pbytes;
   size_t pev_used = 0;
+  // per-category time breakdown of every launch (benchmark instrumentation)
+  bool bd = false;
+  int cur_cat = 0;
+  std::vector<cudaEvent_t> bev;
+  std::vector<int> bcat;
+  size_t bev_used = 0;
 
   template <typename T> T* alloc(size_t n) {
     void* ptr = nullptr;
@@ -261,6 +267,7 @@ struct Prob {
     if (scal_h) cudaFreeHost(scal_h);
     for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
     for (auto e : pev) cudaEventDestroy(e);
+    for (auto e : bev) cudaEventDestroy(e);
   }
 };
 
@@ -269,10 +276,27 @@ struct Prob {
 // launch tally and checked immediately.
 template <typename... KArgs, typename... Args>
 static void launch(Prob& P, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
+  const bool rec = P.bd && P.bev_used + 2 <= P.bev.size();
+  if (rec) CK(cudaEventRecord(P.bev[P.bev_used], P.stream));
   kern<<<grid, block, smem, P.stream>>>(static_cast<KArgs>(args)...);
   ++P.nlaunch;
   KCHECK();
+  if (rec) {
+    CK(cudaEventRecord(P.bev[P.bev_used + 1], P.stream));
+    P.bev_used += 2;
+    P.bcat.push_back(P.cur_cat);
+  }
 }
+
+// Launch categories of the breakdown instrumentation.
+enum { CAT_OTHER = 0, CAT_FINE, CAT_STENCIL, CAT_TRANSFER, CAT_VECTOR, CAT_SETUP, CAT_COARSE, CAT_OC, CAT_SENS,
+       CAT_COUNT };
+struct CatScope {
+  Prob& P;
+  int old;
+  CatScope(Prob& p, int c) : P(p), old(p.cur_cat) { P.cur_cat = c; }
+  ~CatScope() { P.cur_cat = old; }
+};
 
 static Geo level_geo(const Prob& P, int l) {
   int ne[3] = {P.nel[0], P.nel[1], P.nel[2]};
@@ -321,27 +345,27 @@ static const CUtensorMap& fine_map(Prob& P, const T* base, int kind) {
   if (kind == 0) {
     uint64_t dims[4] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny, 3};
     uint64_t str[3] = {g.pz * sz, g.plane * sz, g.n * sz};
-    uint32_t box[4] = {TMA_ZB, BX + 1, 1, 3};
+    uint32_t box[4] = {TMA_ZB, 2 * BX + 1, 1, 3};
     m = encode_map(base, tma_dt<T>(), 4, dims, str, box);
   } else {
     uint64_t dims[3] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny};
     uint64_t str[2] = {g.pz * sz, g.plane * sz};
-    uint32_t box[3] = {TMA_ZB, BX, 1};
+    uint32_t box[3] = {TMA_ZB, 2 * BX, 1};
     m = encode_map(base, tma_dt<T>(), 3, dims, str, box);
   }
   return P.tmaps.emplace(key, m).first->second;
 }
 
 template <int BX>
-static const CUtensorMap& mask_map(Prob& P) {
-  auto key = std::make_pair((const void*)P.mask16, 1000 + BX);
+static const CUtensorMap& flag_map(Prob& P) {
+  auto key = std::make_pair((const void*)P.eflag16, 1000 + BX);
   auto it = P.tmaps.find(key);
   if (it != P.tmaps.end()) return it->second;
   const Geo& g = P.g0;
   uint64_t dims[3] = {(uint64_t)P.mpz, (uint64_t)g.nx, (uint64_t)g.ny};
   uint64_t str[2] = {(uint64_t)P.mpz, (uint64_t)P.mpz * g.nx};
-  uint32_t box[3] = {TMA_ZB, BX + 1, 1};
-  return P.tmaps.emplace(key, encode_map(P.mask16, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims, str, box)).first->second;
+  uint32_t box[3] = {TMA_ZB, 2 * BX, 1};
+  return P.tmaps.emplace(key, encode_map(P.eflag16, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims, str, box)).first->second;
 }
 
 static size_t vbytes(int prec) { return prec == EDGE_FP64 ? sizeof(double) : sizeof(float); }
@@ -352,6 +376,14 @@ static const int FINE2_NW = 4;
 
 static dim3 fine3_grid(const Geo& g, int& ly) {
   const unsigned tz = cdiv(g.nz, 31), tx = cdiv(g.nx, FINE_BX - 1);
+  const long long want = 148LL * 4;
+  long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
+  chunks = std::min<long long>(chunks, g.ny);
+  ly = (int)cdiv(g.ny, chunks);
+  return dim3(tz, tx, cdiv(g.ny, ly));
+}
+static dim3 fine3_grid_v3(const Geo& g, int bx, int& ly) {
+  const unsigned tz = cdiv(g.nz, 15), tx = cdiv(g.nx, 2 * bx - 1);
   const long long want = 148LL * 4;
   long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
   chunks = std::min<long long>(chunks, g.ny);
@@ -382,6 +414,7 @@ template <> struct TypeOps<float> {
 // input vector + E + the epilogue's per-DOF traffic (BC mask excluded).
 template <typename T, class Epi>
 static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
+  CatScope cat(P, CAT_FINE);
   const Geo& g = P.g0;
   const T* E = TypeOps<T>::E(P);
   const bool rec = P.prof && P.pev_used + 2 <= P.pev.size();
@@ -396,9 +429,9 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
         attr = true;
       }
       int ly;
-      dim3 grid = fine3_grid(g, ly);
+      dim3 grid = fine3_grid_v3(g, FINE_BX, ly);
       launch(P, k_fine3_tma<T, Epi, FINE_BX, NS>, grid, dim3(32, FINE_BX), smem, g, fine_map<T, FINE_BX>(P, u, 0),
-             mask_map<FINE_BX>(P), fine_map<T, FINE_BX>(P, E, 1), u, (const uint8_t*)P.mask, cast3<T>(P.ei.k3), ly,
+             flag_map<FINE_BX>(P), fine_map<T, FINE_BX>(P, E, 1), u, (const uint8_t*)P.mask, cast3<T>(P.ei.k3), ly,
              epi, P.part, P.ticket, dot_dst, P.err);
     } else if (P.dim == 3) {
       int ly;
@@ -442,6 +475,7 @@ static void fine_apply_dense(Prob& P, const T* u, Epi epi, double* dot_dst) {
 
 template <typename T, class Epi>
 static void st_apply(Prob& P, const Geo& g, const T* u, const T* S, Epi epi, double* dot_dst) {
+  CatScope cat(P, CAT_STENCIL);
   if (g.dim == 3)
     launch(P, k_st3_apply<T, T, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
   else
@@ -501,6 +535,7 @@ __global__ void k_pcg_check_bb(PcgState* st) {
 // ------------------------------------------------------------------ multigrid setup
 template <typename T, typename TD0>
 static void mg_setup(Prob& P) {
+  CatScope cat(P, CAT_SETUP);
   const int L = P.n_level;
   const Geo& g0 = P.g0;
   const T* E = TypeOps<T>::E(P);
@@ -568,6 +603,7 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
   const Geo& g = Lv.g;
   const long long nv = (long long)g.dof * g.n;
   if (l == P.n_level) {
+    CatScope cat(P, CAT_COARSE);
     launch(P, k_coarse_solve<T, T>, cdiv((long long)P.nd * 32, 256), 256, 0, g, P.Ainv, P.nd, b, out);
     KCHECK();
     return;
@@ -610,19 +646,23 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     }
     const T* xcur = first ? x : out;
     Level& Lc = P.lv[l + 1];
+    P.cur_cat = CAT_TRANSFER;
     if (P.dim == 3)
       launch(P, k_restrict3<T, T>, dim3(cdiv(Lc.g.nz, 64), Lc.g.nx, Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
     else
       launch(P, k_restrict2<T, T>, dim3(cdiv(Lc.g.nx, 64), Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
     KCHECK();
+    P.cur_cat = CAT_VECTOR;
     vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr);
     T* e1 = (T*)Lv.ea;
     T* e2 = (T*)Lv.eb;
+    P.cur_cat = CAT_TRANSFER;
     if (P.dim == 3)
       launch(P, k_prolong3<T, T>, dim3(cdiv(g.nz, 64), g.nx, g.ny), 64, 0, g, Lc.g, (const T*)Lc.res, e1);
     else
       launch(P, k_prolong2<T, T>, dim3(cdiv(g.nx, 64), g.ny), 64, 0, g, Lc.g, (const T*)Lc.res, e1);
     KCHECK();
+    P.cur_cat = CAT_VECTOR;
     const bool last_visit = (vis == visits - 1);
     if (P.n_smooth >= 1) {
       for (int s = 0; s < P.n_smooth - 1; ++s) {
@@ -695,6 +735,7 @@ static void mg_allocate(Prob& P) {
 // ------------------------------------------------------------------ PCG
 template <typename T, typename TD0>
 static void pcg_fp64(Prob& P, double tol, int maxiter) {
+  CatScope cat(P, CAT_VECTOR);
   // b64, x64 are set; T == double
   const Geo& g = P.g0;
   const long long nv = (long long)g.dof * g.n;
@@ -744,6 +785,7 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
 static const double REPLACE_DROP = 1e-2;
 
 static void pcg_mixed(Prob& P, double tol, int maxiter) {
+  CatScope cat(P, CAT_VECTOR);
   const Geo& g = P.g0;
   const long long nv = (long long)g.dof * g.n;
   double* r = P.r64;
@@ -901,7 +943,7 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     P.mask = P.alloc<uint8_t>(g.n);
     if (dim == 3) {
       P.mpz = (g.nz + 15) & ~15;
-      P.mask16 = P.alloc<uint8_t>((size_t)g.ny * g.nx * P.mpz);
+      P.eflag16 = P.alloc<uint8_t>((size_t)g.ny * g.nx * P.mpz);
     }
     P.eflag = P.alloc<uint8_t>(g.n);
     P.err = P.alloc<int>(1);
@@ -967,7 +1009,8 @@ int edge_set_constraints(edge_problem* p, const uint8_t* cons_dev) {
   if (!p || !cons_dev) fail(EDGE_EINVAL, "null argument");
   Prob& P = p->P;
   launch(P, k_mask_from_user, cdiv(P.g0.n, 256), 256, 0, P.g0, cons_dev, P.mask);
-  if (P.mask16) launch(P, k_mask_pitch16, cdiv(P.g0.n, 256), 256, 0, P.g0, (const uint8_t*)P.mask, P.mask16, P.mpz);
+  if (P.eflag16)
+    launch(P, k_flag_pitch16, cdiv(P.g0.n, 256), 256, 0, P.g0, (const uint8_t*)P.mask, P.eflag16, P.mpz);
   launch(P, k_elem_flags, cdiv(P.g0.n, 256), 256, 0, P.g0, P.mask, P.eflag);
   KCHECK();
   P.has_cons = true;
@@ -1191,6 +1234,43 @@ int edge_mg_level_dense(edge_problem* p, int level, double* out_dev, long long n
   API_END
 }
 
+int edge_breakdown_begin(edge_problem* p, int max_launches) {
+  API_BEGIN
+  if (!p || max_launches < 1) fail(EDGE_EINVAL, "bad argument");
+  Prob& P = p->P;
+  while ((int)P.bev.size() < 2 * max_launches) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    P.bev.push_back(e);
+  }
+  P.bev_used = 0;
+  P.bcat.clear();
+  P.bd = true;
+  API_END
+}
+
+int edge_breakdown_end(edge_problem* p, double* ms_by_cat, int* n_by_cat, int n_cat) {
+  API_BEGIN
+  if (!p || !ms_by_cat || !n_by_cat) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  CK(cudaStreamSynchronize(P.stream));
+  for (int c = 0; c < n_cat; ++c) {
+    ms_by_cat[c] = 0.0;
+    n_by_cat[c] = 0;
+  }
+  for (size_t i = 0; i + 1 < P.bev_used; i += 2) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, P.bev[i], P.bev[i + 1]));
+    const int c = P.bcat[i / 2];
+    if (c < n_cat) {
+      ms_by_cat[c] += t;
+      n_by_cat[c] += 1;
+    }
+  }
+  P.bd = false;
+  API_END
+}
+
 int edge_last_solve_stats(const edge_problem* p, double* setup_ms, double* solve_ms, int* pcg_iters,
                           int* true_residuals) {
   API_BEGIN
@@ -1299,6 +1379,7 @@ int edge_filter_apply_T(edge_filter* f, const double* in_dev, double* out_dev, v
 
 static void oc_run(Prob& P, long long n, const double* rho, const double* dr, double A, double vol, double vf,
                    double move, double* rho_new) {
+  CatScope cat(P, CAT_OC);
   if (n != P.n_el) fail(EDGE_EINVAL, "OC vector length does not match the number of elements");
   const unsigned nb = std::min<unsigned>(ew_blocks(n), 1024);
   launch(P, k_oc_prep, nb, 256, 0, n, rho, dr, A, P.ocp, P.part, P.ticket, P.scal);
@@ -1348,6 +1429,7 @@ int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* r
   API_BEGIN
   if (!p || !f || !rho_dev || !f_dev || !U_dev || !dr_dev) fail(EDGE_EINVAL, "null argument");
   Prob& P = p->P;
+  CatScope cat(P, CAT_SENS);
   const Geo& g = P.g0;
   if (f->n_el != P.n_el) fail(EDGE_EINVAL, "filter and mesh sizes differ");
   double* rf = rho_f_dev ? rho_f_dev : P.rho_f;

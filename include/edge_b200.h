@@ -112,6 +112,11 @@ int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* r
 int edge_profile_begin(edge_problem* p, int max_launches);
 int edge_profile_end(edge_problem* p, double* kernel_ms, double* kernel_bytes, int* kernel_launches,
                      long long* total_launches);
+/* Per-category device time of every library launch between begin and end (categories:
+ * 0 other, 1 fine operator, 2 coarse stencils, 3 transfers, 4 vector/PCG, 5 hierarchy
+ * setup, 6 coarsest solve, 7 OC update, 8 filter/sensitivities). */
+int edge_breakdown_begin(edge_problem* p, int max_launches);
+int edge_breakdown_end(edge_problem* p, double* ms_by_cat, int* n_by_cat, int n_cat);
 /* Kernel timing of the last edge_mg_solve (ms), for the benchmarks. */
 int edge_last_solve_stats(const edge_problem* p, double* setup_ms, double* solve_ms, int* pcg_iters,
                           int* true_residuals);
