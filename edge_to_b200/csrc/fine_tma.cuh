@@ -246,7 +246,9 @@ k_fine3_tma(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_
     const uint8_t fl = flag_of(k);   // element row ey: covers this layer's 8 corners
     const T Ee = reinterpret_cast<const T*>(smem + (k % NS) * Tile::STAGE + Tile::E_OFF)[eoff];
     T hi[2][2][3];
-    load_plane(k + 1, ey + 1, fl, hi);
+    // the new plane is also the lower face of element row ey+1, which reuses these values:
+    // mask by both rows' flags (row ey may be the ghost row below the grid, flagged 0)
+    load_plane(k + 1, ey + 1, fl | flag_of(k + 1), hi);
     T own_hi[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) own_hi[c] = hi[0][0][c];
