@@ -242,7 +242,8 @@ def run_ours(args, cfg_name):
                    "n_level": cfg["n_level"], "rtol": cfg["tol"], "precision": args.precision,
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "l2": "working set > 126 MB L2 (no flush needed)",
-                   "pcg_iters_per_step": pcg, "compliance_last": comp_last},
+                   "pcg_iters_per_step": pcg, "compliance_last": comp_last,
+                   "fine_tile": opt.solver.tuned},
         "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_wht + fused epilogues)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,

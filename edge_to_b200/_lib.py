@@ -33,6 +33,8 @@ _SIGS = {
     "edge_process_grad": (ctypes.c_int, [vp, vp, vp]),
     "edge_uses_transform": (ctypes.c_int, [vp]),
     "edge_set_tma": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_set_fine_tile": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    "edge_autotune_fine": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_double_p, c_int_p, c_int_p]),
     "edge_mg_config": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                       c_int_p, ctypes.c_int, ctypes.c_int]),
     "edge_mg_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_double_p, c_int_p]),

@@ -205,6 +205,8 @@ struct Prob {
   uint8_t* eflag = nullptr;
   int* err = nullptr;          // set by kernels whose bounded waits expired
   bool use_tma = true;
+  int tile_variant = 0;    // (BX, NS): 0 (8,4) 1 (8,3) 2 (8,2) 3 (4,4) 4 (4,3)
+  int blocks_per_sm = 4;   // y-chunking target of the fine kernel
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
   double* E64 = nullptr;
   float* E32 = nullptr;
@@ -409,6 +411,27 @@ template <> struct TypeOps<float> {
   static const float* K0b(const Prob& P) { return P.dK0bf; }
 };
 
+// One launch of the TMA fine kernel with BX warps and NS stages per block; the number of
+// y-chunks follows P.blocks_per_sm (the grid aims at that many resident blocks per SM).
+template <typename T, class Epi, int BX, int NS>
+static void fine3_tma_launch(Prob& P, const T* u, const T* E, Epi epi, double* dot_dst) {
+  const Geo& g = P.g0;
+  constexpr int smem = tma_smem_bytes<T, BX, NS>();
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(k_fine3_tma<T, Epi, BX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  const unsigned tz = cdiv(g.nz, 15), tx = cdiv(g.nx, 2 * BX - 1);
+  const long long want = 148LL * P.blocks_per_sm;
+  long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
+  chunks = std::min<long long>(chunks, g.ny);
+  const int ly = (int)cdiv(g.ny, chunks);
+  launch(P, k_fine3_tma<T, Epi, BX, NS>, dim3(tz, tx, cdiv(g.ny, ly)), dim3(32, BX), smem, g,
+         fine_map<T, BX>(P, u, 0), flag_map<BX>(P), fine_map<T, BX>(P, E, 1), u, (const uint8_t*)P.mask,
+         cast3<T>(P.ei.k3), ly, epi, P.part, P.ticket, dot_dst, P.err);
+}
+
 // Fine-level operator with epilogue.  u, E in type T.  When profiling is on, each launch is
 // bracketed by CUDA events on the problem's stream and its algorithmic bytes recorded:
 // input vector + E + the epilogue's per-DOF traffic (BC mask excluded).
@@ -421,18 +444,13 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
   if (rec) CK(cudaEventRecord(P.pev[P.pev_used], P.stream));
   if (P.ei.wht) {
     if (P.dim == 3 && P.use_tma) {
-      constexpr int NS = 4;
-      constexpr int smem = tma_smem_bytes<T, FINE_BX, NS>();
-      static bool attr = false;
-      if (!attr) {
-        CK(cudaFuncSetAttribute(k_fine3_tma<T, Epi, FINE_BX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr = true;
+      switch (P.tile_variant) {
+        case 0: fine3_tma_launch<T, Epi, 8, 4>(P, u, E, epi, dot_dst); break;
+        case 1: fine3_tma_launch<T, Epi, 8, 3>(P, u, E, epi, dot_dst); break;
+        case 2: fine3_tma_launch<T, Epi, 8, 2>(P, u, E, epi, dot_dst); break;
+        case 3: fine3_tma_launch<T, Epi, 4, 4>(P, u, E, epi, dot_dst); break;
+        default: fine3_tma_launch<T, Epi, 4, 3>(P, u, E, epi, dot_dst); break;
       }
-      int ly;
-      dim3 grid = fine3_grid_v3(g, FINE_BX, ly);
-      launch(P, k_fine3_tma<T, Epi, FINE_BX, NS>, grid, dim3(32, FINE_BX), smem, g, fine_map<T, FINE_BX>(P, u, 0),
-             flag_map<FINE_BX>(P), fine_map<T, FINE_BX>(P, E, 1), u, (const uint8_t*)P.mask, cast3<T>(P.ei.k3), ly,
-             epi, P.part, P.ticket, dot_dst, P.err);
     } else if (P.dim == 3) {
       int ly;
       dim3 grid = fine3_grid(g, ly);
@@ -996,6 +1014,72 @@ int edge_set_stream(edge_problem* p, void* stream) {
 }
 
 int edge_uses_transform(const edge_problem* p) { return p && p->P.ei.wht ? 1 : 0; }
+
+int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm) {
+  API_BEGIN
+  if (!p || variant < 0 || variant > 4 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
+  p->P.tile_variant = variant;
+  p->P.blocks_per_sm = blocks_per_sm;
+  API_END
+}
+
+// Autotuner: times every (tile variant, y-chunking) of the fine operator on the current E
+// with the product epilogue in the given precision and keeps the fastest.  Needs E set.
+int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms, int* best_variant,
+                       int* best_bps) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  Prob& P = p->P;
+  if (!P.has_rho) fail(EDGE_ESTATE, "rho not set");
+  if (P.dim != 3 || !P.ei.wht || !P.use_tma) {
+    if (best_ms) *best_ms = 0;
+    if (best_variant) *best_variant = P.tile_variant;
+    if (best_bps) *best_bps = P.blocks_per_sm;
+    return EDGE_OK;
+  }
+  const Geo& g = P.g0;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  double best = 1e30;
+  int bv = P.tile_variant, bb = P.blocks_per_sm;
+  const int bps_list[4] = {2, 4, 8, 16};
+  for (int v = 0; v < 5; ++v)
+    for (int bi = 0; bi < 4; ++bi) {
+      P.tile_variant = v;
+      P.blocks_per_sm = bps_list[bi];
+      auto run = [&]() {
+        if (precision == EDGE_FP64) {
+          EpiStore<double, double> e{P.r64, g.n};
+          fine_apply<double>(P, P.x64, e, nullptr);
+        } else {
+          EpiStore<float, float> e{(float*)P.q, g.n};
+          fine_apply<float>(P, (const float*)P.p, e, nullptr);
+        }
+      };
+      run();
+      CK(cudaEventRecord(a, P.stream));
+      for (int r = 0; r < reps; ++r) run();
+      CK(cudaEventRecord(b, P.stream));
+      CK(cudaEventSynchronize(b));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, a, b));
+      if (ms / reps < best) {
+        best = ms / reps;
+        bv = v;
+        bb = bps_list[bi];
+      }
+    }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  check_err(P);
+  P.tile_variant = bv;
+  P.blocks_per_sm = bb;
+  if (best_ms) *best_ms = best;
+  if (best_variant) *best_variant = bv;
+  if (best_bps) *best_bps = bb;
+  API_END
+}
 
 int edge_set_tma(edge_problem* p, int enable) {
   API_BEGIN

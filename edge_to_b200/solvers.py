@@ -30,7 +30,7 @@ class Solver:
 class CuMultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="splu", matrix_free=False, low_level_tol=1e-8, low_level_maxiter=5000,
-                 min_omega=0.4, omega_boost=1.06, precision="fp64"):
+                 min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True):
         if not isinstance(kernel, CuStructuredStiffnessKernel):
             raise TypeError("CuMultiGrid needs the package's CuStructuredStiffnessKernel")
         self.kernel = kernel
@@ -63,6 +63,8 @@ class CuMultiGrid(Solver):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.last_iters = 0
         self._configured = None
+        self.autotune = autotune
+        self.tuned = None
 
     def reset(self):
         self.last_x0 = None
@@ -78,12 +80,26 @@ class CuMultiGrid(Solver):
                   float(self.min_omega), 1 if self.cycle == "w" else 0, w, len(self.w_level), prec)
         self._configured = key
 
+    def tune(self):
+        """Pick the fine-operator tile (warps, TMA stages, y-chunking) by timing each on the
+        current density (the project's autotuner); runs once, on the first solve."""
+        if self.tuned is not None or not self.autotune or not self.kernel.has_rho:
+            return self.tuned
+        ms, v, b = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        prec = _lib.EDGE_FP64 if self.precision == "fp64" else _lib.EDGE_MIXED
+        self.kernel._bind_stream()
+        _lib.call("edge_autotune_fine", self.kernel.handle, prec, 5, ctypes.byref(ms), ctypes.byref(v),
+                  ctypes.byref(b))
+        self.tuned = {"variant": v.value, "blocks_per_sm": b.value, "ms": ms.value}
+        return self.tuned
+
     def solve(self, rhs, rho=None, use_last=True):
         if not (self.kernel.has_rho or rho is not None):
             raise ValueError("Solver requires a density vector to be passed or set on the kernel.")
         if rho is not None:
             self.kernel.set_rho(rho)
         self._configure()
+        self.tune()
         f = _as_dev_f64(rhs)
         if use_last and self.last_x0 is not None:
             x = self.last_x0

@@ -59,6 +59,13 @@ int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
 /* Tuning/testing switch: 1 (default) stages 3-D fine-level tiles with TMA, 0 uses the
  * cooperative-load version of the same kernel. */
 int edge_set_tma(edge_problem* p, int enable);
+/* Fine-kernel tile: variant 0..4 = (warps, TMA stages) (8,4) (8,3) (8,2) (4,4) (4,3), and
+ * the target of resident blocks per SM that sets the y-chunking of the grid. */
+int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm);
+/* Autotuner: times every tile variant and y-chunking on the current density with the plain
+ * operator in `precision` (reps launches each), keeps the fastest, reports it. */
+int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms, int* best_variant,
+                       int* best_bps);
 /* 1 when the element matrix has the box structure used by the transform kernels */
 int edge_uses_transform(const edge_problem* p);
 
