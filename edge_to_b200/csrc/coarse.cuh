@@ -97,7 +97,7 @@ k_st3_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi 
     Au[0] = c00 * u0 + c01 * u1 + c02 * u2;
     Au[1] = c01 * u0 + c11 * u1 + c12 * u2;
     Au[2] = c02 * u0 + c12 * u1 + c22 * u2;
-#pragma unroll 1
+#pragma unroll
     for (int nb = 14; nb < 27; ++nb) {
       const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
       const long long off = (long long)dy * g.plane + (long long)dx * g.pz + dz;
