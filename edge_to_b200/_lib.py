@@ -48,6 +48,9 @@ _SIGS = {
     "edge_filter_apply_T": (ctypes.c_int, [vp, vp, vp, vp]),
     "edge_oc_update": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                       vp, c_double_p, c_int_p, c_double_p]),
+    "edge_oc_update_static": (ctypes.c_int, [ctypes.c_longlong, vp, vp, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, vp, c_double_p, c_int_p, c_double_p,
+                                             vp]),
     "edge_simp_solve_and_process": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, vp, ctypes.c_int,
                                                    ctypes.c_double, ctypes.c_int, c_double_p, vp, vp, c_double_p,
                                                    c_int_p]),

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -911,6 +912,54 @@ struct edge_filter {
   }
 };
 
+// ------------------------------------------------------------------ OC update without a workspace
+// edge_oc_update_static runs the OC kernels of edge_oc_update on a fixed workspace that is a
+// file-scope device array, so the call allocates nothing.  One workspace per device: calls
+// whose work overlaps on one device (two streams, two host threads) race on it.
+constexpr long long OC_STATIC_MAX_EL = 1LL << 20;   // elements; the ocP cache is 8 MiB
+constexpr unsigned OC_STATIC_MAX_BLOCKS = 1024;     // reduction partials, as edge_oc_update
+struct OcStaticScratch {
+  OcState st;                                  // bisection state, rewritten by k_oc_static_init
+  double scal[2];                              // sum(ocP_raw), sum((rho_new - rho)^2)
+  unsigned ticket;                             // grid-reduction counter: zero when a kernel starts
+  double part[OC_STATIC_MAX_BLOCKS * OC_NODES];
+  double ocp[OC_STATIC_MAX_EL];
+};
+static __device__ __align__(256) OcStaticScratch g_oc_scratch;
+
+// Device address of g_oc_scratch for the current device, looked up once per device (the
+// lookup is the only set-up; the first call on a device performs it).
+static OcStaticScratch* oc_static_scratch() {
+  static std::mutex mu;
+  static OcStaticScratch* addr[128] = {};
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) fail(EDGE_EINVAL, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_oc_scratch);
+    if (e != cudaSuccess || !ptr)
+      fail(EDGE_ECUDA, std::string("cudaGetSymbolAddress(OC workspace): ") + cudaGetErrorString(e));
+    addr[dev] = static_cast<OcStaticScratch*>(ptr);
+  }
+  return addr[dev];
+}
+
+// Start state of one OC update: bracket [1e-9, 1e9] (TopOpt/_cuda.py:260-261), counter zero.
+__global__ void k_oc_static_init(OcStaticScratch* s, double vf, double vol) {
+  OcState init{};
+  init.l1 = 1e-9;
+  init.l2 = 1e9;
+  init.last = 0.5 * (init.l1 + init.l2);
+  init.vf = vf;
+  init.vol = vol;
+  s->st = init;
+  s->scal[0] = 0.0;
+  s->scal[1] = 0.0;
+  s->ticket = 0u;
+}
+
 #define API_BEGIN try {
 #define API_END                 \
   }                             \
@@ -1503,6 +1552,45 @@ int edge_oc_update(edge_problem* p, const double* rho_dev, const double* dr_dev,
   if (lambda_out) *lambda_out = P.oc_h->last;
   if (steps_out) *steps_out = P.oc_h->steps;
   if (sqchange_out) *sqchange_out = P.scal_h[1];
+  API_END
+}
+
+int edge_oc_update_static(long long n, const double* rho_dev, const double* dr_dev, double A, double vol, double vf,
+                          double move, double* rho_new_dev, double* lambda_out, int* steps_out, double* sqchange_out,
+                          void* stream) {
+  API_BEGIN
+  if (!rho_dev || !dr_dev || !rho_new_dev) fail(EDGE_EINVAL, "null argument");
+  if (n <= 0) fail(EDGE_EINVAL, "n must be positive");
+  if (n > OC_STATIC_MAX_EL)
+    fail(EDGE_EINVAL, "n = " + std::to_string(n) + " elements exceeds the fixed OC workspace (at most " +
+                          std::to_string(OC_STATIC_MAX_EL) + " elements); use edge_oc_update");
+  OcStaticScratch* s = oc_static_scratch();
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned nb = std::min<unsigned>(ew_blocks(n), OC_STATIC_MAX_BLOCKS);
+  k_oc_static_init<<<1, 1, 0, st>>>(s, vf, vol);
+  k_oc_prep<<<nb, 256, 0, st>>>(n, rho_dev, dr_dev, A, s->ocp, s->part, &s->ticket, &s->scal[0]);
+  k_oc_floor<<<nb, 256, 0, st>>>(n, s->ocp, &s->scal[0]);
+  KCHECK();
+  OcState h{};
+  const int max_pass = (200 + OC_DEPTH - 1) / OC_DEPTH;
+  for (int pass = 0; pass < max_pass; ++pass) {
+    k_oc_pass<<<nb, 256, 0, st>>>(n, rho_dev, s->ocp, A, move, &s->st, s->part, &s->ticket);
+    if ((pass & 3) == 3) {
+      KCHECK();
+      CK(cudaMemcpyAsync(&h, &s->st, sizeof(OcState), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (h.done) break;
+    }
+  }
+  k_oc_final<<<nb, 256, 0, st>>>(n, rho_dev, s->ocp, move, &s->st, rho_new_dev, s->part, &s->ticket, &s->scal[1]);
+  KCHECK();
+  double chg = 0.0;
+  CK(cudaMemcpyAsync(&h, &s->st, sizeof(OcState), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&chg, &s->scal[1], sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (lambda_out) *lambda_out = h.last;
+  if (steps_out) *steps_out = h.steps;
+  if (sqchange_out) *sqchange_out = chg;
   API_END
 }
 

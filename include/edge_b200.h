@@ -104,6 +104,23 @@ int edge_filter_apply_T(edge_filter* f, const double* in_dev, double* out_dev, v
 int edge_oc_update(edge_problem* p, const double* rho_dev, const double* dr_dev, double A, double vol, double vf,
                    double move, double* rho_new_dev, double* lambda_out, int* steps_out, double* sqchange_out);
 
+/* The same OC update for callers that must not allocate device memory, and need no
+ * problem handle: for example an optimiser whose sensitivities come from another solver,
+ * running where every byte of device memory belongs to another allocator's pool, or where
+ * creating an edge_problem (which allocates the multigrid workspaces) is not wanted.
+ * No counterpart in the reference.  n elements of uniform measure A, on `stream`.
+ * It allocates nothing: its workspace is a fixed 8.1 MiB device array inside the library,
+ * so n is limited to 1,048,576 elements (larger n: EDGE_EINVAL; use edge_oc_update).  The
+ * first call on a device looks up that array's address; make that first call before any
+ * stream capture.  The call zeroes the workspace's reduction counter itself; nothing has to
+ * be initialised by the caller.  There is one workspace per device: calls whose work
+ * overlaps on the same device (different streams or host threads) race and give wrong
+ * results, so order them on one stream or synchronise between them.  Results equal
+ * edge_oc_update's for the same inputs. */
+int edge_oc_update_static(long long n, const double* rho_dev, const double* dr_dev, double A, double vol, double vf,
+                          double move, double* rho_new_dev, double* lambda_out, int* steps_out,
+                          double* sqchange_out, void* stream);
+
 /* ---- one SIMP analysis, fused.  Replaces TopOpt.solve_and_process (TopOpt/_cuda.py:282-302)
  * for SingleMaterial: rho_f = H rho, E = clip(rho_f^p, void, 1), solve, c = f.U,
  * dr = H^T (p clip(rho_f, void, 1)^(p-1) dk). */
