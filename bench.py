@@ -33,10 +33,10 @@ CONFIGS = {
     "cantilever_128x64x64": dict(nel=(128, 64, 64), vf=0.1, rmin=2.0, n_level=4, tol=1e-6),
     "cantilever_64x32x32": dict(nel=(64, 32, 32), vf=0.12, rmin=1.5, n_level=4, tol=1e-6),
 }
-# Mean PCG iterations per SIMP solve of the FP64 path on cantilever_256x128x128 (measured
-# by this benchmark on a B200, see profiles/); the CPU arms use it to turn a timed matvec
-# into SIMP iterations/s, since both run the same FP64 algorithm.
-PCG_ITERS_FP64_CFG5 = 40.0
+# Mean PCG iterations per SIMP solve of the FP64 path on cantilever_256x128x128 (this
+# benchmark on a B200: 139, 135 and 172 in the first timed steps); the CPU arms use it to
+# turn a timed matvec into SIMP iterations/s, since both run the same FP64 algorithm.
+PCG_ITERS_FP64_CFG5 = 149.0
 
 
 def dist_env():
@@ -60,8 +60,8 @@ def traffic_from_profile(config):
     if not os.path.exists(p):
         return None
     try:
-        d = json.load(open(p))
-        return d.get(config)
+        d = json.load(open(p)).get(config)
+        return None if d is None else d.get("dram_bytes_per_launch")
     except Exception:
         return None
 
@@ -135,10 +135,75 @@ def build_problem(cfg, precision):
     return opt, rho
 
 
+def timed_steps(opt, rho, dr, it, steps, ws, local, profile=True):
+    """`steps` SIMP iterations between barriers + synchronisation, CUDA events on the
+    library's stream (torch's current stream); returns the max-over-ranks time."""
+    import ctypes
+    import torch
+    from edge_to_b200 import _lib
+    stream = torch.cuda.current_stream()
+    h = opt.kernel.handle
+    pcg = []
+    clocks = ClockSampler(local)
+    _barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    if profile:
+        _lib.call("edge_profile_begin", h, 200000)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    torch.cuda.nvtx.range_push("edge_timed")      # lets ncu --nvtx-include select the timed launches
+    c = None
+    for _ in range(steps):
+        rho = opt.update_design(rho, dr)
+        c, dr, res = opt.solve_and_process(rho, it)
+        pcg.append(opt.last_stats.get("pcg_iters", 0))
+        it += 1
+    torch.cuda.nvtx.range_pop()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    _barrier(ws)
+    prof = None
+    if profile:
+        kms, kby, kl, tl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int(), ctypes.c_longlong()
+        _lib.call("edge_profile_end", h, ctypes.byref(kms), ctypes.byref(kby), ctypes.byref(kl), ctypes.byref(tl))
+        prof = dict(kernel_ms=kms.value, kernel_bytes=kby.value, kernel_launches=kl.value, launches=int(tl.value))
+    clk = clocks.stop()
+    t_ms = _max_over_ranks(e0.elapsed_time(e1), ws)
+    return dict(rho=rho, dr=dr, it=it, t_ms=t_ms, pcg=pcg, compliance=float(c), prof=prof, clocks=clk)
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([v], device="cuda")
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def warm(opt, rho, warmup):
+    """Initial analysis + `warmup` untimed SIMP iterations."""
+    c, dr, res = opt.solve_and_process(rho, 0)
+    it = 0
+    for _ in range(warmup):
+        rho = opt.update_design(rho, dr)
+        c, dr, res = opt.solve_and_process(rho, it)
+        it += 1
+    return rho, dr, it
+
+
 def run_ours(args, cfg_name):
     import numpy as np
     import torch
-    from edge_to_b200 import _lib
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     if ws > 1:
@@ -147,57 +212,19 @@ def run_ours(args, cfg_name):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     cfg = CONFIGS[cfg_name]
     opt, rho = build_problem(cfg, args.precision)
-    # initial analysis + warm-up steps (untimed)
-    c, dr, res = opt.solve_and_process(rho, 0)
-    it = 0
-    for _ in range(args.warmup):
-        rho = opt.update_design(rho, dr)
-        c, dr, res = opt.solve_and_process(rho, it)
-        it += 1
-    stream = torch.cuda.current_stream()
-    h = opt.kernel.handle
-    pcg = []
-
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+    rho, dr, it = warm(opt, rho, args.warmup)
 
     # ---------------- device-timed region: inputs resident in HBM
-    clocks = ClockSampler(local)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    _lib.call("edge_profile_begin", h, 200000)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        rho = opt.update_design(rho, dr)
-        c, dr, res = opt.solve_and_process(rho, it)
-        pcg.append(opt.last_stats.get("pcg_iters", 0))
-        it += 1
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    import ctypes
-    kms, kby, kl, tl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int(), ctypes.c_longlong()
-    _lib.call("edge_profile_end", h, ctypes.byref(kms), ctypes.byref(kby), ctypes.byref(kl), ctypes.byref(tl))
-    clk = clocks.stop()
-    t_ms = e0.elapsed_time(e1)
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
-    comp_last = float(c)
+    m = timed_steps(opt, rho, dr, it, args.steps, ws, local)
+    rho, dr, it, t_ms, prof = m["rho"], m["dr"], m["it"], m["t_ms"], m["prof"]
 
     # ---------------- end-to-end: design on the host, copies inside the timed region
+    stream = torch.cuda.current_stream()
     rho_h = torch.empty(rho.numel(), dtype=torch.float64, pin_memory=True)
     rho_h.copy_(rho.cpu())
     out_h = torch.empty_like(rho_h)
     dr_e = dr
-    barrier()
+    _barrier(ws)
     torch.cuda.synchronize()
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
@@ -212,22 +239,36 @@ def run_ours(args, cfg_name):
         it += 1
     s1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = s0.elapsed_time(s1)
+    e2e_ms = _max_over_ranks(s0.elapsed_time(s1), ws)
+    bd = breakdown(opt, rho, dr, it) if args.breakdown else None
+    tuned = opt.solver.tuned
+    del opt, rho, dr, rho_h, out_h
+
+    # ---------------- the plain FP64 path on the same workload, same steps (the metric's
+    # denominator), when the timed path is the mixed-precision one
+    fp64 = None
+    if args.precision == "mixed" and not args.no_fp64_compare:
+        torch.cuda.empty_cache()
+        opt64, rho64 = build_problem(cfg, "fp64")
+        rho64, dr64, it64 = warm(opt64, rho64, args.warmup)
+        f = timed_steps(opt64, rho64, dr64, it64, args.steps, ws, local, profile=False)
+        fp64 = {"value": ws * args.steps / (f["t_ms"] / 1e3), "ms_per_step": f["t_ms"] / args.steps,
+                "pcg_iters_per_step": f["pcg"], "compliance_last": f["compliance"]}
+        del opt64, rho64, dr64
     if ws > 1:
         import torch.distributed as dist
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
         dist.destroy_process_group()
     if rank != 0:
         return None
     n_el = int(np.prod(cfg["nel"]))
     peak, peak_kind = peaks()
-    achieved = (kby.value / (kms.value / 1e3) / 1e9) if kms.value > 0 else None
+    kms, kby = prof["kernel_ms"], prof["kernel_bytes"]
+    achieved = (kby / prof["kernel_launches"]) / (kms / prof["kernel_launches"] / 1e3) / 1e9 if kms > 0 else None
     traffic = traffic_from_profile(cfg_name)
+    value = ws * args.steps / (t_ms / 1e3)
     line = {
         "metric": METRIC,
-        "value": ws * args.steps / (t_ms / 1e3),
+        "value": value,
         "unit": "iter/s",
         "n_gpus": ws,
         "steps": args.steps,
@@ -242,23 +283,30 @@ def run_ours(args, cfg_name):
                    "n_level": cfg["n_level"], "rtol": cfg["tol"], "precision": args.precision,
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "l2": "working set > 126 MB L2 (no flush needed)",
-                   "pcg_iters_per_step": pcg, "compliance_last": comp_last,
-                   "fine_tile": opt.solver.tuned},
-        "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_wht + fused epilogues)",
+                   "pcg_iters_per_step": m["pcg"], "compliance_last": m["compliance"],
+                   "fine_tile": tuned},
+        "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_tma + fused epilogues)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "traffic": traffic, "launches": kl.value, "kernel_ms": kms.value,
-                     "share_of_step": kms.value / t_ms if t_ms else None},
+                     "traffic": traffic, "traffic_case": "ncu DRAM bytes of one plain-product launch"
+                     if traffic else None, "launches": prof["kernel_launches"], "kernel_ms": kms,
+                     "algorithmic_bytes_per_launch": kby / max(1, prof["kernel_launches"]),
+                     "share_of_step": kms / t_ms if t_ms else None},
         "e2e": {"value": args.steps / (e2e_ms / 1e3), "unit": "iter/s", "h2d_bytes_per_step": 8 * n_el,
                 "d2h_bytes_per_step": 8 * n_el + 8},
-        "gpu_launches": int(tl.value),
-        "clocks": clk,
+        "gpu_launches": prof["launches"],
+        "clocks": m["clocks"],
     }
-    if args.breakdown:
-        line["breakdown_ms_per_step"] = breakdown(opt, rho, dr, it)
+    if fp64 is not None:
+        line["fp64_path"] = fp64
+        line["mixed_over_fp64"] = value / fp64["value"]
+        line["compliance_rel_err_vs_fp64"] = abs(m["compliance"] - fp64["compliance_last"]) / abs(
+            fp64["compliance_last"])
+    if bd is not None:
+        line["breakdown_ms_per_step"] = bd
     if ws == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, pcg_iters=float(np.mean(pcg)) if pcg else PCG_ITERS_FP64_CFG5,
-                                            reps=2)
+        line["cpu_baseline"] = cpu_baseline(cfg, pcg_iters=float(np.mean(m["pcg"])) if m["pcg"] else
+                                            PCG_ITERS_FP64_CFG5, reps=2)
     return line
 
 
@@ -370,7 +418,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="skip timing the plain FP64 path beside the mixed-precision one")
     ap.add_argument("--config", default="cantilever_256x128x128", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec"])
