@@ -2,9 +2,12 @@
 
 Drop-in names (EDGETO/__init__.py, TopOpt/__init__.py, solvers/__init__.py,
 kernels/__init__.py, geom/__init__.py): CuStructuredMesh2D/3D, CuStructuredStiffnessKernel,
-CuStructuredFilter2D/3D, CuMultiGrid, CuTopOpt, SingleMaterial, auto_stiffness.
+CuStructuredFilter2D/3D, CuMultiGrid, CuTopOpt, SingleMaterial, auto_stiffness; beyond the
+reference, SIMPObjective (differentiable compliance / mechanism objectives, autograd.py).
 Arrays are torch CUDA tensors; the compute runs in libedge_b200.so (sm_100a).
 """
+from . import autograd
+from .autograd import SIMPObjective
 from .filters import CuStructuredFilter2D, CuStructuredFilter3D, FilterKernel
 from .kernels import CuStructuredStiffnessKernel, StiffnessKernel
 from .material import MaterialModel, SingleMaterial
@@ -17,4 +20,5 @@ __all__ = [
     "CuStructuredMesh2D", "CuStructuredMesh3D", "StructuredMesh", "CuStructuredStiffnessKernel", "StiffnessKernel",
     "CuStructuredFilter2D", "CuStructuredFilter3D", "FilterKernel", "CuMultiGrid", "CuTopOpt", "SingleMaterial",
     "MaterialModel", "auto_stiffness", "hexahedron_element_stiffness", "quadrilateral_element_stiffness",
+    "SIMPObjective",
 ]

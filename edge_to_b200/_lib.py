@@ -31,6 +31,8 @@ _SIGS = {
     "edge_matvec_f32": (ctypes.c_int, [vp, vp, vp]),
     "edge_diagonal": (ctypes.c_int, [vp, vp]),
     "edge_process_grad": (ctypes.c_int, [vp, vp, vp]),
+    "edge_process_grad_adjoint": (ctypes.c_int, [vp, vp, vp, vp]),
+    "edge_set_springs": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), c_double_p]),
     "edge_uses_transform": (ctypes.c_int, [vp]),
     "edge_set_tma": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_fine_tile": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),

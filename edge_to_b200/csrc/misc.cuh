@@ -404,6 +404,97 @@ __global__ void k_pcg_p(long long n, TP* __restrict__ p, const TP* __restrict__ 
     p[i] = Conv<TP>::from((double)Conv<double>::from(z[i]) + beta * (double)Conv<double>::from(p[i]));
 }
 
+// ------------------------------------------------------------------ point springs and adjoint sensitivity
+// Grounded springs on single DOFs (the compliant-mechanism input/output springs): in the
+// slot layout, out[f] += sign * k * x[f] for every unconstrained spring DOF f = c*n + slot,
+// and *dot += sum k x[f]^2 when dot is given (the p.Ap term of PCG).  One block.
+template <typename TX, typename TO>
+__global__ void k_springs(int ns, const long long* __restrict__ flat, const double* __restrict__ kk, long long n,
+                          const uint8_t* __restrict__ mask, const TX* __restrict__ x, TO* __restrict__ out,
+                          double sign, double* dot) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+    const long long f = flat[t];
+    const long long s = f % n;
+    const int c = (int)(f / n);
+    if ((mask[s] >> c) & 1) continue;
+    const double xv = (double)Conv<double>::from(x[f]);
+    out[f] = Conv<TO>::from((double)Conv<double>::from(out[f]) + sign * kk[t] * xv);
+    acc += kk[t] * xv * xv;
+  }
+  const double tot = block_sum(acc, sh);
+  if (dot && threadIdx.x == 0) *dot += tot;
+}
+
+// The springs on the diagonal of K (user layout; constrained DOFs keep their 1).
+__global__ void k_springs_diag(int ns, const long long* __restrict__ flat, const long long* __restrict__ user,
+                               const double* __restrict__ kk, long long n, const uint8_t* __restrict__ mask,
+                               double* __restrict__ diag) {
+  for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+    const long long f = flat[t];
+    if ((mask[f % n] >> (int)(f / n)) & 1) continue;
+    diag[user[t]] += kk[t];
+  }
+}
+
+// Adjoint sensitivity of a linear functional: dk_e = -v_e^T K0 u_e, by polarisation of the
+// element energy: v^T K0 u = ((u+v)^T K0 (u+v) - (u-v)^T K0 (u-v)) / 4.
+__global__ void k_dk2(const Geo g, const double* __restrict__ U, const double* __restrict__ V, KHat3<double> K3,
+                      KHat2<double> K2, const double* __restrict__ K0b, int wht, double* __restrict__ dk) {
+  const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nel = (long long)nelx * nely * nelz;
+  if (e >= nel) return;
+  double val;
+  if (g.dim == 3) {
+    const int k = (int)(e % nelz), j = (int)((e / nelz) % nely), i = (int)(e / ((long long)nelz * nely));
+    double a[8][3], b[8][3];
+    for (int q = 0; q < 8; ++q) {
+      const long long s = g.slot3(i + (q & 1), j + ((q >> 1) & 1), k + ((q >> 2) & 1));
+      for (int c = 0; c < 3; ++c) {
+        const double u = U[c * g.n + s], v = V[c * g.n + s];
+        a[q][c] = u + v;
+        b[q][c] = u - v;
+      }
+    }
+    if (wht) {
+      val = -0.25 * (elem3_energy(K3, a) - elem3_energy(K3, b));
+    } else {
+      double acc = 0.0;
+      for (int r = 0; r < 24; ++r) {
+        double t = 0.0;
+        for (int q = 0; q < 24; ++q) t += K0b[r * 24 + q] * 0.5 * (a[q / 3][q % 3] + b[q / 3][q % 3]);
+        acc += 0.5 * (a[r / 3][r % 3] - b[r / 3][r % 3]) * t;
+      }
+      val = -acc;
+    }
+  } else {
+    const int j = (int)(e % nely), i = (int)(e / nely);
+    double a[4][2], b[4][2];
+    for (int q = 0; q < 4; ++q) {
+      const long long s = g.slot2(i + (q & 1), j + ((q >> 1) & 1));
+      for (int c = 0; c < 2; ++c) {
+        const double u = U[c * g.n + s], v = V[c * g.n + s];
+        a[q][c] = u + v;
+        b[q][c] = u - v;
+      }
+    }
+    if (wht) {
+      val = -0.25 * (elem2_energy(K2, a) - elem2_energy(K2, b));
+    } else {
+      double acc = 0.0;
+      for (int r = 0; r < 8; ++r) {
+        double t = 0.0;
+        for (int q = 0; q < 8; ++q) t += K0b[r * 8 + q] * 0.5 * (a[q / 2][q % 2] + b[q / 2][q % 2]);
+        acc += 0.5 * (a[r / 2][r % 2] - b[r / 2][r % 2]) * t;
+      }
+      val = -acc;
+    }
+  }
+  dk[e] = val;
+}
+
 // ------------------------------------------------------------------ OC bisection (TopOpt/_cuda.py:242-280)
 // ocP = max(1e-12, rho * sqrt(max(-dr/A, 0))) with NaN -> 0; the all-zero fallback of
 // MaterialModels.py:87-88 is applied by k_oc_fallback when sum(ocP_raw) == 0.

@@ -208,6 +208,12 @@ struct Prob {
   bool use_tma = true;
   int tile_variant = 0;    // (BX, NS): 0 (8,4) 1 (8,3) 2 (8,2) 3 (4,4) 4 (4,3)
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
+  // grounded point springs (slot-layout flat index, user DOF index, stiffness)
+  static constexpr int MAX_SPRINGS = 64;
+  int n_springs = 0;
+  long long* spr_flat = nullptr;
+  long long* spr_user = nullptr;
+  double* spr_k = nullptr;
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
   double* E64 = nullptr;
   float* E32 = nullptr;
@@ -511,6 +517,14 @@ static void level_apply(Prob& P, int l, const T* u, Epi epi, double* dot_dst = n
 
 static unsigned ew_blocks(long long n) { return (unsigned)std::min<long long>(cdiv(n, 256), 148LL * 16); }
 
+// out += sign * S x for the point springs (slot layout), and *dot += x^T S x when given.
+template <typename TX, typename TO>
+static void springs_apply(Prob& P, const TX* x, TO* out, double sign, double* dot) {
+  if (P.n_springs == 0) return;
+  launch(P, k_springs<TX, TO>, 1, 64, 0, P.n_springs, (const long long*)P.spr_flat, (const double*)P.spr_k,
+         P.g0.n, (const uint8_t*)P.mask, x, out, sign, dot);
+}
+
 // ------------------------------------------------------------------ small kernels
 template <typename TB, typename TD, typename TO>
 __global__ void k_jacobi0(long long n, const TB* __restrict__ b, const TD* __restrict__ dinv, TO* __restrict__ x,
@@ -769,6 +783,7 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
   {
     EpiResid<double, double, double> e{P.b64, r, g.n};
     fine_apply<double>(P, x, e, nullptr);
+    springs_apply(P, (const double*)x, r, -1.0, nullptr);
   }
   launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, P.b64, P.b64, P.part,
                                                                                        P.ticket, &P.st->bb);
@@ -782,6 +797,7 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
     {
       EpiStoreDot<double> e{q, g.n};
       fine_apply<double>(P, p, e, &P.st->pq);
+      springs_apply(P, (const double*)p, q, 1.0, &P.st->pq);
     }
     launch(P, k_pcg_xr<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, x, p, r, q, P.st,
                                                                                            P.part, P.ticket, (float*)nullptr);
@@ -817,6 +833,7 @@ static void pcg_mixed(Prob& P, double tol, int maxiter) {
   auto true_residual = [&]() {
     EpiResid<double, double, double> e{P.b64, r, g.n};
     fine_apply<double>(P, x, e, nullptr);
+    springs_apply(P, (const double*)x, r, -1.0, nullptr);
     launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)r, (const double*)r, P.part, P.ticket, &P.st->rr);
     launch(P, k_copy<double, float>, ew_blocks(nv), 256, 0, nv, (const double*)r, r32);
     ++P.last_true_res;
@@ -834,6 +851,7 @@ static void pcg_mixed(Prob& P, double tol, int maxiter) {
     {
       EpiStoreDot<float> e{q, g.n};
       fine_apply<float>(P, p, e, &P.st->pq);
+      springs_apply(P, (const float*)p, q, 1.0, &P.st->pq);
     }
     launch(P, k_pcg_xr<double, float>, nb, 256, 0, nv, x, (const float*)p, r, (const float*)q, P.st, P.part, P.ticket,
            r32);
@@ -1137,6 +1155,7 @@ int edge_set_tma(edge_problem* p, int enable) {
   API_END
 }
 
+
 int edge_set_constraints(edge_problem* p, const uint8_t* cons_dev) {
   API_BEGIN
   if (!p || !cons_dev) fail(EDGE_EINVAL, "null argument");
@@ -1170,6 +1189,7 @@ int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev) {
   launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, u_dev, P.b64);
   EpiStore<double, double> e{P.r64, g.n};
   fine_apply<double>(P, P.b64, e, nullptr);
+  springs_apply(P, (const double*)P.b64, P.r64, 1.0, nullptr);
   launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, P.r64, out_dev);
   KCHECK();
   API_END
@@ -1187,6 +1207,7 @@ int edge_matvec_f32(edge_problem* p, const double* u_dev, double* out_dev) {
   launch(P, k_user_to_slots<float>, cdiv(g.n, 256), 256, 0, g, u_dev, u32);
   EpiStore<float, float> e{o32, g.n};
   fine_apply<float>(P, u32, e, nullptr);
+  springs_apply(P, (const float*)u32, o32, 1.0, nullptr);
   launch(P, k_slots_to_user<float>, cdiv(g.n, 256), 256, 0, g, (const float*)o32, out_dev);
   API_END
 }
@@ -1201,6 +1222,7 @@ int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev) {
   launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, u_dev, P.b64);
   EpiStore<double, double> e{P.r64, g.n};
   fine_apply_dense<double>(P, P.b64, e, nullptr);
+  springs_apply(P, (const double*)P.b64, P.r64, 1.0, nullptr);
   launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, P.r64, out_dev);
   KCHECK();
   API_END
@@ -1213,6 +1235,9 @@ int edge_diagonal(edge_problem* p, double* diag_dev) {
   if (!P.has_rho) fail(EDGE_ESTATE, "Rho has not been set. diagonal works only after setting rho or if rho is provided.");
   const Geo& g = P.g0;
   launch(P, k_fine_dinv<double, double>, cdiv(g.n, 256), 256, 0, g, P.E64, P.mask, P.dK0diag, P.r64, diag_dev);
+  if (P.n_springs)
+    launch(P, k_springs_diag, 1, 64, 0, P.n_springs, (const long long*)P.spr_flat, (const long long*)P.spr_user,
+           (const double*)P.spr_k, g.n, (const uint8_t*)P.mask, diag_dev);
   KCHECK();
   API_END
 }
@@ -1226,6 +1251,63 @@ int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev) {
   launch(P, k_dk<double>, cdiv(P.n_el, 256), 256, 0, g, P.b64, P.ei.k3, P.ei.k2, P.dK0b, P.ei.wht ? 1 : 0, dk_dev,
                                                          nullptr, nullptr, 0.0, 0.0);
   KCHECK();
+  API_END
+}
+
+int edge_process_grad_adjoint(edge_problem* p, const double* U_dev, const double* V_dev, double* dk_dev) {
+  API_BEGIN
+  if (!p || !U_dev || !V_dev || !dk_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  const Geo& g = P.g0;
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, U_dev, P.b64);
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, V_dev, P.r64);
+  launch(P, k_dk2, cdiv(P.n_el, 256), 256, 0, g, (const double*)P.b64, (const double*)P.r64, P.ei.k3, P.ei.k2,
+         (const double*)P.dK0b, P.ei.wht ? 1 : 0, dk_dev);
+  KCHECK();
+  API_END
+}
+
+int edge_set_springs(edge_problem* p, int n, const long long* dofs, const double* k) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  Prob& P = p->P;
+  if (n < 0 || n > Prob::MAX_SPRINGS)
+    fail(EDGE_EINVAL, "number of springs must be in [0, " + std::to_string(Prob::MAX_SPRINGS) + "]");
+  if (n > 0 && (!dofs || !k)) fail(EDGE_EINVAL, "null argument");
+  const Geo& g = P.g0;
+  const long long ndof = P.n_dof;
+  std::vector<long long> flat(n), user(n);
+  std::vector<double> kv(n);
+  for (int t = 0; t < n; ++t) {
+    if (dofs[t] < 0 || dofs[t] >= ndof) fail(EDGE_EINVAL, "spring DOF index out of range");
+    if (!(k[t] >= 0.0) || !std::isfinite(k[t])) fail(EDGE_EINVAL, "spring stiffness must be finite and >= 0");
+    const long long node = dofs[t] / g.dof;
+    const int c = (int)(dofs[t] % g.dof);
+    long long slot;
+    if (g.dim == 3) {
+      const long long per_j = (long long)g.nx * g.nz;
+      const int j = (int)(node / per_j), i = (int)((node % per_j) / g.nz), kz = (int)(node % g.nz);
+      slot = g.slot3(i, j, kz);
+    } else {
+      const int j = (int)(node / g.nx), i = (int)(node % g.nx);
+      slot = g.slot2(i, j);
+    }
+    flat[t] = (long long)c * g.n + slot;
+    user[t] = dofs[t];
+    kv[t] = k[t];
+  }
+  if (!P.spr_flat) {
+    P.spr_flat = P.alloc<long long>(Prob::MAX_SPRINGS);
+    P.spr_user = P.alloc<long long>(Prob::MAX_SPRINGS);
+    P.spr_k = P.alloc<double>(Prob::MAX_SPRINGS);
+  }
+  CK(cudaStreamSynchronize(P.stream));
+  if (n) {
+    CK(cudaMemcpy(P.spr_flat, flat.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.spr_user, user.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(P.spr_k, kv.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  P.n_springs = n;
   API_END
 }
 

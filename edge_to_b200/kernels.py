@@ -174,5 +174,28 @@ class CuStructuredStiffnessKernel(StiffnessKernel):
         _lib.call("edge_process_grad", self._h, _lib.ptr(U), _lib.ptr(self.dk))
         return self.dk
 
+    # --------------------------------------------------------------- beyond the reference
+    def set_springs(self, dofs, stiffness):
+        """Grounded point springs K_ii += k on DOF indices ``dofs`` (the compliant-mechanism
+        input/output springs); every product and PCG solve includes them.  ``dofs=[]``
+        removes them.  The reference has no springs (its only objective is compliance)."""
+        d = np.ascontiguousarray(np.asarray(dofs, dtype=np.int64).reshape(-1))
+        k = np.broadcast_to(np.asarray(stiffness, dtype=np.float64), d.shape).copy()
+        self._bind_stream()
+        _lib.call("edge_set_springs", self._h, int(d.size), d.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                  k.ctypes.data_as(_lib.c_double_p))
+        self.springs = (d, k)
+
+    def process_grad_adjoint(self, U, V):
+        """dk_e = -v_e^T K0 u_e: the element sensitivity dJ/dE_e of a linear objective
+        J = l.u whose adjoint solution K v = l is V (for compliance V = U and this equals
+        process_grad)."""
+        U = _as_dev_f64(U)
+        V = _as_dev_f64(V)
+        out = torch.empty(self.n_elements, dtype=torch.float64, device="cuda")
+        self._bind_stream()
+        _lib.call("edge_process_grad_adjoint", self._h, _lib.ptr(U), _lib.ptr(V), _lib.ptr(out))
+        return out
+
 
 StructuredStiffnessKernel = CuStructuredStiffnessKernel

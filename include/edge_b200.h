@@ -52,6 +52,14 @@ int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev);
 int edge_diagonal(edge_problem* p, double* diag_dev);
 /* kernels/_cuda.py:152-156 : dk_e = -u_e^T K0 u_e */
 int edge_process_grad(edge_problem* p, const double* U_dev, double* dk_dev);
+/* Adjoint sensitivity for a linear objective J = l.u with K u = f and K v = l:
+ * dk_e = -v_e^T K0 u_e (dJ/dE_e).  No counterpart in the reference (compliance only). */
+int edge_process_grad_adjoint(edge_problem* p, const double* U_dev, const double* V_dev, double* dk_dev);
+/* Grounded point springs added to K: K_ii += k on the n user DOF indices (host arrays, at
+ * most 64; a constrained DOF keeps its identity row).  They enter every product, the PCG
+ * operator and the diagonal; the multigrid preconditioner is built from K without them.
+ * n = 0 removes them.  No counterpart in the reference (compliant-mechanism springs). */
+int edge_set_springs(edge_problem* p, int n, const long long* dofs, const double* k);
 /* The same product through the FP32 operator of the mixed-precision solver. */
 int edge_matvec_f32(edge_problem* p, const double* u_dev, double* out_dev);
 /* Same product through the dense node-centric kernel (an independent path for tests). */
