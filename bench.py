@@ -359,6 +359,8 @@ def run_matvec(args, cfg_name):
     u = torch.randn(k.shape[0], generator=g, device="cuda", dtype=torch.float64)
     from edge_to_b200 import _lib
     out = torch.empty_like(u)
+    if args.tile is not None:
+        _lib.call("edge_set_fine_tile", k.handle, args.tile, args.tile_bps)
 
     def apply():
         if args.precision == "fp64":
@@ -379,7 +381,7 @@ def run_matvec(args, cfg_name):
     w = 8 if args.precision == "fp64" else 4
     alg = 2 * w * n_dof + w * n_el
     peak, kind = peaks()
-    return {"mode": "matvec", "workload": cfg_name, "ms_per_matvec": ms, "algorithmic_bytes": alg,
+    return {"mode": "matvec", "workload": cfg_name, "tile": args.tile, "ms_per_matvec": ms, "algorithmic_bytes": alg,
             "GBps": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak, "peak_source": kind,
             "note": "includes the user-layout <-> slot-layout conversions of edge_matvec"}
 
@@ -424,6 +426,8 @@ def main():
     ap.add_argument("--config", default="cantilever_256x128x128", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec"])
+    ap.add_argument("--tile", type=int, default=None, help="matvec mode: fine-kernel tile variant (0-8)")
+    ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--breakdown", action="store_true",
                     help="extra untimed step with per-category launch timing (events on every launch)")
     args = ap.parse_args()

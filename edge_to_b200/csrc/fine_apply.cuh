@@ -36,6 +36,11 @@ template <typename T, typename TO> struct EpiStore {
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) out[c * n + s] = Conv<TO>::from(Au[c]);
   }
+  struct Pre {};
+  EDGE_D Pre pre(long long) const { return {}; }
+  EDGE_D void apply(long long s, const T* own, const T* Au, const Pre&, double& acc) const {
+    operator()(s, 3, own, Au, acc);
+  }
 };
 
 // out = A u and acc += u . (A u)   (PCG: q = A p, p.q)
@@ -50,6 +55,10 @@ template <typename T> struct EpiStoreDot {
       out[c * n + s] = Au[c];
       acc += (double)own[c] * (double)Au[c];
     }
+  }  struct Pre {};
+  EDGE_D Pre pre(long long) const { return {}; }
+  EDGE_D void apply(long long s, const T* own, const T* Au, const Pre&, double& acc) const {
+    operator()(s, 3, own, Au, acc);
   }
 };
 
@@ -63,6 +72,17 @@ template <typename T, typename TB, typename TO> struct EpiResid {
   EDGE_D void init() {}
   EDGE_D void operator()(long long s, int dof, const T* own, const T* Au, double& acc) const {
     for (int c = 0; c < dof; ++c) r[c * n + s] = Conv<TO>::from(Conv<T>::from(b[c * n + s]) - Au[c]);
+  }
+  struct Pre {
+    T b[3];
+  };
+  EDGE_D Pre pre(long long s) const {
+    Pre p;
+    for (int c = 0; c < 3; ++c) p.b[c] = Conv<T>::from(b[c * n + s]);
+    return p;
+  }
+  EDGE_D void apply(long long s, const T* own, const T* Au, const Pre& p, double& acc) const {
+    for (int c = 0; c < 3; ++c) r[c * n + s] = Conv<TO>::from(p.b[c] - Au[c]);
   }
 };
 
@@ -83,6 +103,20 @@ template <typename T, typename TB, typename TD> struct EpiJacobi {
       const long long q = c * n + s;
       xo[q] = own[c] + w * Conv<T>::from(dinv[q]) * (Conv<T>::from(b[q]) - Au[c]);
     }
+  }
+  struct Pre {
+    T b[3], d[3];
+  };
+  EDGE_D Pre pre(long long s) const {
+    Pre p;
+    for (int c = 0; c < 3; ++c) {
+      p.b[c] = Conv<T>::from(b[c * n + s]);
+      p.d[c] = Conv<T>::from(dinv[c * n + s]);
+    }
+    return p;
+  }
+  EDGE_D void apply(long long s, const T* own, const T* Au, const Pre& p, double& acc) const {
+    for (int c = 0; c < 3; ++c) xo[c * n + s] = own[c] + w * p.d[c] * (p.b[c] - Au[c]);
   }
 };
 
@@ -108,6 +142,29 @@ template <typename T, typename TB, typename TD, typename TX, bool DOT, typename 
       TX v = Conv<TX>::from(Conv<T>::from(xbase[q]) + e);
       xo[q] = v;
       if (DOT) acc += (double)dotv[q] * (double)v;
+    }
+  }
+  struct Pre {
+    T b[3], d[3], xb[3];
+    TV dv[DOT ? 3 : 1];
+  };
+  EDGE_D Pre pre(long long s) const {
+    Pre p;
+    for (int c = 0; c < 3; ++c) {
+      const long long q = c * n + s;
+      p.b[c] = Conv<T>::from(b[q]);
+      p.d[c] = Conv<T>::from(dinv[q]);
+      p.xb[c] = Conv<T>::from(xbase[q]);
+      if constexpr (DOT) p.dv[c] = dotv[q];
+    }
+    return p;
+  }
+  EDGE_D void apply(long long s, const T* own, const T* Au, const Pre& p, double& acc) const {
+    for (int c = 0; c < 3; ++c) {
+      const T e = own[c] + w * p.d[c] * (p.b[c] - Au[c]);
+      const TX v = Conv<TX>::from(p.xb[c] + e);
+      xo[c * n + s] = v;
+      if constexpr (DOT) acc += (double)p.dv[c] * (double)v;
     }
   }
 };

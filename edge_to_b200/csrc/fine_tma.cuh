@@ -242,6 +242,11 @@ k_fine3_tma(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_
 
   for (int k = 0; k + 1 < np; ++k) {
     const int ey = p0 + k;
+    // epilogue inputs of this layer's output node, loaded before the element math so
+    // their latency overlaps it
+    typename Epi::Pre pre;
+    const bool wr = (ey >= y0) && writer;
+    if (wr) pre = epi.pre(s_base + (long long)ey * g.plane);
     if (ok) ok = mbar_wait(&bar[(k + 1) % NS], ((k + 1) / NS) & 1);
     const uint8_t fl = flag_of(k);   // element row ey: covers this layer's 8 corners
     const T Ee = reinterpret_cast<const T*>(smem + (k % NS) * Tile::STAGE + Tile::E_OFF)[eoff];
@@ -302,7 +307,7 @@ k_fine3_tma(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_
 #pragma unroll
       for (int c = 0; c < 3; ++c) fromL[c] = (w > 0) ? sX[xb][w - 1][zl][c] : T(0);
     }
-    if (ey >= y0 && writer) {
+    if (wr) {
       // own node = corner (0,0) of element row ey; its flag fl says whether it may be constrained
       const long long s_out = s_base + (long long)ey * g.plane;
       T own[3], Au[3];
@@ -320,7 +325,7 @@ k_fine3_tma(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_
             Au[c] = own[c];
           }
       }
-      epi(s_out, 3, own, Au, dacc);
+      epi.apply(s_out, own, Au, pre, dacc);
     }
 #pragma unroll
     for (int a = 0; a < 2; ++a)

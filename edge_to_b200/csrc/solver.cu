@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/edge_b200.h"
@@ -23,6 +24,7 @@
 #include "element_op.cuh"
 #include "fine_apply.cuh"
 #include "fine_tma.cuh"
+#include "fine_pk.cuh"
 #include "misc.cuh"
 
 namespace edge {
@@ -206,7 +208,10 @@ struct Prob {
   uint8_t* eflag = nullptr;
   int* err = nullptr;          // set by kernels whose bounded waits expired
   bool use_tma = true;
-  int tile_variant = 0;    // (BX, NS): 0 (8,4) 1 (8,3) 2 (8,2) 3 (4,4) 4 (4,3)
+  int tile_variant = 0;    // k_fine3_tma (BX, NS): 0 (8,4) 1 (8,3) 2 (8,2) 3 (4,4) 4 (4,3);
+                           // FP32 only, k_fine3_pk (BX, NS, min blocks/SM): 5 (4,3,1) 6 (4,3,4)
+                           // 7 (2,3,8) 8 (4,4,4)
+  KHat3P k3p;              // packed transformed element operator (FP32 pairs)
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
   // grounded point springs (slot-layout flat index, user DOF index, stiffness)
   static constexpr int MAX_SPRINGS = 64;
@@ -377,6 +382,56 @@ static const CUtensorMap& flag_map(Prob& P) {
   return P.tmaps.emplace(key, encode_map(P.eflag16, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims, str, box)).first->second;
 }
 
+// Maps of the packed-pair kernel (FP32): u box 24 x (4BX+1) x 1 x 3, E box 24 x 4BX x 1,
+// flags 48 x 4BX x 1.
+template <int BX>
+static const CUtensorMap& pk_map(Prob& P, const float* base, int kind) {
+  auto key = std::make_pair((const void*)base, 2000 + kind * 16 + BX);
+  auto it = P.tmaps.find(key);
+  if (it != P.tmaps.end()) return it->second;
+  const Geo& g = P.g0;
+  const uint64_t sz = sizeof(float);
+  CUtensorMap m;
+  if (kind == 0) {
+    uint64_t dims[4] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny, 3};
+    uint64_t str[3] = {g.pz * sz, g.plane * sz, g.n * sz};
+    uint32_t box[4] = {PK_ZB, 4 * BX + 1, 1, 3};
+    m = encode_map(base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, dims, str, box);
+  } else {
+    uint64_t dims[3] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny};
+    uint64_t str[2] = {g.pz * sz, g.plane * sz};
+    uint32_t box[3] = {PK_ZB, 4 * BX, 1};
+    m = encode_map(base, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, dims, str, box);
+  }
+  return P.tmaps.emplace(key, m).first->second;
+}
+
+template <int BX>
+static const CUtensorMap& pk_flag_map(Prob& P) {
+  auto key = std::make_pair((const void*)P.eflag16, 3000 + BX);
+  auto it = P.tmaps.find(key);
+  if (it != P.tmaps.end()) return it->second;
+  const Geo& g = P.g0;
+  uint64_t dims[3] = {(uint64_t)P.mpz, (uint64_t)g.nx, (uint64_t)g.ny};
+  uint64_t str[2] = {(uint64_t)P.mpz, (uint64_t)P.mpz * g.nx};
+  uint32_t box[3] = {PK_FB, 4 * BX, 1};
+  return P.tmaps.emplace(key, encode_map(P.eflag16, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, dims, str, box)).first->second;
+}
+
+static KHat3P pack3(const KHat3<double>& k) {
+  KHat3P o;
+  for (int c = 0; c < 3; ++c)
+    for (int h = 0; h < 8; ++h) {
+      const float a = (float)k.dg[c][h];
+      o.dg[c][h].v = make_float2(a, a);
+      for (int d = 0; d < 3; ++d) {
+        const float b = (float)k.of[c][d][h];
+        o.of[c][d][h].v = make_float2(b, b);
+      }
+    }
+  return o;
+}
+
 static size_t vbytes(int prec) { return prec == EDGE_FP64 ? sizeof(double) : sizeof(float); }
 
 // ------------------------------------------------------------------ launch helpers
@@ -439,6 +494,26 @@ static void fine3_tma_launch(Prob& P, const T* u, const T* E, Epi epi, double* d
          cast3<T>(P.ei.k3), ly, epi, P.part, P.ticket, dot_dst, P.err);
 }
 
+// One launch of the packed-pair FP32 kernel (BX warps, NS stages).
+template <class Epi, int BX, int NS, int MINB>
+static void fine3_pk_launch(Prob& P, const float* u, const float* E, Epi epi, double* dot_dst) {
+  const Geo& g = P.g0;
+  constexpr int smem = pk_smem_bytes<BX, NS>();
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(k_fine3_pk<Epi, BX, NS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  const unsigned tz = cdiv(g.nz, 15), tx = cdiv(g.nx, 4 * BX - 1);
+  const long long want = 148LL * P.blocks_per_sm;
+  long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
+  chunks = std::min<long long>(chunks, g.ny);
+  const int ly = (int)cdiv(g.ny, chunks);
+  launch(P, k_fine3_pk<Epi, BX, NS, MINB>, dim3(tz, tx, cdiv(g.ny, ly)), dim3(32, BX), smem, g, pk_map<BX>(P, u, 0),
+         pk_flag_map<BX>(P), pk_map<BX>(P, E, 1), u, (const uint8_t*)P.mask, P.k3p, ly, epi, P.part, P.ticket,
+         dot_dst, P.err);
+}
+
 // Fine-level operator with epilogue.  u, E in type T.  When profiling is on, each launch is
 // bracketed by CUDA events on the problem's stream and its algorithmic bytes recorded:
 // input vector + E + the epilogue's per-DOF traffic (BC mask excluded).
@@ -450,7 +525,20 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
   const bool rec = P.prof && P.pev_used + 2 <= P.pev.size();
   if (rec) CK(cudaEventRecord(P.pev[P.pev_used], P.stream));
   if (P.ei.wht) {
-    if (P.dim == 3 && P.use_tma) {
+    bool packed = false;
+    if constexpr (std::is_same<T, float>::value) {
+      if (P.dim == 3 && P.use_tma && P.tile_variant >= 5) {
+        switch (P.tile_variant) {
+          case 5: fine3_pk_launch<Epi, 4, 3, 1>(P, u, E, epi, dot_dst); break;
+          case 6: fine3_pk_launch<Epi, 4, 3, 4>(P, u, E, epi, dot_dst); break;
+          case 7: fine3_pk_launch<Epi, 2, 3, 8>(P, u, E, epi, dot_dst); break;
+          default: fine3_pk_launch<Epi, 4, 4, 4>(P, u, E, epi, dot_dst); break;
+        }
+        packed = true;
+      }
+    }
+    if (packed) {
+    } else if (P.dim == 3 && P.use_tma) {
       switch (P.tile_variant) {
         case 0: fine3_tma_launch<T, Epi, 8, 4>(P, u, E, epi, dot_dst); break;
         case 1: fine3_tma_launch<T, Epi, 8, 3>(P, u, E, epi, dot_dst); break;
@@ -1013,6 +1101,7 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     P.n_el = (long long)nel[0] * nel[1] * (dim == 3 ? nel[2] : 1);
     P.n_dof = (long long)P.g0.nx * P.g0.ny * P.g0.nz * dim;
     analyse_element(dim, K0, P.ei);
+    if (dim == 3) P.k3p = pack3(P.ei.k3);
     const int nk = P.ei.nk;
     P.dK0b = P.alloc<double>(nk * nk);
     CK(cudaMemcpy(P.dK0b, P.ei.K0b, nk * nk * sizeof(double), cudaMemcpyHostToDevice));
@@ -1084,7 +1173,7 @@ int edge_uses_transform(const edge_problem* p) { return p && p->P.ei.wht ? 1 : 0
 
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm) {
   API_BEGIN
-  if (!p || variant < 0 || variant > 4 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
+  if (!p || variant < 0 || variant > 8 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
   p->P.tile_variant = variant;
   p->P.blocks_per_sm = blocks_per_sm;
   API_END
@@ -1111,17 +1200,32 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
   double best = 1e30;
   int bv = P.tile_variant, bb = P.blocks_per_sm;
   const int bps_list[4] = {2, 4, 8, 16};
-  for (int v = 0; v < 5; ++v)
+  const int nvar = precision == EDGE_FP64 ? 5 : 9;  // variants 5..8: packed-pair FP32 kernel
+  for (int v = 0; v < nvar; ++v)
     for (int bi = 0; bi < 4; ++bi) {
       P.tile_variant = v;
       P.blocks_per_sm = bps_list[bi];
+      // time the smoother sweep (the most frequent fine-level launch) once the multigrid is
+      // configured, else the plain product; buffer contents do not matter for timing
+      const bool sweep = P.n_level >= 0 && !P.lv.empty() && P.lv[0].dinv;
       auto run = [&]() {
         if (precision == EDGE_FP64) {
-          EpiStore<double, double> e{P.r64, g.n};
-          fine_apply<double>(P, P.x64, e, nullptr);
+          if (sweep) {
+            EpiJacobi<double, double, double> e{P.b64, (const double*)P.lv[0].dinv, P.r64, &P.st->omega, 1.0, g.n};
+            fine_apply<double>(P, P.x64, e, nullptr);
+          } else {
+            EpiStore<double, double> e{P.r64, g.n};
+            fine_apply<double>(P, P.x64, e, nullptr);
+          }
         } else {
-          EpiStore<float, float> e{(float*)P.q, g.n};
-          fine_apply<float>(P, (const float*)P.p, e, nullptr);
+          if (sweep && P.prec == EDGE_MIXED) {
+            EpiJacobi<float, float, __nv_bfloat16> e{P.r32, (const __nv_bfloat16*)P.lv[0].dinv, (float*)P.q,
+                                                     &P.st->omega, 1.0, g.n};
+            fine_apply<float>(P, (const float*)P.p, e, nullptr);
+          } else {
+            EpiStore<float, float> e{(float*)P.q, g.n};
+            fine_apply<float>(P, (const float*)P.p, e, nullptr);
+          }
         }
       };
       run();

@@ -269,3 +269,58 @@ def test_fp32_operator_accuracy():
         b = torch.empty_like(a)
         _lib.call("edge_matvec_f32", k.handle, _lib.ptr(u), _lib.ptr(b))
         assert rel(b.cpu(), a.cpu()) < 1e-5
+
+
+@pytest.mark.parametrize("nel", [(4, 4, 4), (7, 5, 3), (40, 9, 33), (9, 33, 65), (3, 3, 130), (20, 20, 47), (66, 17, 31)])
+def test_fp32_tile_variants_agree(nel):
+    """Every FP32 fine-kernel tile (k_fine3_tma 0-4, packed-pair k_fine3_pk 5-8) gives K(E) u
+    to single precision on ragged grids with boundary conditions and void elements."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    rng = np.random.default_rng(sum(nel) + 7)
+    mesh = _mesh(3, nel, None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    g = Grid(nel)
+    E = rng.uniform(1e-3, 1, g.n_el)
+    E[rng.random(g.n_el) < 0.2] = 1e-9
+    u = rng.standard_normal(g.n_dof)
+    cons = np.where(rng.random(g.n_dof) < 0.1)[0]
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    k.add_constraints(cons)
+    ref = ops.assemble(g, elements.hex8_stiffness(1, 1, 1, 1, 0.3), E, cons) @ u
+    ut = torch.as_tensor(u, device="cuda")
+    outs = []
+    for v in range(9):
+        for bps in (2, 16):
+            _lib.call("edge_set_fine_tile", k.handle, v, bps)
+            b = torch.empty_like(ut)
+            _lib.call("edge_matvec_f32", k.handle, _lib.ptr(ut), _lib.ptr(b))
+            outs.append(b.cpu().numpy())
+            assert rel(outs[-1], ref) < 2e-6, (v, bps)
+    for o in outs[10:]:
+        assert rel(o, outs[8]) < 1e-6
+
+
+def test_packed_kernel_in_mixed_solve():
+    """Mixed-precision PCG with the packed-pair FP32 kernel follows the k_fine3_tma run."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(9)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    mesh = _mesh(3, (32, 16, 16), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision="mixed", autotune=False)
+    res = []
+    for v in (4, 5, 8):
+        _lib.call("edge_set_fine_tile", k.handle, v, 8)
+        x, r = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
+        res.append((x.cpu().numpy().copy(), s.last_iters, r))
+    for x, it, r in res[1:]:
+        assert abs(it - res[0][1]) <= 2 and r < 1e-8
+        assert rel(x, res[0][0]) < 1e-6
