@@ -386,6 +386,40 @@ def run_matvec(args, cfg_name):
             "note": "includes the user-layout <-> slot-layout conversions of edge_matvec"}
 
 
+def run_tiles(args, cfg_name):
+    """Profiling helper: device time of every fine-kernel tile variant (plain product and
+    smoother sweep, CUDA events around `steps` launches) on the workload's grid after one
+    SIMP analysis, so E, the boundary conditions and the multigrid are the live ones."""
+    import ctypes
+    import torch
+    from edge_to_b200 import _lib
+    opt, rho = build_problem(CONFIGS[cfg_name], args.precision)
+    opt.solve_and_process(rho, 0)
+    torch.cuda.synchronize()
+    h = opt.kernel.handle
+    prec = 1 if args.precision == "mixed" else 0
+    nvar = 5 if args.precision == "fp64" else (13 if _lib.lib().edge_uses_cube_form(h) else 9)
+    k = opt.kernel
+    n_dof, n_el = k.shape[0], k.n_elements
+    w = 8 if args.precision == "fp64" else 4
+    plain_bytes = 2 * w * n_dof + w * n_el
+    sweep_bytes = plain_bytes + n_dof * (w + (8 if args.precision == "fp64" else 2) + 0)
+    peak, kind = peaks()
+    rows = []
+    ms = ctypes.c_double()
+    for v in range(nvar):
+        for bps in (2, 4, 8, 16):
+            r = {"variant": v, "bps": bps}
+            for sweep in (0, 1):
+                _lib.call("edge_time_fine", h, prec, v, bps, sweep, max(1, args.steps), ctypes.byref(ms))
+                b = sweep_bytes if sweep else plain_bytes
+                r["sweep_us" if sweep else "plain_us"] = round(ms.value * 1e3, 2)
+                r["sweep_frac" if sweep else "plain_frac"] = round(b / (ms.value / 1e3) / 1e9 / peak, 3)
+            rows.append(r)
+    return {"mode": "tiles", "workload": cfg_name, "precision": args.precision, "peak_GBps": peak,
+            "peak_source": kind, "plain_bytes": plain_bytes, "sweep_bytes": sweep_bytes, "tiles": rows}
+
+
 def run_reference(args, cfg_name):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -425,8 +459,8 @@ def main():
                     help="skip timing the plain FP64 path beside the mixed-precision one")
     ap.add_argument("--config", default="cantilever_256x128x128", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="simp", choices=["simp", "matvec"])
-    ap.add_argument("--tile", type=int, default=None, help="matvec mode: fine-kernel tile variant (0-8)")
+    ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles"])
+    ap.add_argument("--tile", type=int, default=None, help="matvec mode: fine-kernel tile variant (0-12)")
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--breakdown", action="store_true",
                     help="extra untimed step with per-category launch timing (events on every launch)")
@@ -436,6 +470,8 @@ def main():
         line = run_reference(args, args.config)
     elif args.mode == "matvec":
         line = run_matvec(args, args.config)
+    elif args.mode == "tiles":
+        line = run_tiles(args, args.config)
     else:
         line = run_ours(args, args.config)
     if line is not None:

@@ -34,9 +34,12 @@ _SIGS = {
     "edge_process_grad_adjoint": (ctypes.c_int, [vp, vp, vp, vp]),
     "edge_set_springs": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), c_double_p]),
     "edge_uses_transform": (ctypes.c_int, [vp]),
+    "edge_uses_cube_form": (ctypes.c_int, [vp]),
     "edge_set_tma": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_fine_tile": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
     "edge_autotune_fine": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_double_p, c_int_p, c_int_p]),
+    "edge_time_fine": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      c_double_p]),
     "edge_mg_config": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                       c_int_p, ctypes.c_int, ctypes.c_int]),
     "edge_mg_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_double_p, c_int_p]),

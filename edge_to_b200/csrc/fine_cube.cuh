@@ -1,0 +1,542 @@
+// Packed-pair fine-level operator for cube elements (3-D, FP32), sm_100a.
+//
+// The tiling, TMA staging and node-combination scheme are those of k_fine3_pk (two
+// neighbouring element columns per thread in float2 registers, y-marching blocks, a ring
+// of cp.async.bulk.tensor stages, transform-domain carry of the upper-face part).  Three
+// things differ:
+//
+//  * The transformed element operator is applied in its block form.  For a cube element
+//    (equal edge lengths) of an isotropic material, Khat (element_op.cuh) splits into
+//      - a 3x3 block {(1,x),(2,y),(4,z)} with equal diagonals and equal off-diagonals
+//        (normal strains): v = nd*u + no*(u1+u2+u3),
+//      - three rank-1 2x2 blocks {(1,y),(2,x)}, {(1,z),(4,x)}, {(2,z),(4,y)} with all
+//        four entries equal (shear strains): v1 = v2 = sh*(u1+u2),
+//      - three 2x2 blocks {(3,x),(6,z)}, {(3,y),(5,z)}, {(5,x),(6,y)} with equal diagonals
+//        (bending modes): v1 = bd*u1 + bo*u2, v2 = bo*u1 + bd*u2,
+//      - a 3x3 block {(3,z),(5,y),(6,x)} like the first (twist): v = td*u + to*(sum),
+//      - a diagonal for h = 7 (the hourglass mode): v = h7*u,
+//    so eight coefficients describe it.  They are scaled by E once per element (8 packed
+//    multiplies) and the block products take 33 more, against 66 for the general sparse
+//    form, and the coefficients stay in registers for the whole kernel.  The host checks
+//    every one of the 576 entries of Khat against this model before choosing the kernel.
+//  * The y loop is unrolled by two so that the lower and upper planes swap roles without
+//    register copies.
+//  * The h = 0 transform coefficient (rigid translation) is never formed: its output is
+//    zero, and the carry for (hx, hz) = (0, 0) is kept with the opposite sign so that the
+//    y stage needs no negation.
+//
+//  * The epilogue's per-node inputs (right-hand side, Jacobi diagonal, correction base,
+//    FP64 dot vector) travel through the same TMA ring as u, one box per array and plane,
+//    so the epilogue reads shared memory instead of waiting on global loads; this keeps
+//    the smoother sweep close to the plain product although the kernel runs few warps.
+//
+// TMA boxes, strides and alignments are those of k_fine3_pk, plus the staged arrays: FP32
+// and FP64 boxes start at z0-1 rounded down to 4 nodes (16 / 32 bytes), BF16 boxes at z0-1
+// rounded down to 8 nodes (16 bytes; the 3-D fine level pads z to a multiple of 8 so that
+// BF16 rows are 16-byte strided).  Every mbarrier wait is bounded (fast try first, then
+// the clocked wait of fine_tma.cuh).  No multicast.
+#pragma once
+#include "fine_pk.cuh"
+
+namespace edge {
+
+// Block-form coefficients of a cube element's Khat (already divided by 8 like KHat3).
+struct KCube {
+  float nd, no, sh, bd, bo, td, to, h7;
+};
+
+EDGE_D bool mbar_wait_fast(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  if (ok) return true;
+  return mbar_wait(bar, parity);
+}
+
+// v = E * Khat u in block form; uh / vh indexed [h][c], h = hx | hy<<1 | hz<<2; h = 0 is
+// neither read nor written.
+EDGE_D void khat_cube(const P2 kc[8], P2 E, const P2 uh[8][3], P2 vh[8][3]) {
+  P2 k[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) k[i] = kc[i] * E;
+  {  // normal strains
+    const P2 t = k[1] * (uh[1][0] + uh[2][1] + uh[4][2]);
+    vh[1][0] = pfma(k[0], uh[1][0], t);
+    vh[2][1] = pfma(k[0], uh[2][1], t);
+    vh[4][2] = pfma(k[0], uh[4][2], t);
+  }
+  {  // shear strains
+    const P2 a = k[2] * (uh[1][1] + uh[2][0]);
+    vh[1][1] = a;
+    vh[2][0] = a;
+    const P2 b = k[2] * (uh[1][2] + uh[4][0]);
+    vh[1][2] = b;
+    vh[4][0] = b;
+    const P2 c = k[2] * (uh[2][2] + uh[4][1]);
+    vh[2][2] = c;
+    vh[4][1] = c;
+  }
+  // bending pairs
+  auto pair = [&](int h1, int c1, int h2, int c2) {
+    const P2 a = uh[h1][c1], b = uh[h2][c2];
+    vh[h1][c1] = pfma(k[4], b, k[3] * a);
+    vh[h2][c2] = pfma(k[4], a, k[3] * b);
+  };
+  pair(3, 0, 6, 2);
+  pair(3, 1, 5, 2);
+  pair(5, 0, 6, 1);
+  {  // twist
+    const P2 t = k[6] * (uh[3][2] + uh[5][1] + uh[6][0]);
+    vh[3][2] = pfma(k[5], uh[3][2], t);
+    vh[5][1] = pfma(k[5], uh[5][1], t);
+    vh[6][0] = pfma(k[5], uh[6][0], t);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) vh[7][c] = k[7] * uh[7][c];
+}
+
+// ------------------------------------------------------------------ staged epilogues
+// Each epilogue names the arrays it reads per output node (kN of them, element types kT),
+// loads its inputs from the stage of the output plane (load, before the stage is recycled)
+// and finishes the node (apply).  sp[i] points at component 0 of array i for this node;
+// cs4 / cs2 are the component strides (elements) of 4/8-byte and 2-byte boxes.
+enum : int { ST_F32 = 0, ST_BF16 = 1, ST_F64 = 2 };
+EDGE_HD constexpr int st_width(int t) { return t == ST_BF16 ? 32 : 24; }
+EDGE_HD constexpr int st_esize(int t) { return t == ST_BF16 ? 2 : (t == ST_F64 ? 8 : 4); }
+
+struct SEStore {  // out = A u
+  float* out;
+  long long n;
+  static constexpr int kN = 0;
+  static constexpr bool kDot = false;
+  EDGE_HD static constexpr int kT(int i) { return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 0 : 0; }
+  struct In {};
+  EDGE_D void init() {}
+  EDGE_D In load(const unsigned char* const*, int, int) const { return {}; }
+  EDGE_D void apply(long long s, const float*, const float* Au, const In&, double&) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c * n + s] = Au[c];
+  }
+};
+
+struct SEStoreDot {  // out = A u, acc += u . A u
+  float* out;
+  long long n;
+  static constexpr int kN = 0;
+  static constexpr bool kDot = true;
+  EDGE_HD static constexpr int kT(int i) { return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 0 : 0; }
+  struct In {};
+  EDGE_D void init() {}
+  EDGE_D In load(const unsigned char* const*, int, int) const { return {}; }
+  EDGE_D void apply(long long s, const float* own, const float* Au, const In&, double& acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      out[c * n + s] = Au[c];
+      acc += (double)own[c] * (double)Au[c];
+    }
+  }
+};
+
+struct SEResid {  // r = b - A u
+  float* r;
+  long long n;
+  static constexpr int kN = 1;
+  static constexpr bool kDot = false;
+  EDGE_HD static constexpr int kT(int i) { return i == 0 ? ST_F32 : i == 1 ? 0 : i == 2 ? 0 : 0; }
+  struct In {
+    float b[3];
+  };
+  EDGE_D void init() {}
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int) const {
+    In v;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
+    return v;
+  }
+  EDGE_D void apply(long long s, const float*, const float* Au, const In& v, double&) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r[c * n + s] = v.b[c] - Au[c];
+  }
+};
+
+struct SEJacobi {  // xo = u + w Dinv (b - A u)
+  float* xo;
+  const double* omega;
+  double wscale;
+  long long n;
+  float w;
+  static constexpr int kN = 2;
+  static constexpr bool kDot = false;
+  EDGE_HD static constexpr int kT(int i) { return i == 0 ? ST_F32 : i == 1 ? ST_BF16 : i == 2 ? 0 : 0; }
+  struct In {
+    float b[3], d[3];
+  };
+  EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2) const {
+    In v;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
+      v.d[c] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(sp[1])[c * cs2]);
+    }
+    return v;
+  }
+  EDGE_D void apply(long long s, const float* own, const float* Au, const In& v, double&) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) xo[c * n + s] = own[c] + w * v.d[c] * (v.b[c] - Au[c]);
+  }
+};
+
+// last post-smoothing sweep with the correction: xo = xbase + e + w Dinv (b - A e), e = u;
+// with DOT, acc += dotv . xo with dotv in FP64
+template <bool DOT> struct SEJacobiAdd {
+  float* xo;
+  const double* omega;
+  double wscale;
+  long long n;
+  float w;
+  static constexpr int kN = DOT ? 4 : 3;
+  static constexpr bool kDot = DOT;
+  EDGE_HD static constexpr int kT(int i) { return i == 0 ? ST_F32 : i == 1 ? ST_BF16 : i == 2 ? ST_F32 : ST_F64; }
+  struct In {
+    float b[3], d[3], xb[3];
+    double dv[DOT ? 3 : 1];
+  };
+  EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2) const {
+    In v;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
+      v.d[c] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(sp[1])[c * cs2]);
+      v.xb[c] = reinterpret_cast<const float*>(sp[2])[c * cs4];
+      if constexpr (DOT) v.dv[c] = reinterpret_cast<const double*>(sp[3])[c * cs4];
+    }
+    return v;
+  }
+  EDGE_D void apply(long long s, const float* own, const float* Au, const In& v, double& acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float x = v.xb[c] + (own[c] + w * v.d[c] * (v.b[c] - Au[c]));
+      xo[c * n + s] = x;
+      if constexpr (DOT) acc += v.dv[c] * (double)x;
+    }
+  }
+};
+
+// Stage layout of the cube kernel: the k_fine3_pk stage followed by the staged arrays.
+template <int BX, class SE> struct CubeTile {
+  using B = PkTile<BX>;
+  static constexpr int ROWS = 4 * BX;  // staged rows: the block's output node rows
+  static constexpr int up(int b) { return (b + 127) & ~127; }
+  static constexpr int sbytes(int t) { return 3 * ROWS * st_width(t) * st_esize(t); }
+  static constexpr int s_off(int i) {
+    int o = B::STAGE;
+    for (int j = 0; j < i; ++j) o += up(sbytes(SE::kT(j)));
+    return o;
+  }
+  static constexpr int tx_bytes() {
+    int t = B::TX_BYTES;
+    for (int j = 0; j < SE::kN; ++j) t += sbytes(SE::kT(j));
+    return t;
+  }
+  static constexpr int STAGE = s_off(SE::kN);
+  static constexpr int TX_BYTES = tx_bytes();
+  static constexpr int X_BYTES = B::X_BYTES;
+};
+
+template <int BX, int NS, class SE>
+constexpr int cube_smem_bytes() {
+  return NS * CubeTile<BX, SE>::STAGE + CubeTile<BX, SE>::X_BYTES + 128 + 16 * NS;
+}
+
+template <class SE, int BX, int NS, int MINB>
+__global__ void __launch_bounds__(32 * BX, MINB)
+k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_constant__ CUtensorMap mapF,
+             const __grid_constant__ CUtensorMap mapE, const float* __restrict__ u, const uint8_t* __restrict__ mask,
+             const __grid_constant__ CUtensorMap mapS0, const __grid_constant__ CUtensorMap mapS1,
+             const __grid_constant__ CUtensorMap mapS2, const __grid_constant__ CUtensorMap mapS3, const KCube KC,
+             const int ly, SE epi, double* part, unsigned* ticket, double* dot_dst, int* err) {
+  using Tile = CubeTile<BX, SE>;
+  using PT = PkTile<BX>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  typedef float XArr[2][BX][16][3];
+  XArr& sX = *reinterpret_cast<XArr*>(smem + NS * Tile::STAGE);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + NS * Tile::STAGE + Tile::X_BYTES);
+
+  const int lane = threadIdx.x & 31, w = threadIdx.y, tid = threadIdx.x + 32 * w;
+  const int zl = lane & 15, xh = lane >> 4;
+  const int c0 = 2 * (2 * w + xh);  // first element column of the pair
+  const int z0 = blockIdx.x * 15, x0 = blockIdx.y * (4 * BX - 1);
+  const int y0 = blockIdx.z * ly;
+  const int y1 = min(y0 + ly, g.ny);
+  const int ez = z0 - 1 + zl, exa = x0 - 1 + c0;
+  const int zs4 = (z0 >= 1) ? ((z0 - 1) & ~3) : -4;
+  const int zo4 = (z0 - 1) - zs4;
+  const int zs16 = (z0 >= 1) ? ((z0 - 1) & ~15) : -16;
+  const int zo16 = (z0 - 1) - zs16;
+  const int zs8 = (z0 >= 1) ? ((z0 - 1) & ~7) : -8;
+  const int zo8 = (z0 - 1) - zs8;
+  const long long n = g.n;
+  const int p0 = y0 - 1;
+  const int np = y1 - p0 + 1;
+  const bool zok = (zl >= 1) && (ez < g.nz);
+  const bool writerA = zok && (c0 >= 1) && (exa < g.nx);
+  const bool writerB = zok && (exa + 1 < g.nx);
+  epi.init();
+  bool ok = true;
+  P2 kc[8];
+  kc[0] = pk(KC.nd, KC.nd);
+  kc[1] = pk(KC.no, KC.no);
+  kc[2] = pk(KC.sh, KC.sh);
+  kc[3] = pk(KC.bd, KC.bd);
+  kc[4] = pk(KC.bo, KC.bo);
+  kc[5] = pk(KC.td, KC.td);
+  kc[6] = pk(KC.to, KC.to);
+  kc[7] = pk(KC.h7, KC.h7);
+
+  if (tid == 0) {
+    for (int s = 0; s < NS; ++s) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int k) {
+    const int s = k % NS;
+    unsigned char* st = smem + s * Tile::STAGE;
+    const int p = p0 + k;
+    mbar_expect_tx(&bar[s], Tile::TX_BYTES);
+    tma_load_4d(st + PT::U_OFF, &mapU, zs4, x0 - 1, p, 0, &bar[s]);
+    tma_load_3d(st + PT::F_OFF, &mapF, zs16, x0 - 1, p, &bar[s]);
+    tma_load_3d(st + PT::E_OFF, &mapE, zs4, x0 - 1, p, &bar[s]);
+    const CUtensorMap* ms[4] = {&mapS0, &mapS1, &mapS2, &mapS3};
+#pragma unroll
+    for (int i = 0; i < SE::kN; ++i)
+      tma_load_4d(st + Tile::s_off(i), ms[i], SE::kT(i) == ST_BF16 ? zs8 : zs4, x0 - 1, p, 0, &bar[s]);
+  };
+  if (tid == 0)
+    for (int k = 0; k < NS && k < np; ++k) issue(k);
+
+  constexpr int UC = PT::NR * PK_ZB;  // component stride in a stage (words)
+  const int uoff = c0 * PK_ZB + zo4 + zl;
+  const int foff = c0 * PK_FB + zo16 + zl;
+
+  // The 3 node rows x 2 z of plane p (stage k), masked on constrained DOFs when `fl` says
+  // some corner of the pair may be constrained; x-z transformed into t, and the thread's
+  // two own nodes (rows c0, c0+1 at z = ez) returned raw.
+  auto load_plane = [&](int k, int p, uint8_t fl, P2 t[2][2][3], float ownA[3], float ownB[3]) {
+    const float* su = reinterpret_cast<const float*>(smem + (k % NS) * Tile::STAGE + PT::U_OFF) + uoff;
+    float s[3][2][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s[r][dz][c] = su[c * UC + r * PK_ZB + dz];
+    if (__any_sync(0xffffffffu, fl != 0)) {
+      if (fl) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int dz = 0; dz < 2; ++dz) {
+            const int ii = exa + r, kk = ez + dz;
+            if (ii >= 0 && ii < g.nx && kk >= 0 && kk < g.nz && p >= 0 && p < g.ny) {
+              const uint8_t m = __ldg(mask + g.slot3(ii, p, kk));
+#pragma unroll
+              for (int c = 0; c < 3; ++c)
+                if ((m >> c) & 1) s[r][dz][c] = 0.f;
+            }
+          }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ownA[c] = s[0][0][c];
+      ownB[c] = s[1][0][c];
+    }
+    // x stage (scalar, written straight into the pair registers), then z stage (packed)
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        t[0][dz][c] = pk(s[0][dz][c] + s[1][dz][c], s[1][dz][c] + s[2][dz][c]);
+        t[1][dz][c] = pk(s[0][dz][c] - s[1][dz][c], s[1][dz][c] - s[2][dz][c]);
+      }
+#pragma unroll
+    for (int hx = 0; hx < 2; ++hx)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const P2 a = t[hx][0][c], b = t[hx][1][c];
+        t[hx][0][c] = a + b;
+        t[hx][1][c] = a - b;
+      }
+  };
+  auto flags_of = [&](int k, uint8_t& fa, uint8_t& fb) {
+    const uint8_t* sf = smem + (k % NS) * Tile::STAGE + PT::F_OFF + foff;
+    fa = sf[0];
+    fb = sf[PK_FB];
+  };
+
+  P2 pa[2][2][3], pb[2][2][3];  // x-z transforms of two consecutive planes (roles alternate)
+  P2 car[2][2][3];              // carry to the next plane; car[0][0] holds the negated value
+  float oAa[3], oBa[3], oAb[3], oBb[3];
+  if (ok) ok = mbar_wait_fast(&bar[0], 0);
+  {
+    uint8_t fa, fb;
+    flags_of(0, fa, fb);
+    load_plane(0, p0, fa | fb, pa, oAa, oBa);
+  }
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) car[a][b][c] = pk(0.f, 0.f);
+  double dacc = 0.0;
+  const long long sA_base = g.slot3(max(exa, 0), 0, max(ez, 0));
+  const long long sB_base = g.slot3(exa + 1, 0, max(ez, 0));
+
+  // One layer: element row ey = p0 + k between plane k (lo, already transformed) and plane
+  // k+1 (loaded into hi); writes the outputs of plane ey.
+  auto layer = [&](int k, P2 (&lo)[2][2][3], P2 (&hi)[2][2][3], float (&oA)[3], float (&oB)[3], float (&oAn)[3],
+                   float (&oBn)[3]) {
+    const int ey = p0 + k;
+    const long long sA = sA_base + (long long)ey * g.plane;
+    const long long sB = sB_base + (long long)ey * g.plane;
+    const bool wrA = (ey >= y0) && writerA, wrB = (ey >= y0) && writerB;
+    if (ok) ok = mbar_wait_fast(&bar[(k + 1) % NS], ((k + 1) / NS) & 1);
+    uint8_t fa, fb, fa1, fb1;
+    flags_of(k, fa, fb);
+    flags_of(k + 1, fa1, fb1);
+    const float* sE = reinterpret_cast<const float*>(smem + (k % NS) * Tile::STAGE + PT::E_OFF) + uoff;
+    const P2 Ee = pk(sE[0], sE[PK_ZB]);
+    load_plane(k + 1, ey + 1, fa | fb | fa1 | fb1, hi, oAn, oBn);
+    P2 uh[8][3];
+#pragma unroll
+    for (int hx = 0; hx < 2; ++hx)
+#pragma unroll
+      for (int hz = 0; hz < 2; ++hz)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (hx | hz) uh[hx | (hz << 2)][c] = lo[hx][hz][c] + hi[hx][hz][c];
+          uh[hx | 2 | (hz << 2)][c] = lo[hx][hz][c] - hi[hx][hz][c];
+        }
+    P2 vh[8][3];
+    khat_cube(kc, Ee, uh, vh);
+    P2 cur[2][2][3];
+#pragma unroll
+    for (int hx = 0; hx < 2; ++hx)
+#pragma unroll
+      for (int hz = 0; hz < 2; ++hz)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const P2 b = vh[hx | 2 | (hz << 2)][c];
+          if (hx | hz) {
+            const P2 a = vh[hx | (hz << 2)][c];
+            cur[hx][hz][c] = car[hx][hz][c] + (a + b);
+            car[hx][hz][c] = a - b;
+          } else {  // a = 0: carry kept as +b, subtracted next layer
+            cur[0][0][c] = b - car[0][0][c];
+            car[0][0][c] = b;
+          }
+        }
+    wht_xz(cur);  // cur[ax][az][c]: contributions of the pair's two elements to plane ey
+    P2 gx[2][3];
+#pragma unroll
+    for (int ax = 0; ax < 2; ++ax)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float2 up = cur[ax][1][c].v;
+        const P2 sh = pk(__shfl_up_sync(0xffffffffu, up.x, 1, 16), __shfl_up_sync(0xffffffffu, up.y, 1, 16));
+        gx[ax][c] = cur[ax][0][c] + sh;
+      }
+    float AuA[3], AuB[3], fromL[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      AuB[c] = gx[1][c].v.x + gx[0][c].v.y;
+      fromL[c] = __shfl_up_sync(0xffffffffu, gx[1][c].v.y, 16);
+    }
+    // the output plane's staged epilogue inputs, read before the stage is recycled
+    typename SE::In inA, inB;
+    {
+      const unsigned char* st = smem + (k % NS) * Tile::STAGE;
+      const unsigned char* spA[4];
+      const unsigned char* spB[4];
+#pragma unroll
+      for (int i = 0; i < SE::kN; ++i) {
+        const int t = SE::kT(i);
+        const int e = c0 * st_width(t) + (t == ST_BF16 ? zo8 : zo4) + zl;
+        spA[i] = st + Tile::s_off(i) + e * st_esize(t);
+        spB[i] = spA[i] + st_width(t) * st_esize(t);
+      }
+      constexpr int cs4 = Tile::ROWS * st_width(ST_F32), cs2 = Tile::ROWS * st_width(ST_BF16);
+      if (wrA) inA = epi.load(spA, cs4, cs2);
+      if (wrB) inB = epi.load(spB, cs4, cs2);
+    }
+    const int xb = k & 1;
+    if (xh == 1)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sX[xb][w][zl][c] = gx[1][c].v.y;
+    __syncthreads();
+    if (tid == 0 && k + NS < np) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(k + NS);
+    }
+    if (xh == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) fromL[c] = (w > 0) ? sX[xb][w - 1][zl][c] : 0.f;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) AuA[c] = gx[0][c].v.x + fromL[c];
+    if (wrA) {
+      float own[3], Au[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        own[c] = oA[c];
+        Au[c] = AuA[c];
+      }
+      if (fa) {
+        const uint8_t m = __ldg(mask + sA);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          if ((m >> c) & 1) {
+            own[c] = __ldg(u + c * n + sA);
+            Au[c] = own[c];
+          }
+      }
+      epi.apply(sA, own, Au, inA, dacc);
+    }
+    if (wrB) {
+      float own[3], Au[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        own[c] = oB[c];
+        Au[c] = AuB[c];
+      }
+      if (fb) {
+        const uint8_t m = __ldg(mask + sB);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          if ((m >> c) & 1) {
+            own[c] = __ldg(u + c * n + sB);
+            Au[c] = own[c];
+          }
+      }
+      epi.apply(sB, own, Au, inB, dacc);
+    }
+  };
+
+  int k = 0;
+  for (; k + 2 < np; k += 2) {
+    layer(k, pa, pb, oAa, oBa, oAb, oBb);
+    layer(k + 1, pb, pa, oAb, oBb, oAa, oBa);
+  }
+  if (k + 1 < np) layer(k, pa, pb, oAa, oBa, oAb, oBb);
+  if (!ok) atomicOr(err, 1);
+  finish_dot(epi, dacc, part, ticket, dot_dst);
+}
+
+}  // namespace edge

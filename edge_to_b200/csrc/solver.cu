@@ -25,6 +25,7 @@
 #include "fine_apply.cuh"
 #include "fine_tma.cuh"
 #include "fine_pk.cuh"
+#include "fine_cube.cuh"
 #include "misc.cuh"
 
 namespace edge {
@@ -210,8 +211,11 @@ struct Prob {
   bool use_tma = true;
   int tile_variant = 0;    // k_fine3_tma (BX, NS): 0 (8,4) 1 (8,3) 2 (8,2) 3 (4,4) 4 (4,3);
                            // FP32 only, k_fine3_pk (BX, NS, min blocks/SM): 5 (4,3,1) 6 (4,3,4)
-                           // 7 (2,3,8) 8 (4,4,4)
+                           // 7 (2,3,8) 8 (4,4,4); FP32 cube elements only, k_fine3_cube:
+                           // 9 (4,3,2) 10 (4,4,2) 11 (2,3,4) 12 (8,3,1)
   KHat3P k3p;              // packed transformed element operator (FP32 pairs)
+  KCube kcube;             // block form of the same operator (cube elements)
+  bool cube = false;       // kcube reproduces every entry of the transformed operator
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
   // grounded point springs (slot-layout flat index, user DOF index, stiffness)
   static constexpr int MAX_SPRINGS = 64;
@@ -312,11 +316,15 @@ struct CatScope {
   ~CatScope() { P.cur_cat = old; }
 };
 
+// The 3-D fine level pads z to 8 nodes so that its BF16 rows (the Jacobi diagonal) are
+// 16-byte aligned TMA sources; coarser levels and 2-D pad to 4.
+static int fine_zalign(int dim, int level) { return (dim == 3 && level == 0) ? 8 : 4; }
+
 static Geo level_geo(const Prob& P, int l) {
   int ne[3] = {P.nel[0], P.nel[1], P.nel[2]};
   for (int i = 0; i < l; ++i)
     for (int d = 0; d < 3; ++d) ne[d] /= 2;
-  return make_geo(P.dim, ne[0], ne[1], P.dim == 3 ? ne[2] : 0);
+  return make_geo(P.dim, ne[0], ne[1], P.dim == 3 ? ne[2] : 0, fine_zalign(P.dim, l));
 }
 
 // ------------------------------------------------------------------ TMA tensor maps
@@ -432,6 +440,50 @@ static KHat3P pack3(const KHat3<double>& k) {
   return o;
 }
 
+// Block form of a cube element's transformed operator (fine_cube.cuh): read the eight
+// coefficients off KHat3 and accept them only if the model reproduces all 576 entries.
+static bool cube_form(const KHat3<double>& k, KCube& out) {
+  const double nd = k.dg[0][1], no = k.of[0][1][1], sh = k.dg[1][1], bd = k.dg[0][3], bo = k.of[0][2][3],
+               td = k.dg[2][3], to = k.of[2][1][3], h7 = k.dg[0][7];
+  // model entries: M[(h,c)][(h2,c2)]
+  double M[8][3][8][3] = {};
+  auto set_sym = [&](int h1, int c1, int h2, int c2, double v) {
+    M[h1][c1][h2][c2] = v;
+    M[h2][c2][h1][c1] = v;
+  };
+  const int N[3][2] = {{1, 0}, {2, 1}, {4, 2}}, TW[3][2] = {{3, 2}, {5, 1}, {6, 0}};
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      M[N[a][0]][N[a][1]][N[b][0]][N[b][1]] = a == b ? nd : no;
+      M[TW[a][0]][TW[a][1]][TW[b][0]][TW[b][1]] = a == b ? td : to;
+    }
+  const int SH[3][4] = {{1, 1, 2, 0}, {1, 2, 4, 0}, {2, 2, 4, 1}}, BE[3][4] = {{3, 0, 6, 2}, {3, 1, 5, 2}, {5, 0, 6, 1}};
+  for (int i = 0; i < 3; ++i) {
+    M[SH[i][0]][SH[i][1]][SH[i][0]][SH[i][1]] = sh;
+    M[SH[i][2]][SH[i][3]][SH[i][2]][SH[i][3]] = sh;
+    set_sym(SH[i][0], SH[i][1], SH[i][2], SH[i][3], sh);
+    M[BE[i][0]][BE[i][1]][BE[i][0]][BE[i][1]] = bd;
+    M[BE[i][2]][BE[i][3]][BE[i][2]][BE[i][3]] = bd;
+    set_sym(BE[i][0], BE[i][1], BE[i][2], BE[i][3], bo);
+  }
+  for (int c = 0; c < 3; ++c) M[7][c][7][c] = h7;
+  // actual entries from KHat3 (diagonal + the coupling pattern), zero elsewhere
+  double mx = 0.0, dev = 0.0;
+  for (int h = 0; h < 8; ++h)
+    for (int c = 0; c < 3; ++c)
+      for (int h2 = 0; h2 < 8; ++h2)
+        for (int c2 = 0; c2 < 3; ++c2) {
+          double a = 0.0;
+          if (h2 == h && c2 == c) a = k.dg[c][h];
+          else if (c2 != c && h2 == (h ^ (1 << c) ^ (1 << c2)) && (((h >> c) & 1) != ((h >> c2) & 1))) a = k.of[c][c2][h];
+          mx = std::max(mx, std::fabs(a));
+          dev = std::max(dev, std::fabs(a - M[h][c][h2][c2]));
+        }
+  if (!(mx > 0.0) || dev > 1e-12 * mx) return false;
+  out = KCube{(float)(nd - no), (float)no, (float)sh, (float)bd, (float)bo, (float)(td - to), (float)to, (float)h7};
+  return true;
+}
+
 static size_t vbytes(int prec) { return prec == EDGE_FP64 ? sizeof(double) : sizeof(float); }
 
 // ------------------------------------------------------------------ launch helpers
@@ -514,6 +566,94 @@ static void fine3_pk_launch(Prob& P, const float* u, const float* E, Epi epi, do
          dot_dst, P.err);
 }
 
+// Staged form (fine_cube.cuh) of the solver's FP32 fine-level epilogues; `arr` receives the
+// arrays the kernel stages through TMA, in the order of SE::kT.
+template <class Epi> struct StagedOf {
+  static constexpr bool ok = false;
+};
+template <> struct StagedOf<EpiStore<float, float>> {
+  static constexpr bool ok = true;
+  using SE = SEStore;
+  static SE make(const EpiStore<float, float>& e, const void**) { return SE{e.out, e.n}; }
+};
+template <> struct StagedOf<EpiStoreDot<float>> {
+  static constexpr bool ok = true;
+  using SE = SEStoreDot;
+  static SE make(const EpiStoreDot<float>& e, const void**) { return SE{e.out, e.n}; }
+};
+template <> struct StagedOf<EpiResid<float, float, float>> {
+  static constexpr bool ok = true;
+  using SE = SEResid;
+  static SE make(const EpiResid<float, float, float>& e, const void** arr) {
+    arr[0] = e.b;
+    return SE{e.r, e.n};
+  }
+};
+template <> struct StagedOf<EpiJacobi<float, float, __nv_bfloat16>> {
+  static constexpr bool ok = true;
+  using SE = SEJacobi;
+  static SE make(const EpiJacobi<float, float, __nv_bfloat16>& e, const void** arr) {
+    arr[0] = e.b;
+    arr[1] = e.dinv;
+    return SE{e.xo, e.omega, e.wscale, e.n, 0.f};
+  }
+};
+template <bool DOT, typename TV> struct StagedOf<EpiJacobiAdd<float, float, __nv_bfloat16, float, DOT, TV>> {
+  static constexpr bool ok = !DOT || std::is_same<TV, double>::value;  // the staged dot vector is FP64
+  using SE = SEJacobiAdd<DOT>;
+  static SE make(const EpiJacobiAdd<float, float, __nv_bfloat16, float, DOT, TV>& e, const void** arr) {
+    arr[0] = e.b;
+    arr[1] = e.dinv;
+    arr[2] = e.xbase;
+    if (DOT) arr[3] = e.dotv;
+    return SE{e.xo, e.omega, e.wscale, e.n, 0.f};
+  }
+};
+
+// Tensor map of a staged epilogue array [3][n] (slot layout) of element type t: boxes of
+// st_width(t) z-nodes x 4*BX node rows x 1 plane x 3 components.
+template <int BX>
+static const CUtensorMap& stage_map(Prob& P, const void* base, int t) {
+  auto key = std::make_pair(base, 4000 + t * 16 + BX);
+  auto it = P.tmaps.find(key);
+  if (it != P.tmaps.end()) return it->second;
+  const Geo& g = P.g0;
+  const uint64_t sz = (uint64_t)st_esize(t);
+  const CUtensorMapDataType dt = t == ST_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                 : t == ST_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                               : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  uint64_t dims[4] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny, 3};
+  uint64_t str[3] = {g.pz * sz, g.plane * sz, g.n * sz};
+  uint32_t box[4] = {(uint32_t)st_width(t), 4 * BX, 1, 3};
+  return P.tmaps.emplace(key, encode_map(base, dt, 4, dims, str, box)).first->second;
+}
+
+template <class Epi, int BX, int NS, int MINB>
+static void fine3_cube_launch(Prob& P, const float* u, const float* E, Epi epi0, double* dot_dst) {
+  using ST = StagedOf<Epi>;
+  using SE = typename ST::SE;
+  const void* arr[4] = {nullptr, nullptr, nullptr, nullptr};
+  SE epi = ST::make(epi0, arr);
+  const Geo& g = P.g0;
+  constexpr int smem = cube_smem_bytes<BX, NS, SE>();
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(k_fine3_cube<SE, BX, NS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  const CUtensorMap& mu = pk_map<BX>(P, u, 0);
+  const CUtensorMap* ms[4];
+  for (int i = 0; i < 4; ++i) ms[i] = i < SE::kN ? &stage_map<BX>(P, arr[i], SE::kT(i)) : &mu;
+  const unsigned tz = cdiv(g.nz, 15), tx = cdiv(g.nx, 4 * BX - 1);
+  const long long want = 148LL * P.blocks_per_sm;
+  long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
+  chunks = std::min<long long>(chunks, g.ny);
+  const int ly = (int)cdiv(g.ny, chunks);
+  launch(P, k_fine3_cube<SE, BX, NS, MINB>, dim3(tz, tx, cdiv(g.ny, ly)), dim3(32, BX), smem, g, mu,
+         pk_flag_map<BX>(P), pk_map<BX>(P, E, 1), u, (const uint8_t*)P.mask, *ms[0], *ms[1], *ms[2], *ms[3],
+         P.kcube, ly, epi, P.part, P.ticket, dot_dst, P.err);
+}
+
 // Fine-level operator with epilogue.  u, E in type T.  When profiling is on, each launch is
 // bracketed by CUDA events on the problem's stream and its algorithmic bytes recorded:
 // input vector + E + the epilogue's per-DOF traffic (BC mask excluded).
@@ -527,7 +667,19 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
   if (P.ei.wht) {
     bool packed = false;
     if constexpr (std::is_same<T, float>::value) {
-      if (P.dim == 3 && P.use_tma && P.tile_variant >= 5) {
+      if constexpr (StagedOf<Epi>::ok) {
+        if (P.dim == 3 && P.use_tma && P.tile_variant >= 9 && P.cube) {
+          switch (P.tile_variant) {
+            case 9: fine3_cube_launch<Epi, 4, 3, 2>(P, u, E, epi, dot_dst); break;
+            case 10: fine3_cube_launch<Epi, 4, 4, 2>(P, u, E, epi, dot_dst); break;
+            case 11: fine3_cube_launch<Epi, 2, 3, 4>(P, u, E, epi, dot_dst); break;
+            default: fine3_cube_launch<Epi, 8, 3, 1>(P, u, E, epi, dot_dst); break;
+          }
+          packed = true;
+        }
+      }
+      if (packed) {
+      } else if (P.dim == 3 && P.use_tma && P.tile_variant >= 5) {
         switch (P.tile_variant) {
           case 5: fine3_pk_launch<Epi, 4, 3, 1>(P, u, E, epi, dot_dst); break;
           case 6: fine3_pk_launch<Epi, 4, 3, 4>(P, u, E, epi, dot_dst); break;
@@ -1097,11 +1249,14 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     P.dim = dim;
     P.prec = precision;
     for (int d = 0; d < dim; ++d) P.nel[d] = nel[d];
-    P.g0 = make_geo(dim, nel[0], nel[1], dim == 3 ? nel[2] : 0);
+    P.g0 = make_geo(dim, nel[0], nel[1], dim == 3 ? nel[2] : 0, fine_zalign(dim, 0));
     P.n_el = (long long)nel[0] * nel[1] * (dim == 3 ? nel[2] : 1);
     P.n_dof = (long long)P.g0.nx * P.g0.ny * P.g0.nz * dim;
     analyse_element(dim, K0, P.ei);
-    if (dim == 3) P.k3p = pack3(P.ei.k3);
+    if (dim == 3) {
+      P.k3p = pack3(P.ei.k3);
+      P.cube = P.ei.wht && cube_form(P.ei.k3, P.kcube);
+    }
     const int nk = P.ei.nk;
     P.dK0b = P.alloc<double>(nk * nk);
     CK(cudaMemcpy(P.dK0b, P.ei.K0b, nk * nk * sizeof(double), cudaMemcpyHostToDevice));
@@ -1170,17 +1325,64 @@ int edge_set_stream(edge_problem* p, void* stream) {
 }
 
 int edge_uses_transform(const edge_problem* p) { return p && p->P.ei.wht ? 1 : 0; }
+int edge_uses_cube_form(const edge_problem* p) { return p && p->P.cube ? 1 : 0; }
 
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm) {
   API_BEGIN
-  if (!p || variant < 0 || variant > 8 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
+  if (!p || variant < 0 || variant > 12 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
   p->P.tile_variant = variant;
   p->P.blocks_per_sm = blocks_per_sm;
   API_END
 }
 
+// Average device time of `reps` fine-operator launches with the current tile, the smoother
+// sweep epilogue (sweep = true; needs the multigrid allocated) or the plain product; buffer
+// contents do not matter for timing.
+static double time_fine(Prob& P, int precision, bool sweep, int reps) {
+  const Geo& g = P.g0;
+  auto run = [&]() {
+    if (precision == EDGE_FP64) {
+      if (sweep) {
+        EpiJacobi<double, double, double> e{P.b64, (const double*)P.lv[0].dinv, P.r64, &P.st->omega, 1.0, g.n};
+        fine_apply<double>(P, P.x64, e, nullptr);
+      } else {
+        EpiStore<double, double> e{P.r64, g.n};
+        fine_apply<double>(P, P.x64, e, nullptr);
+      }
+    } else {
+      if (sweep) {
+        EpiJacobi<float, float, __nv_bfloat16> e{P.r32, (const __nv_bfloat16*)P.lv[0].dinv, (float*)P.q,
+                                                 &P.st->omega, 1.0, g.n};
+        fine_apply<float>(P, (const float*)P.p, e, nullptr);
+      } else {
+        EpiStore<float, float> e{(float*)P.q, g.n};
+        fine_apply<float>(P, (const float*)P.p, e, nullptr);
+      }
+    }
+  };
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  run();
+  CK(cudaEventRecord(a, P.stream));
+  for (int r = 0; r < reps; ++r) run();
+  CK(cudaEventRecord(b, P.stream));
+  CK(cudaEventSynchronize(b));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms / reps;
+}
+
+static bool can_time_sweep(const Prob& P, int precision) {
+  if (P.n_level < 0 || P.lv.empty() || !P.lv[0].dinv) return false;
+  return precision == EDGE_FP64 ? P.prec == EDGE_FP64 : P.prec == EDGE_MIXED;
+}
+
 // Autotuner: times every (tile variant, y-chunking) of the fine operator on the current E
-// with the product epilogue in the given precision and keeps the fastest.  Needs E set.
+// (smoother sweep once the multigrid is configured, the most frequent fine-level launch;
+// else the plain product) and keeps the fastest.  Needs E set.
 int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms, int* best_variant,
                        int* best_bps) {
   API_BEGIN
@@ -1193,62 +1395,47 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
     if (best_bps) *best_bps = P.blocks_per_sm;
     return EDGE_OK;
   }
-  const Geo& g = P.g0;
-  cudaEvent_t a, b;
-  CK(cudaEventCreate(&a));
-  CK(cudaEventCreate(&b));
   double best = 1e30;
   int bv = P.tile_variant, bb = P.blocks_per_sm;
   const int bps_list[4] = {2, 4, 8, 16};
-  const int nvar = precision == EDGE_FP64 ? 5 : 9;  // variants 5..8: packed-pair FP32 kernel
+  // variants 5..8: packed-pair FP32 kernel; 9..12: its cube-element form
+  const int nvar = precision == EDGE_FP64 ? 5 : (P.cube ? 13 : 9);
+  const bool sweep = can_time_sweep(P, precision);
   for (int v = 0; v < nvar; ++v)
     for (int bi = 0; bi < 4; ++bi) {
       P.tile_variant = v;
       P.blocks_per_sm = bps_list[bi];
-      // time the smoother sweep (the most frequent fine-level launch) once the multigrid is
-      // configured, else the plain product; buffer contents do not matter for timing
-      const bool sweep = P.n_level >= 0 && !P.lv.empty() && P.lv[0].dinv;
-      auto run = [&]() {
-        if (precision == EDGE_FP64) {
-          if (sweep) {
-            EpiJacobi<double, double, double> e{P.b64, (const double*)P.lv[0].dinv, P.r64, &P.st->omega, 1.0, g.n};
-            fine_apply<double>(P, P.x64, e, nullptr);
-          } else {
-            EpiStore<double, double> e{P.r64, g.n};
-            fine_apply<double>(P, P.x64, e, nullptr);
-          }
-        } else {
-          if (sweep && P.prec == EDGE_MIXED) {
-            EpiJacobi<float, float, __nv_bfloat16> e{P.r32, (const __nv_bfloat16*)P.lv[0].dinv, (float*)P.q,
-                                                     &P.st->omega, 1.0, g.n};
-            fine_apply<float>(P, (const float*)P.p, e, nullptr);
-          } else {
-            EpiStore<float, float> e{(float*)P.q, g.n};
-            fine_apply<float>(P, (const float*)P.p, e, nullptr);
-          }
-        }
-      };
-      run();
-      CK(cudaEventRecord(a, P.stream));
-      for (int r = 0; r < reps; ++r) run();
-      CK(cudaEventRecord(b, P.stream));
-      CK(cudaEventSynchronize(b));
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, a, b));
-      if (ms / reps < best) {
-        best = ms / reps;
+      const double ms = time_fine(P, precision, sweep, reps);
+      if (ms < best) {
+        best = ms;
         bv = v;
         bb = bps_list[bi];
       }
     }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
   check_err(P);
   P.tile_variant = bv;
   P.blocks_per_sm = bb;
   if (best_ms) *best_ms = best;
   if (best_variant) *best_variant = bv;
   if (best_bps) *best_bps = bb;
+  API_END
+}
+
+int edge_time_fine(edge_problem* p, int precision, int variant, int blocks_per_sm, int sweep, int reps,
+                   double* ms) {
+  API_BEGIN
+  if (!p || !ms || reps < 1 || variant < 0 || variant > 12 || blocks_per_sm < 1 || blocks_per_sm > 64)
+    fail(EDGE_EINVAL, "bad argument");
+  Prob& P = p->P;
+  if (!P.has_rho) fail(EDGE_ESTATE, "rho not set");
+  if (sweep && !can_time_sweep(P, precision)) fail(EDGE_ESTATE, "the sweep needs the multigrid of this precision");
+  const int v0 = P.tile_variant, b0 = P.blocks_per_sm;
+  P.tile_variant = variant;
+  P.blocks_per_sm = blocks_per_sm;
+  *ms = time_fine(P, precision, sweep != 0, reps);
+  P.tile_variant = v0;
+  P.blocks_per_sm = b0;
+  check_err(P);
   API_END
 }
 

@@ -67,15 +67,25 @@ int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
 /* Tuning/testing switch: 1 (default) stages 3-D fine-level tiles with TMA, 0 uses the
  * cooperative-load version of the same kernel. */
 int edge_set_tma(edge_problem* p, int enable);
-/* Fine-kernel tile: variant 0..4 = (warps, TMA stages) (8,4) (8,3) (8,2) (4,4) (4,3), and
- * the target of resident blocks per SM that sets the y-chunking of the grid. */
+/* Fine-kernel tile: variant 0..4 = k_fine3_tma (warps, TMA stages) (8,4) (8,3) (8,2) (4,4)
+ * (4,3); FP32 only: 5..8 = packed-pair k_fine3_pk, 9..12 = its cube-element block form
+ * k_fine3_cube (used when edge_uses_cube_form is 1, else 9..12 run k_fine3_pk); and the
+ * target of resident blocks per SM that sets the y-chunking of the grid. */
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm);
 /* Autotuner: times every tile variant and y-chunking on the current density with the plain
  * operator in `precision` (reps launches each), keeps the fastest, reports it. */
 int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms, int* best_variant,
                        int* best_bps);
+/* Benchmark helper: average device time (ms) of `reps` fine-operator launches with the given
+ * tile, with the smoother-sweep epilogue (sweep != 0; needs edge_mg_config/solve of that
+ * precision) or the plain product.  The problem's own tile choice is left unchanged. */
+int edge_time_fine(edge_problem* p, int precision, int variant, int blocks_per_sm, int sweep, int reps,
+                   double* ms);
 /* 1 when the element matrix has the box structure used by the transform kernels */
 int edge_uses_transform(const edge_problem* p);
+/* 1 when the transformed element matrix has the cube block form (eight coefficients) used by
+ * the k_fine3_cube tiles (equal edge lengths, isotropic material) */
+int edge_uses_cube_form(const edge_problem* p);
 
 /* ---- geometric multigrid PCG.  Replaces CuMultiGrid (solvers/_multigrid_cuda.py:15-242).
  * cycle_w != 0 reproduces cycle == 'w' (second coarse visit on the levels in w_levels).

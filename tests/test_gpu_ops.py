@@ -273,8 +273,9 @@ def test_fp32_operator_accuracy():
 
 @pytest.mark.parametrize("nel", [(4, 4, 4), (7, 5, 3), (40, 9, 33), (9, 33, 65), (3, 3, 130), (20, 20, 47), (66, 17, 31)])
 def test_fp32_tile_variants_agree(nel):
-    """Every FP32 fine-kernel tile (k_fine3_tma 0-4, packed-pair k_fine3_pk 5-8) gives K(E) u
-    to single precision on ragged grids with boundary conditions and void elements."""
+    """Every FP32 fine-kernel tile (k_fine3_tma 0-4, packed-pair k_fine3_pk 5-8, its cube form
+    k_fine3_cube 9-12) gives K(E) u to single precision on ragged grids with boundary
+    conditions and void elements."""
     import torch
     import edge_to_b200 as eb
     from edge_to_b200 import _lib
@@ -291,7 +292,8 @@ def test_fp32_tile_variants_agree(nel):
     ref = ops.assemble(g, elements.hex8_stiffness(1, 1, 1, 1, 0.3), E, cons) @ u
     ut = torch.as_tensor(u, device="cuda")
     outs = []
-    for v in range(9):
+    assert _lib.lib().edge_uses_cube_form(k.handle) == 1
+    for v in range(13):
         for bps in (2, 16):
             _lib.call("edge_set_fine_tile", k.handle, v, bps)
             b = torch.empty_like(ut)
@@ -317,7 +319,7 @@ def test_packed_kernel_in_mixed_solve():
     k.set_rho(torch.as_tensor(E, device="cuda"))
     s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision="mixed", autotune=False)
     res = []
-    for v in (4, 5, 8):
+    for v in (4, 5, 8, 9, 10):
         _lib.call("edge_set_fine_tile", k.handle, v, 8)
         x, r = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
         res.append((x.cpu().numpy().copy(), s.last_iters, r))
