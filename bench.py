@@ -150,6 +150,8 @@ def timed_steps(opt, rho, dr, it, steps, ws, local, profile=True):
     clocks.start()
     if profile:
         _lib.call("edge_profile_begin", h, 200000)
+    n_before = ctypes.c_longlong()
+    _lib.call("edge_launch_count", h, ctypes.byref(n_before))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -164,14 +166,17 @@ def timed_steps(opt, rho, dr, it, steps, ws, local, profile=True):
     e1.record(stream)
     torch.cuda.synchronize()
     _barrier(ws)
+    n_after = ctypes.c_longlong()
+    _lib.call("edge_launch_count", h, ctypes.byref(n_after))
     prof = None
     if profile:
         kms, kby, kl, tl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int(), ctypes.c_longlong()
         _lib.call("edge_profile_end", h, ctypes.byref(kms), ctypes.byref(kby), ctypes.byref(kl), ctypes.byref(tl))
-        prof = dict(kernel_ms=kms.value, kernel_bytes=kby.value, kernel_launches=kl.value, launches=int(tl.value))
+        prof = dict(kernel_ms=kms.value, kernel_bytes=kby.value, kernel_launches=kl.value)
     clk = clocks.stop()
     t_ms = _max_over_ranks(e0.elapsed_time(e1), ws)
-    return dict(rho=rho, dr=dr, it=it, t_ms=t_ms, pcg=pcg, compliance=float(c), prof=prof, clocks=clk)
+    return dict(rho=rho, dr=dr, it=it, t_ms=t_ms, pcg=pcg, compliance=float(c), prof=prof, clocks=clk,
+                launches=n_after.value - n_before.value)
 
 
 def _barrier(ws):
@@ -214,9 +219,14 @@ def run_ours(args, cfg_name):
     opt, rho = build_problem(cfg, args.precision)
     rho, dr, it = warm(opt, rho, args.warmup)
 
-    # ---------------- device-timed region: inputs resident in HBM
-    m = timed_steps(opt, rho, dr, it, args.steps, ws, local)
-    rho, dr, it, t_ms, prof = m["rho"], m["dr"], m["it"], m["t_ms"], m["prof"]
+    # ---------------- device-timed region: inputs resident in HBM; each solve is one CUDA
+    # graph launch (per-launch events cannot sit inside a graph, so none are recorded here)
+    m = timed_steps(opt, rho, dr, it, args.steps, ws, local, profile=False)
+    rho, dr, it, t_ms = m["rho"], m["dr"], m["it"], m["t_ms"]
+    # ---------------- one more step with CUDA events around every fine-operator launch (the
+    # host-driven loop, same launches) for the live roofline of the dominant kernel
+    pm = timed_steps(opt, rho, dr, it, 1, ws, local, profile=True)
+    rho, dr, it, prof = pm["rho"], pm["dr"], pm["it"], pm["prof"]
 
     # ---------------- end-to-end: design on the host, copies inside the timed region
     stream = torch.cuda.current_stream()
@@ -285,16 +295,18 @@ def run_ours(args, cfg_name):
                    "l2": "working set > 126 MB L2 (no flush needed)",
                    "pcg_iters_per_step": m["pcg"], "compliance_last": m["compliance"],
                    "fine_tile": tuned},
-        "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_tma + fused epilogues)",
+        "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_cube/_pk/_tma + fused epilogues)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                      "traffic": traffic, "traffic_case": "ncu DRAM bytes of one plain-product launch"
                      if traffic else None, "launches": prof["kernel_launches"], "kernel_ms": kms,
                      "algorithmic_bytes_per_launch": kby / max(1, prof["kernel_launches"]),
-                     "share_of_step": kms / t_ms if t_ms else None},
+                     "share_of_step": kms / pm["t_ms"] if pm["t_ms"] else None,
+                     "timing": "CUDA events around every fine-operator launch of one SIMP step run right "
+                               "after the timed steps (host-driven PCG loop, same kernels and tiles)"},
         "e2e": {"value": args.steps / (e2e_ms / 1e3), "unit": "iter/s", "h2d_bytes_per_step": 8 * n_el,
                 "d2h_bytes_per_step": 8 * n_el + 8},
-        "gpu_launches": prof["launches"],
+        "gpu_launches": m["launches"],
         "clocks": m["clocks"],
     }
     if fp64 is not None:
@@ -394,11 +406,17 @@ def run_tiles(args, cfg_name):
     import torch
     from edge_to_b200 import _lib
     opt, rho = build_problem(CONFIGS[cfg_name], args.precision)
-    opt.solve_and_process(rho, 0)
-    torch.cuda.synchronize()
     h = opt.kernel.handle
+    if args.tile is None:
+        opt.solve_and_process(rho, 0)
+    else:  # one tile (profiling): hierarchy built without a solve, so few launches precede it
+        opt.kernel.set_rho(torch.full((opt.kernel.n_elements,), CONFIGS[cfg_name]["vf"] ** 3, dtype=torch.float64,
+                                      device="cuda"))
+        opt.solver._configure()
+        _lib.call("edge_mg_setup", h)
+    torch.cuda.synchronize()
     prec = 1 if args.precision == "mixed" else 0
-    nvar = 5 if args.precision == "fp64" else (13 if _lib.lib().edge_uses_cube_form(h) else 9)
+    nvar = 5 if args.precision == "fp64" else (15 if _lib.lib().edge_uses_cube_form(h) else 9)
     k = opt.kernel
     n_dof, n_el = k.shape[0], k.n_elements
     w = 8 if args.precision == "fp64" else 4
@@ -407,8 +425,10 @@ def run_tiles(args, cfg_name):
     peak, kind = peaks()
     rows = []
     ms = ctypes.c_double()
-    for v in range(nvar):
-        for bps in (2, 4, 8, 16):
+    variants = [args.tile] if args.tile is not None else list(range(nvar))
+    bps_list = [args.tile_bps] if args.tile is not None else [2, 4, 8, 16]
+    for v in variants:
+        for bps in bps_list:
             r = {"variant": v, "bps": bps}
             for sweep in (0, 1):
                 _lib.call("edge_time_fine", h, prec, v, bps, sweep, max(1, args.steps), ctypes.byref(ms))
@@ -416,8 +436,24 @@ def run_tiles(args, cfg_name):
                 r["sweep_us" if sweep else "plain_us"] = round(ms.value * 1e3, 2)
                 r["sweep_frac" if sweep else "plain_frac"] = round(b / (ms.value / 1e3) / 1e9 / peak, 3)
             rows.append(r)
+    levels = []
+    cfg = CONFIGS[cfg_name]
+    for lvl in range(1, cfg["n_level"]):
+        ne = [v >> lvl for v in cfg["nel"]]
+        nodes = (ne[0] + 1) * (ne[1] + 1) * (ne[2] + 1)
+        # stencil (123 coefficients) + u, b, Dinv, out per node
+        b = nodes * (123 * w + 4 * 3 * w)
+        row = {"level": lvl, "nodes": nodes}
+        for name, qmax in (("thread", 0), ("quad", 1 << 40)):
+            _lib.call("edge_set_stencil_quad", h, qmax)
+            _lib.call("edge_time_level", h, lvl, max(1, args.steps), ctypes.byref(ms))
+            row[name + "_us"] = round(ms.value * 1e3, 2)
+            row[name + "_frac"] = round(b / (ms.value / 1e3) / 1e9 / peak, 3)
+        levels.append(row)
+    _lib.call("edge_set_stencil_quad", h, 200000)
     return {"mode": "tiles", "workload": cfg_name, "precision": args.precision, "peak_GBps": peak,
-            "peak_source": kind, "plain_bytes": plain_bytes, "sweep_bytes": sweep_bytes, "tiles": rows}
+            "peak_source": kind, "plain_bytes": plain_bytes, "sweep_bytes": sweep_bytes, "tiles": rows,
+            "stencil_levels": levels}
 
 
 def run_reference(args, cfg_name):
@@ -460,7 +496,7 @@ def main():
     ap.add_argument("--config", default="cantilever_256x128x128", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles"])
-    ap.add_argument("--tile", type=int, default=None, help="matvec mode: fine-kernel tile variant (0-12)")
+    ap.add_argument("--tile", type=int, default=None, help="matvec/tiles mode: fine-kernel tile variant (0-14)")
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--breakdown", action="store_true",
                     help="extra untimed step with per-category launch timing (events on every launch)")

@@ -38,6 +38,10 @@ _SIGS = {
     "edge_set_tma": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_fine_tile": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
     "edge_autotune_fine": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_double_p, c_int_p, c_int_p]),
+    "edge_set_stencil_quad": (ctypes.c_int, [vp, ctypes.c_longlong]),
+    "edge_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_launch_count": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "edge_time_level": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_double_p]),
     "edge_time_fine": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       c_double_p]),
     "edge_mg_config": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,

@@ -127,6 +127,71 @@ k_st3_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi 
   finish_dot(epi, dacc, part, ticket, dot_dst);
 }
 
+// Latency-oriented variant for small levels, where a sweep is a handful of dependent load
+// round trips rather than a bandwidth problem: four lanes per node share the 26 neighbour
+// terms (term t = 4m + lane; terms 0..12 are the stored upper blocks, 13..25 the transposed
+// blocks of the lower neighbours), every load is unconditional (a neighbour outside the grid
+// reads this node's own slot and is replaced by zero), the four partial sums are combined
+// by two xor-shuffles (the same fixed order on every lane, so results are reproducible) and
+// lane 0 of the group adds the centre block and runs the epilogue.
+template <typename T, typename TS, class Epi>
+__global__ void __launch_bounds__(128)
+k_st3_apply_q(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
+              double* dot_dst) {
+  const long long s0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 2;
+  const int q = threadIdx.x & 3;
+  const long long n = g.n;
+  epi.init();
+  double dacc = 0.0;
+  const long long s = s0 < n ? s0 : n - 1;
+  const int k = (int)(s % g.pz), i = (int)((s / g.pz) % g.nx), j = (int)(s / g.plane);
+  const bool valid = s0 < n && k < g.nz;
+  T Au[3] = {T(0), T(0), T(0)};
+#pragma unroll
+  for (int m = 0; m < 7; ++m) {
+    const int t = 4 * m + q;
+    const bool lower = t >= 13;
+    const int nbi = min(lower ? t - 13 : t, 12);
+    const int nb = 14 + nbi;
+    const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
+    const int sg = lower ? -1 : 1;
+    const bool in = t < 26 && valid && i + sg * dx >= 0 && i + sg * dx < g.nx && j + sg * dy >= 0 &&
+                    j + sg * dy < g.ny && k + sg * dz >= 0 && k + sg * dz < g.nz;
+    const long long off = sg * ((long long)dy * g.plane + (long long)dx * g.pz + dz);
+    const long long sn = in ? s + off : s;
+    const TS* Sb = S + (long long)(6 + nbi * 9) * n + (lower ? sn : s);
+    const int cs = lower ? 1 : 3, ds = lower ? 3 : 1;
+    T v[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const T a = __ldg(u + c * n + sn);
+      v[c] = in ? a : T(0);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      Au[c] += Conv<T>::from(__ldg(Sb + (long long)(c * cs) * n)) * v[0] +
+               Conv<T>::from(__ldg(Sb + (long long)(c * cs + ds) * n)) * v[1] +
+               Conv<T>::from(__ldg(Sb + (long long)(c * cs + 2 * ds) * n)) * v[2];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Au[c] += __shfl_xor_sync(0xffffffffu, Au[c], 1);
+    Au[c] += __shfl_xor_sync(0xffffffffu, Au[c], 2);
+  }
+  if (q == 0 && valid) {
+    const T u0 = __ldg(u + s), u1 = __ldg(u + n + s), u2 = __ldg(u + 2 * n + s);
+    const T c00 = Conv<T>::from(__ldg(S + s)), c01 = Conv<T>::from(__ldg(S + n + s)),
+            c02 = Conv<T>::from(__ldg(S + 2 * n + s)), c11 = Conv<T>::from(__ldg(S + 3 * n + s)),
+            c12 = Conv<T>::from(__ldg(S + 4 * n + s)), c22 = Conv<T>::from(__ldg(S + 5 * n + s));
+    Au[0] += c00 * u0 + c01 * u1 + c02 * u2;
+    Au[1] += c01 * u0 + c11 * u1 + c12 * u2;
+    Au[2] += c02 * u0 + c12 * u1 + c22 * u2;
+    T own[3] = {u0, u1, u2};
+    epi(s, 3, own, Au, dacc);
+  }
+  finish_dot(epi, dacc, part, ticket, dot_dst);
+}
+
 template <typename T, typename TS, class Epi>
 __global__ void __launch_bounds__(128)
 k_st2_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,

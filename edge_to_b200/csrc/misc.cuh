@@ -336,7 +336,9 @@ struct PcgState {
   double res;     // ||r|| / ||f||
   double omega;   // smoother weight for the next V-cycle
   double tol, min_omega, d_omega;
+  double last_replace;      // ||r||/||f|| at the last true-residual replacement (mixed precision)
   int iter, maxiter, done;  // done: 1 converged, 2 maxiter
+  int n_true;               // replacements made inside the iteration loop
 };
 
 // x += alpha p ; r -= alpha q ; rr = r.r with alpha = rz_new / pq.  The finisher
@@ -387,6 +389,8 @@ __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__
 __global__ void k_pcg_true_res(PcgState* st) {
   const double R = sqrt(st->rr) / sqrt(st->bb);
   st->res = R;
+  st->last_replace = R;
+  st->n_true += 1;
   if (R < st->tol) {
     st->done = 1;
   } else {
@@ -396,12 +400,23 @@ __global__ void k_pcg_true_res(PcgState* st) {
   }
 }
 
-// p = z + beta p
+// p = z + beta p, or p = z before the first iteration (iter == 0)
 template <typename TP>
 __global__ void k_pcg_p(long long n, TP* __restrict__ p, const TP* __restrict__ z, const PcgState* st) {
-  const double beta = st->rz_new / st->rz;
+  const bool first = st->iter == 0;
+  const double beta = first ? 0.0 : st->rz_new / st->rz;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    p[i] = Conv<TP>::from((double)Conv<double>::from(z[i]) + beta * (double)Conv<double>::from(p[i]));
+    p[i] = first ? z[i] : Conv<TP>::from((double)Conv<double>::from(z[i]) + beta * (double)Conv<double>::from(p[i]));
+}
+
+// Loop control of the graph-captured PCG: the while node repeats while no stop reason is set;
+// the if node (mixed precision) computes a true residual when the recurrence has converged
+// or has dropped by `drop` since the last replacement.
+__global__ void k_cond_while(cudaGraphConditionalHandle h, const PcgState* st) {
+  cudaGraphSetConditional(h, st->done == 0 ? 1u : 0u);
+}
+__global__ void k_cond_replace(cudaGraphConditionalHandle h, const PcgState* st, double drop) {
+  cudaGraphSetConditional(h, (st->done == 1 || st->res < drop * st->last_replace) ? 1u : 0u);
 }
 
 // ------------------------------------------------------------------ point springs and adjoint sensitivity

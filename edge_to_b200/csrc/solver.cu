@@ -212,11 +212,20 @@ struct Prob {
   int tile_variant = 0;    // k_fine3_tma (BX, NS): 0 (8,4) 1 (8,3) 2 (8,2) 3 (4,4) 4 (4,3);
                            // FP32 only, k_fine3_pk (BX, NS, min blocks/SM): 5 (4,3,1) 6 (4,3,4)
                            // 7 (2,3,8) 8 (4,4,4); FP32 cube elements only, k_fine3_cube:
-                           // 9 (4,3,2) 10 (4,4,2) 11 (2,3,4) 12 (8,3,1)
+                           // 9 (4,3,2) 10 (4,4,2) 11 (2,3,4) 12 (8,3,1) 13 (4,3,4) 14 (4,4,4)
   KHat3P k3p;              // packed transformed element operator (FP32 pairs)
   KCube kcube;             // block form of the same operator (cube elements)
   bool cube = false;       // kcube reproduces every entry of the transformed operator
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
+  long long st_quad_max = 200000;  // 3-D stencil levels with at most this many slots use k_st3_apply_q
+  // CUDA graph of one solve (hierarchy set-up + the whole PCG loop under a while node)
+  bool use_graph = true;
+  cudaGraph_t sg_graph = nullptr;
+  cudaGraphExec_t sg_exec = nullptr;
+  std::vector<double> sg_key;
+  long long sg_pro = 0, sg_body = 0, sg_if = 0;  // launches per section, for the launch tally
+  cudaStream_t cap[3] = {nullptr, nullptr, nullptr};
+  std::string graph_error;
   // grounded point springs (slot-layout flat index, user DOF index, stiffness)
   static constexpr int MAX_SPRINGS = 64;
   int n_springs = 0;
@@ -279,6 +288,10 @@ struct Prob {
     return (T*)ptr;
   }
   ~Prob() {
+    if (sg_exec) cudaGraphExecDestroy(sg_exec);
+    if (sg_graph) cudaGraphDestroy(sg_graph);
+    for (int i = 0; i < 3; ++i)
+      if (cap[i]) cudaStreamDestroy(cap[i]);
     for (void* a : allocs) cudaFree(a);
     if (st_h) cudaFreeHost(st_h);
     if (oc_h) cudaFreeHost(oc_h);
@@ -673,7 +686,9 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
             case 9: fine3_cube_launch<Epi, 4, 3, 2>(P, u, E, epi, dot_dst); break;
             case 10: fine3_cube_launch<Epi, 4, 4, 2>(P, u, E, epi, dot_dst); break;
             case 11: fine3_cube_launch<Epi, 2, 3, 4>(P, u, E, epi, dot_dst); break;
-            default: fine3_cube_launch<Epi, 8, 3, 1>(P, u, E, epi, dot_dst); break;
+            case 12: fine3_cube_launch<Epi, 8, 3, 1>(P, u, E, epi, dot_dst); break;
+            case 13: fine3_cube_launch<Epi, 4, 3, 4>(P, u, E, epi, dot_dst); break;
+            default: fine3_cube_launch<Epi, 4, 4, 4>(P, u, E, epi, dot_dst); break;
           }
           packed = true;
         }
@@ -741,7 +756,10 @@ static void fine_apply_dense(Prob& P, const T* u, Epi epi, double* dot_dst) {
 template <typename T, class Epi>
 static void st_apply(Prob& P, const Geo& g, const T* u, const T* S, Epi epi, double* dot_dst) {
   CatScope cat(P, CAT_STENCIL);
-  if (g.dim == 3)
+  if (g.dim == 3 && g.n <= P.st_quad_max)
+    launch(P, k_st3_apply_q<T, T, Epi>, dim3(cdiv(g.n * 4, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket,
+           dot_dst);
+  else if (g.dim == 3)
     launch(P, k_st3_apply<T, T, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
   else
     launch(P, k_st2_apply<T, T, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
@@ -796,13 +814,18 @@ __global__ void k_pcg_init(PcgState* st, double tol, int maxiter, double min_ome
   st->done = 0;
   st->rz = st->rz_new = st->pq = st->rr = st->alpha = st->beta = 0.0;
   st->res = 0.0;
+  st->last_replace = 1.0;
+  st->n_true = 0;
 }
-__global__ void k_pcg_check_bb(PcgState* st) {
+__global__ void k_pcg_check_bb(PcgState* st, const int* chol_status) {
   // ||f|| == 0: nothing to solve, report residual 0 like a converged solve
   if (st->bb == 0.0) {
     st->done = 1;
     st->res = 0.0;
   }
+  // the coarsest factorisation failed (only reachable inside a graph, where the host
+  // checks the status after the solve): stop before iterating on a broken preconditioner
+  if (*chol_status) st->done = 3;
 }
 
 // ------------------------------------------------------------------ multigrid setup
@@ -1006,51 +1029,42 @@ static void mg_allocate(Prob& P) {
 }
 
 // ------------------------------------------------------------------ PCG
-template <typename T, typename TD0>
-static void pcg_fp64(Prob& P, double tol, int maxiter) {
+// The solve is built from four pieces (prologue, iteration body, and for mixed precision the
+// true-residual replacement) that run either from a host loop (one status read per
+// iteration) or inside one CUDA graph (solve_graph below) whose while node repeats the body
+// and whose if node runs the replacement, so the two drivers execute the same launches.
+//
+// FP64: every level, vector and operator in FP64 (solvers/_multigrid_cuda.py:188-241).
+static void pcg64_prologue(Prob& P, double tol, int maxiter) {
   CatScope cat(P, CAT_VECTOR);
-  // b64, x64 are set; T == double
   const Geo& g = P.g0;
   const long long nv = (long long)g.dof * g.n;
-  double* r = P.r64;
-  double* x = P.x64;
+  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
+  {  // r = b - A x
+    EpiResid<double, double, double> e{P.b64, P.r64, g.n};
+    fine_apply<double>(P, (const double*)P.x64, e, nullptr);
+    springs_apply(P, (const double*)P.x64, P.r64, -1.0, nullptr);
+  }
+  launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, (const double*)P.b64,
+         (const double*)P.b64, P.part, P.ticket, &P.st->bb);
+  launch(P, k_pcg_check_bb, 1, 1, 0, P.st, (const int*)P.chol_status);
+}
+static void pcg64_body(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
   double* p = (double*)P.p;
   double* q = (double*)P.q;
   double* z = (double*)P.lv[0].res;
-  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
-  KCHECK();
-  // r = b - A x ; bb = b.b
+  vcycle<double, double, double>(P, 0, P.r64, z, P.r64, &P.st->rz_new);
+  launch(P, k_pcg_p<double>, ew_blocks(nv), 256, 0, nv, p, (const double*)z, (const PcgState*)P.st);
   {
-    EpiResid<double, double, double> e{P.b64, r, g.n};
-    fine_apply<double>(P, x, e, nullptr);
-    springs_apply(P, (const double*)x, r, -1.0, nullptr);
+    EpiStoreDot<double> e{q, g.n};
+    fine_apply<double>(P, (const double*)p, e, &P.st->pq);
+    springs_apply(P, (const double*)p, q, 1.0, &P.st->pq);
   }
-  launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, P.b64, P.b64, P.part,
-                                                                                       P.ticket, &P.st->bb);
-  KCHECK();
-  launch(P, k_pcg_check_bb, 1, 1, 0, P.st);
-  vcycle<double, TD0, double>(P, 0, r, z, r, &P.st->rz_new);
-  launch(P, k_copy<double, double>, ew_blocks(nv), 256, 0, nv, z, p);
-  KCHECK();
-  int it = 0;
-  for (;;) {
-    {
-      EpiStoreDot<double> e{q, g.n};
-      fine_apply<double>(P, p, e, &P.st->pq);
-      springs_apply(P, (const double*)p, q, 1.0, &P.st->pq);
-    }
-    launch(P, k_pcg_xr<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, x, p, r, q, P.st,
-                                                                                           P.part, P.ticket, (float*)nullptr);
-    KCHECK();
-    CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
-    CK(cudaStreamSynchronize(P.stream));
-    ++it;
-    if (P.st_h->done) break;
-    vcycle<double, TD0, double>(P, 0, r, z, r, &P.st->rz_new);
-    launch(P, k_pcg_p<double>, ew_blocks(nv), 256, 0, nv, p, z, P.st);
-    KCHECK();
-  }
-  P.last_iters = P.st_h->iter;
+  launch(P, k_pcg_xr<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, P.x64, (const double*)p,
+         P.r64, (const double*)q, P.st, P.part, P.ticket, (float*)nullptr);
 }
 
 // Mixed precision: FP32 operator, V-cycle and search directions; FP64 solution, residual
@@ -1059,54 +1073,79 @@ static void pcg_fp64(Prob& P, double tol, int maxiter) {
 // before convergence is declared.
 static const double REPLACE_DROP = 1e-2;
 
-static void pcg_mixed(Prob& P, double tol, int maxiter) {
+static void pcgmx_true_residual(Prob& P) {
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
+  EpiResid<double, double, double> e{P.b64, P.r64, g.n};
+  fine_apply<double>(P, (const double*)P.x64, e, nullptr);
+  springs_apply(P, (const double*)P.x64, P.r64, -1.0, nullptr);
+  launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.r64, (const double*)P.r64, P.part, P.ticket,
+         &P.st->rr);
+  launch(P, k_copy<double, float>, ew_blocks(nv), 256, 0, nv, (const double*)P.r64, P.r32);
+}
+static void pcgmx_prologue(Prob& P, double tol, int maxiter) {
   CatScope cat(P, CAT_VECTOR);
   const Geo& g = P.g0;
   const long long nv = (long long)g.dof * g.n;
-  double* r = P.r64;
-  double* x = P.x64;
-  float* r32 = P.r32;
-  float* p = (float*)P.p;
-  float* q = (float*)P.q;
-  float* z = (float*)P.lv[0].res;
   const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
-  auto true_residual = [&]() {
-    EpiResid<double, double, double> e{P.b64, r, g.n};
-    fine_apply<double>(P, x, e, nullptr);
-    springs_apply(P, (const double*)x, r, -1.0, nullptr);
-    launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)r, (const double*)r, P.part, P.ticket, &P.st->rr);
-    launch(P, k_copy<double, float>, ew_blocks(nv), 256, 0, nv, (const double*)r, r32);
-    ++P.last_true_res;
-  };
-  P.last_true_res = 0;
   launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
   launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.b64, (const double*)P.b64, P.part, P.ticket,
          &P.st->bb);
-  true_residual();
-  launch(P, k_pcg_check_bb, 1, 1, 0, P.st);
-  vcycle<float, __nv_bfloat16, double>(P, 0, r32, z, r, &P.st->rz_new);
-  launch(P, k_copy<float, float>, ew_blocks(nv), 256, 0, nv, (const float*)z, p);
-  double last_replace = 1.0;
-  for (;;) {
-    {
-      EpiStoreDot<float> e{q, g.n};
-      fine_apply<float>(P, p, e, &P.st->pq);
-      springs_apply(P, (const float*)p, q, 1.0, &P.st->pq);
+  pcgmx_true_residual(P);
+  launch(P, k_pcg_check_bb, 1, 1, 0, P.st, (const int*)P.chol_status);
+}
+static void pcgmx_body(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
+  float* p = (float*)P.p;
+  float* q = (float*)P.q;
+  float* z = (float*)P.lv[0].res;
+  vcycle<float, __nv_bfloat16, double>(P, 0, P.r32, z, P.r64, &P.st->rz_new);
+  launch(P, k_pcg_p<float>, ew_blocks(nv), 256, 0, nv, p, (const float*)z, (const PcgState*)P.st);
+  {
+    EpiStoreDot<float> e{q, g.n};
+    fine_apply<float>(P, (const float*)p, e, &P.st->pq);
+    springs_apply(P, (const float*)p, q, 1.0, &P.st->pq);
+  }
+  launch(P, k_pcg_xr<double, float>, nb, 256, 0, nv, P.x64, (const float*)p, P.r64, (const float*)q, P.st, P.part,
+         P.ticket, P.r32);
+}
+static void pcgmx_replace(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  pcgmx_true_residual(P);
+  launch(P, k_pcg_true_res, 1, 1, 0, P.st);
+}
+
+static void read_state(Prob& P) {
+  CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaStreamSynchronize(P.stream));
+}
+
+// Host-driven loop (used while profiling with per-launch events, or with graphs disabled).
+static void pcg_host(Prob& P, double tol, int maxiter) {
+  const bool mixed = P.prec != EDGE_FP64;
+  if (mixed)
+    pcgmx_prologue(P, tol, maxiter);
+  else
+    pcg64_prologue(P, tol, maxiter);
+  read_state(P);
+  P.last_true_res = mixed ? 1 : 0;
+  while (!P.st_h->done) {
+    if (mixed) {
+      pcgmx_body(P);
+      read_state(P);
+      if (P.st_h->done == 1 || P.st_h->res < REPLACE_DROP * P.st_h->last_replace) {
+        pcgmx_replace(P);
+        read_state(P);
+        ++P.last_true_res;
+      }
+    } else {
+      pcg64_body(P);
+      read_state(P);
     }
-    launch(P, k_pcg_xr<double, float>, nb, 256, 0, nv, x, (const float*)p, r, (const float*)q, P.st, P.part, P.ticket,
-           r32);
-    CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
-    CK(cudaStreamSynchronize(P.stream));
-    if (P.st_h->done == 1 || P.st_h->res < REPLACE_DROP * last_replace) {
-      true_residual();
-      launch(P, k_pcg_true_res, 1, 1, 0, P.st);
-      CK(cudaMemcpyAsync(P.st_h, P.st, sizeof(PcgState), cudaMemcpyDeviceToHost, P.stream));
-      CK(cudaStreamSynchronize(P.stream));
-      last_replace = P.st_h->res;
-    }
-    if (P.st_h->done) break;
-    vcycle<float, __nv_bfloat16, double>(P, 0, r32, z, r, &P.st->rz_new);
-    launch(P, k_pcg_p<float>, ew_blocks(nv), 256, 0, nv, p, (const float*)z, P.st);
   }
   P.last_iters = P.st_h->iter;
 }
@@ -1125,24 +1164,169 @@ static void ensure_mg(Prob& P) {
   if (P.n_level < 0) fail(EDGE_ESTATE, "multigrid not configured (edge_mg_config)");
 }
 
-static void solve_internal(Prob& P, double tol, int maxiter) {
-  ensure_mg(P);
-  if (!P.has_rho) fail(EDGE_ESTATE, "Solver requires a density vector to be passed or set on the kernel.");
-  CK(cudaEventRecord(P.ev[0], P.stream));
+static void mg_setup_prec(Prob& P) {
   if (P.prec == EDGE_FP64)
     mg_setup<double, double>(P);
   else
     mg_setup<float, __nv_bfloat16>(P);
+}
+
+// Capture parameters of the solve graph: anything baked into its launches.
+static std::vector<double> graph_key(const Prob& P, double tol, int maxiter) {
+  std::vector<double> k = {(double)P.prec, tol, (double)maxiter, (double)P.n_level, (double)P.n_smooth, P.omega,
+                           P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
+                           (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons};
+  for (int l : P.w_levels) k.push_back((double)l);
+  return k;
+}
+
+// Records one solve (hierarchy set-up, PCG prologue, and the iteration loop as a while node
+// whose body holds, for mixed precision, the replacement as an if node) into P.sg_exec.
+// Captured on the library's own streams so that the caller's stream may be the legacy
+// default stream; touches only buffers the problem owns.
+static void capture_solve(Prob& P, double tol, int maxiter) {
+  const bool mixed = P.prec != EDGE_FP64;
+  for (int i = 0; i < 3; ++i)
+    if (!P.cap[i]) CK(cudaStreamCreateWithFlags(&P.cap[i], cudaStreamNonBlocking));
+  if (P.sg_exec) {
+    CK(cudaGraphExecDestroy(P.sg_exec));
+    P.sg_exec = nullptr;
+  }
+  if (P.sg_graph) {
+    CK(cudaGraphDestroy(P.sg_graph));
+    P.sg_graph = nullptr;
+  }
+  cudaStream_t user = P.stream;
+  const long long n0 = P.nlaunch;
+  long long n1 = 0, n2 = 0, n3 = 0;
+  int depth = 0;  // captures open
+  try {
+    P.stream = P.cap[0];
+    CK(cudaStreamBeginCapture(P.cap[0], cudaStreamCaptureModeThreadLocal));
+    depth = 1;
+    mg_setup_prec(P);
+    if (mixed)
+      pcgmx_prologue(P, tol, maxiter);
+    else
+      pcg64_prologue(P, tol, maxiter);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t nd;
+    CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &g, &deps, &nd));
+    cudaGraphConditionalHandle hw;
+    CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
+    launch(P, k_cond_while, 1, 1, 0, hw, (const PcgState*)P.st);
+    n1 = P.nlaunch;
+    CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, g, deps, nd, &wp));
+    CK(cudaStreamUpdateCaptureDependencies(P.cap[0], &wnode, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    P.stream = P.cap[1];
+    CK(cudaStreamBeginCaptureToGraph(P.cap[1], body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    depth = 2;
+    if (mixed) {
+      pcgmx_body(P);
+      cudaGraph_t gb;
+      CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
+      cudaGraphConditionalHandle hr;
+      CK(cudaGraphConditionalHandleCreate(&hr, gb, 0, cudaGraphCondAssignDefault));
+      launch(P, k_cond_replace, 1, 1, 0, hr, (const PcgState*)P.st, REPLACE_DROP);
+      CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hr;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t inode;
+      CK(cudaGraphAddNode(&inode, gb, deps, nd, &ip));
+      CK(cudaStreamUpdateCaptureDependencies(P.cap[1], &inode, 1, cudaStreamSetCaptureDependencies));
+      n2 = P.nlaunch;
+      P.stream = P.cap[2];
+      CK(cudaStreamBeginCaptureToGraph(P.cap[2], ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal));
+      depth = 3;
+      pcgmx_replace(P);
+      CK(cudaStreamEndCapture(P.cap[2], nullptr));
+      depth = 2;
+      n3 = P.nlaunch;
+      P.stream = P.cap[1];
+    } else {
+      pcg64_body(P);
+    }
+    launch(P, k_cond_while, 1, 1, 0, hw, (const PcgState*)P.st);
+    CK(cudaStreamEndCapture(P.cap[1], nullptr));
+    depth = 1;
+    P.stream = P.cap[0];
+    CK(cudaStreamEndCapture(P.cap[0], &P.sg_graph));
+    depth = 0;
+    CK(cudaGraphInstantiate(&P.sg_exec, P.sg_graph, 0));
+  } catch (...) {
+    for (int d = depth; d >= 1; --d) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(P.cap[d - 1], &junk);
+      if (d == 1 && junk) cudaGraphDestroy(junk);
+    }
+    cudaGetLastError();
+    P.stream = user;
+    P.nlaunch = n0;
+    throw;
+  }
+  P.stream = user;
+  const long long n4 = P.nlaunch;
+  P.sg_pro = n1 - n0;
+  if (mixed) {
+    P.sg_if = n3 - n2;
+    P.sg_body = (n2 - n1) + (n4 - n3);
+  } else {
+    P.sg_if = 0;
+    P.sg_body = n4 - n1;
+  }
+  P.nlaunch = n0;
+  P.sg_key = graph_key(P, tol, maxiter);
+}
+
+static void solve_graph(Prob& P, double tol, int maxiter) {
+  if (!P.sg_exec || P.sg_key != graph_key(P, tol, maxiter)) capture_solve(P, tol, maxiter);
+  CK(cudaEventRecord(P.ev[0], P.stream));
+  CK(cudaGraphLaunch(P.sg_exec, P.stream));
+  CK(cudaEventRecord(P.ev[2], P.stream));
+  int status = 0;
+  CK(cudaMemcpyAsync(&status, P.chol_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+  read_state(P);
+  if (status) fail(EDGE_ENOTPD, "coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
+  P.last_iters = P.st_h->iter;
+  P.last_true_res = (P.prec != EDGE_FP64) ? 1 + P.st_h->n_true : 0;
+  P.nlaunch += P.sg_pro + P.sg_body * (long long)P.st_h->iter + P.sg_if * (long long)P.st_h->n_true;
+}
+
+static void solve_internal(Prob& P, double tol, int maxiter) {
+  ensure_mg(P);
+  if (!P.has_rho) fail(EDGE_ESTATE, "Solver requires a density vector to be passed or set on the kernel.");
+  if (P.use_graph && !P.prof && !P.bd) {
+    solve_graph(P, tol, maxiter);
+    check_err(P);
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, P.ev[0], P.ev[2]));
+    P.last_setup_ms = 0.0;  // inside the graph: counted in the solve time
+    P.last_solve_ms = ms;
+    return;
+  }
+  CK(cudaEventRecord(P.ev[0], P.stream));
+  mg_setup_prec(P);
   CK(cudaEventRecord(P.ev[1], P.stream));
   // check the coarse factorisation
   int status = 0;
   CK(cudaMemcpyAsync(&status, P.chol_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
   CK(cudaStreamSynchronize(P.stream));
   if (status) fail(EDGE_ENOTPD, "coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
-  if (P.prec == EDGE_FP64)
-    pcg_fp64<double, double>(P, tol, maxiter);
-  else
-    pcg_mixed(P, tol, maxiter);
+  pcg_host(P, tol, maxiter);
   CK(cudaEventRecord(P.ev[2], P.stream));
   CK(cudaEventSynchronize(P.ev[2]));
   check_err(P);
@@ -1230,6 +1414,31 @@ __global__ void k_oc_static_init(OcStaticScratch* s, double vf, double vol) {
     return EDGE_ECUDA;          \
   }                             \
   return EDGE_OK;
+
+// Average device time of `reps` Jacobi sweeps of the stencil operator on level l >= 1, in
+// the problem's precision (the hierarchy must be built).
+template <typename T>
+static double time_level(Prob& P, int l, int reps) {
+  Level& Lv = P.lv[l];
+  const Geo& g = Lv.g;
+  auto run = [&]() {
+    EpiJacobi<T, T, T> e{(const T*)Lv.b, (const T*)Lv.dinv, (T*)Lv.xb, &P.st->omega, 1.0, g.n};
+    st_apply<T>(P, g, (const T*)Lv.xa, (const T*)Lv.S, e, nullptr);
+  };
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  run();
+  CK(cudaEventRecord(a, P.stream));
+  for (int r = 0; r < reps; ++r) run();
+  CK(cudaEventRecord(b, P.stream));
+  CK(cudaEventSynchronize(b));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms / reps;
+}
 
 extern "C" {
 
@@ -1324,12 +1533,33 @@ int edge_set_stream(edge_problem* p, void* stream) {
   API_END
 }
 
+int edge_launch_count(const edge_problem* p, long long* n) {
+  API_BEGIN
+  if (!p || !n) fail(EDGE_EINVAL, "null argument");
+  *n = p->P.nlaunch;
+  API_END
+}
+
+int edge_set_graph(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.use_graph = enable != 0;
+  API_END
+}
+
+int edge_set_stencil_quad(edge_problem* p, long long max_slots) {
+  API_BEGIN
+  if (!p || max_slots < 0) fail(EDGE_EINVAL, "bad argument");
+  p->P.st_quad_max = max_slots;
+  API_END
+}
+
 int edge_uses_transform(const edge_problem* p) { return p && p->P.ei.wht ? 1 : 0; }
 int edge_uses_cube_form(const edge_problem* p) { return p && p->P.cube ? 1 : 0; }
 
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm) {
   API_BEGIN
-  if (!p || variant < 0 || variant > 12 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
+  if (!p || variant < 0 || variant > 14 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
   p->P.tile_variant = variant;
   p->P.blocks_per_sm = blocks_per_sm;
   API_END
@@ -1399,7 +1629,7 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
   int bv = P.tile_variant, bb = P.blocks_per_sm;
   const int bps_list[4] = {2, 4, 8, 16};
   // variants 5..8: packed-pair FP32 kernel; 9..12: its cube-element form
-  const int nvar = precision == EDGE_FP64 ? 5 : (P.cube ? 13 : 9);
+  const int nvar = precision == EDGE_FP64 ? 5 : (P.cube ? 15 : 9);
   const bool sweep = can_time_sweep(P, precision);
   for (int v = 0; v < nvar; ++v)
     for (int bi = 0; bi < 4; ++bi) {
@@ -1421,10 +1651,19 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
   API_END
 }
 
+int edge_time_level(edge_problem* p, int level, int reps, double* ms) {
+  API_BEGIN
+  if (!p || !ms || reps < 1) fail(EDGE_EINVAL, "bad argument");
+  Prob& P = p->P;
+  if (P.lv.empty() || level < 1 || level >= P.n_level) fail(EDGE_EINVAL, "level must be a smoothed coarse level");
+  *ms = P.prec == EDGE_FP64 ? time_level<double>(P, level, reps) : time_level<float>(P, level, reps);
+  API_END
+}
+
 int edge_time_fine(edge_problem* p, int precision, int variant, int blocks_per_sm, int sweep, int reps,
                    double* ms) {
   API_BEGIN
-  if (!p || !ms || reps < 1 || variant < 0 || variant > 12 || blocks_per_sm < 1 || blocks_per_sm > 64)
+  if (!p || !ms || reps < 1 || variant < 0 || variant > 14 || blocks_per_sm < 1 || blocks_per_sm > 64)
     fail(EDGE_EINVAL, "bad argument");
   Prob& P = p->P;
   if (!P.has_rho) fail(EDGE_ESTATE, "rho not set");
@@ -1644,6 +1883,7 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
     P.n_level = n_level;
     P.prec = precision;
     P.tmaps.clear();
+    P.sg_key.clear();  // the solve graph refers to the old buffers: capture again
     mg_allocate(P);
   }
   API_END

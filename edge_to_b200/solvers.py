@@ -30,7 +30,7 @@ class Solver:
 class CuMultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="splu", matrix_free=False, low_level_tol=1e-8, low_level_maxiter=5000,
-                 min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True):
+                 min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True, graph=True):
         if not isinstance(kernel, CuStructuredStiffnessKernel):
             raise TypeError("CuMultiGrid needs the package's CuStructuredStiffnessKernel")
         self.kernel = kernel
@@ -65,19 +65,23 @@ class CuMultiGrid(Solver):
         self._configured = None
         self.autotune = autotune
         self.tuned = None
+        # graph=True: each solve (hierarchy set-up + the whole PCG loop) is one CUDA graph
+        # launch with device-side loop control; False: host-driven loop, same launches
+        self.graph = graph
 
     def reset(self):
         self.last_x0 = None
 
     def _configure(self):
         key = (self.n_level, self.n_smooth, self.max_omega, self.min_omega, self.cycle, tuple(self.w_level),
-               self.precision)
+               self.precision, bool(self.graph))
         if self._configured == key:
             return
         w = _lib.int_array(self.w_level) if self.w_level else None
         prec = _lib.EDGE_FP64 if self.precision == "fp64" else _lib.EDGE_MIXED
         _lib.call("edge_mg_config", self.kernel.handle, int(self.n_level), int(self.n_smooth), float(self.max_omega),
                   float(self.min_omega), 1 if self.cycle == "w" else 0, w, len(self.w_level), prec)
+        _lib.call("edge_set_graph", self.kernel.handle, 1 if self.graph else 0)
         self._configured = key
 
     def tune(self):

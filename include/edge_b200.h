@@ -68,8 +68,8 @@ int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
  * cooperative-load version of the same kernel. */
 int edge_set_tma(edge_problem* p, int enable);
 /* Fine-kernel tile: variant 0..4 = k_fine3_tma (warps, TMA stages) (8,4) (8,3) (8,2) (4,4)
- * (4,3); FP32 only: 5..8 = packed-pair k_fine3_pk, 9..12 = its cube-element block form
- * k_fine3_cube (used when edge_uses_cube_form is 1, else 9..12 run k_fine3_pk); and the
+ * (4,3); FP32 only: 5..8 = packed-pair k_fine3_pk, 9..14 = its cube-element block form
+ * k_fine3_cube (used when edge_uses_cube_form is 1, else 9..14 run k_fine3_pk); and the
  * target of resident blocks per SM that sets the y-chunking of the grid. */
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm);
 /* Autotuner: times every tile variant and y-chunking on the current density with the plain
@@ -81,6 +81,22 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
  * precision) or the plain product.  The problem's own tile choice is left unchanged. */
 int edge_time_fine(edge_problem* p, int precision, int variant, int blocks_per_sm, int sweep, int reps,
                    double* ms);
+/* Kernel launches made through this problem so far (a launch inside a graph counts once per
+ * execution; edge_profile_begin resets the tally). */
+int edge_launch_count(const edge_problem* p, long long* n);
+/* enable != 0 (the default): edge_mg_solve and edge_simp_solve_and_process run the
+ * multigrid set-up and the whole PCG loop as one CUDA graph launch (a while node repeats
+ * the iteration, an if node makes the mixed-precision residual replacement; captured on the
+ * first solve and again when a solver setting changes).  0: the same launches from a host
+ * loop that reads the solver state once per iteration.  Per-launch profiling
+ * (edge_profile_begin, edge_breakdown_begin) always uses the host loop. */
+int edge_set_graph(edge_problem* p, int enable);
+/* Coarse 3-D levels with at most max_slots slots use the four-lanes-per-node stencil kernel
+ * (latency-bound small levels); larger levels one thread per node.  Default 200000. */
+int edge_set_stencil_quad(edge_problem* p, long long max_slots);
+/* Benchmark helper: average device time (ms) of `reps` Jacobi sweeps of the stencil operator
+ * on coarse level 1 <= level < n_level, in the problem's precision (hierarchy built). */
+int edge_time_level(edge_problem* p, int level, int reps, double* ms);
 /* 1 when the element matrix has the box structure used by the transform kernels */
 int edge_uses_transform(const edge_problem* p);
 /* 1 when the transformed element matrix has the cube block form (eight coefficients) used by

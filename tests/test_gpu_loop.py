@@ -117,7 +117,18 @@ def test_mixed_precision_mbb_against_reference(golden):
 
 
 def test_mixed_vs_fp64_cantilever():
-    """3-D cantilever, 5 SIMP iterations at rtol 1e-6: mixed vs FP64 compliance within 1e-6."""
+    """3-D cantilever at rtol 1e-6.  One solve: each precision's compliance within 1e-6 of a
+    tight (rtol 1e-12) FP64 solve.  Five SIMP iterations: the mixed and FP64 trajectories
+    within 2e-6 (each side carries its own rtol-1e-6 solution error) and rho within 1e-5."""
+    import torch
+    exact = _cant((64, 32, 32), 0.12, 1.5, dict(tol=1e-12, n_level=4, maxiter=2000), "fp64")
+    rho0 = torch.full((64 * 32 * 32,), 0.12, dtype=torch.float64, device="cuda")
+    c_exact = float(exact.solve_and_process(rho0, 0)[0])
+    for prec in ("fp64", "mixed"):
+        opt = _cant((64, 32, 32), 0.12, 1.5, dict(tol=1e-6, n_level=4, maxiter=1000), prec)
+        c = float(opt.solve_and_process(rho0, 0)[0])
+        print(prec, "single-solve compliance rel err vs rtol-1e-12 FP64", abs(c - c_exact) / c_exact)
+        assert abs(c - c_exact) / c_exact <= 1e-6
     res = {}
     for prec in ("fp64", "mixed"):
         opt = _cant((64, 32, 32), 0.12, 1.5, dict(tol=1e-6, n_level=4, maxiter=1000), prec)
@@ -126,5 +137,5 @@ def test_mixed_vs_fp64_cantilever():
         res[prec] = (np.array(hist["comp_history"]), rho.cpu().numpy(), opt.solver.last_iters)
     err = np.abs(res["mixed"][0] - res["fp64"][0]) / res["fp64"][0]
     print("mixed vs fp64 compliance rel err", err, "pcg iters", res["fp64"][2], res["mixed"][2])
-    assert err.max() <= 1e-6
+    assert err.max() <= 2e-6
     assert np.abs(res["mixed"][1] - res["fp64"][1]).max() <= 1e-5

@@ -274,7 +274,7 @@ def test_fp32_operator_accuracy():
 @pytest.mark.parametrize("nel", [(4, 4, 4), (7, 5, 3), (40, 9, 33), (9, 33, 65), (3, 3, 130), (20, 20, 47), (66, 17, 31)])
 def test_fp32_tile_variants_agree(nel):
     """Every FP32 fine-kernel tile (k_fine3_tma 0-4, packed-pair k_fine3_pk 5-8, its cube form
-    k_fine3_cube 9-12) gives K(E) u to single precision on ragged grids with boundary
+    k_fine3_cube 9-14) gives K(E) u to single precision on ragged grids with boundary
     conditions and void elements."""
     import torch
     import edge_to_b200 as eb
@@ -293,7 +293,7 @@ def test_fp32_tile_variants_agree(nel):
     ut = torch.as_tensor(u, device="cuda")
     outs = []
     assert _lib.lib().edge_uses_cube_form(k.handle) == 1
-    for v in range(13):
+    for v in range(15):
         for bps in (2, 16):
             _lib.call("edge_set_fine_tile", k.handle, v, bps)
             b = torch.empty_like(ut)
@@ -326,3 +326,60 @@ def test_packed_kernel_in_mixed_solve():
     for x, it, r in res[1:]:
         assert abs(it - res[0][1]) <= 2 and r < 1e-8
         assert rel(x, res[0][0]) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_stencil_kernels_agree_in_solve(precision):
+    """The one-thread-per-node and four-lanes-per-node coarse stencil kernels give the same
+    PCG run (same iteration count, solutions equal to rounding)."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(11)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    mesh = _mesh(3, (32, 16, 16), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision=precision, autotune=False)
+    res = []
+    for qmax in (0, 1 << 40):
+        _lib.call("edge_set_stencil_quad", k.handle, qmax)
+        x, r = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
+        res.append((x.cpu().numpy().copy(), s.last_iters, r))
+    (x0, it0, r0), (x1, it1, r1) = res
+    assert abs(it0 - it1) <= (0 if precision == "fp64" else 1) and r0 < 1e-8 and r1 < 1e-8
+    assert rel(x1, x0) < (1e-12 if precision == "fp64" else 1e-7)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_and_host_loop_agree(precision):
+    """One CUDA-graph solve (while node over the PCG iteration, if node for the residual
+    replacement) and the host-driven loop run the same launches: same iteration count and
+    true-residual count, solutions equal to rounding; a second graph solve with a changed
+    tolerance captures again."""
+    import torch
+    import edge_to_b200 as eb
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(5)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    mesh = _mesh(3, (32, 16, 16), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    f = torch.as_tensor(p.f, device="cuda")
+    out = {}
+    for graph in (False, True):
+        s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision=precision, autotune=False,
+                           graph=graph)
+        x, r = s.solve(f, use_last=False)
+        out[graph] = (x.cpu().numpy().copy(), s.last_iters, s.stats()["true_residuals"], r)
+    (x0, it0, t0, r0), (x1, it1, t1, r1) = out[False], out[True]
+    assert it0 == it1 and t0 == t1 and r0 < 1e-8 and r1 < 1e-8
+    assert rel(x1, x0) < 1e-12
+    s.tol = 1e-6
+    x2, r2 = s.solve(f, use_last=False)
+    assert r2 < 1e-6 and s.last_iters < it1
