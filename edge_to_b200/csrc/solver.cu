@@ -238,6 +238,8 @@ struct Prob {
   bool has_rho = false, has_cons = false;
   // MG configuration
   int n_level = -1, n_smooth = 3;
+  std::vector<int> level_sweeps;  // per-level sweep counts (pre = post); levels past its end use n_smooth
+  int sweeps(int l) const { return l < (int)level_sweeps.size() ? level_sweeps[l] : n_smooth; }
   double omega = 0.5, min_omega = 0.4;
   bool cycle_w = false;
   std::vector<int> w_levels;
@@ -909,6 +911,7 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
   T* x = (T*)Lv.xa;
   T* y = (T*)Lv.xb;
   T* r = (T*)Lv.r;
+  const int nsm = P.sweeps(l);
   auto sweep = [&](const T* bb, T* in, T* outv) {
     if (l == 0) {
       EpiJacobi<T, T, TD0> e{bb, (const TD0*)Lv.dinv, outv, om, ws, g.n};
@@ -919,13 +922,13 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     }
   };
   // pre-smoothing from x = 0
-  if (P.n_smooth >= 1) {
+  if (nsm >= 1) {
     if (l == 0)
       launch(P, k_jacobi0<T, TD0, T>, ew_blocks(nv), 256, 0, nv, b, (const TD0*)Lv.dinv, x, om, ws);
     else
       launch(P, k_jacobi0<T, T, T>, ew_blocks(nv), 256, 0, nv, b, (const T*)Lv.dinv, x, om, ws);
     KCHECK();
-    for (int s = 1; s < P.n_smooth; ++s) {
+    for (int s = 1; s < nsm; ++s) {
       sweep(b, x, y);
       std::swap(x, y);
     }
@@ -960,8 +963,8 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     KCHECK();
     P.cur_cat = CAT_VECTOR;
     const bool last_visit = (vis == visits - 1);
-    if (P.n_smooth >= 1) {
-      for (int s = 0; s < P.n_smooth - 1; ++s) {
+    if (nsm >= 1) {
+      for (int s = 0; s < nsm - 1; ++s) {
         sweep(r, e1, e2);
         std::swap(e1, e2);
       }
@@ -1177,6 +1180,8 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter) {
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons};
   for (int l : P.w_levels) k.push_back((double)l);
+  k.push_back(-1.0);
+  for (int v : P.level_sweeps) k.push_back((double)v);
   return k;
 }
 
@@ -1533,6 +1538,15 @@ int edge_set_stream(edge_problem* p, void* stream) {
   API_END
 }
 
+int edge_mg_set_sweeps(edge_problem* p, const int* sweeps, int n) {
+  API_BEGIN
+  if (!p || n < 0 || (n > 0 && !sweeps)) fail(EDGE_EINVAL, "bad argument");
+  for (int i = 0; i < n; ++i)
+    if (sweeps[i] < 0 || sweeps[i] > 16) fail(EDGE_EINVAL, "sweep counts must be in 0..16");
+  p->P.level_sweeps.assign(sweeps, sweeps + n);
+  API_END
+}
+
 int edge_launch_count(const edge_problem* p, long long* n) {
   API_BEGIN
   if (!p || !n) fail(EDGE_EINVAL, "null argument");
@@ -1879,6 +1893,14 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
         cudaFree(q);
         P.allocs.erase(it);
       }
+    }
+    // p and q are shared by both precisions (FP64-sized, read as FP32 by the mixed path): the
+    // operator never writes their padding slots, which the PCG vector kernels sweep over, so
+    // bytes left by the other precision must not survive a switch
+    if (precision != P.prec) {
+      const size_t nv = (size_t)P.g0.dof * P.g0.n;
+      CK(cudaMemsetAsync(P.p, 0, nv * sizeof(double), P.stream));
+      CK(cudaMemsetAsync(P.q, 0, nv * sizeof(double), P.stream));
     }
     P.n_level = n_level;
     P.prec = precision;

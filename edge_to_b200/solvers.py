@@ -30,7 +30,7 @@ class Solver:
 class CuMultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="splu", matrix_free=False, low_level_tol=1e-8, low_level_maxiter=5000,
-                 min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True, graph=True):
+                 min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True, graph=True, tune_sweeps=None):
         if not isinstance(kernel, CuStructuredStiffnessKernel):
             raise TypeError("CuMultiGrid needs the package's CuStructuredStiffnessKernel")
         self.kernel = kernel
@@ -68,6 +68,11 @@ class CuMultiGrid(Solver):
         # graph=True: each solve (hierarchy set-up + the whole PCG loop) is one CUDA graph
         # launch with device-side loop control; False: host-driven loop, same launches
         self.graph = graph
+        # tune_sweeps (default: on for precision="mixed", off for "fp64", which keeps the
+        # reference's n_smooth on every level): per-level smoothing sweeps chosen by timing
+        # whole solves of the first system; the converged solution meets the same tolerance
+        self.tune_sweeps = (precision == "mixed") if tune_sweeps is None else bool(tune_sweeps)
+        self.sweeps = None
 
     def reset(self):
         self.last_x0 = None
@@ -97,6 +102,44 @@ class CuMultiGrid(Solver):
         self.tuned = {"variant": v.value, "blocks_per_sm": b.value, "ms": ms.value}
         return self.tuned
 
+    SWEEP_CANDIDATES = ("1", "1,2", "2", "1,3", "n")
+
+    def tune_sweep_counts(self, f):
+        """Pick per-level smoothing sweeps (fine level first) by timing one solve of K x = f
+        from x = 0 for each candidate pattern ("1,2": one sweep on the fine level, two on
+        every coarser level; "n": n_smooth everywhere, the reference's V-cycle) and keep the
+        fastest that converges.  Runs once, on the first solve; needs the density set."""
+        if self.sweeps is not None or not self.tune_sweeps or not self.kernel.has_rho:
+            return self.sweeps
+        f = _as_dev_f64(f)
+        stream = torch.cuda.current_stream()
+        x = torch.empty_like(f)
+        res, its = ctypes.c_double(), ctypes.c_int()
+        best = None
+        self.kernel._bind_stream()
+        for cand in self.SWEEP_CANDIDATES:
+            if cand == "n":
+                pattern = [self.n_smooth] * self.n_level
+            else:
+                v = [int(t) for t in cand.split(",")]
+                pattern = [v[0]] + [v[-1]] * (self.n_level - 1)
+            _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(pattern), len(pattern))
+            x.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), 0, float(self.tol),
+                      int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            if res.value < self.tol and (best is None or ms < best[0]):
+                best = (ms, pattern, its.value)
+        if best is None:  # nothing converged within maxiter: keep the reference's sweeps
+            best = (0.0, [self.n_smooth] * self.n_level, 0)
+        _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(best[1]), len(best[1]))
+        self.sweeps = {"per_level": best[1], "solve_ms": best[0], "pcg_iters": best[2]}
+        return self.sweeps
+
     def solve(self, rhs, rho=None, use_last=True):
         if not (self.kernel.has_rho or rho is not None):
             raise ValueError("Solver requires a density vector to be passed or set on the kernel.")
@@ -104,6 +147,7 @@ class CuMultiGrid(Solver):
             self.kernel.set_rho(rho)
         self._configure()
         self.tune()
+        self.tune_sweep_counts(rhs)
         f = _as_dev_f64(rhs)
         if use_last and self.last_x0 is not None:
             x = self.last_x0

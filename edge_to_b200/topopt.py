@@ -173,11 +173,12 @@ class CuTopOpt:
     def _solve_and_process_fused(self, rho, iteration):
         sv = self.solver
         sv._configure()
-        if sv.autotune and sv.tuned is None:
-            # the autotuner needs a density on the kernel: use this iteration's SIMP field
+        if (sv.autotune and sv.tuned is None) or (sv.tune_sweeps and sv.sweeps is None):
+            # the autotuners need a density on the kernel: use this iteration's SIMP field
             rho_f = self.filter_kernel.dot(rho)
             self.kernel.set_rho(self.material_model(rho_f, iteration))
             sv.tune()
+            sv.tune_sweep_counts(self.f)
         pen = float(self.material_model.current_penalty(iteration))
         use_last = self.reuse_sol and sv.last_x0 is not None
         if sv.last_x0 is None or not use_last:

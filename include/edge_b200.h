@@ -81,6 +81,11 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
  * precision) or the plain product.  The problem's own tile choice is left unchanged. */
 int edge_time_fine(edge_problem* p, int precision, int variant, int blocks_per_sm, int sweep, int reps,
                    double* ms);
+/* Per-level smoothing sweeps (pre- and post-smoothing each), sweeps[l] for level l < n;
+ * levels from n on use edge_mg_config's n_smooth (n = 0 restores that everywhere).  The
+ * reference smooths every level n_smooth times (solvers/_multigrid_cuda.py:133-186); this
+ * is the knob the sweep autotuner of the mixed-precision solver turns. */
+int edge_mg_set_sweeps(edge_problem* p, const int* sweeps, int n);
 /* Kernel launches made through this problem so far (a launch inside a graph counts once per
  * execution; edge_profile_begin resets the tally). */
 int edge_launch_count(const edge_problem* p, long long* n);

@@ -317,7 +317,8 @@ def test_packed_kernel_in_mixed_solve():
     k = eb.CuStructuredStiffnessKernel(mesh)
     k.add_constraints(np.asarray(p.cons))
     k.set_rho(torch.as_tensor(E, device="cuda"))
-    s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision="mixed", autotune=False)
+    s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision="mixed", autotune=False,
+                       tune_sweeps=False)
     res = []
     for v in (4, 5, 8, 9, 10):
         _lib.call("edge_set_fine_tile", k.handle, v, 8)
@@ -343,7 +344,8 @@ def test_stencil_kernels_agree_in_solve(precision):
     k = eb.CuStructuredStiffnessKernel(mesh)
     k.add_constraints(np.asarray(p.cons))
     k.set_rho(torch.as_tensor(E, device="cuda"))
-    s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision=precision, autotune=False)
+    s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision=precision, autotune=False,
+                       tune_sweeps=False)
     res = []
     for qmax in (0, 1 << 40):
         _lib.call("edge_set_stencil_quad", k.handle, qmax)
@@ -374,7 +376,7 @@ def test_graph_and_host_loop_agree(precision):
     out = {}
     for graph in (False, True):
         s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision=precision, autotune=False,
-                           graph=graph)
+                           graph=graph, tune_sweeps=False)
         x, r = s.solve(f, use_last=False)
         out[graph] = (x.cpu().numpy().copy(), s.last_iters, s.stats()["true_residuals"], r)
     (x0, it0, t0, r0), (x1, it1, t1, r1) = out[False], out[True]
@@ -383,3 +385,56 @@ def test_graph_and_host_loop_agree(precision):
     s.tol = 1e-6
     x2, r2 = s.solve(f, use_last=False)
     assert r2 < 1e-6 and s.last_iters < it1
+
+
+def test_sweep_autotuner_mixed():
+    """The mixed-precision solver picks per-level sweep counts on its first solve; the solve
+    still meets the tolerance and matches a tight FP64 solve; the FP64 solver keeps n_smooth."""
+    import torch
+    import edge_to_b200 as eb
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(3)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    f = torch.as_tensor(p.f, device="cuda")
+    xs = {}
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-8)):
+        mesh = _mesh(3, (32, 16, 16), None)
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        k.add_constraints(np.asarray(p.cons))
+        k.set_rho(torch.as_tensor(E, device="cuda"))
+        s = eb.CuMultiGrid(mesh, k, tol=tol, n_level=3, maxiter=500, precision=prec, autotune=False)
+        x, r = s.solve(f, use_last=False)
+        assert r < tol
+        xs[prec] = (x.cpu().numpy(), s.sweeps)
+    assert xs["fp64"][1] is None
+    sw = xs["mixed"][1]
+    assert sw is not None and len(sw["per_level"]) == 3 and all(1 <= v <= 3 for v in sw["per_level"])
+    assert rel(xs["mixed"][0], xs["fp64"][0]) < 1e-6
+
+
+def test_precision_switch_on_one_problem():
+    """An FP64 solve followed by a mixed-precision solve on the same kernel handle: the mixed
+    solve converges like on a fresh handle (buffers shared by both precisions are cleared)."""
+    import torch
+    import edge_to_b200 as eb
+    p = topopt.cantilever_problem(16, 8, 8, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=2, maxiter=500,
+                                                                     variant="gpu"))
+    rng = np.random.default_rng(4)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    f = torch.as_tensor(p.f, device="cuda")
+    out = []
+    for first64 in (False, True):
+        mesh = _mesh(3, (16, 8, 8), None)
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        k.add_constraints(np.asarray(p.cons))
+        k.set_rho(torch.as_tensor(E, device="cuda"))
+        if first64:
+            eb.CuMultiGrid(mesh, k, tol=1e-10, n_level=2, maxiter=500, precision="fp64", autotune=False).solve(
+                f, use_last=False)
+        s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=2, maxiter=500, precision="mixed", autotune=False,
+                           tune_sweeps=False)
+        x, r = s.solve(f, use_last=False)
+        out.append((x.cpu().numpy(), s.last_iters, r))
+    assert out[1][2] < 1e-8 and out[1][1] == out[0][1]
+    assert rel(out[1][0], out[0][0]) < 1e-12
