@@ -228,6 +228,7 @@ def run_ours(args, cfg_name):
     # host-driven loop, same launches) for the live roofline of the dominant kernel
     pm = timed_steps(opt, rho, dr, it, 1, ws, local, profile=True)
     rho, dr, it, prof = pm["rho"], pm["dr"], pm["it"], pm["prof"]
+    rho_chk, c_chk = rho.detach().clone(), pm["compliance"]  # checked against a tight FP64 solve below
 
     # ---------------- end-to-end: design on the host, copies inside the timed region
     stream = torch.cuda.current_stream()
@@ -266,6 +267,13 @@ def run_ours(args, cfg_name):
         f = timed_steps(opt64, rho64, dr64, it64, args.steps, ws, local, profile=False)
         fp64 = {"value": ws * args.steps / (f["t_ms"] / 1e3), "ms_per_step": f["t_ms"] / args.steps,
                 "pcg_iters_per_step": f["pcg"], "compliance_last": f["compliance"]}
+        # accuracy of each path against an rtol-1e-10 FP64 solve of the same design (its own
+        # last design), outside every timed region
+        opt64.solver.tol, opt64.solver.maxiter = 1e-10, 4000
+        c_t64 = float(opt64.solve_and_process(f["rho"], f["it"])[0])
+        c_tmx = float(opt64.solve_and_process(rho_chk, f["it"])[0])
+        fp64["compliance_rel_err_vs_tight_fp64"] = abs(f["compliance"] - c_t64) / abs(c_t64)
+        fp64["mixed_compliance_rel_err_vs_tight_fp64"] = abs(c_chk - c_tmx) / abs(c_tmx)
         del opt64, rho64, dr64
     if ws > 1:
         import torch.distributed as dist
@@ -316,6 +324,7 @@ def run_ours(args, cfg_name):
         line["mixed_over_fp64"] = value / fp64["value"]
         line["compliance_rel_err_vs_fp64"] = abs(m["compliance"] - fp64["compliance_last"]) / abs(
             fp64["compliance_last"])
+        line["compliance_rel_err_vs_tight_fp64"] = fp64.pop("mixed_compliance_rel_err_vs_tight_fp64")
     if bd is not None:
         line["breakdown_ms_per_step"] = bd
     if ws == 1 and not args.no_cpu_baseline:
