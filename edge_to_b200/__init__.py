@@ -2,7 +2,7 @@
 
 Drop-in names (EDGETO/__init__.py, TopOpt/__init__.py, solvers/__init__.py,
 kernels/__init__.py, geom/__init__.py): CuStructuredMesh2D/3D, CuStructuredStiffnessKernel,
-CuStructuredFilter2D/3D, CuMultiGrid, CuTopOpt, SingleMaterial, auto_stiffness; beyond the
+CuStructuredFilter2D/3D, CuMultiGrid, CuCG, CuTopOpt, SingleMaterial, auto_stiffness; beyond the
 reference, SIMPObjective (differentiable compliance / mechanism objectives, autograd.py).
 Arrays are torch CUDA tensors; the compute runs in libedge_b200.so (sm_100a).
 """
@@ -13,12 +13,12 @@ from .kernels import CuStructuredStiffnessKernel, StiffnessKernel
 from .material import MaterialModel, SingleMaterial
 from .mesh import CuStructuredMesh2D, CuStructuredMesh3D, StructuredMesh
 from .physics import auto_stiffness, hexahedron_element_stiffness, quadrilateral_element_stiffness
-from .solvers import CuMultiGrid
+from .solvers import CuMultiGrid, CuCG
 from .topopt import CuTopOpt
 
 __all__ = [
     "CuStructuredMesh2D", "CuStructuredMesh3D", "StructuredMesh", "CuStructuredStiffnessKernel", "StiffnessKernel",
-    "CuStructuredFilter2D", "CuStructuredFilter3D", "FilterKernel", "CuMultiGrid", "CuTopOpt", "SingleMaterial",
+    "CuStructuredFilter2D", "CuStructuredFilter3D", "FilterKernel", "CuMultiGrid", "CuCG", "CuTopOpt", "SingleMaterial",
     "MaterialModel", "auto_stiffness", "hexahedron_element_stiffness", "quadrilateral_element_stiffness",
     "SIMPObjective",
 ]

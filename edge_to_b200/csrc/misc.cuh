@@ -409,6 +409,67 @@ __global__ void k_pcg_p(long long n, TP* __restrict__ p, const TP* __restrict__ 
     p[i] = first ? z[i] : Conv<TP>::from((double)Conv<double>::from(z[i]) + beta * (double)Conv<double>::from(p[i]));
 }
 
+// Unpreconditioned CG as PCG with z = r: r.z of the current residual is its r.r.
+__global__ void k_cg_rz(PcgState* st) { st->rz_new = st->rr; }
+// Report the true relative residual ||f - A x|| / ||f|| (st->rr holds the true r.r).
+__global__ void k_final_res(PcgState* st) { st->res = st->bb > 0.0 ? sqrt(st->rr) / sqrt(st->bb) : 0.0; }
+
+// FEA_integrals (TopOpt/_solver.py:80-137 with the structured kernel of core/_ops.py:1032-1058):
+// per element, strain = B u_e, stress = D strain (D unscaled, as in the reference), strain
+// energy = 1/2 w_e u_e^T K0 u_e.  u_e is gathered from the user-layout displacement in the
+// reference's corner order (core/_geom.py:20-57); B (nb x nk), D (nb x nb) and K0 (nk x nk) are
+// row-major in that order.  One thread per element (a post-processing call, not a hot path).
+__global__ void k_fea_integrals(int dim, int nelx, int nely, int nelz, long long nel, const double* __restrict__ U,
+                                const double* __restrict__ w, const double* __restrict__ K0,
+                                const double* __restrict__ B, const double* __restrict__ D, int nb,
+                                double* __restrict__ strain, double* __restrict__ stress, double* __restrict__ energy) {
+  const int nc = dim == 3 ? 8 : 4, nk = nc * dim;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nel; e += (long long)gridDim.x * blockDim.x) {
+    long long nid[8];
+    if (dim == 3) {
+      const int i = (int)(e / ((long long)nely * nelz)), j = (int)((e / nelz) % nely), k = (int)(e % nelz);
+      const long long nx = nelx + 1, nz = nelz + 1;
+      auto node = [&](int a, int b, int c) { return (long long)b * nx * nz + (long long)a * nz + c; };
+      nid[0] = node(i, j, k);
+      nid[1] = node(i + 1, j, k);
+      nid[2] = node(i + 1, j + 1, k);
+      nid[3] = node(i, j + 1, k);
+      nid[4] = node(i, j, k + 1);
+      nid[5] = node(i + 1, j, k + 1);
+      nid[6] = node(i + 1, j + 1, k + 1);
+      nid[7] = node(i, j + 1, k + 1);
+    } else {
+      const int i = (int)(e / nely), j = (int)(e % nely);
+      const long long nx = nelx + 1;
+      nid[0] = (long long)j * nx + i;
+      nid[1] = (long long)j * nx + i + 1;
+      nid[2] = (long long)(j + 1) * nx + i + 1;
+      nid[3] = (long long)(j + 1) * nx + i;
+    }
+    double u[24];
+    for (int m = 0; m < nk; ++m) u[m] = U[nid[m / dim] * dim + m % dim];
+    double eps[6];
+    for (int b = 0; b < nb; ++b) {
+      double a = 0.0;
+      for (int m = 0; m < nk; ++m) a += B[b * nk + m] * u[m];
+      eps[b] = a;
+      strain[e * nb + b] = a;
+    }
+    for (int b = 0; b < nb; ++b) {
+      double a = 0.0;
+      for (int c = 0; c < nb; ++c) a += D[b * nb + c] * eps[c];
+      stress[e * nb + b] = a;
+    }
+    double en = 0.0;
+    for (int m = 0; m < nk; ++m) {
+      double a = 0.0;
+      for (int n2 = 0; n2 < nk; ++n2) a += K0[m * nk + n2] * u[n2];
+      en += u[m] * a;
+    }
+    energy[e] = 0.5 * w[e] * en;
+  }
+}
+
 // Loop control of the graph-captured PCG: the while node repeats while no stop reason is set;
 // the if node (mixed precision) computes a true residual when the recurrence has converged
 // or has dropped by `drop` since the last replacement.

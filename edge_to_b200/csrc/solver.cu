@@ -200,6 +200,7 @@ struct Prob {
   std::vector<void*> allocs;
   // element / operator data
   double* dK0b = nullptr;
+  double* dK0ref = nullptr;  // element matrix in the reference's corner order
   float* dK0bf = nullptr;
   double* dK0diag = nullptr;
   double* dQ = nullptr;
@@ -1070,6 +1071,55 @@ static void pcg64_body(Prob& P) {
          P.r64, (const double*)q, P.st, P.part, P.ticket, (float*)nullptr);
 }
 
+// Plain CG (no preconditioner), the reference's CG solver (solvers/_gpu.py:11-58, cupyx cg
+// with M = None): the FP64 PCG pieces with z = r.
+static void cg_prologue(Prob& P, double tol, int maxiter) {
+  CatScope cat(P, CAT_VECTOR);
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
+  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, 0.0, 0.0);
+  {
+    EpiResid<double, double, double> e{P.b64, P.r64, g.n};
+    fine_apply<double>(P, (const double*)P.x64, e, nullptr);
+    springs_apply(P, (const double*)P.x64, P.r64, -1.0, nullptr);
+  }
+  launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.b64, (const double*)P.b64, P.part, P.ticket,
+         &P.st->bb);
+  launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.r64, (const double*)P.r64, P.part, P.ticket,
+         &P.st->rr);
+  launch(P, k_pcg_check_bb, 1, 1, 0, P.st, (const int*)P.zero_int);
+}
+static void cg_body(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  double* p = (double*)P.p;
+  double* q = (double*)P.q;
+  launch(P, k_cg_rz, 1, 1, 0, P.st);
+  launch(P, k_pcg_p<double>, ew_blocks(nv), 256, 0, nv, p, (const double*)P.r64, (const PcgState*)P.st);
+  {
+    EpiStoreDot<double> e{q, g.n};
+    fine_apply<double>(P, (const double*)p, e, &P.st->pq);
+    springs_apply(P, (const double*)p, q, 1.0, &P.st->pq);
+  }
+  launch(P, k_pcg_xr<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, P.x64, (const double*)p,
+         P.r64, (const double*)q, P.st, P.part, P.ticket, (float*)nullptr);
+}
+// True residual after the loop (the reference recomputes ||f - K x|| / ||f||); r64 is
+// scratch at that point.
+static void cg_epilogue(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  EpiResid<double, double, double> e{P.b64, P.r64, g.n};
+  fine_apply<double>(P, (const double*)P.x64, e, nullptr);
+  springs_apply(P, (const double*)P.x64, P.r64, -1.0, nullptr);
+  launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, (const double*)P.r64,
+         (const double*)P.r64, P.part, P.ticket, &P.st->rr);
+  launch(P, k_final_res, 1, 1, 0, P.st);
+}
+
 // Mixed precision: FP32 operator, V-cycle and search directions; FP64 solution, residual
 // recurrence, dot products, coarse solve, and true residuals r = b - A x (FP64 operator
 // with FP64 E) that replace the recurrence every time it has dropped by REPLACE_DROP and
@@ -1175,8 +1225,8 @@ static void mg_setup_prec(Prob& P) {
 }
 
 // Capture parameters of the solve graph: anything baked into its launches.
-static std::vector<double> graph_key(const Prob& P, double tol, int maxiter) {
-  std::vector<double> k = {(double)P.prec, tol, (double)maxiter, (double)P.n_level, (double)P.n_smooth, P.omega,
+static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, bool cg = false) {
+  std::vector<double> k = {cg ? -1.0 : (double)P.prec, tol, (double)maxiter, (double)P.n_level, (double)P.n_smooth, P.omega,
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons};
   for (int l : P.w_levels) k.push_back((double)l);
@@ -1189,8 +1239,8 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter) {
 // whose body holds, for mixed precision, the replacement as an if node) into P.sg_exec.
 // Captured on the library's own streams so that the caller's stream may be the legacy
 // default stream; touches only buffers the problem owns.
-static void capture_solve(Prob& P, double tol, int maxiter) {
-  const bool mixed = P.prec != EDGE_FP64;
+static void capture_solve(Prob& P, double tol, int maxiter, bool cg = false) {
+  const bool mixed = !cg && P.prec != EDGE_FP64;
   for (int i = 0; i < 3; ++i)
     if (!P.cap[i]) CK(cudaStreamCreateWithFlags(&P.cap[i], cudaStreamNonBlocking));
   if (P.sg_exec) {
@@ -1203,17 +1253,21 @@ static void capture_solve(Prob& P, double tol, int maxiter) {
   }
   cudaStream_t user = P.stream;
   const long long n0 = P.nlaunch;
-  long long n1 = 0, n2 = 0, n3 = 0;
+  long long n1 = 0, n2 = 0, n3 = 0, n4e = 0;
   int depth = 0;  // captures open
   try {
     P.stream = P.cap[0];
     CK(cudaStreamBeginCapture(P.cap[0], cudaStreamCaptureModeThreadLocal));
     depth = 1;
-    mg_setup_prec(P);
-    if (mixed)
-      pcgmx_prologue(P, tol, maxiter);
-    else
-      pcg64_prologue(P, tol, maxiter);
+    if (cg)
+      cg_prologue(P, tol, maxiter);
+    else {
+      mg_setup_prec(P);
+      if (mixed)
+        pcgmx_prologue(P, tol, maxiter);
+      else
+        pcg64_prologue(P, tol, maxiter);
+    }
     cudaStreamCaptureStatus cs;
     cudaGraph_t g;
     const cudaGraphNode_t* deps;
@@ -1262,6 +1316,8 @@ static void capture_solve(Prob& P, double tol, int maxiter) {
       depth = 2;
       n3 = P.nlaunch;
       P.stream = P.cap[1];
+    } else if (cg) {
+      cg_body(P);
     } else {
       pcg64_body(P);
     }
@@ -1269,6 +1325,8 @@ static void capture_solve(Prob& P, double tol, int maxiter) {
     CK(cudaStreamEndCapture(P.cap[1], nullptr));
     depth = 1;
     P.stream = P.cap[0];
+    n4e = P.nlaunch;
+    if (cg) cg_epilogue(P);
     CK(cudaStreamEndCapture(P.cap[0], &P.sg_graph));
     depth = 0;
     CK(cudaGraphInstantiate(&P.sg_exec, P.sg_graph, 0));
@@ -1284,8 +1342,8 @@ static void capture_solve(Prob& P, double tol, int maxiter) {
     throw;
   }
   P.stream = user;
-  const long long n4 = P.nlaunch;
-  P.sg_pro = n1 - n0;
+  const long long n4 = n4e, n5 = P.nlaunch;
+  P.sg_pro = (n1 - n0) + (n5 - n4);  // prologue and epilogue run once
   if (mixed) {
     P.sg_if = n3 - n2;
     P.sg_body = (n2 - n1) + (n4 - n3);
@@ -1294,20 +1352,20 @@ static void capture_solve(Prob& P, double tol, int maxiter) {
     P.sg_body = n4 - n1;
   }
   P.nlaunch = n0;
-  P.sg_key = graph_key(P, tol, maxiter);
+  P.sg_key = graph_key(P, tol, maxiter, cg);
 }
 
-static void solve_graph(Prob& P, double tol, int maxiter) {
-  if (!P.sg_exec || P.sg_key != graph_key(P, tol, maxiter)) capture_solve(P, tol, maxiter);
+static void solve_graph(Prob& P, double tol, int maxiter, bool cg = false) {
+  if (!P.sg_exec || P.sg_key != graph_key(P, tol, maxiter, cg)) capture_solve(P, tol, maxiter, cg);
   CK(cudaEventRecord(P.ev[0], P.stream));
   CK(cudaGraphLaunch(P.sg_exec, P.stream));
   CK(cudaEventRecord(P.ev[2], P.stream));
   int status = 0;
-  CK(cudaMemcpyAsync(&status, P.chol_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+  if (!cg) CK(cudaMemcpyAsync(&status, P.chol_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
   read_state(P);
   if (status) fail(EDGE_ENOTPD, "coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
   P.last_iters = P.st_h->iter;
-  P.last_true_res = (P.prec != EDGE_FP64) ? 1 + P.st_h->n_true : 0;
+  P.last_true_res = cg ? 1 : ((P.prec != EDGE_FP64) ? 1 + P.st_h->n_true : 0);
   P.nlaunch += P.sg_pro + P.sg_body * (long long)P.st_h->iter + P.sg_if * (long long)P.st_h->n_true;
 }
 
@@ -1474,6 +1532,8 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     const int nk = P.ei.nk;
     P.dK0b = P.alloc<double>(nk * nk);
     CK(cudaMemcpy(P.dK0b, P.ei.K0b, nk * nk * sizeof(double), cudaMemcpyHostToDevice));
+    P.dK0ref = P.alloc<double>(nk * nk);
+    CK(cudaMemcpy(P.dK0ref, K0, nk * nk * sizeof(double), cudaMemcpyHostToDevice));
     std::vector<float> kf(nk * nk);
     for (int i = 0; i < nk * nk; ++i) kf[i] = (float)P.ei.K0b[i];
     P.dK0bf = P.alloc<float>(nk * nk);
@@ -1929,6 +1989,42 @@ int edge_mg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_l
   CK(cudaStreamSynchronize(P.stream));
   if (residual_out) *residual_out = P.st_h->res;
   if (iters_out) *iters_out = P.st_h->iter;
+  API_END
+}
+
+int edge_cg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
+                  double* residual_out, int* iters_out) {
+  API_BEGIN
+  if (!p || !f_dev || !x_dev) fail(EDGE_EINVAL, "null argument");
+  if (tol <= 0.0 || maxiter < 1) fail(EDGE_EINVAL, "tol must be > 0 and maxiter >= 1");
+  Prob& P = p->P;
+  if (!P.has_rho) fail(EDGE_ESTATE, "Solver requires a density vector to be passed or set on the kernel.");
+  const Geo& g = P.g0;
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, f_dev, P.b64);
+  if (use_last)
+    launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, x_dev, P.x64);
+  else
+    CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
+  solve_graph(P, tol, maxiter, true);
+  check_err(P);
+  launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, P.x64, x_dev);
+  CK(cudaStreamSynchronize(P.stream));
+  if (residual_out) *residual_out = P.st_h->res;
+  if (iters_out) *iters_out = P.st_h->iter;
+  API_END
+}
+
+int edge_fea_integrals(edge_problem* p, const double* U_dev, const double* w_dev, const double* B_dev,
+                       const double* D_dev, int nb, double* strain_dev, double* stress_dev, double* energy_dev) {
+  API_BEGIN
+  if (!p || !U_dev || !w_dev || !B_dev || !D_dev || !strain_dev || !stress_dev || !energy_dev)
+    fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  if (nb < 1 || nb > 6) fail(EDGE_EINVAL, "strain size must be in 1..6");
+  launch(P, k_fea_integrals, std::min<unsigned>(cdiv(P.n_el, 128), 148u * 32u), 128, 0, P.dim, P.nel[0], P.nel[1],
+         P.dim == 3 ? P.nel[2] : 1, P.n_el, U_dev, w_dev, (const double*)P.dK0ref, B_dev, D_dev, nb, strain_dev,
+         stress_dev, energy_dev);
+  CK(cudaStreamSynchronize(P.stream));
   API_END
 }
 

@@ -174,6 +174,27 @@ class CuStructuredStiffnessKernel(StiffnessKernel):
         _lib.call("edge_process_grad", self._h, _lib.ptr(U), _lib.ptr(self.dk))
         return self.dk
 
+    def fea_integrals(self, w, U, B, D):
+        """Per-element strain = B u_e, stress = D strain and strain energy 1/2 w_e u_e^T K0 u_e
+        (the structured path of TopOpt/_solver.py:80-137); B, D: the mesh's B_single, D_single.
+        Returns (strain [n_el, nb], stress [n_el, nb], strain_energy [n_el]) on the device."""
+        w = _as_dev_f64(w)
+        U = _as_dev_f64(U)
+        Bt = torch.as_tensor(np.ascontiguousarray(np.asarray(B, dtype=np.float64)), device="cuda")
+        Dt = torch.as_tensor(np.ascontiguousarray(np.asarray(D, dtype=np.float64)), device="cuda")
+        nb = Bt.shape[0]
+        if Bt.shape[1] != self.elements_size * self.dof or Dt.shape != (nb, nb):
+            raise ValueError("B must be nb x (element nodes * dof) and D nb x nb")
+        if w.numel() != self.n_elements or U.numel() != self.shape[0]:
+            raise ValueError("weights / displacement size does not match the mesh")
+        strain = torch.empty((self.n_elements, nb), dtype=torch.float64, device="cuda")
+        stress = torch.empty_like(strain)
+        energy = torch.empty(self.n_elements, dtype=torch.float64, device="cuda")
+        self._bind_stream()
+        _lib.call("edge_fea_integrals", self._h, _lib.ptr(U), _lib.ptr(w), _lib.ptr(Bt), _lib.ptr(Dt), int(nb),
+                  _lib.ptr(strain), _lib.ptr(stress), _lib.ptr(energy))
+        return strain, stress, energy
+
     # --------------------------------------------------------------- beyond the reference
     def set_springs(self, dofs, stiffness):
         """Grounded point springs K_ii += k on DOF indices ``dofs`` (the compliant-mechanism

@@ -173,3 +173,49 @@ class CuMultiGrid(Solver):
 
 
 MultiGrid = CuMultiGrid
+
+
+class CuCG(Solver):
+    """Conjugate gradients without a preconditioner on the matrix-free stiffness operator:
+    the reference's CG solver (solvers/_gpu.py:11-58, cupyx cg with M = None; the returned
+    residual is recomputed as ||f - K x|| / ||f||).  Works on any grid extent (the multigrid
+    needs element counts divisible by 2**n_level).  The iteration runs on the device as one
+    CUDA graph launch.  matrix_free=False in the reference assembles K first; the product
+    and hence the iterates are the same, so here it only records the choice."""
+
+    def __init__(self, kernel, maxiter=1000, tol=1e-5, matrix_free=None):
+        if not isinstance(kernel, CuStructuredStiffnessKernel):
+            raise TypeError("CuCG needs the package's CuStructuredStiffnessKernel")
+        self.kernel = kernel
+        self.last_x0 = None
+        self.tol = tol
+        self.maxiter = maxiter
+        self.matrix_free = True if matrix_free is None else bool(matrix_free)
+        self.last_iters = 0
+
+    def reset(self):
+        self.last_x0 = None
+
+    def solve(self, rhs, rho=None, use_last=True):
+        if not (self.kernel.has_rho or rho is not None):
+            raise ValueError("Solver requires a density vector to be passed or set on the kernel.")
+        if rho is not None:
+            self.kernel.set_rho(rho)
+        f = _as_dev_f64(rhs)
+        if use_last and self.last_x0 is not None:
+            x = self.last_x0.clone()
+            warm = 1
+        else:
+            x = torch.zeros_like(f)
+            warm = 0
+        res, its = ctypes.c_double(), ctypes.c_int()
+        self.kernel._bind_stream()
+        _lib.call("edge_cg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
+                  int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
+        if use_last:  # the reference keeps the warm start only on this branch
+            self.last_x0 = x
+        self.last_iters = its.value
+        return x, res.value
+
+
+CG = CuCG

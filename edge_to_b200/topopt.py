@@ -154,6 +154,26 @@ class CuTopOpt:
         return rho_new.reshape(-1)
 
     # ----------------------------------------------------------------- analysis (TopOpt/_cuda.py:282-302)
+    def FEA_integrals(self, rho):
+        """Strain, stress, strain energy and von Mises stress per element for the design rho
+        (TopOpt/_cuda.py:78-129): E = the material's 'plain' value (rho clipped to [void, 1]),
+        one solve of K(E) u = f warm-started from the last solution, then the element
+        integrals on the device (edge_fea_integrals).  Returns torch tensors on the device."""
+        rho_ = self.material_model(_as_dev_f64(rho).reshape(-1), 1e6, plain=True)
+        self.kernel.set_rho(rho_)
+        U, residual = self.solver.solve(self.f, use_last=True)
+        if residual > 1e-5:
+            logger.warning(f"Solver residual is above 1e-5 ({residual:.4e}). Consider higher iterations (rerun "
+                           f"this function and more iteration from prior solve will be applied).")
+        strain, stress, strain_energy = self.kernel.fea_integrals(rho_, U, self.mesh.B_single, self.mesh.D_single)
+        s = stress
+        if self.mesh.nodes.shape[1] == 2:
+            von_mises = torch.sqrt(s[:, 0] ** 2 + s[:, 1] ** 2 - s[:, 0] * s[:, 1] + 3 * s[:, 2] ** 2)
+        else:
+            von_mises = torch.sqrt(0.5 * ((s[:, 0] - s[:, 1]) ** 2 + (s[:, 1] - s[:, 2]) ** 2 + (s[:, 2] - s[:, 0]) ** 2
+                                          + 6 * (s[:, 3] ** 2 + s[:, 4] ** 2 + s[:, 5] ** 2)))
+        return strain, stress, strain_energy, von_mises
+
     def solve_and_process(self, rho, iteration):
         rho = _as_dev_f64(rho).reshape(-1)
         if self.fused:

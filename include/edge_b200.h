@@ -81,6 +81,22 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
  * precision) or the plain product.  The problem's own tile choice is left unchanged. */
 int edge_time_fine(edge_problem* p, int precision, int variant, int blocks_per_sm, int sweep, int reps,
                    double* ms);
+/* ---- FEA_integrals.  Replaces TopOpt/_solver.py:80-137 (TopOpt/_cuda.py:78-129) for
+ * structured meshes: per element (reference element order) strain = B u_e, stress = D strain,
+ * strain energy = 1/2 w_e u_e^T K0 u_e, with u_e from the user-layout displacement U in the
+ * reference's corner order.  B is nb x (corners*dim), D nb x nb, row-major (the mesh's
+ * B_single, D_single); w per element (the reference passes the 'plain' material values).
+ * Outputs: strain, stress [n_el][nb], energy [n_el].  All pointers are device memory. */
+int edge_fea_integrals(edge_problem* p, const double* U_dev, const double* w_dev, const double* B_dev,
+                       const double* D_dev, int nb, double* strain_dev, double* stress_dev, double* energy_dev);
+/* ---- conjugate gradients without a preconditioner.  Replaces the reference's CG solver
+ * (solvers/_gpu.py:11-58: cupyx.scipy.sparse.linalg.cg on the matrix-free kernel, M = None,
+ * stop at ||r|| <= tol ||f||, residual reported as ||f - K x|| / ||f||).  FP64; needs the
+ * density set; no multigrid configuration.  Runs as one CUDA graph launch (while node),
+ * captured on the first call.  use_last: start from x_dev (user layout) instead of zero.
+ * Does not fail on non-convergence: *iters_out == maxiter and the residual tell. */
+int edge_cg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
+                  double* residual_out, int* iters_out);
 /* Per-level smoothing sweeps (pre- and post-smoothing each), sweeps[l] for level l < n;
  * levels from n on use edge_mg_config's n_smooth (n = 0 restores that everywhere).  The
  * reference smooths every level n_smooth times (solvers/_multigrid_cuda.py:133-186); this

@@ -45,6 +45,16 @@ def dk(grid: Grid, K0, u):
     return -np.einsum("ea,ab,eb->e", ue, K0, ue)
 
 
+def fea_integrals(grid: Grid, K0, B, D, w, u):
+    """Element strain = B u_e, stress = D strain, strain energy = 1/2 w_e u_e^T K0 u_e
+    (core/_ops.py:1032-1058, the structured path of TopOpt/_solver.py:80-137)."""
+    ue = np.asarray(u)[grid.dof_map()]
+    strain = ue @ np.asarray(B).T
+    stress = strain @ np.asarray(D).T
+    energy = 0.5 * np.asarray(w) * np.einsum("ea,ab,eb->e", ue, K0, ue)
+    return strain, stress, energy
+
+
 def matvec_free(grid: Grid, K0, E, u, cons_mask=None):
     """Matrix-free K(E) u on the structured grid by corner slicing (numpy, for large grids).
 

@@ -311,6 +311,46 @@ def make_grad():
     print("grad: comp", comp, "res", res)
 
 
+def make_fea():
+    """FEA_integrals (TopOpt/_solver.py:80-137 and its structured kernel, core/_ops.py:1032-1058):
+    op-level with a random displacement on 2-D and 3-D grids, and the whole call (material
+    'plain' clip, solve, integrals) on a small MBB beam with a random design."""
+    ref = _REF
+    from EDGETO.core._ops import FEA_Integrals_node_basis_parallel
+    out = {}
+    rng = np.random.default_rng(11)
+    for tag, mesh in (("2d", ref.StructuredMesh2D(13, 7, 13.0, 7.0, stiffness=_stiff(0.3))),
+                      ("3d", ref.StructuredMesh3D(6, 5, 4, 6.0, 5.0, 4.0, stiffness=_stiff(0.3)))):
+        k = ref.StructuredStiffnessKernel(mesh)
+        nel = mesh.elements.shape[0]
+        w = rng.uniform(1e-3, 1.0, nel)
+        U = rng.standard_normal(mesh.nodes.shape[0] * mesh.dof)
+        strain, stress, energy = FEA_Integrals_node_basis_parallel(
+            mesh.K_single, mesh.D_single, mesh.B_single, k.elements_flat, nel, w, U, mesh.dof,
+            mesh.elements_size, mesh.B_single.shape[0])
+        out.update({f"{tag}_w": w, f"{tag}_U": U, f"{tag}_strain": strain, f"{tag}_stress": stress,
+                    f"{tag}_energy": energy, f"{tag}_B": mesh.B_single, f"{tag}_D": mesh.D_single})
+    # whole call on a 24x12 MBB beam
+    mesh = ref.StructuredMesh2D(24, 12, 24.0, 12.0, stiffness=_stiff(0.3))
+    mat = ref.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=0.5)
+    k = ref.StructuredStiffnessKernel(mesh)
+    filt = ref.StructuredFilter2D(mesh, 1.5)
+    solver = ref.MultiGrid(mesh, k, tol=1e-12, n_level=2, maxiter=4000)
+    opt = ref.TopOpt(mesh, mat, k, solver, filt, max_iter=1, verbose=False)
+    nodes = mesh.nodes
+    left = np.where(np.isclose(nodes[:, 0], 0.0))[0]
+    opt.add_BC_nodal(left, np.array([[True, False]]))
+    br = np.where(np.isclose(nodes[:, 0], 24.0) & np.isclose(nodes[:, 1], 0.0))[0]
+    opt.add_BC_nodal(br, np.array([[False, True]]))
+    tl = np.where(np.isclose(nodes[:, 0], 0.0) & np.isclose(nodes[:, 1], 12.0))[0]
+    opt.add_F_nodal(tl, np.array([[0.0, -1.0]]))
+    rho = rng.uniform(0.05, 1.0, mesh.elements.shape[0])
+    strain, stress, energy, vm = opt.FEA_integrals(rho)
+    out.update(call_rho=rho, call_strain=strain, call_stress=stress, call_energy=energy, call_vm=np.asarray(vm))
+    np.savez_compressed(os.path.join(HERE, "fea.npz"), **out)
+    print("fea: energy sum", float(np.sum(energy)))
+
+
 _REF = None
 
 if __name__ == "__main__":
@@ -318,7 +358,8 @@ if __name__ == "__main__":
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
     _REF = _import_reference()
-    jobs = {"kat": make_kat, "ops": make_ops, "mbb": make_loop_mbb, "cant": make_loop_cant3d, "grad": make_grad}
+    jobs = {"kat": make_kat, "ops": make_ops, "mbb": make_loop_mbb, "cant": make_loop_cant3d, "grad": make_grad,
+            "fea": make_fea}
     for name, fn in jobs.items():
         if args.only and name not in args.only.split(","):
             continue

@@ -1,0 +1,108 @@
+"""Solvers beyond the multigrid: CuCG (the reference's unpreconditioned CG,
+solvers/_gpu.py:11-58) on grids of any extent, checked against direct solves and scipy's CG
+on the oracle's assembled matrix.
+
+Tolerances: solutions to 1e-6 relative of the direct solve at tol 1e-10 (the error bound of
+CG at that residual times the matrix's conditioning on these small grids); iteration counts
+within 2 of scipy's CG (same recurrences, different summation order).
+"""
+import numpy as np
+import pytest
+
+from oracle import ops, topopt
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _problem(nel, seed, lo=0.05):
+    import torch
+    import edge_to_b200 as eb
+    p = topopt.mbb_problem(*nel) if len(nel) == 2 else topopt.cantilever_problem(*nel)
+    rng = np.random.default_rng(seed)
+    E = np.clip(rng.uniform(lo, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    st = lambda x: eb.auto_stiffness(x, 1.0, 0.3)  # noqa: E731
+    mesh = (eb.CuStructuredMesh2D(*nel, *[float(v) for v in nel], stiffness=st) if len(nel) == 2 else
+            eb.CuStructuredMesh3D(*nel, *[float(v) for v in nel], stiffness=st))
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    K = ops.assemble(p.grid, p.K0, E, p.cons)
+    return p, k, K, torch.as_tensor(p.f, device="cuda")
+
+
+@pytest.mark.parametrize("nel", [(61, 23), (13, 7, 5)])
+def test_cg_matches_direct_solve(nel):
+    import scipy.sparse.linalg as sla
+    import edge_to_b200 as eb
+    p, k, K, f = _problem(nel, 1)
+    s = eb.CuCG(k, maxiter=20000, tol=1e-10)
+    x, r = s.solve(f, use_last=False)
+    xd = sla.spsolve(K.tocsc(), p.f)
+    xg = x.cpu().numpy()
+    true_res = np.linalg.norm(p.f - K @ xg) / np.linalg.norm(p.f)
+    # the loop stops on the recurrence residual; the reported one is the true residual, which
+    # rounding keeps within a small factor of the tolerance (the reference reports the same)
+    assert r < 1e-9 and abs(r - true_res) <= 1e-3 * true_res + 1e-14
+    assert rel(xg, xd) < 1e-6
+    assert s.last_x0 is None  # the reference keeps a warm start only when use_last is set
+
+
+def test_cg_iterations_follow_scipy_cg():
+    import scipy.sparse.linalg as sla
+    import edge_to_b200 as eb
+    p, k, K, f = _problem((9, 5, 4), 2, lo=0.5)
+    count = []
+    sla.cg(K, p.f, rtol=1e-8, atol=0.0, maxiter=5000, callback=lambda xk: count.append(1))
+    s = eb.CuCG(k, maxiter=5000, tol=1e-8)
+    x, r = s.solve(f)
+    assert abs(s.last_iters - len(count)) <= 2, (s.last_iters, len(count))
+    # warm start: the second solve of the same system starts at the solution
+    x2, r2 = s.solve(f)
+    assert s.last_iters <= 1 and r2 < 1e-8
+
+
+def test_cg_does_not_raise_on_maxiter():
+    import edge_to_b200 as eb
+    p, k, K, f = _problem((31, 17), 3)
+    s = eb.CuCG(k, maxiter=7, tol=1e-12)
+    x, r = s.solve(f, use_last=False)
+    assert s.last_iters == 7 and r > 1e-12 and np.isfinite(r)
+
+
+def test_fea_integrals_against_reference(golden):
+    """edge_fea_integrals equals the reference's element integrals (random displacements, 1e-12),
+    and CuTopOpt.FEA_integrals equals the reference's whole call on a 24x12 MBB beam with a
+    random design (both solved to 1e-12: 1e-8)."""
+    import torch
+    import edge_to_b200 as eb
+    z = golden("fea.npz")
+    st = lambda x: eb.auto_stiffness(x, 1.0, 0.3)  # noqa: E731
+    for tag, nel in (("2d", (13, 7)), ("3d", (6, 5, 4))):
+        mesh = (eb.CuStructuredMesh2D(*nel, *[float(v) for v in nel], stiffness=st) if len(nel) == 2 else
+                eb.CuStructuredMesh3D(*nel, *[float(v) for v in nel], stiffness=st))
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        s, ss, en = k.fea_integrals(z[f"{tag}_w"], z[f"{tag}_U"], mesh.B_single, mesh.D_single)
+        for a, b in ((s, z[f"{tag}_strain"]), (ss, z[f"{tag}_stress"]), (en, z[f"{tag}_energy"])):
+            assert rel(a.cpu().numpy(), b) <= 1e-12, tag
+    mesh = eb.CuStructuredMesh2D(24, 12, 24.0, 12.0, stiffness=st)
+    mat = eb.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=0.5)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    filt = eb.CuStructuredFilter2D(mesh, 1.5)
+    solver = eb.CuMultiGrid(mesh, k, tol=1e-12, n_level=2, maxiter=4000)
+    opt = eb.CuTopOpt(mesh, mat, k, solver, filt, max_iter=1, verbose=False)
+    nodes = mesh.nodes
+    opt.add_BC_nodal(np.where(np.isclose(nodes[:, 0], 0.0))[0], np.array([[True, False]]))
+    opt.add_BC_nodal(np.where(np.isclose(nodes[:, 0], 24.0) & np.isclose(nodes[:, 1], 0.0))[0],
+                     np.array([[False, True]]))
+    opt.add_F_nodal(np.where(np.isclose(nodes[:, 0], 0.0) & np.isclose(nodes[:, 1], 12.0))[0],
+                    np.array([[0.0, -1.0]]))
+    strain, stress, energy, vm = opt.FEA_integrals(torch.as_tensor(z["call_rho"], device="cuda"))
+    for a, b in ((strain, z["call_strain"]), (stress, z["call_stress"]), (energy, z["call_energy"]),
+                 (vm, z["call_vm"])):
+        assert rel(a.cpu().numpy(), b) <= 1e-8

@@ -145,3 +145,23 @@ def test_gradient_random_rho(golden):
     comp, dr, res, U = p.solve_and_process(z["rho"])
     assert abs(comp - float(z["compliance"])) / comp < 1e-8
     assert rel(dr, z["dr"]) < 1e-7
+
+
+def test_fea_integrals_oracle_and_element_matrices(golden):
+    """Oracle element integrals (strain, stress, strain energy) equal the reference's on random
+    displacements, and this package's meshes build the reference's B_single / D_single."""
+    import edge_to_b200 as eb
+    from oracle import elements
+    z = golden("fea.npz")
+    for tag, nel in (("2d", (13, 7)), ("3d", (6, 5, 4))):
+        g = Grid(nel)
+        K0 = elements.q4_stiffness(1, 1, E=1.0, nu=0.3) if g.dim == 2 else elements.hex8_stiffness(1, 1, 1, E=1.0,
+                                                                                                   nu=0.3)
+        st, ss, en = ops.fea_integrals(g, K0, z[f"{tag}_B"], z[f"{tag}_D"], z[f"{tag}_w"], z[f"{tag}_U"])
+        for a, b in ((st, z[f"{tag}_strain"]), (ss, z[f"{tag}_stress"]), (en, z[f"{tag}_energy"])):
+            assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+        stiff = lambda x: eb.auto_stiffness(x, 1.0, 0.3)  # noqa: E731
+        mesh = (eb.CuStructuredMesh2D(*nel, *[float(v) for v in nel], stiffness=stiff) if g.dim == 2 else
+                eb.CuStructuredMesh3D(*nel, *[float(v) for v in nel], stiffness=stiff))
+        assert np.abs(mesh.B_single - z[f"{tag}_B"]).max() <= 1e-13
+        assert np.abs(mesh.D_single - z[f"{tag}_D"]).max() <= 1e-13
