@@ -10,6 +10,7 @@ coarse_solver only selects between equivalent exact solves.
 """
 import ctypes
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -25,6 +26,87 @@ class Solver:
 
     def reset(self):
         pass
+
+
+class _PaddedGrid:
+    """Embedding of a structured problem whose element counts are not all divisible by
+    2**n_level into the next grid that is: the real grid keeps its numbering in the lower
+    corner, padding elements have zero stiffness and every node that touches only padding
+    elements is constrained (identity rows, zero load).  The padded system restricted to the
+    real DOFs is the original one, and its solution is zero on the padding, so a solve on the
+    padded grid answers the original problem while the multigrid coarsens cleanly.  (The
+    reference's multigrid has no such handling: on odd extents its prolongation is not the
+    restriction's transpose and PCG stalls.)"""
+
+    def __init__(self, kernel, n_level):
+        from .mesh import CuStructuredMesh2D, CuStructuredMesh3D
+        mesh = kernel.mesh
+        m = 2 ** n_level
+        nel = [int(v) for v in mesh.nel]
+        pad = [(v + m - 1) // m * m for v in nel]
+        h = [float(L) / n for L, n in zip(mesh.dim, nel)]
+        elem = (mesh.K_single, mesh.D_single, mesh.B_single, float(mesh.A_single[0]))
+        stiff = lambda x0: elem  # noqa: E731  (the real mesh's element, so K0 is identical)
+        if len(nel) == 2:
+            pm = CuStructuredMesh2D(pad[0], pad[1], pad[0] * h[0], pad[1] * h[1], stiffness=stiff)
+        else:
+            pm = CuStructuredMesh3D(pad[0], pad[1], pad[2], pad[0] * h[0], pad[1] * h[1], pad[2] * h[2],
+                                    stiffness=stiff)
+        self.nel, self.pad = nel, pad
+        self.kernel = CuStructuredStiffnessKernel(pm)
+        dof = kernel.dof
+        if len(nel) == 2:
+            i, j = np.meshgrid(np.arange(nel[0]), np.arange(nel[1]), indexing="ij")
+            el = (i * pad[1] + j).ravel()                                    # e = i*nely + j
+            jn, in_ = np.meshgrid(np.arange(nel[1] + 1), np.arange(nel[0] + 1), indexing="ij")
+            nodes = (jn * (pad[0] + 1) + in_).ravel()                        # n = j*(nelx+1) + i
+            pj, pi = np.meshgrid(np.arange(pad[1] + 1), np.arange(pad[0] + 1), indexing="ij")
+            outside = ((pi > nel[0]) | (pj > nel[1])).ravel()
+        else:
+            i, j, k = np.meshgrid(np.arange(nel[0]), np.arange(nel[1]), np.arange(nel[2]), indexing="ij")
+            el = (i * pad[1] * pad[2] + j * pad[2] + k).ravel()             # e = i*ny*nz + j*nz + k
+            jn, in_, kn = np.meshgrid(np.arange(nel[1] + 1), np.arange(nel[0] + 1), np.arange(nel[2] + 1),
+                                      indexing="ij")
+            nodes = (jn * (pad[0] + 1) * (pad[2] + 1) + in_ * (pad[2] + 1) + kn).ravel()  # n = j*nx*nz + i*nz + k
+            pj, pi, pk = np.meshgrid(np.arange(pad[1] + 1), np.arange(pad[0] + 1), np.arange(pad[2] + 1),
+                                     indexing="ij")
+            outside = ((pi > nel[0]) | (pj > nel[1]) | (pk > nel[2])).ravel()
+        self.el_map = torch.as_tensor(el, device="cuda")
+        self.dof_map = torch.as_tensor((nodes[:, None] * dof + np.arange(dof)[None, :]).ravel(), device="cuda")
+        self.pad_dofs = torch.as_tensor(
+            (np.nonzero(outside)[0][:, None] * dof + np.arange(dof)[None, :]).ravel(), device="cuda")
+        self._cons_key = None
+        self._springs_key = None
+
+    def sync(self, kernel):
+        """Copy the real kernel's density, constraints and springs onto the padded kernel."""
+        kp = self.kernel
+        E = torch.zeros(kp.n_elements, dtype=torch.float64, device="cuda")
+        E[self.el_map] = _as_dev_f64(kernel.rho).reshape(-1)
+        kp.set_rho(E)
+        key = (kernel.constraints.data_ptr(), int(kernel.constraints.sum().item()), kernel.has_con)
+        if key != self._cons_key:
+            c = torch.zeros(kp.shape[0], dtype=torch.bool, device="cuda")
+            c[self.dof_map] = kernel.constraints
+            c[self.pad_dofs] = True
+            kp.set_constraints(torch.nonzero(c).reshape(-1))
+            self._cons_key = key
+        springs = getattr(kernel, "springs", None)
+        skey = None if springs is None else (tuple(springs[0].tolist()), tuple(springs[1].tolist()))
+        if skey != self._springs_key:
+            if springs is None:
+                kp.set_springs([], [])
+            else:
+                kp.set_springs(self.dof_map[torch.as_tensor(springs[0], device="cuda")].cpu().numpy(), springs[1])
+            self._springs_key = skey
+
+    def embed(self, v):
+        out = torch.zeros(self.kernel.shape[0], dtype=torch.float64, device="cuda")
+        out[self.dof_map] = _as_dev_f64(v).reshape(-1)
+        return out
+
+    def extract(self, v):
+        return v[self.dof_map]
 
 
 class CuMultiGrid(Solver):
@@ -73,9 +155,20 @@ class CuMultiGrid(Solver):
         # whole solves of the first system; the converged solution meets the same tolerance
         self.tune_sweeps = (precision == "mixed") if tune_sweeps is None else bool(tune_sweeps)
         self.sweeps = None
+        # element counts not divisible by 2**n_level: solve on a padded grid (_PaddedGrid)
+        self._pad = None
+        self._inner = None
+        if any(int(v) % (2 ** n_level) for v in mesh.nel):
+            self._pad = _PaddedGrid(kernel, n_level)
+            self._inner = CuMultiGrid(self._pad.kernel.mesh, self._pad.kernel, maxiter=maxiter, tol=tol,
+                                      n_smooth=n_smooth, omega=omega, n_level=n_level, cycle=cycle, w_level=w_level,
+                                      min_omega=min_omega, omega_boost=omega_boost, precision=precision,
+                                      autotune=autotune, graph=graph, tune_sweeps=tune_sweeps)
 
     def reset(self):
         self.last_x0 = None
+        if self._inner is not None:
+            self._inner.reset()
 
     def _configure(self):
         key = (self.n_level, self.n_smooth, self.max_omega, self.min_omega, self.cycle, tuple(self.w_level),
@@ -140,11 +233,29 @@ class CuMultiGrid(Solver):
         self.sweeps = {"per_level": best[1], "solve_ms": best[0], "pcg_iters": best[2]}
         return self.sweeps
 
+    @property
+    def padded(self):
+        """True when this solver works on a padded copy of the grid (odd extents)."""
+        return self._pad is not None
+
+    def _solve_padded(self, rhs, use_last):
+        inner = self._inner
+        inner.tol, inner.maxiter = self.tol, self.maxiter
+        self._pad.sync(self.kernel)
+        xp, res = inner.solve(self._pad.embed(rhs), use_last=use_last)
+        x = self._pad.extract(xp)
+        self.last_x0 = x
+        self.last_iters = inner.last_iters
+        self.tuned, self.sweeps = inner.tuned, inner.sweeps
+        return x, res
+
     def solve(self, rhs, rho=None, use_last=True):
         if not (self.kernel.has_rho or rho is not None):
             raise ValueError("Solver requires a density vector to be passed or set on the kernel.")
         if rho is not None:
             self.kernel.set_rho(rho)
+        if self._pad is not None:
+            return self._solve_padded(rhs, use_last)
         self._configure()
         self.tune()
         self.tune_sweep_counts(rhs)
@@ -165,6 +276,8 @@ class CuMultiGrid(Solver):
         return x, res.value
 
     def stats(self):
+        if self._inner is not None:
+            return self._inner.stats()
         a, b = ctypes.c_double(), ctypes.c_double()
         i, t = ctypes.c_int(), ctypes.c_int()
         _lib.call("edge_last_solve_stats", self.kernel.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(i),

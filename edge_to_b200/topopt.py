@@ -64,7 +64,7 @@ class CuTopOpt:
     def fused(self):
         return (isinstance(self.kernel, CuStructuredStiffnessKernel) and isinstance(self.solver, CuMultiGrid)
                 and isinstance(self.filter_kernel, _CuStructuredFilter) and isinstance(self.material_model, SingleMaterial)
-                and self.solver.kernel is self.kernel)
+                and self.solver.kernel is self.kernel and not self.solver.padded)
 
     # ----------------------------------------------------------------- BCs and loads (TopOpt/_cuda.py:131-240)
     def reset_BC(self):

@@ -106,3 +106,60 @@ def test_fea_integrals_against_reference(golden):
     for a, b in ((strain, z["call_strain"]), (stress, z["call_stress"]), (energy, z["call_energy"]),
                  (vm, z["call_vm"])):
         assert rel(a.cpu().numpy(), b) <= 1e-8
+
+
+class _Direct:
+    """Exact solve for the oracle's SIMP loop on grids the reference multigrid cannot coarsen."""
+
+    def solve(self, K, f, use_last=True):
+        import scipy.sparse.linalg as sla
+        return sla.spsolve(K.tocsc(), f), 0.0
+
+
+@pytest.mark.parametrize("nel,n_level", [((61, 23), 3), ((13, 7, 5), 2)])
+def test_padded_multigrid_on_odd_extents(nel, n_level):
+    """Element counts not divisible by 2**n_level: CuMultiGrid solves on a padded grid and
+    returns the direct solution of the original system (the reference's multigrid stalls)."""
+    import scipy.sparse.linalg as sla
+    import edge_to_b200 as eb
+    p, k, K, f = _problem(nel, 5)
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-8)):
+        s = eb.CuMultiGrid(k.mesh, k, tol=tol, n_level=n_level, maxiter=500, precision=prec)
+        assert s.padded
+        x, r = s.solve(f, use_last=False)
+        xd = sla.spsolve(K.tocsc(), p.f)
+        assert r < tol and s.last_iters < 200, (prec, r, s.last_iters)
+        assert rel(x.cpu().numpy(), xd) < (1e-6 if prec == "fp64" else 1e-4)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_simp_loop_on_odd_mbb_beam(precision):
+    """Ten SIMP iterations on a 61x23 MBB beam (not coarsenable by the reference multigrid):
+    compliance history against the oracle's loop with exact solves."""
+    import torch
+    import edge_to_b200 as eb
+    nelx, nely = 61, 23
+    ref = topopt.mbb_problem(nelx, nely, vf=0.5, rmin=1.5)
+    ref.solver = _Direct()
+    rho_ref, hist = ref.optimize(0.5, 10)
+    st = lambda x: eb.auto_stiffness(x, 1.0, 0.3)  # noqa: E731
+    mesh = eb.CuStructuredMesh2D(nelx, nely, float(nelx), float(nely), stiffness=st)
+    mat = eb.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=0.5)
+    mat.init_desvars = lambda nel, **kw: torch.full((nel,), 0.5, dtype=torch.float64, device="cuda")
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    filt = eb.CuStructuredFilter2D(mesh, 1.5)
+    solver = eb.CuMultiGrid(mesh, k, tol=1e-10 if precision == "fp64" else 1e-8, n_level=3, maxiter=1000,
+                            precision=precision)
+    opt = eb.CuTopOpt(mesh, mat, k, solver, filt, max_iter=10, ch_tol=0, fun_tol=0, verbose=False)
+    nodes = mesh.nodes
+    opt.add_BC_nodal(np.where(np.isclose(nodes[:, 0], 0.0))[0], np.array([[True, False]]))
+    opt.add_BC_nodal(np.where(np.isclose(nodes[:, 0], nelx) & np.isclose(nodes[:, 1], 0.0))[0],
+                     np.array([[False, True]]))
+    opt.add_F_nodal(np.where(np.isclose(nodes[:, 0], 0.0) & np.isclose(nodes[:, 1], nely))[0],
+                    np.array([[0.0, -1.0]]))
+    assert not opt.fused
+    rho, flag, h = opt.optimize(save_comp_history=True)
+    c = np.array(h["comp_history"])
+    err = np.abs(c - np.array(hist["comp"])) / np.array(hist["comp"])
+    assert err.max() < (1e-8 if precision == "fp64" else 1e-6), err
+    assert np.abs(rho.cpu().numpy() - rho_ref).max() < (1e-6 if precision == "fp64" else 1e-4)
