@@ -467,6 +467,37 @@ def run_tiles(args, cfg_name):
             "stencil_levels": levels}
 
 
+def run_batch(args):
+    """Batching configuration: 256 randomized 2-D problems of uneven size (edge_to_b200.batch),
+    spread over host threads with one CUDA stream each; value = problem-iterations per second
+    (one SIMP iteration of one problem = filter + SIMP law + GMG-PCG solve + sensitivities + OC)."""
+    import numpy as np
+    import torch
+    from edge_to_b200 import batch
+    torch.cuda.set_device(0)
+    n = args.batch_size
+    specs = [batch.random_spec(i, seed=0) for i in range(n)]
+    b = batch.BatchSIMP(specs, precision=args.precision, tol=1e-6, maxiter=1000, n_threads=args.batch_threads)
+    b.step(args.warmup)               # initial analysis, autotuners, warm-up iterations
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = b.step(args.steps)
+    clk = clocks.stop()
+    pcg = [int(np.mean(it["pcg"][-args.steps:])) for it in b.items]
+    dofs = [2 * (sp["nelx"] + 1) * (sp["nely"] + 1) for sp in specs]
+    return {"metric": "SIMP problem-iterations/s, 256 random uneven 2-D problems", "value": n * args.steps / (ms / 1e3),
+            "unit": "problem-iter/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+bf16/f64",
+            "data": "synthetic: seeded random problems (edge_to_b200.batch.random_spec, seed 0)",
+            "config": {"workload": f"batch{n}_2d", "problems": n, "dof_total": int(np.sum(dofs)),
+                       "elements_total": int(sum(sp["nelx"] * sp["nely"] for sp in specs)),
+                       "rtol": 1e-6, "precision": args.precision, "threads_streams": b.n_threads,
+                       "padded_problems": int(sum(it["opt"].solver.padded for it in b.items)),
+                       "pcg_iters_mean": float(np.mean(pcg))},
+            "clocks": clk}
+
+
 def run_reference(args, cfg_name):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -511,12 +542,18 @@ def main():
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--n-smooth", type=int, default=3,
                     help="default smoothing sweeps of the timed path (the FP64 path keeps the reference's 3)")
+    ap.add_argument("--batch", action="store_true",
+                    help="the batching configuration (random uneven 2-D problems) instead of --config")
+    ap.add_argument("--batch-size", type=int, default=256)
+    ap.add_argument("--batch-threads", type=int, default=16)
     ap.add_argument("--breakdown", action="store_true",
                     help="extra untimed step with per-category launch timing (events on every launch)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         line = run_reference(args, args.config)
+    elif args.batch:
+        line = run_batch(args)
     elif args.mode == "matvec":
         line = run_matvec(args, args.config)
     elif args.mode == "tiles":

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <cmath>
@@ -346,13 +347,17 @@ static Geo level_geo(const Prob& P, int l) {
 // ------------------------------------------------------------------ TMA tensor maps
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
+// Queried once per process (problems may live on different host threads).
 static void get_encode() {
-  if (g_encode) return;
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-  if (q != cudaDriverEntryPointSuccess || !fn) fail(EDGE_ECUDA, "cuTensorMapEncodeTiled not available");
-  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  static std::once_flag once;
+  std::call_once(once, []() {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && fn)
+      g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  });
+  if (!g_encode) fail(EDGE_ECUDA, "cuTensorMapEncodeTiled not available");
 }
 
 static CUtensorMap encode_map(const void* base, CUtensorMapDataType dt, int rank, const uint64_t* dims,
@@ -547,8 +552,8 @@ template <typename T, class Epi, int BX, int NS>
 static void fine3_tma_launch(Prob& P, const T* u, const T* E, Epi epi, double* dot_dst) {
   const Geo& g = P.g0;
   constexpr int smem = tma_smem_bytes<T, BX, NS>();
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<bool> attr{false};  // setting the attribute twice is harmless
+  if (!attr.load()) {
     CK(cudaFuncSetAttribute(k_fine3_tma<T, Epi, BX, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }
@@ -567,8 +572,8 @@ template <class Epi, int BX, int NS, int MINB>
 static void fine3_pk_launch(Prob& P, const float* u, const float* E, Epi epi, double* dot_dst) {
   const Geo& g = P.g0;
   constexpr int smem = pk_smem_bytes<BX, NS>();
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<bool> attr{false};  // setting the attribute twice is harmless
+  if (!attr.load()) {
     CK(cudaFuncSetAttribute(k_fine3_pk<Epi, BX, NS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }
@@ -652,8 +657,8 @@ static void fine3_cube_launch(Prob& P, const float* u, const float* E, Epi epi0,
   SE epi = ST::make(epi0, arr);
   const Geo& g = P.g0;
   constexpr int smem = cube_smem_bytes<BX, NS, SE>();
-  static bool attr = false;
-  if (!attr) {
+  static std::atomic<bool> attr{false};  // setting the attribute twice is harmless
+  if (!attr.load()) {
     CK(cudaFuncSetAttribute(k_fine3_cube<SE, BX, NS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }

@@ -163,3 +163,26 @@ def test_simp_loop_on_odd_mbb_beam(precision):
     err = np.abs(c - np.array(hist["comp"])) / np.array(hist["comp"])
     assert err.max() < (1e-8 if precision == "fp64" else 1e-6), err
     assert np.abs(rho.cpu().numpy() - rho_ref).max() < (1e-6 if precision == "fp64" else 1e-4)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_of_random_problems_against_oracle(precision):
+    """Random uneven 2-D problems (the batching configuration's generator at reduced sizes)
+    solved concurrently on several streams: every problem's compliance history matches the
+    oracle's SIMP loop with exact solves."""
+    from edge_to_b200 import batch
+    specs = [batch.random_spec(i, seed=100, nelx_range=(20, 44), nely_range=(12, 26)) for i in range(6)]
+    tol = 1e-10 if precision == "fp64" else 1e-8
+    b = batch.BatchSIMP(specs, precision=precision, tol=tol, maxiter=2000, n_threads=3)
+    ms = b.step(6)  # initial analysis + 5 design updates per problem
+    assert ms > 0
+    for spec, item in zip(specs, b.items):
+        ref = topopt.SIMPOracle((spec["nelx"], spec["nely"]), vf=spec["vf"], rmin=spec["rmin"])
+        ref.add_bc_nodal(spec["clamped_nodes"], [[True, True]])
+        ref.add_force_nodal(spec["load_nodes"], spec["forces"])
+        ref.solver = _Direct()
+        _, hist = ref.optimize(spec["vf"], 5)
+        c = np.array(item["comp"])
+        want = np.array([hist["comp0"]] + hist["comp"])
+        err = np.abs(c - want) / np.abs(want)
+        assert err.max() < (1e-7 if precision == "fp64" else 1e-5), (spec["index"], err)
