@@ -114,7 +114,7 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def build_problem(cfg, precision, n_smooth=3):
+def build_problem(cfg, precision, n_smooth=3, graph=True):
     import numpy as np
     import torch
     import edge_to_b200 as eb
@@ -124,7 +124,7 @@ def build_problem(cfg, precision, n_smooth=3):
     k = eb.CuStructuredStiffnessKernel(mesh)
     filt = eb.CuStructuredFilter3D(mesh, cfg["rmin"])
     solver = eb.CuMultiGrid(mesh, k, tol=cfg["tol"], n_level=cfg["n_level"], maxiter=1000, precision=precision,
-                            n_smooth=n_smooth)
+                            n_smooth=n_smooth, graph=graph)
     opt = eb.CuTopOpt(mesh, mat, k, solver, filt, max_iter=1, move=0.2, verbose=False)
     nx, ny, nz = nel[0] + 1, nel[1] + 1, nel[2] + 1
     j, k_ = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
@@ -217,7 +217,7 @@ def run_ours(args, cfg_name):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     cfg = CONFIGS[cfg_name]
-    opt, rho = build_problem(cfg, args.precision, args.n_smooth)
+    opt, rho = build_problem(cfg, args.precision, args.n_smooth, graph=not args.no_graph)
     rho, dr, it = warm(opt, rho, args.warmup)
 
     # ---------------- device-timed region: inputs resident in HBM; each solve is one CUDA
@@ -542,6 +542,8 @@ def main():
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--n-smooth", type=int, default=3,
                     help="default smoothing sweeps of the timed path (the FP64 path keeps the reference's 3)")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="host-driven PCG loop instead of one CUDA graph per solve (same launches; for profilers)")
     ap.add_argument("--batch", action="store_true",
                     help="the batching configuration (random uneven 2-D problems) instead of --config")
     ap.add_argument("--batch-size", type=int, default=256)

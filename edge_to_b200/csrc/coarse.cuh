@@ -36,6 +36,21 @@ EDGE_HD double bnd_total3(int nb) { return nb == 3 ? 3.375 : nb == 2 ? 4.5 : nb 
 EDGE_HD double bnd_total2(int nb) { return nb == 2 ? 2.25 : nb == 1 ? 3.0 : 4.0; }
 EDGE_HD double dist_w(int d) { return d == 0 ? 1.0 : d == 1 ? 0.5 : d == 2 ? 0.25 : 0.125; }
 EDGE_D int is_bnd(int i, int n) { return (i == 0 || i == n - 1) ? 1 : 0; }
+// 1 / bnd_total: the transfers multiply by these instead of dividing (a divide in FP64 is a
+// long instruction sequence; the results differ from the division by rounding only)
+template <typename T> EDGE_D T inv_bnd_total3(int nb) {
+  return nb == 3 ? T(1.0 / 3.375) : nb == 2 ? T(1.0 / 4.5) : nb == 1 ? T(1.0 / 6.0) : T(0.125);
+}
+template <typename T> EDGE_D T inv_bnd_total2(int nb) {
+  return nb == 2 ? T(1.0 / 2.25) : nb == 1 ? T(1.0 / 3.0) : T(0.25);
+}
+// arithmetic type of a transfer producing TO: FP64 for FP64 vectors, FP32 otherwise
+template <typename TO> struct TransferT {
+  using type = float;
+};
+template <> struct TransferT<double> {
+  using type = double;
+};
 
 // ------------------------------------------------------------------ symmetric stencil access
 constexpr int NST3 = 123;
@@ -245,13 +260,16 @@ __global__ void k_st_dinv(const Geo g, const TS* __restrict__ S, TD* __restrict_
 
 // ------------------------------------------------------------------ transfers
 template <typename TI, typename TO>
+// 3-D transfers: one thread per output node; blockIdx.y = plane y, the (z, x) pairs of a plane
+// flattened over blockIdx.x (z fastest).
 __global__ void k_restrict3(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
-  const int K = blockIdx.x * blockDim.x + threadIdx.x;
-  const int I = blockIdx.y, J = blockIdx.z;
-  if (K >= gc.nz) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int J = blockIdx.y;
+  if (t >= gc.nz * gc.nx) return;
+  const int K = t % gc.nz, I = t / gc.nz;
+  using T = typename TransferT<TO>::type;
   const int nb = is_bnd(I, gc.nx) + is_bnd(J, gc.ny) + is_bnd(K, gc.nz);
-  const double W = bnd_total3(nb);
-  double v[3] = {0, 0, 0};
+  T v[3] = {0, 0, 0};
   for (int di = -1; di <= 1; ++di) {
     const int fi = 2 * I + di;
     if (fi < 0 || fi >= gf.nx) continue;
@@ -261,14 +279,15 @@ __global__ void k_restrict3(const Geo gf, const Geo gc, const TI* __restrict__ i
       for (int dk = -1; dk <= 1; ++dk) {
         const int fk = 2 * K + dk;
         if (fk < 0 || fk >= gf.nz) continue;
-        const double w = dist_w(abs(di) + abs(dj) + abs(dk));
+        const T w = (T)dist_w(abs(di) + abs(dj) + abs(dk));
         const long long sf = gf.slot3(fi, fj, fk);
-        for (int c = 0; c < 3; ++c) v[c] += w * (double)Conv<double>::from(in[c * gf.n + sf]);
+        for (int c = 0; c < 3; ++c) v[c] += w * Conv<T>::from(in[c * gf.n + sf]);
       }
     }
   }
+  const T iw = inv_bnd_total3<T>(nb);
   const long long sc = gc.slot3(I, J, K);
-  for (int c = 0; c < 3; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] / W);
+  for (int c = 0; c < 3; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] * iw);
 }
 
 template <typename TI, typename TO>
@@ -276,29 +295,32 @@ __global__ void k_restrict2(const Geo gf, const Geo gc, const TI* __restrict__ i
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   const int J = blockIdx.y;
   if (I >= gc.nx) return;
-  const double W = bnd_total2(is_bnd(I, gc.nx) + is_bnd(J, gc.ny));
-  double v[2] = {0, 0};
+  using T = typename TransferT<TO>::type;
+  const T iw = inv_bnd_total2<T>(is_bnd(I, gc.nx) + is_bnd(J, gc.ny));
+  T v[2] = {0, 0};
   for (int di = -1; di <= 1; ++di) {
     const int fi = 2 * I + di;
     if (fi < 0 || fi >= gf.nx) continue;
     for (int dj = -1; dj <= 1; ++dj) {
       const int fj = 2 * J + dj;
       if (fj < 0 || fj >= gf.ny) continue;
-      const double w = dist_w(abs(di) + abs(dj));
+      const T w = (T)dist_w(abs(di) + abs(dj));
       const long long sf = gf.slot2(fi, fj);
-      for (int c = 0; c < 2; ++c) v[c] += w * (double)Conv<double>::from(in[c * gf.n + sf]);
+      for (int c = 0; c < 2; ++c) v[c] += w * Conv<T>::from(in[c * gf.n + sf]);
     }
   }
   const long long sc = gc.slot2(I, J);
-  for (int c = 0; c < 2; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] / W);
+  for (int c = 0; c < 2; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] * iw);
 }
 
 template <typename TI, typename TO>
 __global__ void k_prolong3(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = blockIdx.y, j = blockIdx.z;
-  if (k >= gf.nz) return;
-  double v[3] = {0, 0, 0};
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (t >= gf.nz * gf.nx) return;
+  const int k = t % gf.nz, i = t / gf.nz;
+  using T = typename TransferT<TO>::type;
+  T v[3] = {0, 0, 0};
   int cnt = 0;
   for (int ci = i / 2; ci <= i / 2 + (i & 1); ++ci) {
     if (ci >= gc.nx) continue;
@@ -306,15 +328,17 @@ __global__ void k_prolong3(const Geo gf, const Geo gc, const TI* __restrict__ in
       if (cj >= gc.ny) continue;
       for (int ck = k / 2; ck <= k / 2 + (k & 1); ++ck) {
         if (ck >= gc.nz) continue;
-        const double W = bnd_total3(is_bnd(ci, gc.nx) + is_bnd(cj, gc.ny) + is_bnd(ck, gc.nz));
+        const T iw = inv_bnd_total3<T>(is_bnd(ci, gc.nx) + is_bnd(cj, gc.ny) + is_bnd(ck, gc.nz));
         const long long sc = gc.slot3(ci, cj, ck);
-        for (int c = 0; c < 3; ++c) v[c] += (double)Conv<double>::from(in[c * gc.n + sc]) / W;
+        for (int c = 0; c < 3; ++c) v[c] += Conv<T>::from(in[c * gc.n + sc]) * iw;
         ++cnt;
       }
     }
   }
+  // cnt is 1, 2, 4 or 8: its reciprocal is exact
+  const T ic = cnt ? T(1) / T(cnt) : T(0);
   const long long sf = gf.slot3(i, j, k);
-  for (int c = 0; c < 3; ++c) out[c * gf.n + sf] = Conv<TO>::from(cnt ? v[c] / cnt : 0.0);
+  for (int c = 0; c < 3; ++c) out[c * gf.n + sf] = Conv<TO>::from(v[c] * ic);
 }
 
 template <typename TI, typename TO>
@@ -322,20 +346,22 @@ __global__ void k_prolong2(const Geo gf, const Geo gc, const TI* __restrict__ in
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= gf.nx) return;
-  double v[2] = {0, 0};
+  using T = typename TransferT<TO>::type;
+  T v[2] = {0, 0};
   int cnt = 0;
   for (int ci = i / 2; ci <= i / 2 + (i & 1); ++ci) {
     if (ci >= gc.nx) continue;
     for (int cj = j / 2; cj <= j / 2 + (j & 1); ++cj) {
       if (cj >= gc.ny) continue;
-      const double W = bnd_total2(is_bnd(ci, gc.nx) + is_bnd(cj, gc.ny));
+      const T iw = inv_bnd_total2<T>(is_bnd(ci, gc.nx) + is_bnd(cj, gc.ny));
       const long long sc = gc.slot2(ci, cj);
-      for (int c = 0; c < 2; ++c) v[c] += (double)Conv<double>::from(in[c * gc.n + sc]) / W;
+      for (int c = 0; c < 2; ++c) v[c] += Conv<T>::from(in[c * gc.n + sc]) * iw;
       ++cnt;
     }
   }
+  const T ic = cnt ? T(1) / T(cnt) : T(0);
   const long long sf = gf.slot2(i, j);
-  for (int c = 0; c < 2; ++c) out[c * gf.n + sf] = Conv<TO>::from(cnt ? v[c] / cnt : 0.0);
+  for (int c = 0; c < 2; ++c) out[c * gf.n + sf] = Conv<TO>::from(v[c] * ic);
 }
 
 // ------------------------------------------------------------------ Galerkin, level 0 -> 1

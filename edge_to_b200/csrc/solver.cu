@@ -953,7 +953,8 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     Level& Lc = P.lv[l + 1];
     P.cur_cat = CAT_TRANSFER;
     if (P.dim == 3)
-      launch(P, k_restrict3<T, T>, dim3(cdiv(Lc.g.nz, 64), Lc.g.nx, Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
+      launch(P, k_restrict3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g, r,
+             (T*)Lc.b);
     else
       launch(P, k_restrict2<T, T>, dim3(cdiv(Lc.g.nx, 64), Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
     KCHECK();
@@ -963,7 +964,8 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     T* e2 = (T*)Lv.eb;
     P.cur_cat = CAT_TRANSFER;
     if (P.dim == 3)
-      launch(P, k_prolong3<T, T>, dim3(cdiv(g.nz, 64), g.nx, g.ny), 64, 0, g, Lc.g, (const T*)Lc.res, e1);
+      launch(P, k_prolong3<T, T>, dim3(cdiv((long long)g.nz * g.nx, 256), g.ny), 256, 0, g, Lc.g,
+             (const T*)Lc.res, e1);
     else
       launch(P, k_prolong2<T, T>, dim3(cdiv(g.nx, 64), g.ny), 64, 0, g, Lc.g, (const T*)Lc.res, e1);
     KCHECK();
@@ -2163,7 +2165,7 @@ static void transfer(int dim, const int* nel, const double* in_dev, double* out_
   if (restrict_) {
     k_user_to_slots<double><<<cdiv(gf.n, 256), 256, 0, s>>>(gf, in_dev, vf);
     if (dim == 3)
-      k_restrict3<double, double><<<dim3(cdiv(gc.nz, 64), gc.nx, gc.ny), 64, 0, s>>>(gf, gc, vf, vc);
+      k_restrict3<double, double><<<dim3(cdiv((long long)gc.nz * gc.nx, 256), gc.ny), 256, 0, s>>>(gf, gc, vf, vc);
     else
       k_restrict2<double, double><<<dim3(cdiv(gc.nx, 64), gc.ny), 64, 0, s>>>(gf, gc, vf, vc);
     k_slots_to_user<double><<<cdiv(gc.n, 256), 256, 0, s>>>(gc, vc, out_dev);
@@ -2171,7 +2173,7 @@ static void transfer(int dim, const int* nel, const double* in_dev, double* out_
     CK(cudaMemsetAsync(vc, 0, (size_t)gc.dof * gc.n * sizeof(double), s));
     k_user_to_slots<double><<<cdiv(gc.n, 256), 256, 0, s>>>(gc, in_dev, vc);
     if (dim == 3)
-      k_prolong3<double, double><<<dim3(cdiv(gf.nz, 64), gf.nx, gf.ny), 64, 0, s>>>(gf, gc, vc, vf);
+      k_prolong3<double, double><<<dim3(cdiv((long long)gf.nz * gf.nx, 256), gf.ny), 256, 0, s>>>(gf, gc, vc, vf);
     else
       k_prolong2<double, double><<<dim3(cdiv(gf.nx, 64), gf.ny), 64, 0, s>>>(gf, gc, vc, vf);
     k_slots_to_user<double><<<cdiv(gf.n, 256), 256, 0, s>>>(gf, vf, out_dev);
