@@ -25,10 +25,12 @@
 //    zero, and the carry for (hx, hz) = (0, 0) is kept with the opposite sign so that the
 //    y stage needs no negation.
 //
-//  * The epilogue's per-node inputs (right-hand side, Jacobi diagonal, correction base,
-//    FP64 dot vector) travel through the same TMA ring as u, one box per array and plane,
+//  * The epilogue's per-node inputs (right-hand side, Jacobi diagonal, correction base)
+//    travel through the same TMA ring as u, one box per array and plane,
 //    so the epilogue reads shared memory instead of waiting on global loads; this keeps
 //    the smoother sweep close to the plain product although the kernel runs few warps.
+//    A stage is refilled at the barrier of the layer after the one that used it, so the
+//    epilogue reads its inputs after the barrier and holds no registers across it.
 //
 // TMA boxes, strides and alignments are those of k_fine3_pk, plus the staged arrays: FP32
 // and FP64 boxes start at z0-1 rounded down to 4 nodes (16 / 32 bytes), BF16 boxes at z0-1
@@ -191,19 +193,19 @@ struct SEJacobi {  // xo = u + w Dinv (b - A u)
 };
 
 // last post-smoothing sweep with the correction: xo = xbase + e + w Dinv (b - A e), e = u;
-// with DOT, acc += dotv . xo with dotv in FP64
+// with DOT, acc += b . xo accumulated in FP64 (the PCG's r.z with the right-hand side b of
+// the V-cycle, which is the residual, as the dot vector: no extra array is staged)
 template <bool DOT> struct SEJacobiAdd {
   float* xo;
   const double* omega;
   double wscale;
   long long n;
   float w;
-  static constexpr int kN = DOT ? 4 : 3;
+  static constexpr int kN = 3;
   static constexpr bool kDot = DOT;
-  EDGE_HD static constexpr int kT(int i) { return i == 0 ? ST_F32 : i == 1 ? ST_BF16 : i == 2 ? ST_F32 : ST_F64; }
+  EDGE_HD static constexpr int kT(int i) { return i == 0 ? ST_F32 : i == 1 ? ST_BF16 : i == 2 ? ST_F32 : 0; }
   struct In {
     float b[3], d[3], xb[3];
-    double dv[DOT ? 3 : 1];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
   EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2) const {
@@ -213,7 +215,6 @@ template <bool DOT> struct SEJacobiAdd {
       v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
       v.d[c] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(sp[1])[c * cs2]);
       v.xb[c] = reinterpret_cast<const float*>(sp[2])[c * cs4];
-      if constexpr (DOT) v.dv[c] = reinterpret_cast<const double*>(sp[3])[c * cs4];
     }
     return v;
   }
@@ -222,7 +223,7 @@ template <bool DOT> struct SEJacobiAdd {
     for (int c = 0; c < 3; ++c) {
       const float x = v.xb[c] + (own[c] + w * v.d[c] * (v.b[c] - Au[c]));
       xo[c * n + s] = x;
-      if constexpr (DOT) acc += v.dv[c] * (double)x;
+      if constexpr (DOT) acc += (double)v.b[c] * (double)x;
     }
   }
 };
@@ -260,6 +261,7 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
              const __grid_constant__ CUtensorMap mapS0, const __grid_constant__ CUtensorMap mapS1,
              const __grid_constant__ CUtensorMap mapS2, const __grid_constant__ CUtensorMap mapS3, const KCube KC,
              const int ly, SE epi, double* part, unsigned* ticket, double* dot_dst, int* err) {
+  static_assert(NS >= 3, "a stage is refilled one layer after its last use");
   using Tile = CubeTile<BX, SE>;
   using PT = PkTile<BX>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -459,7 +461,18 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
       AuB[c] = gx[1][c].v.x + gx[0][c].v.y;
       fromL[c] = __shfl_up_sync(0xffffffffu, gx[1][c].v.y, 16);
     }
-    // the output plane's staged epilogue inputs, read before the stage is recycled
+    const int xb = k & 1;
+    if (xh == 1)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sX[xb][w][zl][c] = gx[1][c].v.y;
+    __syncthreads();
+    // every thread has finished layer k-1, whose epilogue was the last reader of stage k-1:
+    // refill it (with NS >= 3 it is neither stage k nor stage k+1, both still in use)
+    if (tid == 0 && k >= 1 && k - 1 + NS < np) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(k - 1 + NS);
+    }
+    // the output plane's staged epilogue inputs (stage k stays valid until layer k+1)
     typename SE::In inA, inB;
     {
       const unsigned char* st = smem + (k % NS) * Tile::STAGE;
@@ -475,15 +488,6 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
       constexpr int cs4 = Tile::ROWS * st_width(ST_F32), cs2 = Tile::ROWS * st_width(ST_BF16);
       if (wrA) inA = epi.load(spA, cs4, cs2);
       if (wrB) inB = epi.load(spB, cs4, cs2);
-    }
-    const int xb = k & 1;
-    if (xh == 1)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) sX[xb][w][zl][c] = gx[1][c].v.y;
-    __syncthreads();
-    if (tid == 0 && k + NS < np) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(k + NS);
     }
     if (xh == 0) {
 #pragma unroll

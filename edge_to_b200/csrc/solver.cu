@@ -592,6 +592,15 @@ static void fine3_pk_launch(Prob& P, const float* u, const float* E, Epi epi, do
 template <class Epi> struct StagedOf {
   static constexpr bool ok = false;
 };
+template <class Epi> static bool staged_usable(const Epi& e) {
+  if constexpr (StagedOf<Epi>::ok) {
+    if constexpr (std::is_same<typename StagedOf<Epi>::SE, SEJacobiAdd<true>>::value ||
+                  std::is_same<typename StagedOf<Epi>::SE, SEJacobiAdd<false>>::value)
+      return StagedOf<Epi>::usable(e);
+    return true;
+  }
+  return false;
+}
 template <> struct StagedOf<EpiStore<float, float>> {
   static constexpr bool ok = true;
   using SE = SEStore;
@@ -620,13 +629,15 @@ template <> struct StagedOf<EpiJacobi<float, float, __nv_bfloat16>> {
   }
 };
 template <bool DOT, typename TV> struct StagedOf<EpiJacobiAdd<float, float, __nv_bfloat16, float, DOT, TV>> {
-  static constexpr bool ok = !DOT || std::is_same<TV, double>::value;  // the staged dot vector is FP64
+  static constexpr bool ok = true;
   using SE = SEJacobiAdd<DOT>;
-  static SE make(const EpiJacobiAdd<float, float, __nv_bfloat16, float, DOT, TV>& e, const void** arr) {
+  using Epi = EpiJacobiAdd<float, float, __nv_bfloat16, float, DOT, TV>;
+  // the staged form takes its dot with the right-hand side b
+  static bool usable(const Epi& e) { return !DOT || (const void*)e.dotv == (const void*)e.b; }
+  static SE make(const Epi& e, const void** arr) {
     arr[0] = e.b;
     arr[1] = e.dinv;
     arr[2] = e.xbase;
-    if (DOT) arr[3] = e.dotv;
     return SE{e.xo, e.omega, e.wscale, e.n, 0.f};
   }
 };
@@ -689,7 +700,7 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
     bool packed = false;
     if constexpr (std::is_same<T, float>::value) {
       if constexpr (StagedOf<Epi>::ok) {
-        if (P.dim == 3 && P.use_tma && P.tile_variant >= 9 && P.cube) {
+        if (P.dim == 3 && P.use_tma && P.tile_variant >= 9 && P.cube && staged_usable(epi)) {
           switch (P.tile_variant) {
             case 9: fine3_cube_launch<Epi, 4, 3, 2>(P, u, E, epi, dot_dst); break;
             case 10: fine3_cube_launch<Epi, 4, 4, 2>(P, u, E, epi, dot_dst); break;
@@ -1163,7 +1174,8 @@ static void pcgmx_body(Prob& P) {
   float* p = (float*)P.p;
   float* q = (float*)P.q;
   float* z = (float*)P.lv[0].res;
-  vcycle<float, __nv_bfloat16, double>(P, 0, P.r32, z, P.r64, &P.st->rz_new);
+  // r.z with the FP32 copy of the residual (the V-cycle's right-hand side), FP64 accumulation
+  vcycle<float, __nv_bfloat16, float>(P, 0, P.r32, z, P.r32, &P.st->rz_new);
   launch(P, k_pcg_p<float>, ew_blocks(nv), 256, 0, nv, p, (const float*)z, (const PcgState*)P.st);
   {
     EpiStoreDot<float> e{q, g.n};
