@@ -218,7 +218,13 @@ def run_ours(args, cfg_name):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     cfg = CONFIGS[cfg_name]
     opt, rho = build_problem(cfg, args.precision, args.n_smooth, graph=not args.no_graph)
+    if args.coarse_bf16:
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_coarse_bf16", opt.kernel.handle, 1)
     rho, dr, it = warm(opt, rho, args.warmup)
+    # the state the timed steps start from; the end-to-end steps restart from it, so both
+    # measure the same SIMP iterations (later iterations need more PCG iterations)
+    start = (rho.clone(), dr.clone(), it, opt.solver.last_x0.clone() if opt.solver.last_x0 is not None else None)
 
     # ---------------- device-timed region: inputs resident in HBM; each solve is one CUDA
     # graph launch (per-launch events cannot sit inside a graph, so none are recorded here)
@@ -230,12 +236,16 @@ def run_ours(args, cfg_name):
     rho, dr, it, prof = pm["rho"], pm["dr"], pm["it"], pm["prof"]
     rho_chk, c_chk = rho.detach().clone(), pm["compliance"]  # checked against a tight FP64 solve below
 
-    # ---------------- end-to-end: design on the host, copies inside the timed region
+    # ---------------- end-to-end: design on the host, copies inside the timed region, from the
+    # timed steps' starting state
     stream = torch.cuda.current_stream()
-    rho_h = torch.empty(rho.numel(), dtype=torch.float64, pin_memory=True)
-    rho_h.copy_(rho.cpu())
+    rho0, dr_e, it_e, x0 = start
+    if x0 is not None:
+        opt.solver.last_x0.copy_(x0)
+    rho_h = torch.empty(rho0.numel(), dtype=torch.float64, pin_memory=True)
+    rho_h.copy_(rho0.cpu())
     out_h = torch.empty_like(rho_h)
-    dr_e = dr
+    e2e_pcg = []
     _barrier(ws)
     torch.cuda.synchronize()
     s0 = torch.cuda.Event(enable_timing=True)
@@ -244,11 +254,12 @@ def run_ours(args, cfg_name):
     for _ in range(args.steps):
         rho_d = rho_h.to("cuda", non_blocking=True)
         rho_n = opt.update_design(rho_d, dr_e)
-        c, dr_e, res = opt.solve_and_process(rho_n, it)
+        c, dr_e, res = opt.solve_and_process(rho_n, it_e)
         out_h.copy_(rho_n, non_blocking=True)
         comp_host = float(c)  # D2H of the compliance (synchronising)
+        e2e_pcg.append(opt.last_stats.get("pcg_iters", 0))
         rho_h, out_h = out_h, rho_h
-        it += 1
+        it_e += 1
     s1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = _max_over_ranks(s0.elapsed_time(s1), ws)
@@ -315,7 +326,8 @@ def run_ours(args, cfg_name):
                      "timing": "CUDA events around every fine-operator launch of one SIMP step run right "
                                "after the timed steps (host-driven PCG loop, same kernels and tiles)"},
         "e2e": {"value": args.steps / (e2e_ms / 1e3), "unit": "iter/s", "h2d_bytes_per_step": 8 * n_el,
-                "d2h_bytes_per_step": 8 * n_el + 8},
+                "d2h_bytes_per_step": 8 * n_el + 8, "pcg_iters_per_step": e2e_pcg,
+                "note": "the same SIMP iterations as the device-timed steps (restarted from their state)"},
         "gpu_launches": m["launches"],
         "clocks": m["clocks"],
     }
@@ -542,6 +554,7 @@ def main():
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--n-smooth", type=int, default=3,
                     help="default smoothing sweeps of the timed path (the FP64 path keeps the reference's 3)")
+    ap.add_argument("--coarse-bf16", action="store_true", help="mixed path: BF16-stored coarse stencils")
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven PCG loop instead of one CUDA graph per solve (same launches; for profilers)")
     ap.add_argument("--batch", action="store_true",

@@ -189,6 +189,7 @@ struct Level {
   Geo g;
   void *b = nullptr, *xa = nullptr, *xb = nullptr, *r = nullptr, *ea = nullptr, *eb = nullptr, *res = nullptr;
   void* S = nullptr;     // stencil (l >= 1)
+  void* S16 = nullptr;   // BF16 copy of the FP32 stencil, applied when Prob::st_bf16 is set
   void* dinv = nullptr;  // Jacobi inverse diagonal
 };
 
@@ -220,6 +221,7 @@ struct Prob {
   bool cube = false;       // kcube reproduces every entry of the transformed operator
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
   long long st_quad_max = 200000;  // 3-D stencil levels with at most this many slots use k_st3_apply_q
+  bool st_bf16 = false;            // mixed precision: apply the coarse stencils from BF16 copies
   // CUDA graph of one solve (hierarchy set-up + the whole PCG loop under a while node)
   bool use_graph = true;
   cudaGraph_t sg_graph = nullptr;
@@ -772,24 +774,31 @@ static void fine_apply_dense(Prob& P, const T* u, Epi epi, double* dot_dst) {
   KCHECK();
 }
 
-template <typename T, class Epi>
-static void st_apply(Prob& P, const Geo& g, const T* u, const T* S, Epi epi, double* dot_dst) {
+template <typename T, class Epi, typename TS = T>
+static void st_apply(Prob& P, const Geo& g, const T* u, const TS* S, Epi epi, double* dot_dst) {
   CatScope cat(P, CAT_STENCIL);
   if (g.dim == 3 && g.n <= P.st_quad_max)
-    launch(P, k_st3_apply_q<T, T, Epi>, dim3(cdiv(g.n * 4, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket,
+    launch(P, k_st3_apply_q<T, TS, Epi>, dim3(cdiv(g.n * 4, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket,
            dot_dst);
   else if (g.dim == 3)
-    launch(P, k_st3_apply<T, T, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
+    launch(P, k_st3_apply<T, TS, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
   else
-    launch(P, k_st2_apply<T, T, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
+    launch(P, k_st2_apply<T, TS, Epi>, dim3(cdiv(g.n, 128)), dim3(128), 0, g, u, S, epi, P.part, P.ticket, dot_dst);
 }
 
 template <typename T, class Epi>
 static void level_apply(Prob& P, int l, const T* u, Epi epi, double* dot_dst = nullptr) {
-  if (l == 0)
+  if (l == 0) {
     fine_apply<T>(P, u, epi, dot_dst);
-  else
-    st_apply<T>(P, P.lv[l].g, u, (const T*)P.lv[l].S, epi, dot_dst);
+    return;
+  }
+  if constexpr (std::is_same<T, float>::value) {
+    if (P.st_bf16 && P.lv[l].S16) {
+      st_apply<T, Epi, __nv_bfloat16>(P, P.lv[l].g, u, (const __nv_bfloat16*)P.lv[l].S16, epi, dot_dst);
+      return;
+    }
+  }
+  st_apply<T>(P, P.lv[l].g, u, (const T*)P.lv[l].S, epi, dot_dst);
 }
 
 static unsigned ew_blocks(long long n) { return (unsigned)std::min<long long>(cdiv(n, 256), 148LL * 16); }
@@ -884,6 +893,11 @@ static void mg_setup(Prob& P) {
     const Geo& g = P.lv[l].g;
     launch(P, k_st_dinv<T, T>, cdiv(g.n, 256), 256, 0, g, (const T*)P.lv[l].S, (T*)P.lv[l].dinv);
     KCHECK();
+    if (P.st_bf16 && P.lv[l].S16) {  // the Jacobi diagonal above keeps the FP32 centre
+      const long long ns = (long long)nst(P.dim) * g.n;
+      launch(P, k_copy<T, __nv_bfloat16>, ew_blocks(ns), 256, 0, ns, (const T*)P.lv[l].S,
+             (__nv_bfloat16*)P.lv[l].S16);
+    }
   }
   // coarsest: dense FP64 Cholesky and explicit inverse
   const Geo& gL = P.lv[L].g;
@@ -1040,6 +1054,7 @@ static void mg_allocate(Prob& P) {
     if (l > 0) {
       const size_t ns = (size_t)nst(P.dim) * Lv.g.n;
       Lv.S = vb == 8 ? (void*)P.alloc<double>(ns) : (void*)P.alloc<float>(ns);
+      if (vb == 4 && l < L) Lv.S16 = (void*)P.alloc<__nv_bfloat16>(ns);
     }
   }
   const Geo& gL = P.lv[L].g;
@@ -1247,7 +1262,8 @@ static void mg_setup_prec(Prob& P) {
 static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, bool cg = false) {
   std::vector<double> k = {cg ? -1.0 : (double)P.prec, tol, (double)maxiter, (double)P.n_level, (double)P.n_smooth, P.omega,
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
-                           (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons};
+                           (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons,
+                           (double)P.st_bf16};
   for (int l : P.w_levels) k.push_back((double)l);
   k.push_back(-1.0);
   for (int v : P.level_sweeps) k.push_back((double)v);
@@ -1640,6 +1656,13 @@ int edge_set_graph(edge_problem* p, int enable) {
   API_END
 }
 
+int edge_set_coarse_bf16(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.st_bf16 = enable != 0;
+  API_END
+}
+
 int edge_set_stencil_quad(edge_problem* p, long long max_slots) {
   API_BEGIN
   if (!p || max_slots < 0) fail(EDGE_EINVAL, "bad argument");
@@ -1661,9 +1684,23 @@ int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm) {
 // Average device time of `reps` fine-operator launches with the current tile, the smoother
 // sweep epilogue (sweep = true; needs the multigrid allocated) or the plain product; buffer
 // contents do not matter for timing.
-static double time_fine(Prob& P, int precision, bool sweep, int reps) {
+static double time_fine(Prob& P, int precision, bool sweep, int reps, bool mix = false) {
   const Geo& g = P.g0;
   auto run = [&]() {
+    if (mix) {
+      // the fine-level launches of one mixed-precision PCG iteration with one sweep per level:
+      // residual, last sweep + correction + r.z, product + p.q
+      Level& L0 = P.lv[0];
+      const __nv_bfloat16* d = (const __nv_bfloat16*)L0.dinv;
+      EpiResid<float, float, float> e1{P.r32, (float*)L0.r, g.n};
+      fine_apply<float>(P, (const float*)L0.xa, e1, nullptr);
+      EpiJacobiAdd<float, float, __nv_bfloat16, float, true, float> e2{
+          P.r32, d, (const float*)L0.xa, (float*)L0.res, P.r32, &P.st->omega, 1.0, g.n};
+      fine_apply<float>(P, (const float*)L0.ea, e2, &P.st->rz);
+      EpiStoreDot<float> e3{(float*)P.q, g.n};
+      fine_apply<float>(P, (const float*)P.p, e3, &P.st->pq);
+      return;
+    }
     if (precision == EDGE_FP64) {
       if (sweep) {
         EpiJacobi<double, double, double> e{P.b64, (const double*)P.lv[0].dinv, P.r64, &P.st->omega, 1.0, g.n};
@@ -1703,9 +1740,10 @@ static bool can_time_sweep(const Prob& P, int precision) {
   return precision == EDGE_FP64 ? P.prec == EDGE_FP64 : P.prec == EDGE_MIXED;
 }
 
-// Autotuner: times every (tile variant, y-chunking) of the fine operator on the current E
-// (smoother sweep once the multigrid is configured, the most frequent fine-level launch;
-// else the plain product) and keeps the fastest.  Needs E set.
+// Autotuner: times every (tile variant, y-chunking) of the fine operator on the current E and
+// keeps the fastest: once the multigrid is configured, the mixed path's per-iteration mix
+// of fine launches (residual, last sweep with r.z, product with p.q) or the FP64 smoother
+// sweep; else the plain product.  Needs E set.
 int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms, int* best_variant,
                        int* best_bps) {
   API_BEGIN
@@ -1724,11 +1762,12 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
   // variants 5..8: packed-pair FP32 kernel; 9..12: its cube-element form
   const int nvar = precision == EDGE_FP64 ? 5 : (P.cube ? 15 : 9);
   const bool sweep = can_time_sweep(P, precision);
+  const bool mix = sweep && precision != EDGE_FP64;  // time the whole per-iteration mix
   for (int v = 0; v < nvar; ++v)
     for (int bi = 0; bi < 4; ++bi) {
       P.tile_variant = v;
       P.blocks_per_sm = bps_list[bi];
-      const double ms = time_fine(P, precision, sweep, reps);
+      const double ms = time_fine(P, precision, sweep, reps, mix);
       if (ms < best) {
         best = ms;
         bv = v;
@@ -1956,7 +1995,7 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
   if (realloc) {
     // free the old hierarchy
     for (auto& Lv : P.lv) {
-      for (void* q : {Lv.b, Lv.xa, Lv.xb, Lv.r, Lv.ea, Lv.eb, Lv.res, Lv.S, Lv.dinv}) {
+      for (void* q : {Lv.b, Lv.xa, Lv.xb, Lv.r, Lv.ea, Lv.eb, Lv.res, Lv.S, Lv.S16, Lv.dinv}) {
         if (!q) continue;
         auto it = std::find(P.allocs.begin(), P.allocs.end(), q);
         if (it != P.allocs.end()) {

@@ -112,6 +112,10 @@ int edge_launch_count(const edge_problem* p, long long* n);
  * loop that reads the solver state once per iteration.  Per-launch profiling
  * (edge_profile_begin, edge_breakdown_begin) always uses the host loop. */
 int edge_set_graph(edge_problem* p, int enable);
+/* Mixed precision only: enable != 0 applies the coarse-level stencils (levels >= 1, below the
+ * coarsest) from BF16 copies made after each Galerkin set-up (half the bytes of the largest
+ * coarse kernel); the Jacobi diagonals and the Galerkin chain stay FP32.  Default 0. */
+int edge_set_coarse_bf16(edge_problem* p, int enable);
 /* Coarse 3-D levels with at most max_slots slots use the four-lanes-per-node stencil kernel
  * (latency-bound small levels); larger levels one thread per node.  Default 200000. */
 int edge_set_stencil_quad(edge_problem* p, long long max_slots);
