@@ -473,7 +473,7 @@ def run_tiles(args, cfg_name):
             row[name + "_us"] = round(ms.value * 1e3, 2)
             row[name + "_frac"] = round(b / (ms.value / 1e3) / 1e9 / peak, 3)
         levels.append(row)
-    _lib.call("edge_set_stencil_quad", h, 200000)
+    _lib.call("edge_set_stencil_quad", h, 40000)
     return {"mode": "tiles", "workload": cfg_name, "precision": args.precision, "peak_GBps": peak,
             "peak_source": kind, "plain_bytes": plain_bytes, "sweep_bytes": sweep_bytes, "tiles": rows,
             "stencil_levels": levels}

@@ -220,7 +220,7 @@ struct Prob {
   KCube kcube;             // block form of the same operator (cube elements)
   bool cube = false;       // kcube reproduces every entry of the transformed operator
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
-  long long st_quad_max = 200000;  // 3-D stencil levels with at most this many slots use k_st3_apply_q
+  long long st_quad_max = 40000;   // 3-D stencil levels with at most this many slots use k_st3_apply_q
   bool st_bf16 = false;            // mixed precision: apply the coarse stencils from BF16 copies
   // CUDA graph of one solve (hierarchy set-up + the whole PCG loop under a while node)
   bool use_graph = true;

@@ -117,7 +117,8 @@ int edge_set_graph(edge_problem* p, int enable);
  * coarse kernel); the Jacobi diagonals and the Galerkin chain stay FP32.  Default 0. */
 int edge_set_coarse_bf16(edge_problem* p, int enable);
 /* Coarse 3-D levels with at most max_slots slots use the four-lanes-per-node stencil kernel
- * (latency-bound small levels); larger levels one thread per node.  Default 200000. */
+ * (latency-bound small levels); larger levels one thread per node.  Default 40000 (at 70k
+ * slots one thread per node is already faster). */
 int edge_set_stencil_quad(edge_problem* p, long long max_slots);
 /* Benchmark helper: average device time (ms) of `reps` Jacobi sweeps of the stencil operator
  * on coarse level 1 <= level < n_level, in the problem's precision (hierarchy built). */
