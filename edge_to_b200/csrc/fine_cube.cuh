@@ -193,19 +193,20 @@ struct SEJacobi {  // xo = u + w Dinv (b - A u)
 };
 
 // last post-smoothing sweep with the correction: xo = xbase + e + w Dinv (b - A e), e = u;
-// with DOT, acc += b . xo accumulated in FP64 (the PCG's r.z with the right-hand side b of
-// the V-cycle, which is the residual, as the dot vector: no extra array is staged)
+// with DOT, acc += dotv . xo accumulated in FP64, dotv an FP32 array staged like the others
+// (the PCG's r.z with the FP32 copy of the residual)
 template <bool DOT> struct SEJacobiAdd {
   float* xo;
   const double* omega;
   double wscale;
   long long n;
   float w;
-  static constexpr int kN = 3;
+  static constexpr int kN = DOT ? 4 : 3;
   static constexpr bool kDot = DOT;
-  EDGE_HD static constexpr int kT(int i) { return i == 0 ? ST_F32 : i == 1 ? ST_BF16 : i == 2 ? ST_F32 : 0; }
+  EDGE_HD static constexpr int kT(int i) { return i == 0 ? ST_F32 : i == 1 ? ST_BF16 : ST_F32; }
   struct In {
     float b[3], d[3], xb[3];
+    float dv[DOT ? 3 : 1];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
   EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2) const {
@@ -215,6 +216,7 @@ template <bool DOT> struct SEJacobiAdd {
       v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
       v.d[c] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(sp[1])[c * cs2]);
       v.xb[c] = reinterpret_cast<const float*>(sp[2])[c * cs4];
+      if constexpr (DOT) v.dv[c] = reinterpret_cast<const float*>(sp[3])[c * cs4];
     }
     return v;
   }
@@ -223,7 +225,7 @@ template <bool DOT> struct SEJacobiAdd {
     for (int c = 0; c < 3; ++c) {
       const float x = v.xb[c] + (own[c] + w * v.d[c] * (v.b[c] - Au[c]));
       xo[c * n + s] = x;
-      if constexpr (DOT) acc += (double)v.b[c] * (double)x;
+      if constexpr (DOT) acc += (double)v.dv[c] * (double)x;
     }
   }
 };

@@ -345,17 +345,46 @@ struct PcgState {
 // updates res / omega / done as solvers/_multigrid_cuda.py:219-227 and moves rz_new to rz.
 // With r32 != nullptr the updated residual is also written in FP32 (the V-cycle input of
 // the mixed-precision solver).
+// Two-wide vector types for the PCG vector kernels (every vector is 16-byte aligned and
+// holds 3 * n entries with n a multiple of 4, so pairs never straddle the end).
+template <typename T> struct V2;
+template <> struct V2<double> {
+  using type = double2;
+};
+template <> struct V2<float> {
+  using type = float2;
+};
+
 template <typename TX, typename TP>
 __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__ p, TX* __restrict__ r,
                          const TP* __restrict__ q, PcgState* st, double* part, unsigned* ticket,
                          float* __restrict__ r32) {
+  using X2 = typename V2<TX>::type;
+  using P2v = typename V2<TP>::type;
   const double alpha = st->rz_new / st->pq;
   double acc = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const double pi = (double)Conv<double>::from(p[i]);
-    const double qi = (double)Conv<double>::from(q[i]);
-    x[i] = Conv<TX>::from((double)Conv<double>::from(x[i]) + alpha * pi);
-    const double ri = (double)Conv<double>::from(r[i]) - alpha * qi;
+  const long long n2 = n >> 1;
+  X2* __restrict__ x2 = reinterpret_cast<X2*>(x);
+  X2* __restrict__ r2 = reinterpret_cast<X2*>(r);
+  const P2v* __restrict__ p2 = reinterpret_cast<const P2v*>(p);
+  const P2v* __restrict__ q2 = reinterpret_cast<const P2v*>(q);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2; i += (long long)gridDim.x * blockDim.x) {
+    const P2v pv = p2[i], qv = q2[i];
+    X2 xv = x2[i], rv = r2[i];
+    xv.x = Conv<TX>::from((double)xv.x + alpha * (double)pv.x);
+    xv.y = Conv<TX>::from((double)xv.y + alpha * (double)pv.y);
+    const double r0 = (double)rv.x - alpha * (double)qv.x, r1 = (double)rv.y - alpha * (double)qv.y;
+    rv.x = Conv<TX>::from(r0);
+    rv.y = Conv<TX>::from(r1);
+    x2[i] = xv;
+    r2[i] = rv;
+    if (r32) reinterpret_cast<float2*>(r32)[i] = make_float2((float)r0, (float)r1);
+    acc += r0 * r0 + r1 * r1;
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {  // odd length (not produced by this library)
+    const long long i = n - 1;
+    x[i] = Conv<TX>::from((double)x[i] + alpha * (double)p[i]);
+    const double ri = (double)r[i] - alpha * (double)q[i];
     r[i] = Conv<TX>::from(ri);
     if (r32) r32[i] = (float)ri;
     acc += ri * ri;
@@ -403,10 +432,27 @@ __global__ void k_pcg_true_res(PcgState* st) {
 // p = z + beta p, or p = z before the first iteration (iter == 0)
 template <typename TP>
 __global__ void k_pcg_p(long long n, TP* __restrict__ p, const TP* __restrict__ z, const PcgState* st) {
+  using P2v = typename V2<TP>::type;
   const bool first = st->iter == 0;
   const double beta = first ? 0.0 : st->rz_new / st->rz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    p[i] = first ? z[i] : Conv<TP>::from((double)Conv<double>::from(z[i]) + beta * (double)Conv<double>::from(p[i]));
+  const long long n2 = n >> 1;
+  P2v* __restrict__ p2 = reinterpret_cast<P2v*>(p);
+  const P2v* __restrict__ z2 = reinterpret_cast<const P2v*>(z);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2; i += (long long)gridDim.x * blockDim.x) {
+    const P2v zv = z2[i];
+    if (first) {
+      p2[i] = zv;
+    } else {
+      P2v pv = p2[i];
+      pv.x = Conv<TP>::from((double)zv.x + beta * (double)pv.x);
+      pv.y = Conv<TP>::from((double)zv.y + beta * (double)pv.y);
+      p2[i] = pv;
+    }
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const long long i = n - 1;
+    p[i] = first ? z[i] : Conv<TP>::from((double)z[i] + beta * (double)p[i]);
+  }
 }
 
 // Unpreconditioned CG as PCG with z = r: r.z of the current residual is its r.r.

@@ -634,12 +634,13 @@ template <bool DOT, typename TV> struct StagedOf<EpiJacobiAdd<float, float, __nv
   static constexpr bool ok = true;
   using SE = SEJacobiAdd<DOT>;
   using Epi = EpiJacobiAdd<float, float, __nv_bfloat16, float, DOT, TV>;
-  // the staged form takes its dot with the right-hand side b
-  static bool usable(const Epi& e) { return !DOT || (const void*)e.dotv == (const void*)e.b; }
+  // the staged form stages an FP32 dot vector
+  static bool usable(const Epi&) { return !DOT || std::is_same<TV, float>::value; }
   static SE make(const Epi& e, const void** arr) {
     arr[0] = e.b;
     arr[1] = e.dinv;
     arr[2] = e.xbase;
+    if constexpr (DOT) arr[3] = e.dotv;
     return SE{e.xo, e.omega, e.wscale, e.n, 0.f};
   }
 };
