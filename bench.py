@@ -488,11 +488,13 @@ def run_tiles(args, cfg_name):
         # stencil (123 coefficients) + u, b, Dinv, out per node
         b = nodes * (123 * w + 4 * 3 * w)
         row = {"level": lvl, "nodes": nodes}
-        for name, qmax in (("thread", 0), ("quad", 1 << 40)):
+        for name, qmax, pair in (("thread", 0, -1), ("pair", 0, 0), ("quad", 1 << 40, -1)):
             _lib.call("edge_set_stencil_quad", h, qmax)
+            _lib.call("edge_set_stencil_pair", h, pair)
             _lib.call("edge_time_level", h, lvl, max(1, args.steps), ctypes.byref(ms))
             row[name + "_us"] = round(ms.value * 1e3, 2)
             row[name + "_frac"] = round(b / (ms.value / 1e3) / 1e9 / peak, 3)
+        _lib.call("edge_set_stencil_pair", h, 200000)
         levels.append(row)
     _lib.call("edge_set_stencil_quad", h, 40000)
     return {"mode": "tiles", "workload": cfg_name, "precision": args.precision, "peak_GBps": peak,

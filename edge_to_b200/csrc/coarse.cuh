@@ -142,6 +142,120 @@ k_st3_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi 
   finish_dot(epi, dacc, part, ticket, dot_dst);
 }
 
+// Two consecutive z-slots per thread (s0 even, s1 = s0 + 1; the padded row length is a
+// multiple of 4, so both lie in one (x, y) row): the centre blocks, the stored upper blocks
+// and the dz = 0 neighbour values load as 8-byte pairs.  A warp covers 64 slots of one row,
+// so the (x, y) range tests of a direction are warp-uniform branches; the z range test is
+// a select on values loaded from inside the array (a z neighbour outside the grid is the
+// row's padding or the next row's first slot).  Same sums in the same order per node as
+// k_st3_apply.
+template <typename T, typename TS, class Epi>
+__global__ void __launch_bounds__(128)
+k_st3_apply2(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
+             double* dot_dst) {
+  using T2 = typename V2<T>::type;
+  const long long s0 = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  const long long n = g.n;
+  epi.init();
+  double dacc = 0.0;
+  if (s0 < n) {
+    const int k0 = (int)(s0 % g.pz), i = (int)((s0 / g.pz) % g.nx), j = (int)(s0 / g.plane);
+    const bool ok0 = k0 < g.nz, ok1 = k0 + 1 < g.nz;
+    auto ld2 = [&](const T* a, long long s) { return reinterpret_cast<const T2*>(a + s)[0]; };
+    auto lds2 = [&](const TS* a, long long s) -> T2 {
+      if constexpr (std::is_same<TS, T>::value) {
+        return reinterpret_cast<const T2*>(a + s)[0];
+      } else {
+        T2 r;
+        r.x = Conv<T>::from(__ldg(a + s));
+        r.y = Conv<T>::from(__ldg(a + s + 1));
+        return r;
+      }
+    };
+    T2 uc[3], Au[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) uc[c] = ld2(u + c * n, s0);
+    {
+      T2 cc[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) cc[q] = lds2(S + q * n, s0);
+      // rows of the symmetric centre block: (c00 c01 c02; c01 c11 c12; c02 c12 c22)
+      Au[0].x = cc[0].x * uc[0].x + cc[1].x * uc[1].x + cc[2].x * uc[2].x;
+      Au[0].y = cc[0].y * uc[0].y + cc[1].y * uc[1].y + cc[2].y * uc[2].y;
+      Au[1].x = cc[1].x * uc[0].x + cc[3].x * uc[1].x + cc[4].x * uc[2].x;
+      Au[1].y = cc[1].y * uc[0].y + cc[3].y * uc[1].y + cc[4].y * uc[2].y;
+      Au[2].x = cc[2].x * uc[0].x + cc[4].x * uc[1].x + cc[5].x * uc[2].x;
+      Au[2].y = cc[2].y * uc[0].y + cc[4].y * uc[1].y + cc[5].y * uc[2].y;
+    }
+#pragma unroll
+    for (int nb = 14; nb < 27; ++nb) {
+      const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
+      const long long off = (long long)dy * g.plane + (long long)dx * g.pz + dz;
+      const TS* Sb = S + (long long)(6 + (nb - 14) * 9) * n;
+      if (i + dx >= 0 && i + dx < g.nx && j + dy >= 0 && j + dy < g.ny) {  // upper neighbour
+        const bool z0 = k0 + dz >= 0 && k0 + dz < g.nz, z1 = k0 + 1 + dz >= 0 && k0 + 1 + dz < g.nz;
+        const long long sn = s0 + off;
+        // dz = +1 at the end of the last row would read one slot past the array: clamp
+        // (that value is masked by z1 anyway)
+        const long long sn1 = sn + 1 < n ? sn + 1 : n - 1;
+        T2 v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (dz == 0) {
+            v[c] = ld2(u + c * n, sn);
+          } else {
+            v[c].x = __ldg(u + c * n + sn);
+            v[c].y = __ldg(u + c * n + sn1);
+          }
+          v[c].x = z0 ? v[c].x : T(0);
+          v[c].y = z1 ? v[c].y : T(0);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T2 a = lds2(Sb + (c * 3 + 0) * n, s0), b = lds2(Sb + (c * 3 + 1) * n, s0),
+                   d = lds2(Sb + (c * 3 + 2) * n, s0);
+          Au[c].x += a.x * v[0].x + b.x * v[1].x + d.x * v[2].x;
+          Au[c].y += a.y * v[0].y + b.y * v[1].y + d.y * v[2].y;
+        }
+      }
+      if (i - dx >= 0 && i - dx < g.nx && j - dy >= 0 && j - dy < g.ny) {  // lower neighbour
+        const bool z0 = k0 - dz >= 0 && k0 - dz < g.nz, z1 = k0 + 1 - dz >= 0 && k0 + 1 - dz < g.nz;
+        const long long sm = s0 - off;  // sm >= -1 when the (x, y) test holds: clamp the pair start
+        const long long sa = sm < 0 ? 0 : sm;
+        T2 v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          v[c].x = __ldg(u + c * n + sa);
+          v[c].y = __ldg(u + c * n + sm + 1);
+          v[c].x = z0 ? v[c].x : T(0);
+          v[c].y = z1 ? v[c].y : T(0);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          T2 a, b, d;
+          a.x = Conv<T>::from(__ldg(Sb + (0 * 3 + c) * n + sa));
+          a.y = Conv<T>::from(__ldg(Sb + (0 * 3 + c) * n + sm + 1));
+          b.x = Conv<T>::from(__ldg(Sb + (1 * 3 + c) * n + sa));
+          b.y = Conv<T>::from(__ldg(Sb + (1 * 3 + c) * n + sm + 1));
+          d.x = Conv<T>::from(__ldg(Sb + (2 * 3 + c) * n + sa));
+          d.y = Conv<T>::from(__ldg(Sb + (2 * 3 + c) * n + sm + 1));
+          Au[c].x += a.x * v[0].x + b.x * v[1].x + d.x * v[2].x;
+          Au[c].y += a.y * v[0].y + b.y * v[1].y + d.y * v[2].y;
+        }
+      }
+    }
+    if (ok0) {
+      T own[3] = {uc[0].x, uc[1].x, uc[2].x}, A[3] = {Au[0].x, Au[1].x, Au[2].x};
+      epi(s0, 3, own, A, dacc);
+    }
+    if (ok1) {
+      T own[3] = {uc[0].y, uc[1].y, uc[2].y}, A[3] = {Au[0].y, Au[1].y, Au[2].y};
+      epi(s0 + 1, 3, own, A, dacc);
+    }
+  }
+  finish_dot(epi, dacc, part, ticket, dot_dst);
+}
+
 // Latency-oriented variant for small levels, where a sweep is a handful of dependent load
 // round trips rather than a bandwidth problem: four lanes per node share the 26 neighbour
 // terms (term t = 4m + lane; terms 0..12 are the stored upper blocks, 13..25 the transposed

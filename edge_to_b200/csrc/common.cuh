@@ -64,6 +64,16 @@ EDGE_D float to_f(double x) { return (float)x; }
 EDGE_D float to_f(float x) { return x; }
 EDGE_D float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
 
+// Two-wide vector types (pair loads in the PCG vector kernels and the paired stencil; every
+// vector is 16-byte aligned and holds dof * n entries with n a multiple of 4).
+template <typename T> struct V2;
+template <> struct V2<double> {
+  using type = double2;
+};
+template <> struct V2<float> {
+  using type = float2;
+};
+
 template <typename T> struct Conv;
 template <> struct Conv<double> {
   EDGE_D static double from(double x) { return x; }

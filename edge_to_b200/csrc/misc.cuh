@@ -345,15 +345,6 @@ struct PcgState {
 // updates res / omega / done as solvers/_multigrid_cuda.py:219-227 and moves rz_new to rz.
 // With r32 != nullptr the updated residual is also written in FP32 (the V-cycle input of
 // the mixed-precision solver).
-// Two-wide vector types for the PCG vector kernels (every vector is 16-byte aligned and
-// holds 3 * n entries with n a multiple of 4, so pairs never straddle the end).
-template <typename T> struct V2;
-template <> struct V2<double> {
-  using type = double2;
-};
-template <> struct V2<float> {
-  using type = float2;
-};
 
 template <typename TX, typename TP>
 __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__ p, TX* __restrict__ r,

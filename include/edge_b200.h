@@ -112,6 +112,9 @@ int edge_launch_count(const edge_problem* p, long long* n);
  * loop that reads the solver state once per iteration.  Per-launch profiling
  * (edge_profile_begin, edge_breakdown_begin) always uses the host loop. */
 int edge_set_graph(edge_problem* p, int enable);
+/* FP32 3-D coarse levels with at least min_slots slots use two nodes per thread (pair loads
+ * of the centre and stored blocks; default 200000); min_slots < 0: one node per thread. */
+int edge_set_stencil_pair(edge_problem* p, long long min_slots);
 /* Mixed precision only: enable != 0 applies the coarse-level stencils (levels >= 1, below the
  * coarsest) from BF16 copies made after each Galerkin set-up (half the bytes of the largest
  * coarse kernel); the Jacobi diagonals and the Galerkin chain stay FP32.  Default 0. */

@@ -331,8 +331,8 @@ def test_packed_kernel_in_mixed_solve():
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_stencil_kernels_agree_in_solve(precision):
-    """The one-thread-per-node and four-lanes-per-node coarse stencil kernels give the same
-    PCG run (same iteration count, solutions equal to rounding)."""
+    """The one-thread-per-node, two-nodes-per-thread and four-lanes-per-node coarse stencil
+    kernels give the same PCG run (same iteration count, solutions equal to rounding)."""
     import torch
     import edge_to_b200 as eb
     from edge_to_b200 import _lib
@@ -347,13 +347,15 @@ def test_stencil_kernels_agree_in_solve(precision):
     s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision=precision, autotune=False,
                        tune_sweeps=False)
     res = []
-    for qmax in (0, 1 << 40):
+    for qmax, pair in ((0, -1), (1 << 40, -1), (0, 0)):
         _lib.call("edge_set_stencil_quad", k.handle, qmax)
+        _lib.call("edge_set_stencil_pair", k.handle, pair)
         x, r = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
         res.append((x.cpu().numpy().copy(), s.last_iters, r))
-    (x0, it0, r0), (x1, it1, r1) = res
-    assert abs(it0 - it1) <= (0 if precision == "fp64" else 1) and r0 < 1e-8 and r1 < 1e-8
-    assert rel(x1, x0) < (1e-12 if precision == "fp64" else 1e-7)
+    x0, it0, r0 = res[0]
+    for x1, it1, r1 in res[1:]:
+        assert abs(it0 - it1) <= (0 if precision == "fp64" else 1) and r0 < 1e-8 and r1 < 1e-8
+        assert rel(x1, x0) < (1e-12 if precision == "fp64" else 1e-7)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
