@@ -346,6 +346,28 @@ struct PcgState {
 // With r32 != nullptr the updated residual is also written in FP32 (the V-cycle input of
 // the mixed-precision solver).
 
+// Finisher of the x/r update: new r.r, residual, iteration count, stop reason and the
+// next V-cycle's smoother weight (solvers/_multigrid_cuda.py:219-227).
+struct PcgXrFin {
+  PcgState* st;
+  double alpha;
+  EDGE_D void operator()(double t) const {
+    st->alpha = alpha;
+    st->rz = st->rz_new;
+    st->rr = t;
+    const double R = sqrt(t) / sqrt(st->bb);
+    st->res = R;
+    st->iter += 1;
+    if (R < st->tol) {
+      st->done = 1;
+    } else {
+      const double Rc = fmin(fmax(R, st->tol), 1e-1);
+      st->omega = st->min_omega + st->d_omega / 2.0 * exp((-Rc + st->tol) * 500.0);
+      if (st->iter >= st->maxiter) st->done = 2;
+    }
+  }
+};
+
 template <typename TX, typename TP>
 __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__ p, TX* __restrict__ r,
                          const TP* __restrict__ q, PcgState* st, double* part, unsigned* ticket,
@@ -382,26 +404,55 @@ __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__
   }
   __shared__ double sh[32];
   double bt = block_sum(acc, sh);
-  struct Fin {
-    PcgState* st;
-    double alpha;
-    EDGE_D void operator()(double t) const {
-      st->alpha = alpha;
-      st->rz = st->rz_new;
-      st->rr = t;
-      const double R = sqrt(t) / sqrt(st->bb);
-      st->res = R;
-      st->iter += 1;
-      if (R < st->tol) {
-        st->done = 1;
-      } else {
-        const double Rc = fmin(fmax(R, st->tol), 1e-1);
-        st->omega = st->min_omega + st->d_omega / 2.0 * exp((-Rc + st->tol) * 500.0);
-        if (st->iter >= st->maxiter) st->done = 2;
-      }
-    }
-  };
-  grid_reduce_finish(bt, part, ticket, Fin{st, alpha});
+  grid_reduce_finish(bt, part, ticket, PcgXrFin{st, alpha});
+}
+
+// Mixed precision: the same update with the solution kept as an FP32 increment since the last
+// residual replacement (x32 += alpha p); the FP64 solution is only touched when k_fold_x adds
+// the increment in, before every true residual and at the end of the solve.  The residual
+// recurrence stays FP64.
+__global__ void k_pcg_xr_lag(long long n, float* __restrict__ x32, const float* __restrict__ p,
+                             double* __restrict__ r, const float* __restrict__ q, PcgState* st, double* part,
+                             unsigned* ticket, float* __restrict__ r32) {
+  const double alpha = st->rz_new / st->pq;
+  const float af = (float)alpha;
+  double acc = 0.0;
+  const long long n2 = n >> 1;
+  float2* __restrict__ x2 = reinterpret_cast<float2*>(x32);
+  double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
+  const float2* __restrict__ p2 = reinterpret_cast<const float2*>(p);
+  const float2* __restrict__ q2 = reinterpret_cast<const float2*>(q);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2; i += (long long)gridDim.x * blockDim.x) {
+    const float2 pv = p2[i], qv = q2[i];
+    float2 xv = x2[i];
+    double2 rv = r2[i];
+    xv.x += af * pv.x;
+    xv.y += af * pv.y;
+    rv.x -= alpha * (double)qv.x;
+    rv.y -= alpha * (double)qv.y;
+    x2[i] = xv;
+    r2[i] = rv;
+    reinterpret_cast<float2*>(r32)[i] = make_float2((float)rv.x, (float)rv.y);
+    acc += rv.x * rv.x + rv.y * rv.y;
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const long long i = n - 1;
+    x32[i] += af * p[i];
+    r[i] -= alpha * (double)q[i];
+    r32[i] = (float)r[i];
+    acc += r[i] * r[i];
+  }
+  __shared__ double sh[32];
+  double bt = block_sum(acc, sh);
+  grid_reduce_finish(bt, part, ticket, PcgXrFin{st, alpha});
+}
+
+// x64 += x32, x32 = 0
+__global__ void k_fold_x(long long n, double* __restrict__ x, float* __restrict__ x32) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += (double)x32[i];
+    x32[i] = 0.f;
+  }
 }
 
 // Residual replacement: st->rr holds the TRUE residual r.r (b - A x in FP64).  Decides

@@ -259,6 +259,7 @@ struct Prob {
   double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr;
   void *p = nullptr, *q = nullptr;  // type T of the precision mode
   float* r32 = nullptr;
+  float* x32 = nullptr;  // mixed path: FP32 solution increment since the last replacement
   // user-layout scratch for the fused SIMP step
   double *rho_f = nullptr, *gsens = nullptr;
   // reductions
@@ -1184,6 +1185,7 @@ static void pcgmx_prologue(Prob& P, double tol, int maxiter) {
   const long long nv = (long long)g.dof * g.n;
   const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
   launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
+  CK(cudaMemsetAsync(P.x32, 0, nv * sizeof(float), P.stream));
   launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.b64, (const double*)P.b64, P.part, P.ticket,
          &P.st->bb);
   pcgmx_true_residual(P);
@@ -1205,11 +1207,18 @@ static void pcgmx_body(Prob& P) {
     fine_apply<float>(P, (const float*)p, e, &P.st->pq);
     springs_apply(P, (const float*)p, q, 1.0, &P.st->pq);
   }
-  launch(P, k_pcg_xr<double, float>, nb, 256, 0, nv, P.x64, (const float*)p, P.r64, (const float*)q, P.st, P.part,
-         P.ticket, P.r32);
+  launch(P, k_pcg_xr_lag, nb, 256, 0, nv, P.x32, (const float*)p, P.r64, (const float*)q, P.st, P.part, P.ticket,
+         P.r32);
+}
+// x64 += x32 (the FP32 increment of the solution since the last replacement), x32 = 0
+static void pcgmx_fold(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  const long long nv = (long long)P.g0.dof * P.g0.n;
+  launch(P, k_fold_x, ew_blocks(nv), 256, 0, nv, P.x64, P.x32);
 }
 static void pcgmx_replace(Prob& P) {
   CatScope cat(P, CAT_VECTOR);
+  pcgmx_fold(P);
   pcgmx_true_residual(P);
   launch(P, k_pcg_true_res, 1, 1, 0, P.st);
 }
@@ -1242,6 +1251,7 @@ static void pcg_host(Prob& P, double tol, int maxiter) {
       read_state(P);
     }
   }
+  if (mixed) pcgmx_fold(P);  // stopped on maxiter after the last replacement
   P.last_iters = P.st_h->iter;
 }
 
@@ -1370,6 +1380,7 @@ static void capture_solve(Prob& P, double tol, int maxiter, bool cg = false) {
     P.stream = P.cap[0];
     n4e = P.nlaunch;
     if (cg) cg_epilogue(P);
+    if (mixed) pcgmx_fold(P);
     CK(cudaStreamEndCapture(P.cap[0], &P.sg_graph));
     depth = 0;
     CK(cudaGraphInstantiate(&P.sg_exec, P.sg_graph, 0));
@@ -1602,6 +1613,7 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     P.p = P.alloc<double>(nv);  // sized for FP64; the mixed path uses the first half as FP32
     P.q = P.alloc<double>(nv);
     P.r32 = P.alloc<float>(nv);
+    P.x32 = P.alloc<float>(nv);
     P.rho_f = P.alloc<double>(P.n_el);
     P.gsens = P.alloc<double>(P.n_el);
     P.ocp = P.alloc<double>(P.n_el);
