@@ -208,14 +208,9 @@ class CuMultiGrid(Solver):
         stream = torch.cuda.current_stream()
         x = torch.empty_like(f)
         res, its = ctypes.c_double(), ctypes.c_int()
-        best = None
         self.kernel._bind_stream()
-        for cand in self.SWEEP_CANDIDATES:
-            if cand == "n":
-                pattern = [self.n_smooth] * self.n_level
-            else:
-                v = [int(t) for t in cand.split(",")]
-                pattern = [v[0]] + [v[-1]] * (self.n_level - 1)
+
+        def timed_solve(pattern):
             _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(pattern), len(pattern))
             x.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -224,13 +219,30 @@ class CuMultiGrid(Solver):
                       int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
             e1.record(stream)
             e1.synchronize()
-            ms = e0.elapsed_time(e1)
-            if res.value < self.tol and (best is None or ms < best[0]):
-                best = (ms, pattern, its.value)
-        if best is None:  # nothing converged within maxiter: keep the reference's sweeps
+            return e0.elapsed_time(e1), res.value < self.tol, its.value
+
+        runs = []
+        for cand in self.SWEEP_CANDIDATES:
+            if cand == "n":
+                pattern = [self.n_smooth] * self.n_level
+            else:
+                v = [int(t) for t in cand.split(",")]
+                pattern = [v[0]] + [v[-1]] * (self.n_level - 1)
+            ms, ok, it = timed_solve(pattern)
+            if ok:
+                runs.append([ms, pattern, it])
+        if not runs:  # nothing converged within maxiter: keep the reference's sweeps
             best = (0.0, [self.n_smooth] * self.n_level, 0)
+        else:
+            # the leading candidates are often within a few per cent: time the best two again
+            # and decide on the sum
+            runs.sort(key=lambda r: r[0])
+            for r in runs[:2]:
+                ms, ok, _ = timed_solve(r[1])
+                r[0] = r[0] + ms if ok else float("inf")
+            best = tuple(min(runs[:2], key=lambda r: r[0]))
         _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(best[1]), len(best[1]))
-        self.sweeps = {"per_level": best[1], "solve_ms": best[0], "pcg_iters": best[2]}
+        self.sweeps = {"per_level": best[1], "solve_ms": best[0] / (2 if runs else 1), "pcg_iters": best[2]}
         return self.sweeps
 
     @property
