@@ -83,6 +83,15 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi's start-up (NVML initialisation) must not overlap the timed region:
+        # wait for its first sample (at most 10 s)
+        import time
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            if os.path.exists(self.path) and os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -146,9 +155,9 @@ def timed_steps(opt, rho, dr, it, steps, ws, local, profile=True):
     h = opt.kernel.handle
     pcg = []
     clocks = ClockSampler(local)
+    clocks.start()
     _barrier(ws)
     torch.cuda.synchronize()
-    clocks.start()
     if profile:
         _lib.call("edge_profile_begin", h, 200000)
     n_before = ctypes.c_longlong()

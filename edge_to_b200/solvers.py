@@ -197,14 +197,17 @@ class CuMultiGrid(Solver):
 
     SWEEP_CANDIDATES = ("1", "1,2", "2", "1,3", "n")
 
-    def tune_sweep_counts(self, f):
-        """Pick per-level smoothing sweeps (fine level first) by timing one solve of K x = f
-        from x = 0 for each candidate pattern ("1,2": one sweep on the fine level, two on
-        every coarser level; "n": n_smooth everywhere, the reference's V-cycle) and keep the
-        fastest that converges.  Runs once, on the first solve; needs the density set."""
-        if self.sweeps is not None or not self.tune_sweeps or not self.kernel.has_rho:
+    def tune_sweep_counts(self, f, x0=None):
+        """Pick per-level smoothing sweeps (fine level first) by timing one solve of K x = f for
+        each candidate pattern ("1,2": one sweep on the fine level, two on every coarser
+        level; "n": n_smooth everywhere, the reference's V-cycle), every candidate starting
+        from x0, and keep the fastest that converges.  Runs once, on the first warm-started
+        solve (x0 = the previous solution, as in every later SIMP iteration; solves before it
+        use n_smooth); needs the density set."""
+        if self.sweeps is not None or not self.tune_sweeps or not self.kernel.has_rho or x0 is None:
             return self.sweeps
         f = _as_dev_f64(f)
+        x0 = _as_dev_f64(x0).clone()
         stream = torch.cuda.current_stream()
         x = torch.empty_like(f)
         res, its = ctypes.c_double(), ctypes.c_int()
@@ -212,10 +215,10 @@ class CuMultiGrid(Solver):
 
         def timed_solve(pattern):
             _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(pattern), len(pattern))
-            x.zero_()
+            x.copy_(x0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), 0, float(self.tol),
+            _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), 1, float(self.tol),
                       int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
             e1.record(stream)
             e1.synchronize()
@@ -270,7 +273,8 @@ class CuMultiGrid(Solver):
             return self._solve_padded(rhs, use_last)
         self._configure()
         self.tune()
-        self.tune_sweep_counts(rhs)
+        if use_last and self.last_x0 is not None:
+            self.tune_sweep_counts(rhs, self.last_x0)
         f = _as_dev_f64(rhs)
         if use_last and self.last_x0 is not None:
             x = self.last_x0

@@ -193,12 +193,14 @@ class CuTopOpt:
     def _solve_and_process_fused(self, rho, iteration):
         sv = self.solver
         sv._configure()
-        if (sv.autotune and sv.tuned is None) or (sv.tune_sweeps and sv.sweeps is None):
+        tune_sweeps_now = sv.tune_sweeps and sv.sweeps is None and self.reuse_sol and sv.last_x0 is not None
+        if (sv.autotune and sv.tuned is None) or tune_sweeps_now:
             # the autotuners need a density on the kernel: use this iteration's SIMP field
             rho_f = self.filter_kernel.dot(rho)
             self.kernel.set_rho(self.material_model(rho_f, iteration))
             sv.tune()
-            sv.tune_sweep_counts(self.f)
+            if tune_sweeps_now:  # warm-started from the previous solution, like the solves after it
+                sv.tune_sweep_counts(self.f, sv.last_x0)
         pen = float(self.material_model.current_penalty(iteration))
         use_last = self.reuse_sol and sv.last_x0 is not None
         if sv.last_x0 is None or not use_last:
