@@ -233,9 +233,15 @@ def run_ours(args, cfg_name):
         opt.solver.tune_sweeps = False
         opt.solver.sweeps = {"per_level": pat, "fixed": True}
         _l.call("edge_mg_set_sweeps", opt.kernel.handle, _l.int_array(pat), len(pat))
-    if args.coarse_bf16:
+    if args.coarse_fp32:
         from edge_to_b200 import _lib as _l
-        _l.call("edge_set_coarse_bf16", opt.kernel.handle, 1)
+        _l.call("edge_set_coarse_bf16", opt.kernel.handle, 0)
+    if args.residual64:
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_residual32", opt.kernel.handle, 0)
+    if args.pdl:
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_pdl", opt.kernel.handle, 1)
     rho, dr, it = warm(opt, rho, args.warmup)
     # the state the timed steps start from; the end-to-end steps restart from it, so both
     # measure the same SIMP iterations (later iterations need more PCG iterations)
@@ -338,7 +344,10 @@ def run_ours(args, cfg_name):
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "l2": "working set > 126 MB L2 (no flush needed)",
                    "pcg_iters_per_step": m["pcg"], "compliance_last": m["compliance"],
-                   "fine_tile": tuned, "sweeps": sweeps},
+                   "fine_tile": tuned, "sweeps": sweeps,
+                   "coarse_stencils": "fp32" if (args.coarse_fp32 or args.precision == "fp64") else "bf16",
+                   "residual_recurrence": "fp64" if (args.residual64 or args.precision == "fp64") else "fp32",
+                   "programmatic_dependent_launch": args.pdl and not args.no_graph},
         "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_cube/_pk/_tma + fused epilogues)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
@@ -586,7 +595,11 @@ def main():
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--n-smooth", type=int, default=3,
                     help="default smoothing sweeps of the timed path (the FP64 path keeps the reference's 3)")
-    ap.add_argument("--coarse-bf16", action="store_true", help="mixed path: BF16-stored coarse stencils")
+    ap.add_argument("--coarse-fp32", action="store_true",
+                    help="mixed path: apply the coarse stencils in FP32 (default: BF16 copies)")
+    ap.add_argument("--residual64", action="store_true", help="mixed path: FP64-stored residual recurrence")
+    ap.add_argument("--pdl", action="store_true",
+                    help="solve graph with programmatic dependent launch (default: plain stream order)")
     ap.add_argument("--sweeps", default=None,
                     help="per-level smoothing sweeps of the timed path, e.g. 1,1,1,1,1 (no sweep autotuning)")
     ap.add_argument("--no-graph", action="store_true",

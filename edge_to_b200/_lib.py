@@ -40,6 +40,8 @@ _SIGS = {
     "edge_autotune_fine": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, c_double_p, c_int_p, c_int_p]),
     "edge_set_stencil_quad": (ctypes.c_int, [vp, ctypes.c_longlong]),
     "edge_set_coarse_bf16": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_set_residual32": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_set_pdl": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_stencil_pair": (ctypes.c_int, [vp, ctypes.c_longlong]),
     "edge_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_mg_set_sweeps": (ctypes.c_int, [vp, c_int_p, ctypes.c_int]),

@@ -98,12 +98,14 @@ template <typename T, typename TS, class Epi>
 __global__ void __launch_bounds__(128)
 k_st3_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
             double* dot_dst) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long n = g.n;
   epi.init();
   double dacc = 0.0;
   const int k = (int)(s % g.pz), i = (int)((s / g.pz) % g.nx), j = (int)(s / g.plane);
   if (s < n && k < g.nz) {
+    const typename Epi::Pre pe = epi.pre(s);  // epilogue inputs first: their latency overlaps the stencil
     const T u0 = __ldg(u + s), u1 = __ldg(u + n + s), u2 = __ldg(u + 2 * n + s);
     const T c00 = Conv<T>::from(__ldg(S + s)), c01 = Conv<T>::from(__ldg(S + n + s)),
             c02 = Conv<T>::from(__ldg(S + 2 * n + s)), c11 = Conv<T>::from(__ldg(S + 3 * n + s)),
@@ -137,14 +139,15 @@ k_st3_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi 
       }
     }
     T own[3] = {u0, u1, u2};
-    epi(s, 3, own, Au, dacc);
+    epi.apply(s, own, Au, pe, dacc);
   }
   finish_dot(epi, dacc, part, ticket, dot_dst);
 }
 
 // Two consecutive z-slots per thread (s0 even, s1 = s0 + 1; the padded row length is a
-// multiple of 4, so both lie in one (x, y) row): the centre blocks, the stored upper blocks
-// and the dz = 0 neighbour values load as 8-byte pairs.  A warp covers 64 slots of one row,
+// multiple of 4, so both lie in one (x, y) row): the centre blocks, the stored upper blocks,
+// the dz = 0 lower blocks and the dz = 0 neighbour values load as pairs (8 bytes for FP32,
+// 4 bytes for a BF16 stencil copy).  A warp covers 64 slots of one row,
 // so the (x, y) range tests of a direction are warp-uniform branches; the z range test is
 // a select on values loaded from inside the array (a z neighbour outside the grid is the
 // row's padding or the next row's first slot).  Same sums in the same order per node as
@@ -153,6 +156,7 @@ template <typename T, typename TS, class Epi>
 __global__ void __launch_bounds__(128)
 k_st3_apply2(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
              double* dot_dst) {
+  EDGE_PDL_ENTRY();
   using T2 = typename V2<T>::type;
   const long long s0 = 2 * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
   const long long n = g.n;
@@ -161,10 +165,19 @@ k_st3_apply2(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi
   if (s0 < n) {
     const int k0 = (int)(s0 % g.pz), i = (int)((s0 / g.pz) % g.nx), j = (int)(s0 / g.plane);
     const bool ok0 = k0 < g.nz, ok1 = k0 + 1 < g.nz;
+    // epilogue inputs of both slots first (s0 + 1 < n: n is even), overlapping the stencil loads
+    const typename Epi::Pre pe0 = epi.pre(s0), pe1 = epi.pre(s0 + 1);
     auto ld2 = [&](const T* a, long long s) { return reinterpret_cast<const T2*>(a + s)[0]; };
     auto lds2 = [&](const TS* a, long long s) -> T2 {
       if constexpr (std::is_same<TS, T>::value) {
         return reinterpret_cast<const T2*>(a + s)[0];
+      } else if constexpr (std::is_same<TS, __nv_bfloat16>::value) {
+        // s is even and the coefficient arrays start on even slots: one 4-byte load
+        const __nv_bfloat162 h = __ldg(reinterpret_cast<const __nv_bfloat162*>(a + s));
+        T2 r;
+        r.x = Conv<T>::from(__low2bfloat16(h));
+        r.y = Conv<T>::from(__high2bfloat16(h));
+        return r;
       } else {
         T2 r;
         r.x = Conv<T>::from(__ldg(a + s));
@@ -225,20 +238,30 @@ k_st3_apply2(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi
         T2 v[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          v[c].x = __ldg(u + c * n + sa);
-          v[c].y = __ldg(u + c * n + sm + 1);
+          if (dz == 0) {  // off is even (plane and pz are multiples of 4): sm is an aligned pair start >= 0
+            v[c] = ld2(u + c * n, sm);
+          } else {
+            v[c].x = __ldg(u + c * n + sa);
+            v[c].y = __ldg(u + c * n + sm + 1);
+          }
           v[c].x = z0 ? v[c].x : T(0);
           v[c].y = z1 ? v[c].y : T(0);
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           T2 a, b, d;
-          a.x = Conv<T>::from(__ldg(Sb + (0 * 3 + c) * n + sa));
-          a.y = Conv<T>::from(__ldg(Sb + (0 * 3 + c) * n + sm + 1));
-          b.x = Conv<T>::from(__ldg(Sb + (1 * 3 + c) * n + sa));
-          b.y = Conv<T>::from(__ldg(Sb + (1 * 3 + c) * n + sm + 1));
-          d.x = Conv<T>::from(__ldg(Sb + (2 * 3 + c) * n + sa));
-          d.y = Conv<T>::from(__ldg(Sb + (2 * 3 + c) * n + sm + 1));
+          if (dz == 0) {
+            a = lds2(Sb + (0 * 3 + c) * n, sm);
+            b = lds2(Sb + (1 * 3 + c) * n, sm);
+            d = lds2(Sb + (2 * 3 + c) * n, sm);
+          } else {
+            a.x = Conv<T>::from(__ldg(Sb + (0 * 3 + c) * n + sa));
+            a.y = Conv<T>::from(__ldg(Sb + (0 * 3 + c) * n + sm + 1));
+            b.x = Conv<T>::from(__ldg(Sb + (1 * 3 + c) * n + sa));
+            b.y = Conv<T>::from(__ldg(Sb + (1 * 3 + c) * n + sm + 1));
+            d.x = Conv<T>::from(__ldg(Sb + (2 * 3 + c) * n + sa));
+            d.y = Conv<T>::from(__ldg(Sb + (2 * 3 + c) * n + sm + 1));
+          }
           Au[c].x += a.x * v[0].x + b.x * v[1].x + d.x * v[2].x;
           Au[c].y += a.y * v[0].y + b.y * v[1].y + d.y * v[2].y;
         }
@@ -246,11 +269,11 @@ k_st3_apply2(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi
     }
     if (ok0) {
       T own[3] = {uc[0].x, uc[1].x, uc[2].x}, A[3] = {Au[0].x, Au[1].x, Au[2].x};
-      epi(s0, 3, own, A, dacc);
+      epi.apply(s0, own, A, pe0, dacc);
     }
     if (ok1) {
       T own[3] = {uc[0].y, uc[1].y, uc[2].y}, A[3] = {Au[0].y, Au[1].y, Au[2].y};
-      epi(s0 + 1, 3, own, A, dacc);
+      epi.apply(s0 + 1, own, A, pe1, dacc);
     }
   }
   finish_dot(epi, dacc, part, ticket, dot_dst);
@@ -267,6 +290,7 @@ template <typename T, typename TS, class Epi>
 __global__ void __launch_bounds__(128)
 k_st3_apply_q(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
               double* dot_dst) {
+  EDGE_PDL_ENTRY();
   const long long s0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 2;
   const int q = threadIdx.x & 3;
   const long long n = g.n;
@@ -275,6 +299,8 @@ k_st3_apply_q(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Ep
   const long long s = s0 < n ? s0 : n - 1;
   const int k = (int)(s % g.pz), i = (int)((s / g.pz) % g.nx), j = (int)(s / g.plane);
   const bool valid = s0 < n && k < g.nz;
+  typename Epi::Pre pe{};
+  if (q == 0) pe = epi.pre(s);  // the epilogue lane's inputs first (s is clamped into the array)
   T Au[3] = {T(0), T(0), T(0)};
 #pragma unroll
   for (int m = 0; m < 7; ++m) {
@@ -316,7 +342,7 @@ k_st3_apply_q(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Ep
     Au[1] += c01 * u0 + c11 * u1 + c12 * u2;
     Au[2] += c02 * u0 + c12 * u1 + c22 * u2;
     T own[3] = {u0, u1, u2};
-    epi(s, 3, own, Au, dacc);
+    epi.apply(s, own, Au, pe, dacc);
   }
   finish_dot(epi, dacc, part, ticket, dot_dst);
 }
@@ -325,6 +351,7 @@ template <typename T, typename TS, class Epi>
 __global__ void __launch_bounds__(128)
 k_st2_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi epi, double* part, unsigned* ticket,
             double* dot_dst) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long n = g.n;
   epi.init();
@@ -364,6 +391,7 @@ k_st2_apply(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi 
 // Dinv of a stencil level: 1 / centre diagonal.
 template <typename TS, typename TD>
 __global__ void k_st_dinv(const Geo g, const TS* __restrict__ S, TD* __restrict__ dinv) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   for (int c = 0; c < g.dof; ++c) {
@@ -374,28 +402,39 @@ __global__ void k_st_dinv(const Geo g, const TS* __restrict__ S, TD* __restrict_
 
 // ------------------------------------------------------------------ transfers
 template <typename TI, typename TO>
-// 3-D transfers: one thread per output node; blockIdx.y = plane y, the (z, x) pairs of a plane
-// flattened over blockIdx.x (z fastest).
+// 3-D restriction: one thread per coarse node; blockIdx.y = plane y, the (z, x) pairs of a
+// plane flattened over blockIdx.x (z fastest).  The fine z-neighbours 2K and 2K + 1 are one
+// aligned pair load (2K is even and rows are padded to a multiple of 4 slots, so 2K + 1 is
+// inside the row; it is masked when it is past the last node), 2K - 1 a scalar load.  The
+// weights are summed in the order (x, y, z) of the 27-point loop.
 __global__ void k_restrict3(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  EDGE_PDL_ENTRY();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int J = blockIdx.y;
   if (t >= gc.nz * gc.nx) return;
   const int K = t % gc.nz, I = t / gc.nz;
   using T = typename TransferT<TO>::type;
+  using TI2 = typename V2<TI>::type;
   const int nb = is_bnd(I, gc.nx) + is_bnd(J, gc.ny) + is_bnd(K, gc.nz);
+  const bool zm = K >= 1, zp = 2 * K + 1 < gf.nz;
   T v[3] = {0, 0, 0};
+#pragma unroll
   for (int di = -1; di <= 1; ++di) {
     const int fi = 2 * I + di;
     if (fi < 0 || fi >= gf.nx) continue;
+#pragma unroll
     for (int dj = -1; dj <= 1; ++dj) {
       const int fj = 2 * J + dj;
       if (fj < 0 || fj >= gf.ny) continue;
-      for (int dk = -1; dk <= 1; ++dk) {
-        const int fk = 2 * K + dk;
-        if (fk < 0 || fk >= gf.nz) continue;
-        const T w = (T)dist_w(abs(di) + abs(dj) + abs(dk));
-        const long long sf = gf.slot3(fi, fj, fk);
-        for (int c = 0; c < 3; ++c) v[c] += w * Conv<T>::from(in[c * gf.n + sf]);
+      const T w0 = (T)dist_w(abs(di) + abs(dj)), w1 = (T)dist_w(abs(di) + abs(dj) + 1);
+      const long long sf = gf.slot3(fi, fj, 2 * K);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const TI* a = in + c * gf.n + sf;
+        const TI2 pr = __ldg(reinterpret_cast<const TI2*>(a));
+        if (zm) v[c] += w1 * Conv<T>::from(__ldg(a - 1));
+        v[c] += w0 * Conv<T>::from(pr.x);
+        if (zp) v[c] += w1 * Conv<T>::from(pr.y);
       }
     }
   }
@@ -406,6 +445,7 @@ __global__ void k_restrict3(const Geo gf, const Geo gc, const TI* __restrict__ i
 
 template <typename TI, typename TO>
 __global__ void k_restrict2(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  EDGE_PDL_ENTRY();
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   const int J = blockIdx.y;
   if (I >= gc.nx) return;
@@ -427,36 +467,75 @@ __global__ void k_restrict2(const Geo gf, const Geo gc, const TI* __restrict__ i
   for (int c = 0; c < 2; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] * iw);
 }
 
+// 3-D prolongation: one thread per coarse node (ci, cj, ck), which writes its fine children
+// (2ci + a, 2cj + b, 2ck + c), a, b, c in {0, 1}.  A child's value is the mean of its coarse
+// parents (the corners ci..ci+a x cj..cj+b x ck..ck+c that exist), each scaled by the
+// reciprocal of its boundary weight total; the eight corner values are loaded once per thread
+// instead of once per child, and the two z-children of a fine row are one aligned pair store.
+// Launch: blockIdx.y = coarse plane cj, the coarse (z, x) pairs flattened over blockIdx.x.
 template <typename TI, typename TO>
 __global__ void k_prolong3(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  EDGE_PDL_ENTRY();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
-  if (t >= gf.nz * gf.nx) return;
-  const int k = t % gf.nz, i = t / gf.nz;
+  const int cj = blockIdx.y;
+  if (t >= gc.nz * gc.nx) return;
+  const int ck = t % gc.nz, ci = t / gc.nz;
   using T = typename TransferT<TO>::type;
-  T v[3] = {0, 0, 0};
-  int cnt = 0;
-  for (int ci = i / 2; ci <= i / 2 + (i & 1); ++ci) {
-    if (ci >= gc.nx) continue;
-    for (int cj = j / 2; cj <= j / 2 + (j & 1); ++cj) {
-      if (cj >= gc.ny) continue;
-      for (int ck = k / 2; ck <= k / 2 + (k & 1); ++ck) {
-        if (ck >= gc.nz) continue;
-        const T iw = inv_bnd_total3<T>(is_bnd(ci, gc.nx) + is_bnd(cj, gc.ny) + is_bnd(ck, gc.nz));
-        const long long sc = gc.slot3(ci, cj, ck);
-        for (int c = 0; c < 3; ++c) v[c] += Conv<T>::from(in[c * gc.n + sc]) * iw;
-        ++cnt;
+  using TO2 = typename V2<TO>::type;
+  // upper parents that exist, and odd children that exist
+  const bool px = ci + 1 < gc.nx, py = cj + 1 < gc.ny, pz = ck + 1 < gc.nz;
+  const bool fx = 2 * ci + 1 < gf.nx, fy = 2 * cj + 1 < gf.ny, fz = 2 * ck + 1 < gf.nz;
+  T cv[2][2][2][3];  // weighted corner values, 0 where the corner does not exist
+#pragma unroll
+  for (int x = 0; x < 2; ++x)
+#pragma unroll
+    for (int y = 0; y < 2; ++y)
+#pragma unroll
+      for (int z = 0; z < 2; ++z) {
+        const bool ex = (x == 0 || px) && (y == 0 || py) && (z == 0 || pz);
+        const long long sc = gc.slot3(ci + x, cj + y, ck + z);
+        const T iw = inv_bnd_total3<T>(is_bnd(ci + x, gc.nx) + is_bnd(cj + y, gc.ny) + is_bnd(ck + z, gc.nz));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) cv[x][y][z][c] = ex ? Conv<T>::from(__ldg(in + c * gc.n + sc)) * iw : T(0);
+      }
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    if (a == 1 && !fx) continue;
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      if (b == 1 && !fy) continue;
+      // parents per axis: 1, or 2 for an odd child whose upper parent exists; 1/cnt is exact
+      const int cxy = (1 + (a == 1 && px)) * (1 + (b == 1 && py));
+      const T ic0 = T(1) / T(cxy), ic1 = T(1) / T(cxy * (1 + pz));
+      const long long sf = gf.slot3(2 * ci + a, 2 * cj + b, 2 * ck);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        T v0 = 0, v1 = 0;  // the even and the odd z-child
+#pragma unroll
+        for (int x = 0; x <= a; ++x)
+#pragma unroll
+          for (int y = 0; y <= b; ++y) {
+            v0 += cv[x][y][0][c];
+            v1 += cv[x][y][0][c];
+            v1 += cv[x][y][1][c];
+          }
+        TO* o = out + c * gf.n + sf;
+        if (fz) {
+          TO2 w;
+          w.x = Conv<TO>::from(v0 * ic0);
+          w.y = Conv<TO>::from(v1 * ic1);
+          *reinterpret_cast<TO2*>(o) = w;
+        } else {
+          o[0] = Conv<TO>::from(v0 * ic0);
+        }
       }
     }
   }
-  // cnt is 1, 2, 4 or 8: its reciprocal is exact
-  const T ic = cnt ? T(1) / T(cnt) : T(0);
-  const long long sf = gf.slot3(i, j, k);
-  for (int c = 0; c < 3; ++c) out[c * gf.n + sf] = Conv<TO>::from(v[c] * ic);
 }
 
 template <typename TI, typename TO>
 __global__ void k_prolong2(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
+  EDGE_PDL_ENTRY();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= gf.nx) return;
@@ -481,6 +560,7 @@ __global__ void k_prolong2(const Geo gf, const Geo gc, const TI* __restrict__ in
 // ------------------------------------------------------------------ Galerkin, level 0 -> 1
 // Element constraint flags: flag[slot(e)] = 1 if any corner DOF of element e is constrained.
 __global__ void k_elem_flags(const Geo g, const uint8_t* __restrict__ mask, uint8_t* __restrict__ flag) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   uint8_t f = 0;
@@ -520,6 +600,7 @@ __global__ void __launch_bounds__(128)
 k_galerkin3_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
                const uint8_t* __restrict__ eflag, const double* __restrict__ Q, const double* __restrict__ K0b,
                TS* __restrict__ S) {
+  EDGE_PDL_ENTRY();
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int nb = 13 + blockIdx.y;  // centre and upper directions only
   if (sc >= gc.n) return;
@@ -615,6 +696,7 @@ __global__ void __launch_bounds__(128)
 k_galerkin2_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
                const uint8_t* __restrict__ eflag, const double* __restrict__ Q, const double* __restrict__ K0b,
                TS* __restrict__ S) {
+  EDGE_PDL_ENTRY();
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int nb = 4 + blockIdx.y;  // centre and upper directions only
   if (sc >= gc.n) return;
@@ -700,6 +782,7 @@ k_galerkin2_l0(const Geo gf, const Geo gc, const TE* __restrict__ E, const uint8
 template <typename TS>
 __global__ void __launch_bounds__(128)
 k_galerkin3_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __restrict__ Sc) {
+  EDGE_PDL_ENTRY();
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int nb = 13 + blockIdx.y;
   if (sc >= gc.n) return;
@@ -745,6 +828,7 @@ k_galerkin3_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __rest
 template <typename TS>
 __global__ void __launch_bounds__(128)
 k_galerkin2_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __restrict__ Sc) {
+  EDGE_PDL_ENTRY();
   const long long sc = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int nb = 4 + blockIdx.y;
   if (sc >= gc.n) return;
@@ -789,6 +873,7 @@ k_galerkin2_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __rest
 // node_index the unpadded lexicographic index (j, i, k) of the reference.
 template <typename TS>
 __global__ void k_st_to_dense(const Geo g, const TS* __restrict__ S, double* __restrict__ A, int nd) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   const int dof = g.dof;
@@ -827,6 +912,7 @@ __global__ void k_st_to_dense(const Geo g, const TS* __restrict__ S, double* __r
 constexpr int CB = 32;
 
 __global__ void __launch_bounds__(CB * CB / 4) k_chol_diag(double* A, int nd, int K, int* status) {
+  EDGE_PDL_ENTRY();
   __shared__ double t[CB][CB + 1];
   const int k0 = K * CB;
   const int m = min(CB, nd - k0);
@@ -862,6 +948,7 @@ __global__ void __launch_bounds__(CB * CB / 4) k_chol_diag(double* A, int nd, in
 
 // Tile row I = K+1+blockIdx.x: X L_KK^T = A_IK  (X overwrites A_IK)
 __global__ void __launch_bounds__(CB * CB / 4) k_chol_panel(double* A, int nd, int K) {
+  EDGE_PDL_ENTRY();
   __shared__ double L[CB][CB + 1];
   __shared__ double X[CB][CB + 1];
   const int k0 = K * CB;
@@ -890,6 +977,7 @@ __global__ void __launch_bounds__(CB * CB / 4) k_chol_panel(double* A, int nd, i
 
 // Trailing update A_IJ -= A_IK A_JK^T for K < J <= I; blockIdx.x enumerates (I, J).
 __global__ void __launch_bounds__(CB * CB / 4) k_chol_update(double* A, int nd, int K, int nt) {
+  EDGE_PDL_ENTRY();
   __shared__ double P[CB][CB + 1];
   __shared__ double Q[CB][CB + 1];
   const int m = nt - K - 1;  // tiles below K
@@ -921,6 +1009,7 @@ __global__ void __launch_bounds__(CB * CB / 4) k_chol_update(double* A, int nd, 
 
 // U = L^T (row-major), so that both substitutions below read rows.
 __global__ void k_transpose_lower(const double* __restrict__ L, double* __restrict__ U, int nd) {
+  EDGE_PDL_ENTRY();
   const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (q >= (long long)nd * nd) return;
   const int r = (int)(q / nd), c = (int)(q % nd);
@@ -930,6 +1019,7 @@ __global__ void k_transpose_lower(const double* __restrict__ L, double* __restri
 // Column `col` of A^-1 = L^-T L^-1 e_col, one block per column.  U = L^T row-major.
 __global__ void __launch_bounds__(256) k_chol_inverse(const double* __restrict__ L, const double* __restrict__ U,
                                                       double* __restrict__ X, int nd) {
+  EDGE_PDL_ENTRY();
   extern __shared__ double y[];
   const int col = blockIdx.x;
   const int t = threadIdx.x, nt = blockDim.x;
@@ -953,13 +1043,14 @@ __global__ void __launch_bounds__(256) k_chol_inverse(const double* __restrict__
 }
 
 // x = Ainv b on the coarsest level: b and x in slot layout (types TB/TX), Ainv dense FP64.
-// One warp per dense row.
+// Each block first gathers b into shared memory in dense order (nd * sizeof(TB) bytes of
+// dynamic shared memory), then one warp per dense row.
 template <typename TB, typename TX>
 __global__ void k_coarse_solve(const Geo g, const double* __restrict__ Ainv, int nd, const TB* __restrict__ b,
                                TX* __restrict__ x) {
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (row >= nd) return;
+  EDGE_PDL_ENTRY();
+  extern __shared__ __align__(16) unsigned char coarse_smem[];
+  TB* bs = reinterpret_cast<TB*>(coarse_smem);
   const int dof = g.dof;
   auto slot_of = [&](int dn) -> long long {
     const int node = dn / dof;
@@ -970,11 +1061,14 @@ __global__ void k_coarse_solve(const Geo g, const double* __restrict__ Ainv, int
     const int i = node % g.nx, j = node / g.nx;
     return g.slot2(i, j);
   };
+  for (int c = threadIdx.x; c < nd; c += blockDim.x) bs[c] = b[(c % dof) * g.n + slot_of(c)];
+  __syncthreads();
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= nd) return;
+  const double* __restrict__ a = Ainv + (long long)row * nd;
   double acc = 0.0;
-  for (int cidx = lane; cidx < nd; cidx += 32) {
-    const double bv = (double)Conv<double>::from(b[(cidx % dof) * g.n + slot_of(cidx)]);
-    acc += Ainv[(long long)row * nd + cidx] * bv;
-  }
+  for (int c = lane; c < nd; c += 32) acc += a[c] * (double)Conv<double>::from(bs[c]);
   acc = warp_sum(acc);
   if (lane == 0) x[(row % dof) * g.n + slot_of(row)] = Conv<TX>::from(acc);
 }

@@ -55,6 +55,13 @@ inline Geo make_geo(int dim, int nelx, int nely, int nelz, int zalign = 4) {
   return g;
 }
 
+// Programmatic dependent launch.  Inside the captured solve graph kernels are launched with
+// programmatic stream serialization, so a kernel's blocks may be scheduled while the kernel
+// before it is still finishing.  Every kernel therefore waits for that grid to complete (and
+// its memory to be visible) before its first memory access, and then lets its own dependents
+// start launching.  Both instructions are no-ops for a kernel launched without the attribute.
+#define EDGE_PDL_ENTRY() asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory")
+
 // ------------------------------------------------------------------ type helpers
 template <typename T> EDGE_D T ld(const T* p) { return __ldg(p); }
 EDGE_D double to_d(double x) { return x; }

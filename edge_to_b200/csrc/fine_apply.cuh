@@ -188,6 +188,7 @@ template <typename T, typename TE, class Epi, int BX>
 __global__ void __launch_bounds__(32 * BX)
 k_fine3_wht(const Geo g, const T* __restrict__ u, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
             const KHat3<T> K, const int ly, Epi epi, double* part, unsigned* ticket, double* dot_dst) {
+  EDGE_PDL_ENTRY();
   __shared__ T sU[2][3][BX + 1][34];
   __shared__ T sG[2][2][3][BX][33];
   const int lane = threadIdx.x, wx = threadIdx.y, tid = lane + 32 * wx;
@@ -302,6 +303,7 @@ template <typename T, typename TE, class Epi, int NW>
 __global__ void __launch_bounds__(32 * NW)
 k_fine2_wht(const Geo g, const T* __restrict__ u, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
             const KHat2<T> K, const int ly, Epi epi, double* part, unsigned* ticket, double* dot_dst) {
+  EDGE_PDL_ENTRY();
   constexpr int NT = 32 * NW;
   __shared__ T sU[2][2][NT + 2];
   __shared__ T sG[2][2][2][NT + 1];
@@ -397,6 +399,7 @@ template <typename T, typename TE, class Epi>
 __global__ void __launch_bounds__(128)
 k_fine3_dense(const Geo g, const T* __restrict__ u, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
               const T* __restrict__ K0b, Epi epi, double* part, unsigned* ticket, double* dot_dst) {
+  EDGE_PDL_ENTRY();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   const int j = blockIdx.z;
@@ -438,6 +441,7 @@ template <typename T, typename TE, class Epi>
 __global__ void __launch_bounds__(128)
 k_fine2_dense(const Geo g, const T* __restrict__ u, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
               const T* __restrict__ K0b, Epi epi, double* part, unsigned* ticket, double* dot_dst) {
+  EDGE_PDL_ENTRY();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   const long long n = g.n;

@@ -263,6 +263,7 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
              const __grid_constant__ CUtensorMap mapS0, const __grid_constant__ CUtensorMap mapS1,
              const __grid_constant__ CUtensorMap mapS2, const __grid_constant__ CUtensorMap mapS3, const KCube KC,
              const int ly, SE epi, double* part, unsigned* ticket, double* dot_dst, int* err) {
+  EDGE_PDL_ENTRY();
   static_assert(NS >= 3, "a stage is refilled one layer after its last use");
   using Tile = CubeTile<BX, SE>;
   using PT = PkTile<BX>;

@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(32 * BX)
 k_fine3_tma(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_constant__ CUtensorMap mapF,
             const __grid_constant__ CUtensorMap mapE, const T* __restrict__ u, const uint8_t* __restrict__ mask,
             const KHat3<T> K, const int ly, Epi epi, double* part, unsigned* ticket, double* dot_dst, int* err) {
+  EDGE_PDL_ENTRY();
   using Tile = TmaTile<T, BX>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);

@@ -29,6 +29,7 @@ EDGE_D bool node_of_slot(const Geo& g, long long s, int& i, int& j, int& k, long
 
 template <typename TO>
 __global__ void k_user_to_slots(const Geo g, const double* __restrict__ user, TO* __restrict__ v) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   int i, j, k;
@@ -39,6 +40,7 @@ __global__ void k_user_to_slots(const Geo g, const double* __restrict__ user, TO
 
 template <typename TI>
 __global__ void k_slots_to_user(const Geo g, const TI* __restrict__ v, double* __restrict__ user) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   int i, j, k;
@@ -49,6 +51,7 @@ __global__ void k_slots_to_user(const Geo g, const TI* __restrict__ v, double* _
 
 // Per-node constraint bits from the reference's per-DOF boolean array.
 __global__ void k_mask_from_user(const Geo g, const uint8_t* __restrict__ cons, uint8_t* __restrict__ mask) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   int i, j, k;
@@ -64,6 +67,7 @@ __global__ void k_mask_from_user(const Geo g, const uint8_t* __restrict__ cons, 
 // element slot has a constrained DOF.  Slots past the last element (ghosts) are flagged
 // from their existing corners, so f(i,j,k) always covers node (i,j,k) itself.
 __global__ void k_flag_pitch16(const Geo g, const uint8_t* __restrict__ mask, uint8_t* __restrict__ f16, int mpz) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   int i, j, k;
@@ -87,6 +91,7 @@ EDGE_D long long user_elem(const Geo& g, int i, int j, int k) {
 
 template <typename TO>
 __global__ void k_elem_user_to_slots(const Geo g, const double* __restrict__ user, TO* __restrict__ v) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   int i, j, k;
@@ -114,6 +119,7 @@ template <typename TE1, typename TE2>
 __global__ void k_filter_material(const Geo g, const Taps taps, const double* __restrict__ rho,
                                   double* __restrict__ rho_f, TE1* __restrict__ E1, TE2* __restrict__ E2,
                                   double penalty, double vmin, int plain) {
+  EDGE_PDL_ENTRY();
   const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nel = (long long)nelx * nely * nelz;
@@ -151,6 +157,7 @@ __global__ void k_filter_material(const Geo g, const Taps taps, const double* __
 
 // Filter only (H rho), user order in and out.
 __global__ void k_filter(const Geo g, const Taps taps, const double* __restrict__ in, double* __restrict__ out) {
+  EDGE_PDL_ENTRY();
   const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nel = (long long)nelx * nely * nelz;
@@ -177,6 +184,7 @@ __global__ void k_filter(const Geo g, const Taps taps, const double* __restrict_
 
 // Normaliser N_e = sum of in-bounds weights (core/_filter.py:6-40).
 __global__ void k_filter_norm(const Geo g, const Taps taps, double* __restrict__ N) {
+  EDGE_PDL_ENTRY();
   const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nel = (long long)nelx * nely * nelz;
@@ -203,6 +211,7 @@ __global__ void k_filter_norm(const Geo g, const Taps taps, double* __restrict__
 // Transpose: (H^T v)_e = sum_k (w_k / N_{e+o_k}) v_{e+o_k} (core/_filter.py:42-76).
 __global__ void k_filter_T(const Geo g, const Taps taps, const double* __restrict__ N, const double* __restrict__ in,
                            double* __restrict__ out) {
+  EDGE_PDL_ENTRY();
   const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nel = (long long)nelx * nely * nelz;
@@ -235,6 +244,7 @@ template <typename TU>
 __global__ void k_dk(const Geo g, const TU* __restrict__ U, KHat3<double> K3, KHat2<double> K2,
                      const double* __restrict__ K0b, int wht, double* __restrict__ dk, const double* __restrict__ rho_f,
                      double* __restrict__ gout, double penalty, double vmin) {
+  EDGE_PDL_ENTRY();
   const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nel = (long long)nelx * nely * nelz;
@@ -287,6 +297,7 @@ template <typename TE, typename TD>
 __global__ void k_fine_dinv(const Geo g, const TE* __restrict__ E, const uint8_t* __restrict__ mask,
                             const double* __restrict__ K0diag /* [corner][c] bit order */, TD* __restrict__ dinv,
                             double* __restrict__ diag_out) {
+  EDGE_PDL_ENTRY();
   const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (s >= g.n) return;
   int i, j, k;
@@ -317,6 +328,7 @@ __global__ void k_fine_dinv(const Geo g, const TE* __restrict__ E, const uint8_t
 template <typename TA, typename TB>
 __global__ void k_dot(long long n, const TA* __restrict__ a, const TB* __restrict__ b, double* part, unsigned* ticket,
                       double* dst) {
+  EDGE_PDL_ENTRY();
   double acc = 0.0;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
     acc += (double)Conv<double>::from(a[q]) * (double)Conv<double>::from(b[q]);
@@ -372,6 +384,7 @@ template <typename TX, typename TP>
 __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__ p, TX* __restrict__ r,
                          const TP* __restrict__ q, PcgState* st, double* part, unsigned* ticket,
                          float* __restrict__ r32) {
+  EDGE_PDL_ENTRY();
   using X2 = typename V2<TX>::type;
   using P2v = typename V2<TP>::type;
   const double alpha = st->rz_new / st->pq;
@@ -414,6 +427,7 @@ __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__
 __global__ void k_pcg_xr_lag(long long n, float* __restrict__ x32, const float* __restrict__ p,
                              double* __restrict__ r, const float* __restrict__ q, PcgState* st, double* part,
                              unsigned* ticket, float* __restrict__ r32) {
+  EDGE_PDL_ENTRY();
   const double alpha = st->rz_new / st->pq;
   const float af = (float)alpha;
   double acc = 0.0;
@@ -447,8 +461,52 @@ __global__ void k_pcg_xr_lag(long long n, float* __restrict__ x32, const float* 
   grid_reduce_finish(bt, part, ticket, PcgXrFin{st, alpha});
 }
 
+// Mixed precision with an FP32 residual recurrence between the FP64 replacements ("reliable
+// updates": the recurrence only has to stay accurate relative to the residual at the last
+// replacement, which is at most 100 times the current one): x32 += alpha p, r32 -= alpha q
+// as FP32 fused multiply-adds with alpha rounded to FP32, 16-byte accesses, r.r summed per
+// four values in FP32 and accumulated in FP64.
+__global__ void k_pcg_xr32(long long n, float* __restrict__ x32, const float* __restrict__ p,
+                           float* __restrict__ r32, const float* __restrict__ q, PcgState* st, double* part,
+                           unsigned* ticket) {
+  EDGE_PDL_ENTRY();
+  const double alpha = st->rz_new / st->pq;
+  const float af = (float)alpha;
+  double acc = 0.0;
+  const long long n4 = n >> 2;
+  float4* __restrict__ x4 = reinterpret_cast<float4*>(x32);
+  float4* __restrict__ r4 = reinterpret_cast<float4*>(r32);
+  const float4* __restrict__ p4 = reinterpret_cast<const float4*>(p);
+  const float4* __restrict__ q4 = reinterpret_cast<const float4*>(q);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 pv = p4[i], qv = q4[i];
+    float4 xv = x4[i], rv = r4[i];
+    xv.x = fmaf(af, pv.x, xv.x);
+    xv.y = fmaf(af, pv.y, xv.y);
+    xv.z = fmaf(af, pv.z, xv.z);
+    xv.w = fmaf(af, pv.w, xv.w);
+    rv.x = fmaf(-af, qv.x, rv.x);
+    rv.y = fmaf(-af, qv.y, rv.y);
+    rv.z = fmaf(-af, qv.z, rv.z);
+    rv.w = fmaf(-af, qv.w, rv.w);
+    x4[i] = xv;
+    r4[i] = rv;
+    acc += (double)(rv.x * rv.x + rv.y * rv.y + rv.z * rv.z + rv.w * rv.w);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {  // tail (lengths here are multiples of 4)
+    const long long i = 4 * n4 + threadIdx.x;
+    x32[i] = fmaf(af, p[i], x32[i]);
+    r32[i] = fmaf(-af, q[i], r32[i]);
+    acc += (double)r32[i] * (double)r32[i];
+  }
+  __shared__ double sh[32];
+  double bt = block_sum(acc, sh);
+  grid_reduce_finish(bt, part, ticket, PcgXrFin{st, alpha});
+}
+
 // x64 += x32, x32 = 0
 __global__ void k_fold_x(long long n, double* __restrict__ x, float* __restrict__ x32) {
+  EDGE_PDL_ENTRY();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     x[i] += (double)x32[i];
     x32[i] = 0.f;
@@ -458,6 +516,7 @@ __global__ void k_fold_x(long long n, double* __restrict__ x, float* __restrict_
 // Residual replacement: st->rr holds the TRUE residual r.r (b - A x in FP64).  Decides
 // convergence on it; otherwise the iteration continues with the replaced residual.
 __global__ void k_pcg_true_res(PcgState* st) {
+  EDGE_PDL_ENTRY();
   const double R = sqrt(st->rr) / sqrt(st->bb);
   st->res = R;
   st->last_replace = R;
@@ -474,6 +533,7 @@ __global__ void k_pcg_true_res(PcgState* st) {
 // p = z + beta p, or p = z before the first iteration (iter == 0)
 template <typename TP>
 __global__ void k_pcg_p(long long n, TP* __restrict__ p, const TP* __restrict__ z, const PcgState* st) {
+  EDGE_PDL_ENTRY();
   using P2v = typename V2<TP>::type;
   const bool first = st->iter == 0;
   const double beta = first ? 0.0 : st->rz_new / st->rz;
@@ -498,9 +558,11 @@ __global__ void k_pcg_p(long long n, TP* __restrict__ p, const TP* __restrict__ 
 }
 
 // Unpreconditioned CG as PCG with z = r: r.z of the current residual is its r.r.
-__global__ void k_cg_rz(PcgState* st) { st->rz_new = st->rr; }
+__global__ void k_cg_rz(PcgState* st) {
+  EDGE_PDL_ENTRY(); st->rz_new = st->rr; }
 // Report the true relative residual ||f - A x|| / ||f|| (st->rr holds the true r.r).
-__global__ void k_final_res(PcgState* st) { st->res = st->bb > 0.0 ? sqrt(st->rr) / sqrt(st->bb) : 0.0; }
+__global__ void k_final_res(PcgState* st) {
+  EDGE_PDL_ENTRY(); st->res = st->bb > 0.0 ? sqrt(st->rr) / sqrt(st->bb) : 0.0; }
 
 // FEA_integrals (TopOpt/_solver.py:80-137 with the structured kernel of core/_ops.py:1032-1058):
 // per element, strain = B u_e, stress = D strain (D unscaled, as in the reference), strain
@@ -511,6 +573,7 @@ __global__ void k_fea_integrals(int dim, int nelx, int nely, int nelz, long long
                                 const double* __restrict__ w, const double* __restrict__ K0,
                                 const double* __restrict__ B, const double* __restrict__ D, int nb,
                                 double* __restrict__ strain, double* __restrict__ stress, double* __restrict__ energy) {
+  EDGE_PDL_ENTRY();
   const int nc = dim == 3 ? 8 : 4, nk = nc * dim;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nel; e += (long long)gridDim.x * blockDim.x) {
     long long nid[8];
@@ -562,9 +625,11 @@ __global__ void k_fea_integrals(int dim, int nelx, int nely, int nelz, long long
 // the if node (mixed precision) computes a true residual when the recurrence has converged
 // or has dropped by `drop` since the last replacement.
 __global__ void k_cond_while(cudaGraphConditionalHandle h, const PcgState* st) {
+  EDGE_PDL_ENTRY();
   cudaGraphSetConditional(h, st->done == 0 ? 1u : 0u);
 }
 __global__ void k_cond_replace(cudaGraphConditionalHandle h, const PcgState* st, double drop) {
+  EDGE_PDL_ENTRY();
   cudaGraphSetConditional(h, (st->done == 1 || st->res < drop * st->last_replace) ? 1u : 0u);
 }
 
@@ -576,6 +641,7 @@ template <typename TX, typename TO>
 __global__ void k_springs(int ns, const long long* __restrict__ flat, const double* __restrict__ kk, long long n,
                           const uint8_t* __restrict__ mask, const TX* __restrict__ x, TO* __restrict__ out,
                           double sign, double* dot) {
+  EDGE_PDL_ENTRY();
   __shared__ double sh[32];
   double acc = 0.0;
   for (int t = threadIdx.x; t < ns; t += blockDim.x) {
@@ -595,6 +661,7 @@ __global__ void k_springs(int ns, const long long* __restrict__ flat, const doub
 __global__ void k_springs_diag(int ns, const long long* __restrict__ flat, const long long* __restrict__ user,
                                const double* __restrict__ kk, long long n, const uint8_t* __restrict__ mask,
                                double* __restrict__ diag) {
+  EDGE_PDL_ENTRY();
   for (int t = threadIdx.x; t < ns; t += blockDim.x) {
     const long long f = flat[t];
     if ((mask[f % n] >> (int)(f / n)) & 1) continue;
@@ -606,6 +673,7 @@ __global__ void k_springs_diag(int ns, const long long* __restrict__ flat, const
 // element energy: v^T K0 u = ((u+v)^T K0 (u+v) - (u-v)^T K0 (u-v)) / 4.
 __global__ void k_dk2(const Geo g, const double* __restrict__ U, const double* __restrict__ V, KHat3<double> K3,
                       KHat2<double> K2, const double* __restrict__ K0b, int wht, double* __restrict__ dk) {
+  EDGE_PDL_ENTRY();
   const int nelx = g.nx - 1, nely = g.ny - 1, nelz = g.dim == 3 ? g.nz - 1 : 1;
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nel = (long long)nelx * nely * nelz;
@@ -664,6 +732,7 @@ __global__ void k_dk2(const Geo g, const double* __restrict__ U, const double* _
 // MaterialModels.py:87-88 is applied by k_oc_fallback when sum(ocP_raw) == 0.
 __global__ void k_oc_prep(long long n, const double* __restrict__ rho, const double* __restrict__ dr, double A,
                           double* __restrict__ ocp, double* part, unsigned* ticket, double* sum_dst) {
+  EDGE_PDL_ENTRY();
   double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     double v = rho[i] * sqrt(fmax(-dr[i] / A, 0.0));
@@ -677,6 +746,7 @@ __global__ void k_oc_prep(long long n, const double* __restrict__ rho, const dou
 }
 
 __global__ void k_oc_floor(long long n, double* __restrict__ ocp, const double* __restrict__ sum) {
+  EDGE_PDL_ENTRY();
   const bool allzero = (*sum == 0.0);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     double v = allzero ? 1e-3 : ocp[i];
@@ -704,6 +774,7 @@ EDGE_D double oc_rho(double r, double o, double lam, double move) {
 // and 2t+2 (l1 = mid).
 __global__ void __launch_bounds__(256) k_oc_pass(long long n, const double* __restrict__ rho, const double* __restrict__ ocp,
                                                  double A, double move, OcState* st, double* part, unsigned* ticket) {
+  EDGE_PDL_ENTRY();
   if (st->done) return;
   double lam[OC_NODES];
   {
@@ -778,6 +849,7 @@ __global__ void __launch_bounds__(256) k_oc_pass(long long n, const double* __re
 __global__ void k_oc_final(long long n, const double* __restrict__ rho, const double* __restrict__ ocp, double move,
                            const OcState* st, double* __restrict__ rho_new, double* part, unsigned* ticket,
                            double* chg_dst) {
+  EDGE_PDL_ENTRY();
   const double lam = st->last;
   double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {

@@ -221,7 +221,15 @@ struct Prob {
   bool cube = false;       // kcube reproduces every entry of the transformed operator
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
   long long st_quad_max = 40000;   // 3-D stencil levels with at most this many slots use k_st3_apply_q
-  bool st_bf16 = false;            // mixed precision: apply the coarse stencils from BF16 copies
+  bool st_bf16 = true;             // mixed precision: apply the coarse stencils from BF16 copies
+  // mixed precision: the residual recurrence between FP64 replacements is stored in FP32
+  // (arithmetic and r.r in FP64); false keeps an FP64 recurrence with an FP32 copy
+  bool res32 = true;
+  // solve graph: kernels launched with programmatic stream serialization (each kernel's
+  // blocks may be scheduled while its predecessor drains; every kernel waits on entry).
+  // Off by default: at 12.8M DOF the SIMP loop ran 1.5 % slower with it.
+  bool pdl = false;
+  bool capturing = false;  // set while capture_solve records the solve graph
   // FP32 3-D levels with at least st_pair_min slots: two nodes per thread (k_st3_apply2;
   // 21 % faster than one node per thread at 570 k slots, slower at 75 k and in FP64)
   bool st_pair = true;
@@ -320,7 +328,21 @@ template <typename... KArgs, typename... Args>
 static void launch(Prob& P, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
   const bool rec = P.bd && P.bev_used + 2 <= P.bev.size();
   if (rec) CK(cudaEventRecord(P.bev[P.bev_used], P.stream));
-  kern<<<grid, block, smem, P.stream>>>(static_cast<KArgs>(args)...);
+  if (P.pdl && P.capturing) {  // only on the library's own capture streams
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = P.stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+  } else {
+    kern<<<grid, block, smem, P.stream>>>(static_cast<KArgs>(args)...);
+  }
   ++P.nlaunch;
   KCHECK();
   if (rec) {
@@ -824,6 +846,7 @@ static void springs_apply(Prob& P, const TX* x, TO* out, double sign, double* do
 template <typename TB, typename TD, typename TO>
 __global__ void k_jacobi0(long long n, const TB* __restrict__ b, const TD* __restrict__ dinv, TO* __restrict__ x,
                           const double* omega, double wscale) {
+  EDGE_PDL_ENTRY();
   const double w = (*omega) * wscale;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     using Tc = TO;
@@ -833,15 +856,18 @@ __global__ void k_jacobi0(long long n, const TB* __restrict__ b, const TD* __res
 }
 template <typename TA, typename TB, typename TO>
 __global__ void k_add(long long n, const TA* __restrict__ a, const TB* __restrict__ b, TO* __restrict__ o) {
+  EDGE_PDL_ENTRY();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     o[i] = Conv<TO>::from((double)Conv<double>::from(a[i]) + (double)Conv<double>::from(b[i]));
 }
 template <typename TI, typename TO>
 __global__ void k_copy(long long n, const TI* __restrict__ a, TO* __restrict__ o) {
+  EDGE_PDL_ENTRY();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     o[i] = Conv<TO>::from(a[i]);
 }
 __global__ void k_pcg_init(PcgState* st, double tol, int maxiter, double min_omega, double d_omega) {
+  EDGE_PDL_ENTRY();
   st->tol = tol;
   st->maxiter = maxiter;
   st->min_omega = min_omega;
@@ -855,6 +881,7 @@ __global__ void k_pcg_init(PcgState* st, double tol, int maxiter, double min_ome
   st->n_true = 0;
 }
 __global__ void k_pcg_check_bb(PcgState* st, const int* chol_status) {
+  EDGE_PDL_ENTRY();
   // ||f|| == 0: nothing to solve, report residual 0 like a converged solve
   if (st->bb == 0.0) {
     st->done = 1;
@@ -942,7 +969,8 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
   const long long nv = (long long)g.dof * g.n;
   if (l == P.n_level) {
     CatScope cat(P, CAT_COARSE);
-    launch(P, k_coarse_solve<T, T>, cdiv((long long)P.nd * 32, 256), 256, 0, g, P.Ainv, P.nd, b, out);
+    launch(P, k_coarse_solve<T, T>, cdiv((long long)P.nd * 32, 256), 256, (size_t)P.nd * sizeof(T), g, P.Ainv, P.nd,
+           b, out);
     KCHECK();
     return;
   }
@@ -998,7 +1026,7 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     T* e2 = (T*)Lv.eb;
     P.cur_cat = CAT_TRANSFER;
     if (P.dim == 3)
-      launch(P, k_prolong3<T, T>, dim3(cdiv((long long)g.nz * g.nx, 256), g.ny), 256, 0, g, Lc.g,
+      launch(P, k_prolong3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g,
              (const T*)Lc.res, e1);
     else
       launch(P, k_prolong2<T, T>, dim3(cdiv(g.nx, 64), g.ny), 64, 0, g, Lc.g, (const T*)Lc.res, e1);
@@ -1069,6 +1097,12 @@ static void mg_allocate(Prob& P) {
   const Geo& gL = P.lv[L].g;
   P.nd = gL.nx * gL.ny * gL.nz * gL.dof;
   if (P.nd > 8192) fail(EDGE_EINVAL, "coarsest level has " + std::to_string(P.nd) + " DOFs; use more levels (<= 8192)");
+  // k_coarse_solve stages b in shared memory: up to 64 KB for 8192 FP64 values (one constant
+  // limit for every problem, so concurrent set-ups do not race on it)
+  CK(cudaFuncSetAttribute(k_coarse_solve<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          8192 * (int)sizeof(double)));
+  CK(cudaFuncSetAttribute(k_coarse_solve<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          8192 * (int)sizeof(double)));
   P.Adense = P.alloc<double>((size_t)P.nd * P.nd);
   P.Ainv = P.alloc<double>((size_t)P.nd * P.nd);
   P.Ut = P.alloc<double>((size_t)P.nd * P.nd);
@@ -1207,8 +1241,11 @@ static void pcgmx_body(Prob& P) {
     fine_apply<float>(P, (const float*)p, e, &P.st->pq);
     springs_apply(P, (const float*)p, q, 1.0, &P.st->pq);
   }
-  launch(P, k_pcg_xr_lag, nb, 256, 0, nv, P.x32, (const float*)p, P.r64, (const float*)q, P.st, P.part, P.ticket,
-         P.r32);
+  if (P.res32)  // x32 += alpha p, r32 -= alpha q in FP32
+    launch(P, k_pcg_xr32, nb, 256, 0, nv, P.x32, (const float*)p, P.r32, (const float*)q, P.st, P.part, P.ticket);
+  else
+    launch(P, k_pcg_xr_lag, nb, 256, 0, nv, P.x32, (const float*)p, P.r64, (const float*)q, P.st, P.part, P.ticket,
+           P.r32);
 }
 // x64 += x32 (the FP32 increment of the solution since the last replacement), x32 = 0
 static void pcgmx_fold(Prob& P) {
@@ -1281,7 +1318,8 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, boo
   std::vector<double> k = {cg ? -1.0 : (double)P.prec, tol, (double)maxiter, (double)P.n_level, (double)P.n_smooth, P.omega,
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons,
-                           (double)P.st_bf16, (double)P.st_pair, (double)P.st_pair_min};
+                           (double)P.st_bf16, (double)P.st_pair, (double)P.st_pair_min, (double)P.res32,
+                           (double)P.pdl};
   for (int l : P.w_levels) k.push_back((double)l);
   k.push_back(-1.0);
   for (int v : P.level_sweeps) k.push_back((double)v);
@@ -1310,6 +1348,7 @@ static void capture_solve(Prob& P, double tol, int maxiter, bool cg = false) {
   int depth = 0;  // captures open
   try {
     P.stream = P.cap[0];
+    P.capturing = true;
     CK(cudaStreamBeginCapture(P.cap[0], cudaStreamCaptureModeThreadLocal));
     depth = 1;
     if (cg)
@@ -1383,8 +1422,10 @@ static void capture_solve(Prob& P, double tol, int maxiter, bool cg = false) {
     if (mixed) pcgmx_fold(P);
     CK(cudaStreamEndCapture(P.cap[0], &P.sg_graph));
     depth = 0;
+    P.capturing = false;
     CK(cudaGraphInstantiate(&P.sg_exec, P.sg_graph, 0));
   } catch (...) {
+    P.capturing = false;
     for (int d = depth; d >= 1; --d) {
       cudaGraph_t junk = nullptr;
       cudaStreamEndCapture(P.cap[d - 1], &junk);
@@ -1507,6 +1548,7 @@ static OcStaticScratch* oc_static_scratch() {
 
 // Start state of one OC update: bracket [1e-9, 1e9] (TopOpt/_cuda.py:260-261), counter zero.
 __global__ void k_oc_static_init(OcStaticScratch* s, double vf, double vol) {
+  EDGE_PDL_ENTRY();
   OcState init{};
   init.l1 = 1e-9;
   init.l2 = 1e9;
@@ -1688,6 +1730,20 @@ int edge_set_coarse_bf16(edge_problem* p, int enable) {
   API_BEGIN
   if (!p) fail(EDGE_EINVAL, "null handle");
   p->P.st_bf16 = enable != 0;
+  API_END
+}
+
+int edge_set_pdl(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.pdl = enable != 0;
+  API_END
+}
+
+int edge_set_residual32(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.res32 = enable != 0;
   API_END
 }
 
@@ -2252,7 +2308,7 @@ static void transfer(int dim, const int* nel, const double* in_dev, double* out_
     CK(cudaMemsetAsync(vc, 0, (size_t)gc.dof * gc.n * sizeof(double), s));
     k_user_to_slots<double><<<cdiv(gc.n, 256), 256, 0, s>>>(gc, in_dev, vc);
     if (dim == 3)
-      k_prolong3<double, double><<<dim3(cdiv((long long)gf.nz * gf.nx, 256), gf.ny), 256, 0, s>>>(gf, gc, vc, vf);
+      k_prolong3<double, double><<<dim3(cdiv((long long)gc.nz * gc.nx, 256), gc.ny), 256, 0, s>>>(gf, gc, vc, vf);
     else
       k_prolong2<double, double><<<dim3(cdiv(gf.nx, 64), gf.ny), 64, 0, s>>>(gf, gc, vc, vf);
     k_slots_to_user<double><<<cdiv(gf.n, 256), 256, 0, s>>>(gf, vf, out_dev);

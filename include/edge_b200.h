@@ -117,8 +117,20 @@ int edge_set_graph(edge_problem* p, int enable);
 int edge_set_stencil_pair(edge_problem* p, long long min_slots);
 /* Mixed precision only: enable != 0 applies the coarse-level stencils (levels >= 1, below the
  * coarsest) from BF16 copies made after each Galerkin set-up (half the bytes of the largest
- * coarse kernel); the Jacobi diagonals and the Galerkin chain stay FP32.  Default 0. */
+ * coarse kernel); the Jacobi diagonals and the Galerkin chain stay FP32.  Default 1 (at 12.8M
+ * DOF: the same PCG iteration counts as FP32 stencils, 3 % more SIMP iterations/s). */
 int edge_set_coarse_bf16(edge_problem* p, int enable);
+/* Mixed precision only: enable != 0 (default) stores the PCG residual recurrence in FP32
+ * between the FP64 true-residual replacements (each replacement recomputes r = b - A x in FP64
+ * after the recurrence has dropped 100-fold, and before convergence is declared; the update
+ * itself and r.r are computed in FP64).  0: FP64 recurrence plus an FP32 copy for the V-cycle. */
+int edge_set_residual32(edge_problem* p, int enable);
+/* enable != 0: the kernels of the captured solve graph are launched with programmatic stream
+ * serialization (programmatic dependent launch), so that each kernel's blocks can be
+ * scheduled while the previous kernel drains; every kernel waits for its predecessor on
+ * entry.  0 (default): plain stream order (at 12.8M DOF the SIMP loop ran 1.5 % faster so).
+ * Host-driven solves always use plain order. */
+int edge_set_pdl(edge_problem* p, int enable);
 /* Coarse 3-D levels with at most max_slots slots use the four-lanes-per-node stencil kernel
  * (latency-bound small levels); larger levels one thread per node.  Default 40000 (at 70k
  * slots one thread per node is already faster). */

@@ -347,6 +347,7 @@ def test_stencil_kernels_agree_in_solve(precision):
     s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision=precision, autotune=False,
                        tune_sweeps=False)
     res = []
+    _lib.call("edge_set_coarse_bf16", k.handle, 0)  # FP32 stencils first
     for qmax, pair in ((0, -1), (1 << 40, -1), (0, 0)):
         _lib.call("edge_set_stencil_quad", k.handle, qmax)
         _lib.call("edge_set_stencil_pair", k.handle, pair)
@@ -356,16 +357,29 @@ def test_stencil_kernels_agree_in_solve(precision):
     for x1, it1, r1 in res[1:]:
         assert abs(it0 - it1) <= (0 if precision == "fp64" else 1) and r0 < 1e-8 and r1 < 1e-8
         assert rel(x1, x0) < (1e-12 if precision == "fp64" else 1e-7)
+    if precision == "mixed":
+        # BF16 stencil copies: one node per thread and two nodes per thread (4-byte pair loads)
+        _lib.call("edge_set_coarse_bf16", k.handle, 1)
+        bf = []
+        for pair in (-1, 0):
+            _lib.call("edge_set_stencil_quad", k.handle, 0)
+            _lib.call("edge_set_stencil_pair", k.handle, pair)
+            x, r = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
+            bf.append((x.cpu().numpy().copy(), s.last_iters, r))
+        (xa, ia, ra), (xb, ib, rb) = bf
+        assert abs(ia - ib) <= 1 and abs(ia - it0) <= 3 and ra < 1e-8 and rb < 1e-8
+        assert rel(xb, xa) < 1e-7 and rel(xa, x0) < 1e-6
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_graph_and_host_loop_agree(precision):
     """One CUDA-graph solve (while node over the PCG iteration, if node for the residual
     replacement) and the host-driven loop run the same launches: same iteration count and
-    true-residual count, solutions equal to rounding; a second graph solve with a changed
-    tolerance captures again."""
+    true-residual count, solutions equal to rounding; so does the graph with programmatic
+    dependent launch; a second graph solve with a changed tolerance captures again."""
     import torch
     import edge_to_b200 as eb
+    from edge_to_b200 import _lib
     p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
                                                                        variant="gpu"))
     rng = np.random.default_rng(5)
@@ -384,9 +398,42 @@ def test_graph_and_host_loop_agree(precision):
     (x0, it0, t0, r0), (x1, it1, t1, r1) = out[False], out[True]
     assert it0 == it1 and t0 == t1 and r0 < 1e-8 and r1 < 1e-8
     assert rel(x1, x0) < 1e-12
+    # the graph with programmatic dependent launch: the same launches, overlapped
+    _lib.call("edge_set_pdl", k.handle, 1)
+    x3, r3 = s.solve(f, use_last=False)
+    assert s.last_iters == it1 and rel(x3.cpu().numpy(), x1) < 1e-12
+    _lib.call("edge_set_pdl", k.handle, 0)
     s.tol = 1e-6
     x2, r2 = s.solve(f, use_last=False)
     assert r2 < 1e-6 and s.last_iters < it1
+
+
+def test_residual_recurrence_precisions_agree():
+    """Mixed precision with the residual recurrence stored in FP32 (default) and in FP64: both
+    meet the tolerance on the FP64 true residual, take about the same iterations and give the
+    same solution to the tolerance."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(9)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    mesh = _mesh(3, (32, 16, 16), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision="mixed", autotune=False,
+                       tune_sweeps=False)
+    f = torch.as_tensor(p.f, device="cuda")
+    out = {}
+    for r32 in (1, 0):
+        _lib.call("edge_set_residual32", k.handle, r32)
+        x, r = s.solve(f, use_last=False)
+        out[r32] = (x.cpu().numpy().copy(), s.last_iters, r)
+    (x1, i1, r1), (x0, i0, r0) = out[1], out[0]
+    assert r1 < 1e-8 and r0 < 1e-8 and abs(i1 - i0) <= 3
+    assert rel(x1, x0) < 1e-6
 
 
 def test_sweep_autotuner_mixed():
