@@ -2,7 +2,8 @@
 
 Drop-in names (EDGETO/__init__.py, TopOpt/__init__.py, solvers/__init__.py,
 kernels/__init__.py, geom/__init__.py): CuStructuredMesh2D/3D, CuStructuredStiffnessKernel,
-CuStructuredFilter2D/3D, CuMultiGrid, CuCG, CuTopOpt, SingleMaterial, auto_stiffness; beyond the
+CuStructuredFilter2D/3D, CuMultiGrid, CuCG, CuTopOpt, SingleMaterial, PenalizedMultiMaterial,
+auto_stiffness; beyond the
 reference, SIMPObjective (differentiable compliance / mechanism objectives, autograd.py).
 Arrays are torch CUDA tensors; the compute runs in libedge_b200.so (sm_100a).
 """
@@ -10,7 +11,7 @@ from . import autograd
 from .autograd import SIMPObjective
 from .filters import CuStructuredFilter2D, CuStructuredFilter3D, FilterKernel
 from .kernels import CuStructuredStiffnessKernel, StiffnessKernel
-from .material import MaterialModel, SingleMaterial
+from .material import MaterialModel, PenalizedMultiMaterial, SingleMaterial
 from .mesh import CuStructuredMesh2D, CuStructuredMesh3D, StructuredMesh
 from .physics import auto_stiffness, hexahedron_element_stiffness, quadrilateral_element_stiffness
 from .solvers import CuMultiGrid, CuCG
@@ -19,6 +20,6 @@ from .topopt import CuTopOpt
 __all__ = [
     "CuStructuredMesh2D", "CuStructuredMesh3D", "StructuredMesh", "CuStructuredStiffnessKernel", "StiffnessKernel",
     "CuStructuredFilter2D", "CuStructuredFilter3D", "FilterKernel", "CuMultiGrid", "CuCG", "CuTopOpt", "SingleMaterial",
-    "MaterialModel", "auto_stiffness", "hexahedron_element_stiffness", "quadrilateral_element_stiffness",
+    "PenalizedMultiMaterial", "MaterialModel", "auto_stiffness", "hexahedron_element_stiffness", "quadrilateral_element_stiffness",
     "SIMPObjective",
 ]

@@ -863,4 +863,57 @@ __global__ void k_oc_final(long long n, const double* __restrict__ rho, const do
   grid_reduce_finish(bt, part, ticket, DotSink{chg_dst});
 }
 
+// Multi-material SIMP law (PenalizedMultiMaterial, MaterialModels.py:102-205).  rho is the
+// n_el x n_mat row-major design of the reference.  With c_m = clip(rho_m, void, 1),
+// a_m = c_m^p and b_m = 1 - a_m:
+//   E = max(void, sum_m E_m a_m prod_{k != m} b_k)
+//   dE/drho_j = p c_j^(p-1) (E_j prod_{k != j} b_k - sum_{m != j} E_m a_m prod_{k != m, j} b_k)
+// (the derivative of the sum before its clip, as the reference's backward), and with
+// plain != 0: E = clip(sum_m E_m rho_m, void, 1).  One thread per element.
+constexpr int MM_MAX = 8;
+struct MMat {
+  double e[MM_MAX];
+};
+__global__ void k_mm_law(long long n_el, int n_mat, const double* __restrict__ rho, MMat Em, double vd, double pen,
+                         int plain, double* __restrict__ E, double* __restrict__ dE) {
+  EDGE_PDL_ENTRY();
+  for (long long el = blockIdx.x * (long long)blockDim.x + threadIdx.x; el < n_el;
+       el += (long long)gridDim.x * blockDim.x) {
+    const double* r = rho + el * n_mat;
+    if (plain) {
+      double s = 0.0;
+      for (int m = 0; m < n_mat; ++m) s += r[m] * Em.e[m];
+      E[el] = fmin(fmax(s, vd), 1.0);
+      continue;
+    }
+    double c[MM_MAX], a[MM_MAX], b[MM_MAX];
+    for (int m = 0; m < n_mat; ++m) {
+      c[m] = fmin(fmax(r[m], vd), 1.0);
+      a[m] = pow(c[m], pen);
+      b[m] = 1.0 - a[m];
+    }
+    double s = 0.0;
+    for (int m = 0; m < n_mat; ++m) {
+      double t = a[m];
+      for (int k = 0; k < n_mat; ++k)
+        if (k != m) t *= b[k];
+      s += t * Em.e[m];
+    }
+    E[el] = fmax(s, vd);
+    if (dE) {
+      for (int j = 0; j < n_mat; ++j) {
+        const double dj = pen * pow(c[j], pen - 1.0);
+        double g = 0.0;
+        for (int i = 0; i < n_mat; ++i) {
+          double t = 1.0;
+          for (int k = 0; k < n_mat; ++k)
+            if (k != j) t *= (k == i) ? a[k] : b[k];
+          g += (i == j ? dj : -dj) * t * Em.e[i];
+        }
+        dE[el * n_mat + j] = g;
+      }
+    }
+  }
+}
+
 }  // namespace edge

@@ -2318,6 +2318,22 @@ static void transfer(int dim, const int* nel, const double* in_dev, double* out_
   CK(cudaFreeAsync(vc, s));
 }
 
+int edge_mm_law(long long n_el, int n_mat, const double* rho_dev, const double* E_mat, double void_, double penalty,
+                int plain, double* E_dev, double* dE_dev, void* stream) {
+  API_BEGIN
+  if (!rho_dev || !E_mat || !E_dev) fail(EDGE_EINVAL, "null argument");
+  if (n_el < 0 || n_mat < 1 || n_mat > MM_MAX)
+    fail(EDGE_EINVAL, "n_mat must be in 1.." + std::to_string(MM_MAX) + " and n_el >= 0");
+  if (!std::isfinite(penalty) || !std::isfinite(void_)) fail(EDGE_EINVAL, "penalty and void must be finite");
+  if (n_el == 0) return EDGE_OK;
+  MMat em{};
+  for (int m = 0; m < n_mat; ++m) em.e[m] = E_mat[m];
+  k_mm_law<<<std::min<unsigned>(cdiv(n_el, 256), 148u * 16u), 256, 0, (cudaStream_t)stream>>>(
+      n_el, n_mat, rho_dev, em, void_, penalty, plain, E_dev, dE_dev);
+  KCHECK();
+  API_END
+}
+
 int edge_restrict(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream) {
   API_BEGIN
   if (!nel || !in_dev || !out_dev) fail(EDGE_EINVAL, "null argument");

@@ -116,7 +116,14 @@ class CuTopOpt:
         self.f.copy_(torch.from_numpy(f))
 
     # ----------------------------------------------------------------- OC (TopOpt/_cuda.py:242-280)
+    @property
+    def n_sets(self):
+        """Design columns per element (1, or the number of materials of a multi-material law)."""
+        return int(self.material_model.base_properties()["n_sets"])
+
     def update_design(self, rho, df):
+        if self.n_sets > 1:
+            return self._update_design_generic(_as_dev_f64(rho), _as_dev_f64(df))
         rho = _as_dev_f64(rho).reshape(-1)
         df = _as_dev_f64(df).reshape(-1)
         if isinstance(self.material_model, SingleMaterial) and isinstance(self.kernel, CuStructuredStiffnessKernel):
@@ -132,14 +139,17 @@ class CuTopOpt:
         return self._update_design_generic(rho, df)
 
     def _update_design_generic(self, rho, df):
-        rho = rho.reshape(-1, 1)
-        df = df.reshape(-1, 1)
+        """OC with one bisection multiplier per design column (TopOpt/_cuda.py:242-280): every
+        column keeps bisecting until its own (l2 - l1) / (l2 + l1) <= 1e-4, on the material
+        model's ocP and constraint test.  Multi-material designs are (n_el, n_sets)."""
+        size = self.n_sets
+        rho = rho.reshape(-1, size)
+        df = df.reshape(-1, size)
         xU = torch.clamp(rho + self.move, 0.0, 1.0)
         xL = torch.clamp(rho - self.move, 0.0, 1.0)
         As = torch.as_tensor(np.asarray(self.mesh.As), dtype=torch.float64, device="cuda")
         ocP = self.material_model.ocP(df, As, rho)
         ocP = torch.clamp(ocP, min=1e-12)
-        size = self.material_model.base_properties()["n_sets"]
         l1 = 1e-9 * torch.ones(size, dtype=torch.float64, device="cuda")
         l2 = 1e9 * torch.ones(size, dtype=torch.float64, device="cuda")
         lmid = 0.5 * (l1 + l2)
@@ -151,7 +161,7 @@ class CuTopOpt:
             valids = self.material_model.evaluate_constraint(rho_new, As, float(self.mesh.volume))
             l2 = torch.where(valids, lmid, l2)
             l1 = torch.where(~valids, lmid, l1)
-        return rho_new.reshape(-1)
+        return rho_new.reshape(-1) if size == 1 else rho_new
 
     # ----------------------------------------------------------------- analysis (TopOpt/_cuda.py:282-302)
     def FEA_integrals(self, rho):
@@ -175,6 +185,8 @@ class CuTopOpt:
         return strain, stress, strain_energy, von_mises
 
     def solve_and_process(self, rho, iteration):
+        if self.n_sets > 1:
+            return self._solve_and_process_sets(_as_dev_f64(rho), iteration)
         rho = _as_dev_f64(rho).reshape(-1)
         if self.fused:
             return self._solve_and_process_fused(rho, iteration)
@@ -188,6 +200,25 @@ class CuTopOpt:
         dr = dr.reshape(dr.shape[0], -1)
         for i in range(dr.shape[1]):
             dr[:, i] = self.filter_kernel._rmatvec(dr[:, i].contiguous())
+        return compliance, dr, residual
+
+    def _solve_and_process_sets(self, rho, iteration):
+        """solve_and_process for an (n_el, n_sets) design (the reference's call order,
+        TopOpt/_cuda.py:282-302): each column filtered, the material law maps the filtered
+        columns to one E per element, one solve, dr = dE/drho_f * dk per column, each column
+        filtered back with the transpose."""
+        n = self.n_sets
+        rho = rho.reshape(-1, n)
+        rho_ = torch.stack([self.filter_kernel.dot(rho[:, m].contiguous()) for m in range(n)], dim=1)
+        E = self.material_model(rho_, iteration)
+        self.kernel.set_rho(_as_dev_f64(E).reshape(-1))
+        U, residual = self.solver.solve(self.f, use_last=self.reuse_sol)
+        compliance = torch.dot(self.f, U)
+        df = self.kernel.process_grad(U).reshape(-1, 1)
+        dr = _as_dev_f64(self.material_model.grad(rho_, iteration)).reshape(-1, n) * df
+        for m in range(n):
+            dr[:, m] = self.filter_kernel._rmatvec(dr[:, m].contiguous())
+        self._U = U
         return compliance, dr, residual
 
     def _solve_and_process_fused(self, rho, iteration):
@@ -225,11 +256,14 @@ class CuTopOpt:
     def optimize(self, save_comp_history=False, save_change_history=False, save_rho_history=False, rho_init=None,
                  callback=None):
         flag = False
+        n = self.n_sets
         if rho_init is None:
             rho = self.material_model.init_desvars(self.kernel.n_elements)
+        elif n > 1:  # a multi-material start design is taken as given, clipped to [0, 1]
+            rho = torch.clamp(_as_dev_f64(rho_init), 0.0, 1.0)
         else:
             rho = self.material_model(_as_dev_f64(rho_init).reshape(-1), 0, plain=True)
-        rho = _as_dev_f64(rho).reshape(-1)
+        rho = _as_dev_f64(rho).reshape(-1) if n == 1 else _as_dev_f64(rho).reshape(-1, n)
         comp, df, res = self.solve_and_process(rho, 0)
         prog = trange(self.max_iter, disable=logger.getEffectiveLevel() > logging.INFO)
         comp_history, change_history, rho_history = [], [], []

@@ -160,6 +160,15 @@ int edge_mg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_l
 int edge_mg_setup(edge_problem* p);
 int edge_mg_level_dense(edge_problem* p, int level, double* out_dev, long long n);
 
+/* ---- multi-material SIMP law.  Replaces PenalizedMultiMaterial.__forward__ / __backward__
+ * (MaterialModels.py:146-205): rho_dev is the n_el x n_mat row-major design (filtered),
+ * E_mat the n_mat Young's moduli (host array), 1 <= n_mat <= 8.  E_dev (n_el) receives
+ * max(void, sum_m E_m a_m prod_{k!=m} (1 - a_k)), a_m = clip(rho_m, void, 1)^penalty, or with
+ * plain != 0 clip(sum_m E_m rho_m, void, 1); dE_dev (n_el x n_mat, may be NULL; ignored when
+ * plain) receives dE/drho.  Asynchronous on stream. */
+int edge_mm_law(long long n_el, int n_mat, const double* rho_dev, const double* E_mat, double void_, double penalty,
+                int plain, double* E_dev, double* dE_dev, void* stream);
+
 /* ---- grid transfers.  Replace apply_restriction_cuda / apply_prolongation_cuda
  * (core/_mgm_cuda.py:223-314); nel is the FINE grid. */
 int edge_restrict(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream);

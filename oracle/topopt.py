@@ -112,9 +112,67 @@ class SIMPOracle:
         return rho, hist
 
 
-def mbb_problem(nelx=120, nely=40, **kw):
-    """2-D MBB half-beam: left edge u_x = 0, bottom-right node u_y = 0, F = (0,-1) at top-left."""
-    p = SIMPOracle((nelx, nely), **kw)
+def oc_update_sets(rho, dr, A, vol, law, move):
+    """OC of TopOpt/_solver.py:271-311 on an (n_el, n_sets) design, one bisection
+    multiplier per column, each stopping at (l2 - l1) / (l2 + l1) <= 1e-4; ocP and the
+    constraint test from the multi-material law (MaterialModels.py:207-228)."""
+    n = rho.shape[1]
+    A = np.asarray(A, dtype=np.float64).reshape(-1)
+    xU = np.clip(rho + move, 0.0, 1.0)
+    xL = np.clip(rho - move, 0.0, 1.0)
+    ocP = np.maximum(1e-12, law.ocp(dr, A, rho))
+    l1 = 1e-9 * np.ones(n)
+    l2 = 1e9 * np.ones(n)
+    lmid = 0.5 * (l1 + l2)
+    rho_new = np.maximum(0, np.maximum(xL, np.minimum(1.0, np.minimum(xU, ocP / lmid))))
+    while np.any((l2 - l1) / (l2 + l1) > 1e-4):
+        lmid = 0.5 * (l1 + l2)
+        rho_new = np.maximum(0, np.maximum(xL, np.minimum(1.0, np.minimum(xU, ocP / lmid))))
+        valid = law.con(rho_new, A, vol)
+        l2[valid] = lmid[valid]
+        l1[~valid] = lmid[~valid]
+    return rho_new
+
+
+class MultiMaterialSIMPOracle(SIMPOracle):
+    """SIMP with a multi-material law (oracle.material.MultiMaterialLaw) on an (n_el, n_sets)
+    design: every column filtered, E from the law, one exact sparse solve, dr = dE/drho_f dk
+    per column filtered back, OC per column (oc_update_sets)."""
+
+    def __init__(self, nel, law, **kw):
+        super().__init__(nel, void=law.void, penalty=law.penalty, **kw)
+        self.law = law
+
+    def solve_and_process(self, rho):
+        import scipy.sparse.linalg as spla
+        n = self.law.n
+        rho_f = np.stack([ops.filter_apply(self.H, rho[:, m]) for m in range(n)], axis=1)
+        E = self.law.forward(rho_f)
+        K = ops.assemble(self.grid, self.K0, E, self.cons)
+        U = spla.spsolve(K.tocsc(), self.f)
+        comp = float(self.f @ U)
+        dk = ops.dk(self.grid, self.K0, U)
+        dr = self.law.backward(rho_f) * dk.reshape(-1, 1)
+        dr = np.stack([ops.filter_apply_T(self.H, dr[:, m]) for m in range(n)], axis=1)
+        return comp, dr, 0.0, U
+
+    def optimize(self, rho0, n_iter):
+        rho = np.array(rho0, dtype=float).reshape(self.grid.n_el, self.law.n)
+        comp, dr, _, U = self.solve_and_process(rho)
+        hist = {"comp": [], "rho": [], "comp0": comp}
+        for _ in range(n_iter):
+            rho = oc_update_sets(rho, dr, np.array([self.A]), self.vol, self.law, self.move)
+            comp, dr, _, U = self.solve_and_process(rho)
+            hist["comp"].append(comp)
+            hist["rho"].append(rho.copy())
+        self.U = U
+        return rho, hist
+
+
+def mbb_problem(nelx=120, nely=40, law=None, **kw):
+    """2-D MBB half-beam: left edge u_x = 0, bottom-right node u_y = 0, F = (0,-1) at top-left
+    (with a multi-material law: MultiMaterialSIMPOracle)."""
+    p = SIMPOracle((nelx, nely), **kw) if law is None else MultiMaterialSIMPOracle((nelx, nely), law, **kw)
     g = p.grid
     left = np.array([g.node_id(0, j) for j in range(nely + 1)])
     p.add_bc_nodal(left, [[True, False]])

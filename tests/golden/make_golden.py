@@ -23,6 +23,8 @@ Outputs (all small .npz files, committed):
   loop_mbb2d.npz      120x40 MBB half-beam, 100 SIMP iterations, MG-PCG rtol 1e-8
   loop_cant3d.npz     64x32x32 cantilever, first SIMP iterations, 4-level MG rtol 1e-6
   grad_cant3d.npz     32x16x16 cantilever, random rho, compliance and filtered dr
+  fea.npz             FEA_integrals, op level and the whole call
+  multimaterial.npz   PenalizedMultiMaterial law: forward, plain, backward, constraint, ocP
 """
 import argparse
 import os
@@ -351,6 +353,52 @@ def make_fea():
     print("fea: energy sum", float(np.sum(energy)))
 
 
+def make_multimaterial():
+    """PenalizedMultiMaterial (MaterialModels.py:102-235) run on random designs: forward
+    (penalised and plain), backward, the mass constraint and ocP, for two and three
+    materials with per-material masses and for two materials with a shared mass over
+    rho_mat.  The reference's TopOpt loop cannot run this class (its update_design reshapes
+    the design to one column, TopOpt/_solver.py:281), so only the law is pinned here."""
+    from EDGETO.MaterialModels import PenalizedMultiMaterial
+    out = {}
+    rng = np.random.default_rng(21)
+    cases = {
+        "two": dict(n_material=2, mass=np.array([[0.25], [0.25]]), E_mat=np.array([[1.0], [0.5]]), rho_mat=None,
+                    void=1e-6, penalty=3.0),
+        "three": dict(n_material=3, mass=np.array([[0.2], [0.15], [0.1]]), E_mat=np.array([[1.0], [0.6], [0.3]]),
+                      rho_mat=None, void=1e-6, penalty=3.0),
+        "shared": dict(n_material=2, mass=np.array([[0.3]]), E_mat=np.array([[1.0], [0.4]]),
+                       rho_mat=np.array([[1.0], [0.35]]), void=1e-9, penalty=2.5),
+    }
+    nel = 64
+    for tag, kw in cases.items():
+        m = PenalizedMultiMaterial(**kw)
+        n = kw["n_material"]
+        rho = rng.uniform(0.0, 1.0, (nel, n))
+        rho[0, :] = 0.0  # clip edges
+        rho[1, :] = 1.0
+        rho[2, 0] = 1.0
+        E = m(rho, 0)
+        Ep = m(rho, 0, plain=True)
+        dE = m.grad(rho, 0)
+        dg = rng.uniform(0.5, 1.5, nel)
+        vol = float(dg.sum())
+        cons = np.stack([m.evaluate_constraint(rho * s, dg, vol) for s in (0.1, 0.5, 1.0)])
+        df = -rng.uniform(0.0, 2.0, (nel, n))
+        df[3, :] = 0.5  # positive sensitivities: NaN -> 0 in ocP
+        ocP = m.ocP(df, dg, rho)
+        ocP0 = m.ocP(np.abs(df), dg, rho)  # all positive: the 1e-3 fallback
+        out.update({f"{tag}_rho": rho, f"{tag}_E": np.asarray(E).reshape(-1), f"{tag}_Eplain": np.asarray(Ep).reshape(-1),
+                    f"{tag}_dE": np.asarray(dE).reshape(nel, n), f"{tag}_dg": dg, f"{tag}_vol": np.array(vol),
+                    f"{tag}_cons": cons, f"{tag}_df": df, f"{tag}_ocP": ocP, f"{tag}_ocP0": ocP0,
+                    f"{tag}_n": np.array(n), f"{tag}_E_mat": kw["E_mat"].reshape(-1),
+                    f"{tag}_mass": kw["mass"].reshape(-1), f"{tag}_void": np.array(kw["void"]),
+                    f"{tag}_penalty": np.array(kw["penalty"]),
+                    f"{tag}_rho_mat": (kw["rho_mat"].reshape(-1) if kw["rho_mat"] is not None else np.zeros(0))})
+    np.savez_compressed(os.path.join(HERE, "multimaterial.npz"), **out)
+    print("multimaterial: E sums", {t: float(out[f"{t}_E"].sum()) for t in cases})
+
+
 _REF = None
 
 if __name__ == "__main__":
@@ -359,7 +407,7 @@ if __name__ == "__main__":
     args = ap.parse_args()
     _REF = _import_reference()
     jobs = {"kat": make_kat, "ops": make_ops, "mbb": make_loop_mbb, "cant": make_loop_cant3d, "grad": make_grad,
-            "fea": make_fea}
+            "fea": make_fea, "mm": make_multimaterial}
     for name, fn in jobs.items():
         if args.only and name not in args.only.split(","):
             continue
