@@ -1,11 +1,12 @@
-"""Element physics for the structured meshes: Q4 (plane stress / plane strain) and hex8.
+"""Element physics: T3, Q4 (plane stress / plane strain), Tet4 and hex8.
 
 Host-side (numpy) set-up code with the reference's signatures
-(physics/_linelas.py:179-547): ``quadrilateral_element_stiffness``,
+(physics/_linelas.py:1-547): ``triangle_element_stiffness``,
+``tetrahedron_element_stiffness``, ``quadrilateral_element_stiffness``,
 ``hexahedron_element_stiffness``, their area/volume helpers and ``auto_stiffness``.
-Isoparametric elements with full 2x2(x2) Gauss integration; the returned B is the
-Gauss-point average, as in the reference.  Only Q4 / hex8 are provided: triangles and
-tetrahedra belong to the unstructured meshes, which this package does not cover.
+Q4 / hex8 are isoparametric with full 2x2(x2) Gauss integration and return the Gauss-point
+average of B, as in the reference; T3 / Tet4 are constant-strain simplices whose shape
+function gradients are read off the inverse of the coordinate matrix [1 x y (z)].
 """
 import numpy as np
 
@@ -54,6 +55,61 @@ def _iso_D(E, nu):
     D[0, 0] = D[1, 1] = D[2, 2] = 1 - nu
     D[3, 3] = D[4, 4] = D[5, 5] = (1 - 2 * nu) / 2
     return c * D
+
+
+def triangle_element_area(x0s):
+    return _tri_signed_area(np.asarray(x0s, dtype=np.float64))
+
+
+def _simplex_gradients(x0s):
+    """Gradients of the linear shape functions of a simplex (rows: nodes, columns: x, y(, z)):
+    N_i(x) = [1, x] . inv(P)[:, i] with P = [1 | x0s]."""
+    P = np.concatenate([np.ones((x0s.shape[0], 1)), x0s], -1)
+    return np.linalg.inv(P)[1:].T
+
+
+def triangle_element_stiffness(x0s, E=1.0, NU=0.33, e_type=0, t=1.0):
+    """(K 6x6, D 3x3, B 3x6) of a constant-strain triangle (physics/_linelas.py:3-50)."""
+    x0s = np.asarray(x0s, dtype=np.float64)
+    A = _tri_signed_area(x0s)
+    if A < 0:
+        raise Exception("Node Order Is Not Correct")
+    g = _simplex_gradients(x0s)
+    B = np.zeros((3, 6))
+    B[0, 0::2] = g[:, 0]
+    B[1, 1::2] = g[:, 1]
+    B[2, 0::2] = g[:, 1]
+    B[2, 1::2] = g[:, 0]
+    D = _plane_D(E, NU, e_type)
+    return t * A * B.T @ D @ B, D, B
+
+
+def tetrahedron_element_stiffness(x0s, E=1.0, NU=0.33):
+    """(K 12x12, D 6x6, B 6x12) of a linear tetrahedron (physics/_linelas.py:70-176); strain
+    order xx, yy, zz, xy, yz, zx."""
+    x0s = np.asarray(x0s, dtype=np.float64)
+    V = tetrahedron_element_volume(x0s)
+    if V < 0:
+        raise Exception("Node Order Is Not Correct")
+    g = _simplex_gradients(x0s)
+    B = np.zeros((6, 12))
+    for d in range(3):
+        B[d, d::3] = g[:, d]
+    B[3, 0::3], B[3, 1::3] = g[:, 1], g[:, 0]
+    B[4, 1::3], B[4, 2::3] = g[:, 2], g[:, 1]
+    B[5, 0::3], B[5, 2::3] = g[:, 2], g[:, 0]
+    D = _iso_D(E, NU)
+    return V * B.T @ D @ B, D, B
+
+
+def _reordered(fn, x0s, order, dof, E, Nu):
+    """Element matrices of a clockwise (negatively oriented) element: computed on the nodes
+    in `order` and permuted back to the given node order."""
+    K, D, B = fn(x0s[order], E, Nu)
+    idx = (np.asarray(order)[:, None] * dof + np.arange(dof)[None, :]).reshape(-1)
+    inv = np.empty_like(idx)
+    inv[idx] = np.arange(idx.size)
+    return K[inv][:, inv], D, B[:, inv]
 
 
 def quadrilateral_element_stiffness(x0s, E=1.0, NU=0.33, e_type=0, t=1.0):
@@ -111,8 +167,26 @@ def hexahedron_element_stiffness(x0s, E=1.0, nu=0.33):
 
 
 def auto_stiffness(x0s, E, Nu):
-    """(K, D, B, area|volume) for a Q4 (4 nodes in 2-D) or hex8 element (physics/_linelas.py:477-547)."""
+    """(K, D, B, area|volume) of a T3, Tet4, Q4 or hex8 element chosen by its node count and
+    dimension (physics/_linelas.py:477-547).  A negatively oriented triangle or tetrahedron
+    is computed in the reversed (T3) or 0,1,3,2 (Tet4) node order and permuted back, with a
+    positive measure; Q4 and hex8 must be positively oriented (an Exception otherwise, as in
+    the reference, whose final call uses the given order)."""
     x0s = np.asarray(x0s, dtype=np.float64)
+    if x0s.shape[0] == 3:
+        A = _tri_signed_area(x0s)
+        if A < 0:
+            K, D, B = _reordered(triangle_element_stiffness, x0s, [2, 1, 0], 2, E, Nu)
+            return K, D, B, -A
+        K, D, B = triangle_element_stiffness(x0s, E, Nu)
+        return K, D, B, A
+    if x0s.shape[0] == 4 and x0s.shape[1] == 3:
+        V = tetrahedron_element_volume(x0s)
+        if V < 0:
+            K, D, B = _reordered(tetrahedron_element_stiffness, x0s, [0, 1, 3, 2], 3, E, Nu)
+            return K, D, B, -V
+        K, D, B = tetrahedron_element_stiffness(x0s, E, Nu)
+        return K, D, B, V
     if x0s.shape[0] == 4 and x0s.shape[1] == 2:
         A = quadrilateral_element_area(x0s)
         if A < 0:
@@ -125,4 +199,4 @@ def auto_stiffness(x0s, E, Nu):
             A = hexahedron_element_volume(x0s[[4, 5, 6, 7, 0, 1, 2, 3]])
         K, D, B = hexahedron_element_stiffness(x0s, E, Nu)
         return K, D, B, A
-    raise Exception("Element Type Not Supported (structured meshes use Q4 / hex8)")
+    raise Exception("Element Type Not Supported")

@@ -25,6 +25,8 @@ Outputs (all small .npz files, committed):
   grad_cant3d.npz     32x16x16 cantilever, random rho, compliance and filtered dr
   fea.npz             FEA_integrals, op level and the whole call
   multimaterial.npz   PenalizedMultiMaterial law: forward, plain, backward, constraint, ocP
+  general.npz         unstructured meshes (T3, T3+Q4, Tet4, distorted hex8): element
+                      matrices, matvec, diagonal, dk, KD-tree filter
 """
 import argparse
 import os
@@ -399,6 +401,99 @@ def make_multimaterial():
     print("multimaterial: E sums", {t: float(out[f"{t}_E"].sum()) for t in cases})
 
 
+def general_meshes(rng):
+    """Small unstructured meshes (nodes, elements) shared by the fixture script and the tests:
+    'tri' jittered triangles (uniform), 'mixed' triangles and quadrilaterals (general),
+    'tet' jittered tetrahedra with both orientations (uniform), 'hex' distorted hexahedra."""
+    out = {}
+    nx, ny = 6, 4
+    xs, ys = np.meshgrid(np.arange(nx + 1, dtype=float), np.arange(ny + 1, dtype=float), indexing="xy")
+    P = np.stack([xs.ravel(), ys.ravel()], 1)
+    interior = (P[:, 0] > 0) & (P[:, 0] < nx) & (P[:, 1] > 0) & (P[:, 1] < ny)
+    P[interior] += rng.uniform(-0.2, 0.2, (int(interior.sum()), 2))
+    nid = lambda i, j: j * (nx + 1) + i  # noqa: E731
+    tris, mixed = [], []
+    for j in range(ny):
+        for i in range(nx):
+            a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            tris += [[a, b, c], [a, c, d]]
+            if (i + j) % 2 == 0:
+                mixed.append([a, b, c, d])
+            else:
+                mixed += [[a, b, c], [a, c, d]]
+    out["tri"] = (P.copy(), np.array(tris, dtype=np.int64))
+    out["mixed"] = (P.copy(), mixed)
+    nx, ny, nz = 3, 2, 2
+    g = np.stack(np.meshgrid(np.arange(nx + 1.0), np.arange(ny + 1.0), np.arange(nz + 1.0), indexing="ij"), -1)
+    P3 = g.reshape(-1, 3).copy()
+    inner = (P3 > 0).all(1) & (P3 < [nx, ny, nz]).all(1)
+    P3[inner] += rng.uniform(-0.15, 0.15, (int(inner.sum()), 3))
+    nid3 = lambda i, j, k: (i * (ny + 1) + j) * (nz + 1) + k  # noqa: E731
+    tets, hexes = [], []
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                c = [nid3(i + a, j + b, k + e) for (a, b, e) in
+                     ((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1))]
+                hexes.append(c)
+                for t in ((0, 1, 3, 4), (1, 2, 3, 6), (1, 3, 4, 6), (1, 4, 5, 6), (3, 4, 6, 7)):
+                    tets.append([c[q] for q in t])
+    out["tet"] = (P3.copy(), np.array(tets, dtype=np.int64))
+    Ph = P3.copy()
+    out["hex"] = (Ph, np.array(hexes, dtype=np.int64))
+    return out
+
+
+def make_general():
+    """Unstructured meshes through the reference's CPU classes: GeneralMesh (geom/_mesh.py:
+    146-225), UniformStiffnessKernel / GeneralStiffnessKernel (kernels/_processors.py:157-395)
+    and GeneralFilter (geom/_filters.py:256-270): element matrices, areas, centroids, matvec
+    with and without constraints, diagonal, dk and the filter matrix."""
+    from EDGETO.geom._mesh import GeneralMesh
+    from EDGETO.kernels._processors import UniformStiffnessKernel, GeneralStiffnessKernel
+    from EDGETO.geom._filters import GeneralFilter
+    rng = np.random.default_rng(31)
+    out = {}
+    for tag, (P, els) in general_meshes(rng).items():
+        el_arg = np.array(els, dtype=object) if isinstance(els, list) else els
+        if isinstance(els, list):
+            el_arg = np.empty(len(els), dtype=object)
+            for i, e in enumerate(els):
+                el_arg[i] = list(e)
+        mesh = GeneralMesh(P, el_arg, stiffness=_stiff(0.3))
+        k = UniformStiffnessKernel(mesh) if mesh.is_uniform else GeneralStiffnessKernel(mesh)
+        n_el = len(els)
+        ndof = mesh.nodes.shape[0] * mesh.dof
+        rho = rng.uniform(0.1, 1.0, n_el)
+        u = rng.standard_normal(ndof)
+        k.set_rho(rho)
+        mv = np.array(k.dot(u), copy=True)
+        U = rng.standard_normal(ndof)
+        dk = np.array(k.process_grad(U), copy=True)
+        cons = np.unique(rng.choice(ndof, size=max(2, ndof // 8), replace=False))
+        k.set_constraints(cons)
+        mvc = np.array(k.dot(u), copy=True)
+        diag = np.array(k.diagonal(), copy=True)
+        filt = GeneralFilter(mesh, 1.6)
+        H = filt.kernel.toarray()
+        x = rng.uniform(0, 1, n_el)
+        sizes = np.array([len(e) for e in els], dtype=np.int64)
+        flat = np.concatenate([np.asarray(e, dtype=np.int64) for e in els])
+        if mesh.is_uniform:
+            Kflat = np.concatenate([K.reshape(-1) for K in mesh.Ks])
+        else:
+            Kflat = np.asarray(mesh.K_flat)
+        out.update({f"{tag}_nodes": P, f"{tag}_sizes": sizes, f"{tag}_flat": flat,
+                    f"{tag}_uniform": np.array(bool(mesh.is_uniform)), f"{tag}_dof": np.array(mesh.dof),
+                    f"{tag}_centroids": mesh.centeroids, f"{tag}_As": np.asarray(mesh.As).reshape(-1),
+                    f"{tag}_volume": np.array(float(mesh.volume)), f"{tag}_Kflat": Kflat, f"{tag}_rho": rho,
+                    f"{tag}_u": u, f"{tag}_matvec": mv, f"{tag}_U": U, f"{tag}_dk": dk, f"{tag}_cons": cons,
+                    f"{tag}_matvec_con": mvc, f"{tag}_diag_con": diag, f"{tag}_H": H, f"{tag}_fx": x,
+                    f"{tag}_Hx": np.asarray(filt._matvec(x)), f"{tag}_HTx": np.asarray(filt._rmatvec(x))})
+        print(f"general {tag}: n_el {n_el} ndof {ndof} uniform {mesh.is_uniform}")
+    np.savez_compressed(os.path.join(HERE, "general.npz"), **out)
+
+
 _REF = None
 
 if __name__ == "__main__":
@@ -407,7 +502,7 @@ if __name__ == "__main__":
     args = ap.parse_args()
     _REF = _import_reference()
     jobs = {"kat": make_kat, "ops": make_ops, "mbb": make_loop_mbb, "cant": make_loop_cant3d, "grad": make_grad,
-            "fea": make_fea, "mm": make_multimaterial}
+            "fea": make_fea, "mm": make_multimaterial, "general": make_general}
     for name, fn in jobs.items():
         if args.only and name not in args.only.split(","):
             continue

@@ -208,3 +208,52 @@ def test_multimaterial_oracle_loop():
     assert all(b < a for a, b in zip(c, c[1:]))
     assert (rho.mean(axis=0) <= np.array([0.25, 0.15]) * (1 + 1e-4)).all()
     assert (rho >= 0).all() and (rho <= 1).all()
+
+
+GENERAL_TAGS = ("tri", "mixed", "tet", "hex")
+
+
+def test_general_mesh_oracle(golden):
+    """Unstructured meshes (T3, T3+Q4, Tet4 of both orientations, distorted hex8): the oracle's
+    operator with and without constraints, diagonal, dk, centroids and KD-tree filter equal the
+    reference's UniformStiffnessKernel / GeneralStiffnessKernel / GeneralFilter."""
+    from oracle import general
+    z = golden("general.npz")
+    for tag in GENERAL_TAGS:
+        sizes, flat, dof = z[f"{tag}_sizes"], z[f"{tag}_flat"], int(z[f"{tag}_dof"])
+        conn = general.connectivity(sizes, flat)
+        Ks = general.element_matrices(z[f"{tag}_Kflat"], sizes, dof)
+        nodes = z[f"{tag}_nodes"]
+        n_dof = nodes.shape[0] * dof
+        assert bool(z[f"{tag}_uniform"]) == (len(set(sizes.tolist())) == 1)
+        assert rel(general.centroids(nodes, conn), z[f"{tag}_centroids"]) < 1e-14, tag
+        K = general.assemble(n_dof, dof, conn, Ks, z[f"{tag}_rho"])
+        assert rel(K @ z[f"{tag}_u"], z[f"{tag}_matvec"]) < 1e-13, tag
+        Kc = general.assemble(n_dof, dof, conn, Ks, z[f"{tag}_rho"], z[f"{tag}_cons"])
+        assert rel(Kc @ z[f"{tag}_u"], z[f"{tag}_matvec_con"]) < 1e-13, tag
+        assert rel(Kc.diagonal(), z[f"{tag}_diag_con"]) < 1e-13, tag
+        assert rel(general.dk(conn, Ks, z[f"{tag}_U"], dof), z[f"{tag}_dk"]) < 1e-13, tag
+        H = general.filter_matrix(z[f"{tag}_centroids"], 1.6)
+        assert rel(H.toarray(), z[f"{tag}_H"]) < 1e-14, tag
+        assert rel(H @ z[f"{tag}_fx"], z[f"{tag}_Hx"]) < 1e-14, tag
+        assert rel(H.T @ z[f"{tag}_fx"], z[f"{tag}_HTx"]) < 1e-14, tag
+
+
+def test_general_element_matrices_product(golden):
+    """This package's element routines (edge_to_b200.physics.auto_stiffness: T3 and Tet4 via
+    the simplex coordinate matrix, isoparametric Q4 / hex8) reproduce the reference's element
+    matrices and measures on the unstructured fixture meshes, including negatively oriented
+    tetrahedra."""
+    from edge_to_b200 import physics
+    from oracle import general
+    z = golden("general.npz")
+    for tag in GENERAL_TAGS:
+        sizes, flat, dof = z[f"{tag}_sizes"], z[f"{tag}_flat"], int(z[f"{tag}_dof"])
+        conn = general.connectivity(sizes, flat)
+        Ks = general.element_matrices(z[f"{tag}_Kflat"], sizes, dof)
+        nodes = z[f"{tag}_nodes"]
+        for e, c in enumerate(conn):
+            K, D, B, A = physics.auto_stiffness(nodes[c], 1.0, 0.3)
+            assert rel(K, Ks[e]) < 1e-13, (tag, e)
+            assert abs(A - z[f"{tag}_As"][e]) <= 1e-14 * max(1.0, abs(A)), (tag, e)
+        assert abs(sum(z[f"{tag}_As"]) - float(z[f"{tag}_volume"])) < 1e-12
