@@ -12,13 +12,13 @@ from .autograd import SIMPObjective
 from .filters import CuStructuredFilter2D, CuStructuredFilter3D, FilterKernel
 from .kernels import CuStructuredStiffnessKernel, StiffnessKernel
 from .material import MaterialModel, PenalizedMultiMaterial, SingleMaterial
-from .mesh import CuStructuredMesh2D, CuStructuredMesh3D, StructuredMesh
+from .mesh import CuGeneralMesh, CuStructuredMesh2D, CuStructuredMesh3D, GeneralMesh, StructuredMesh
 from .physics import auto_stiffness, hexahedron_element_stiffness, quadrilateral_element_stiffness
 from .solvers import CuMultiGrid, CuCG
 from .topopt import CuTopOpt
 
 __all__ = [
-    "CuStructuredMesh2D", "CuStructuredMesh3D", "StructuredMesh", "CuStructuredStiffnessKernel", "StiffnessKernel",
+    "CuStructuredMesh2D", "CuStructuredMesh3D", "StructuredMesh", "CuGeneralMesh", "GeneralMesh", "CuStructuredStiffnessKernel", "StiffnessKernel",
     "CuStructuredFilter2D", "CuStructuredFilter3D", "FilterKernel", "CuMultiGrid", "CuCG", "CuTopOpt", "SingleMaterial",
     "PenalizedMultiMaterial", "MaterialModel", "auto_stiffness", "hexahedron_element_stiffness", "quadrilateral_element_stiffness",
     "SIMPObjective",

@@ -1,4 +1,5 @@
-"""Structured Q4 / hex8 meshes with the reference's numbering (geom/_mesh.py:81-143).
+"""Structured Q4 / hex8 meshes with the reference's numbering (geom/_mesh.py:81-143), and
+general (unstructured) meshes of T3 / Q4 / Tet4 / hex8 elements (geom/_mesh.py:146-251).
 
 Node and element arrays follow core/_geom.py:4-98 (2-D node j*(nelx+1)+i, element
 i*nely+j; 3-D node j*nx*nz + i*nz + k, element i*nely*nelz + j*nelz + k).  They are
@@ -125,3 +126,64 @@ class CuStructuredMesh3D(_StructuredBase):
 # The CPU-named classes of the reference map to the same GPU meshes here.
 StructuredMesh2D = CuStructuredMesh2D
 StructuredMesh3D = CuStructuredMesh3D
+
+
+class CuGeneralMesh:
+    """Unstructured mesh, drop-in for GeneralMesh / CuGeneralMesh (geom/_mesh.py:146-251).
+
+    ``nodes`` (n x dim) and ``elements`` (an n_el x k integer array, or a sequence of node
+    lists of mixed sizes).  Builds the reference's bookkeeping: ``element_sizes``,
+    ``elements_flat``, ``elements_ptr``, ``centeroids`` (sic, the reference's name: the mean of
+    each element's nodes), ``is_uniform`` (one element size), the per-element matrices from
+    ``stiffness`` (``Ks``, ``Ds``, ``Bs`` stacked when uniform; ``K_flat``/``D_flat``/``B_flat``
+    with ``K_ptr``/``D_ptr``/``B_ptr`` otherwise), ``As`` (n_el x 1), ``dof`` and ``volume``.
+    Nodes that no element uses are removed and the connectivity renumbered; the reference
+    renumbers only ``elements_flat`` and keeps reading ``elements`` with the old numbers, so
+    here ``elements`` is renumbered as well.  Arrays are host numpy arrays: the device copies
+    belong to the stiffness kernel and filter that consume the mesh.
+    """
+
+    def __init__(self, nodes, elements, dtype=np.float64, stiffness=_default_stiffness):
+        nodes = np.asarray(nodes, dtype=dtype)
+        conn = [np.asarray(e, dtype=np.int64).reshape(-1) for e in elements]
+        if not conn:
+            raise ValueError("mesh has no elements")
+        sizes = np.array([c.size for c in conn], dtype=np.int32)
+        self.is_uniform = bool((sizes == sizes[0]).all())
+        self.centeroids = np.stack([nodes[c].mean(axis=0) for c in conn]).astype(dtype)
+        flat = np.concatenate(conn)
+        used = np.unique(flat)
+        if used.size != nodes.shape[0]:
+            remap = -np.ones(nodes.shape[0], dtype=np.int64)
+            remap[used] = np.arange(used.size)
+            conn = [remap[c] for c in conn]
+            flat = remap[flat]
+            nodes = nodes[used]
+        self.nodes = nodes
+        self.element_sizes = sizes
+        self.elements_flat = flat.astype(np.int32)
+        self.elements_ptr = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+        mats = [stiffness(nodes[c]) for c in conn]
+        self.As = np.array([[m[3]] for m in mats], dtype=dtype)
+        if self.is_uniform:
+            self.elements = np.stack(conn).astype(np.int32)
+            self.Ks = np.stack([m[0] for m in mats]).astype(dtype)
+            self.Ds = np.stack([m[1] for m in mats]).astype(dtype)
+            self.Bs = np.stack([m[2] for m in mats]).astype(dtype)
+            self.dof = int(self.Ks.shape[1] // sizes[0])
+        else:
+            self.elements = conn
+            for name, i in (("K", 0), ("D", 1), ("B", 2)):
+                arrs = [np.asarray(m[i], dtype=dtype).reshape(-1) for m in mats]
+                setattr(self, f"{name}_flat", np.concatenate(arrs))
+                setattr(self, f"{name}_ptr", np.concatenate([[0], np.cumsum([a.size for a in arrs])]).astype(np.int32))
+            self.dof = int(np.asarray(mats[-1][0]).shape[0] // sizes[-1])
+        self.volume = float(np.sum(self.As))
+        self.dtype = dtype
+
+    @property
+    def n_elements(self):
+        return len(self.element_sizes)
+
+
+GeneralMesh = CuGeneralMesh
