@@ -422,8 +422,8 @@ __global__ void k_pcg_xr(long long n, TX* __restrict__ x, const TP* __restrict__
 
 // Mixed precision: the same update with the solution kept as an FP32 increment since the last
 // residual replacement (x32 += alpha p); the FP64 solution is only touched when k_fold_x adds
-// the increment in, before every true residual and at the end of the solve.  The residual
-// recurrence stays FP64.
+// the increment in, before every true residual and at the end of the solve.  This variant
+// keeps an FP64 residual recurrence (edge_set_residual32(0)); k_pcg_xr32 is the default.
 __global__ void k_pcg_xr_lag(long long n, float* __restrict__ x32, const float* __restrict__ p,
                              double* __restrict__ r, const float* __restrict__ q, PcgState* st, double* part,
                              unsigned* ticket, float* __restrict__ r32) {

@@ -1196,10 +1196,11 @@ static void cg_epilogue(Prob& P) {
   launch(P, k_final_res, 1, 1, 0, P.st);
 }
 
-// Mixed precision: FP32 operator, V-cycle and search directions; FP64 solution, residual
-// recurrence, dot products, coarse solve, and true residuals r = b - A x (FP64 operator
-// with FP64 E) that replace the recurrence every time it has dropped by REPLACE_DROP and
-// before convergence is declared.
+// Mixed precision: FP32 operator, V-cycle and search directions; FP64 solution (kept as an
+// FP32 increment between replacements), dot products, coarse solve, and true residuals
+// r = b - A x (FP64 operator with FP64 E) that replace the residual recurrence every time it
+// has dropped by REPLACE_DROP and before convergence is declared.  The recurrence itself is
+// stored in FP32 (Prob::res32, default) or FP64.
 static const double REPLACE_DROP = 1e-2;
 
 static void pcgmx_true_residual(Prob& P) {
