@@ -196,13 +196,21 @@ def _barrier(ws):
 
 
 def _max_over_ranks(v, ws):
+    """The maximum of v over the ranks (a CUDA tensor under NCCL, a host tensor under gloo)."""
     if ws == 1:
         return v
     import torch
     import torch.distributed as dist
-    tt = torch.tensor([v], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    tt = torch.tensor([float(v)], dtype=torch.float64, device=dev)
     dist.all_reduce(tt, op=dist.ReduceOp.MAX)
     return float(tt.item())
+
+
+def whole_job_rate(units_per_rank, ws, t_max_ms):
+    """Units processed by all ranks per second, over the slowest rank's time: every rank does
+    the same amount of work (replicas or equal shards), so the job ends with the slowest."""
+    return ws * units_per_rank / (t_max_ms / 1e3)
 
 
 def warm(opt, rho, warmup):
@@ -299,7 +307,7 @@ def run_ours(args, cfg_name):
         opt64, rho64 = build_problem(cfg, "fp64")
         rho64, dr64, it64 = warm(opt64, rho64, args.warmup)
         f = timed_steps(opt64, rho64, dr64, it64, args.steps, ws, local, profile=False)
-        fp64 = {"value": ws * args.steps / (f["t_ms"] / 1e3), "ms_per_step": f["t_ms"] / args.steps,
+        fp64 = {"value": whole_job_rate(args.steps, ws, f["t_ms"]), "ms_per_step": f["t_ms"] / args.steps,
                 "pcg_iters_per_step": f["pcg"], "compliance_last": f["compliance"]}
         # accuracy of each path against an rtol-1e-10 FP64 solve of the same design (its own
         # last design), outside every timed region
@@ -325,7 +333,7 @@ def run_ours(args, cfg_name):
     kms, kby = prof["kernel_ms"], prof["kernel_bytes"]
     achieved = (kby / prof["kernel_launches"]) / (kms / prof["kernel_launches"] / 1e3) / 1e9 if kms > 0 else None
     traffic = traffic_from_profile(cfg_name)
-    value = ws * args.steps / (t_ms / 1e3)
+    value = whole_job_rate(args.steps, ws, t_ms)
     line = {
         "metric": METRIC,
         "value": value,
@@ -357,7 +365,7 @@ def run_ours(args, cfg_name):
                      "share_of_step": kms / pm["t_ms"] if pm["t_ms"] else None,
                      "timing": "CUDA events around every fine-operator launch of one SIMP step run right "
                                "after the timed steps (host-driven PCG loop, same kernels and tiles)"},
-        "e2e": {"value": args.steps / (e2e_ms / 1e3), "unit": "iter/s", "h2d_bytes_per_step": 8 * n_el,
+        "e2e": {"value": whole_job_rate(args.steps, ws, e2e_ms), "unit": "iter/s", "h2d_bytes_per_step": 8 * n_el,
                 "d2h_bytes_per_step": 8 * n_el + 8, "pcg_iters_per_step": e2e_pcg,
                 "note": "the same SIMP iterations as the device-timed steps (restarted from their state)"},
         "gpu_launches": m["launches"],
@@ -521,33 +529,52 @@ def run_tiles(args, cfg_name):
 
 
 def run_batch(args):
-    """Batching configuration: 256 randomized 2-D problems of uneven size (edge_to_b200.batch),
+    """Batching configuration: randomized 2-D problems of uneven size (edge_to_b200.batch),
     spread over host threads with one CUDA stream each; value = problem-iterations per second
-    (one SIMP iteration of one problem = filter + SIMP law + GMG-PCG solve + sensitivities + OC)."""
+    (one SIMP iteration of one problem = filter + SIMP law + GMG-PCG solve + sensitivities + OC).
+    With N ranks every rank solves its own batch_size problems (batch.shard_specs: disjoint
+    seeded problems, no collective on the data path; weak scaling), timed between barriers
+    and taken over the slowest rank."""
     import numpy as np
     import torch
     from edge_to_b200 import batch
-    torch.cuda.set_device(0)
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     n = args.batch_size
-    specs = [batch.random_spec(i, seed=0) for i in range(n)]
+    specs = batch.shard_specs(n, rank, seed=0)
     b = batch.BatchSIMP(specs, precision=args.precision, tol=1e-6, maxiter=1000, n_threads=args.batch_threads)
     b.step(args.warmup)               # initial analysis, autotuners, warm-up iterations
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(local)
     clocks.start()
+    _barrier(ws)
     ms = b.step(args.steps)
+    _barrier(ws)
     clk = clocks.stop()
+    ms = _max_over_ranks(ms, ws)
     pcg = [int(np.mean(it["pcg"][-args.steps:])) for it in b.items]
     dofs = [2 * (sp["nelx"] + 1) * (sp["nely"] + 1) for sp in specs]
-    return {"metric": "SIMP problem-iterations/s, 256 random uneven 2-D problems", "value": n * args.steps / (ms / 1e3),
-            "unit": "problem-iter/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    return {"metric": f"SIMP problem-iterations/s, {n} random uneven 2-D problems per GPU",
+            "value": whole_job_rate(n * args.steps, ws, ms),
+            "unit": "problem-iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32+bf16/f64",
             "data": "synthetic: seeded random problems (edge_to_b200.batch.random_spec, seed 0)",
-            "config": {"workload": f"batch{n}_2d", "problems": n, "dof_total": int(np.sum(dofs)),
-                       "elements_total": int(sum(sp["nelx"] * sp["nely"] for sp in specs)),
+            "config": {"workload": f"batch{n}_2d", "problems": n * ws, "problems_per_gpu": n,
+                       "parallelism": f"independent problems x{ws}" if ws > 1 else "1 GPU",
+                       "dof_total_rank0": int(np.sum(dofs)),
+                       "elements_total_rank0": int(sum(sp["nelx"] * sp["nely"] for sp in specs)),
                        "rtol": 1e-6, "precision": args.precision, "threads_streams": b.n_threads,
-                       "padded_problems": int(sum(it["opt"].solver.padded for it in b.items)),
-                       "pcg_iters_mean": float(np.mean(pcg))},
+                       "padded_problems_rank0": int(sum(it["opt"].solver.padded for it in b.items)),
+                       "pcg_iters_mean_rank0": float(np.mean(pcg))},
             "clocks": clk}
 
 

@@ -49,6 +49,13 @@ def random_spec(index, seed=0, nelx_range=(64, 512), nely_range=(32, 256)):
             "clamped_nodes": clamped, "load_nodes": np.asarray(load_nodes, dtype=np.int64), "forces": forces}
 
 
+def shard_specs(n, rank, seed=0):
+    """The n problems of one rank when the batch runs on several GPUs: problem indices
+    rank * n .. rank * n + n - 1, so every rank has its own seeded problems (rank 0's are the
+    single-GPU batch) and no two ranks share one."""
+    return [random_spec(rank * n + i, seed) for i in range(n)]
+
+
 def _node(nelx, i, j):
     return j * (nelx + 1) + i  # reference 2-D node numbering (core/_geom.py:20-25)
 
