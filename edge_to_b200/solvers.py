@@ -109,6 +109,27 @@ class _PaddedGrid:
         return v[self.dof_map]
 
 
+def pick_sweep_pattern(runs, retime, margin):
+    """Choice of the sweep autotuner among converged runs [ms, pattern, pcg_iters].
+
+    The fastest pattern and the cheapest one (fewest sweeps) are timed again with
+    ``retime(pattern) -> (ms, converged, iters)`` and decided on the sum of both timings.  A
+    pattern with more sweeps must beat the cheapest by ``margin`` (best < margin * cheapest):
+    the iterations that extra sweeps save shrink as the SIMP design sharpens (at 12.8M DOF:
+    17 % fewer PCG iterations in the first timed SIMP step, 5 % in the fifth), so near-ties on
+    the early tuning solve go to fewer sweeps.  Returns (ms summed, pattern, iters)."""
+    runs = sorted(([float(r[0]), list(r[1]), r[2]] for r in runs), key=lambda r: r[0])
+    cheap = min(runs, key=lambda r: (sum(r[1]), r[1]))
+    contenders = [runs[0]] if runs[0] is cheap else [runs[0], cheap]
+    for r in contenders:
+        ms, ok, _ = retime(r[1])
+        r[0] = r[0] + ms if ok else float("inf")
+    best = contenders[0]
+    if len(contenders) == 2 and not best[0] < margin * cheap[0]:
+        best = cheap
+    return tuple(best)
+
+
 class CuMultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="splu", matrix_free=False, low_level_tol=1e-8, low_level_maxiter=5000,
@@ -242,21 +263,7 @@ class CuMultiGrid(Solver):
         if not runs:  # nothing converged within maxiter: keep the reference's sweeps
             best = (0.0, [self.n_smooth] * self.n_level, 0)
         else:
-            # The fastest pattern and the cheapest one (fewest sweeps) are timed again and
-            # decided on the sum.  A pattern with more sweeps must beat the cheapest by the
-            # margin: the iterations that extra sweeps save shrink as the SIMP design sharpens
-            # (at 12.8M DOF: 17 % fewer PCG iterations in the first timed SIMP step, 5 % in
-            # the fifth), so near-ties on this early solve go to fewer sweeps.
-            runs.sort(key=lambda r: r[0])
-            cheap = min(runs, key=lambda r: (sum(r[1]), r[1]))
-            contenders = [runs[0]] if runs[0] is cheap else [runs[0], cheap]
-            for r in contenders:
-                ms, ok, _ = timed_solve(r[1])
-                r[0] = r[0] + ms if ok else float("inf")
-            best = contenders[0]
-            if len(contenders) == 2 and not best[0] < self.SWEEP_MARGIN * cheap[0]:
-                best = cheap
-            best = tuple(best)
+            best = pick_sweep_pattern(runs, timed_solve, self.SWEEP_MARGIN)
         _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(best[1]), len(best[1]))
         self.sweeps = {"per_level": best[1], "solve_ms": best[0] / (2 if runs else 1), "pcg_iters": best[2],
                        "tune_tol": tol, "candidates": candidates}
