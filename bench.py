@@ -8,8 +8,8 @@ A step = one SIMP iteration (OC update + filter + SIMP law + GMG-PCG solve + com
 + sensitivity + filter transpose), warm-started like the reference.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
-  python bench.py --impl reference ...   (CPU reference arm: multi-threaded port of the
-                                           reference's matvec on the host cores)
+  python bench.py --impl reference ...   (CPU reference arm: the reference's CPU SIMP
+                                           iteration, oracle/cpu_simp.py, on the host cores)
 
 Prints one JSON line (rank 0).  `value` is device-timed with inputs resident in HBM;
 `e2e` runs the same steps through the public API with the design kept in pinned host
@@ -33,10 +33,10 @@ CONFIGS = {
     "cantilever_128x64x64": dict(nel=(128, 64, 64), vf=0.1, rmin=2.0, n_level=4, tol=1e-6),
     "cantilever_64x32x32": dict(nel=(64, 32, 32), vf=0.12, rmin=1.5, n_level=4, tol=1e-6),
 }
-# Mean PCG iterations per SIMP solve of the FP64 path on cantilever_256x128x128 (this
-# benchmark on a B200: 139, 135 and 172 in the first timed steps); the CPU arms use it to
-# turn a timed matvec into SIMP iterations/s, since both run the same FP64 algorithm.
-PCG_ITERS_FP64_CFG5 = 149.0
+# rtol of the FP64 oracle trajectory (nearly exact solves) the timed paths are compared with
+ORACLE_RTOL = 1e-10
+# PCG iterations of the CPU reference timed per step (the timed samples of oracle/cpu_simp.py)
+CPU_PCG_SAMPLES = 8
 
 
 def dist_env():
@@ -123,7 +123,7 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def build_problem(cfg, precision, n_smooth=3, graph=True):
+def build_problem(cfg, precision, n_smooth=3, graph=True, maxiter=1000):
     import numpy as np
     import torch
     import edge_to_b200 as eb
@@ -132,7 +132,7 @@ def build_problem(cfg, precision, n_smooth=3, graph=True):
     mat = eb.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=cfg["vf"])
     k = eb.CuStructuredStiffnessKernel(mesh)
     filt = eb.CuStructuredFilter3D(mesh, cfg["rmin"])
-    solver = eb.CuMultiGrid(mesh, k, tol=cfg["tol"], n_level=cfg["n_level"], maxiter=1000, precision=precision,
+    solver = eb.CuMultiGrid(mesh, k, tol=cfg["tol"], n_level=cfg["n_level"], maxiter=maxiter, precision=precision,
                             n_smooth=n_smooth, graph=graph)
     opt = eb.CuTopOpt(mesh, mat, k, solver, filt, max_iter=1, move=0.2, verbose=False)
     nx, ny, nz = nel[0] + 1, nel[1] + 1, nel[2] + 1
@@ -153,7 +153,7 @@ def timed_steps(opt, rho, dr, it, steps, ws, local, profile=True):
     from edge_to_b200 import _lib
     stream = torch.cuda.current_stream()
     h = opt.kernel.handle
-    pcg = []
+    pcg, comps = [], []
     clocks = ClockSampler(local)
     clocks.start()
     _barrier(ws)
@@ -171,6 +171,7 @@ def timed_steps(opt, rho, dr, it, steps, ws, local, profile=True):
         rho = opt.update_design(rho, dr)
         c, dr, res = opt.solve_and_process(rho, it)
         pcg.append(opt.last_stats.get("pcg_iters", 0))
+        comps.append(float(c))  # already on the host: the analysis returns it from a host read
         it += 1
     torch.cuda.nvtx.range_pop()
     e1.record(stream)
@@ -185,7 +186,7 @@ def timed_steps(opt, rho, dr, it, steps, ws, local, profile=True):
         prof = dict(kernel_ms=kms.value, kernel_bytes=kby.value, kernel_launches=kl.value)
     clk = clocks.stop()
     t_ms = _max_over_ranks(e0.elapsed_time(e1), ws)
-    return dict(rho=rho, dr=dr, it=it, t_ms=t_ms, pcg=pcg, compliance=float(c), prof=prof, clocks=clk,
+    return dict(rho=rho, dr=dr, it=it, t_ms=t_ms, pcg=pcg, compliance=float(c), comps=comps, prof=prof, clocks=clk,
                 launches=n_after.value - n_before.value)
 
 
@@ -213,15 +214,29 @@ def whole_job_rate(units_per_rank, ws, t_max_ms):
     return ws * units_per_rank / (t_max_ms / 1e3)
 
 
-def warm(opt, rho, warmup):
-    """Initial analysis + `warmup` untimed SIMP iterations."""
+def warm(opt, rho, warmup, comps=None):
+    """Initial analysis + `warmup` untimed SIMP iterations (compliances appended to comps)."""
     c, dr, res = opt.solve_and_process(rho, 0)
+    if comps is not None:
+        comps.append(float(c))
     it = 0
     for _ in range(warmup):
         rho = opt.update_design(rho, dr)
         c, dr, res = opt.solve_and_process(rho, it)
+        if comps is not None:
+            comps.append(float(c))
         it += 1
     return rho, dr, it
+
+
+def trajectory_diff(comps_a, comps_b, rho_a, rho_b):
+    """Per-iteration relative compliance difference of two SIMP trajectories from the same
+    start, and the largest absolute difference of their designs after the last one."""
+    d = [abs(a - b) / abs(b) for a, b in zip(comps_a, comps_b)]
+    return {"iterations": len(d), "compliance_rel_diff_max": max(d) if d else None,
+            "compliance_rel_diff_last": d[-1] if d else None,
+            "rho_max_abs_diff_last": float((rho_a - rho_b).abs().max()),
+            "compliance_rel_diff_per_iteration": [float(f"{v:.3e}") for v in d]}
 
 
 def run_ours(args, cfg_name):
@@ -234,6 +249,9 @@ def run_ours(args, cfg_name):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     cfg = CONFIGS[cfg_name]
+    cpu_job = None
+    if ws == 1 and not args.no_cpu_baseline:
+        cpu_job = start_cpu_reference(cfg_name, CPU_PCG_SAMPLES, max(1, (os.cpu_count() or 2) - 2))
     opt, rho = build_problem(cfg, args.precision, args.n_smooth, graph=not args.no_graph)
     if args.sweeps:
         from edge_to_b200 import _lib as _l
@@ -250,7 +268,11 @@ def run_ours(args, cfg_name):
     if args.pdl:
         from edge_to_b200 import _lib as _l
         _l.call("edge_set_pdl", opt.kernel.handle, 1)
-    rho, dr, it = warm(opt, rho, args.warmup)
+    if args.no_fuse:
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_fuse", opt.kernel.handle, 0)
+    traj = []
+    rho, dr, it = warm(opt, rho, args.warmup, traj)
     # the state the timed steps start from; the end-to-end steps restart from it, so both
     # measure the same SIMP iterations (later iterations need more PCG iterations)
     start = (rho.clone(), dr.clone(), it, opt.solver.last_x0.clone() if opt.solver.last_x0 is not None else None)
@@ -259,6 +281,8 @@ def run_ours(args, cfg_name):
     # graph launch (per-launch events cannot sit inside a graph, so none are recorded here)
     m = timed_steps(opt, rho, dr, it, args.steps, ws, local, profile=False)
     rho, dr, it, t_ms = m["rho"], m["dr"], m["it"], m["t_ms"]
+    traj += m["comps"]
+    rho_traj = rho.detach().clone()
     # ---------------- one more step with CUDA events around every fine-operator launch (the
     # host-driven loop, same launches) for the live roofline of the dominant kernel
     pm = timed_steps(opt, rho, dr, it, 1, ws, local, profile=True)
@@ -305,10 +329,15 @@ def run_ours(args, cfg_name):
     if args.precision == "mixed" and not args.no_fp64_compare:
         torch.cuda.empty_cache()
         opt64, rho64 = build_problem(cfg, "fp64")
-        rho64, dr64, it64 = warm(opt64, rho64, args.warmup)
+        traj64 = []
+        rho64, dr64, it64 = warm(opt64, rho64, args.warmup, traj64)
         f = timed_steps(opt64, rho64, dr64, it64, args.steps, ws, local, profile=False)
+        traj64 += f["comps"]
         fp64 = {"value": whole_job_rate(args.steps, ws, f["t_ms"]), "ms_per_step": f["t_ms"] / args.steps,
                 "pcg_iters_per_step": f["pcg"], "compliance_last": f["compliance"]}
+        # the two SIMP trajectories (initial analysis, warm-up and timed iterations) from the
+        # same start design, iteration by iteration
+        fp64["trajectory"] = trajectory_diff(traj, traj64, rho_traj, f["rho"])
         # accuracy of each path against an rtol-1e-10 FP64 solve of the same design (its own
         # last design), outside every timed region
         opt64.solver.tol, opt64.solver.maxiter = 1e-10, 4000
@@ -322,7 +351,20 @@ def run_ours(args, cfg_name):
             "compliance": abs(c_chk - c_tmx) / abs(c_tmx),
             "displacement": float(torch.linalg.norm(u_chk - u_t) / torch.linalg.norm(u_t)),
             "dc": float((dr_chk - dr_t).abs().max() / dr_t.abs().max())}
-        del opt64, rho64, dr64
+        rho64_last = f["rho"].detach().clone()
+        del opt64, rho64, dr64, f
+        if not args.no_oracle_trajectory:
+            # the FP64 oracle trajectory: the same SIMP iterations with every solve at rtol
+            # ORACLE_RTOL (nearly exact), against which both timed paths' compliances and
+            # designs are compared iteration by iteration (outside every timed region)
+            torch.cuda.empty_cache()
+            opt_t, rho_t = build_problem(dict(cfg, tol=ORACLE_RTOL), "fp64", maxiter=5000)
+            traj_t = []
+            rho_t, _, _ = warm(opt_t, rho_t, args.warmup + args.steps, traj_t)
+            fp64["oracle"] = {"rtol": ORACLE_RTOL,
+                              "mixed": trajectory_diff(traj, traj_t, rho_traj, rho_t),
+                              "fp64": trajectory_diff(traj64, traj_t, rho64_last, rho_t)}
+            del opt_t, rho_t
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -355,7 +397,8 @@ def run_ours(args, cfg_name):
                    "fine_tile": tuned, "sweeps": sweeps,
                    "coarse_stencils": "fp32" if (args.coarse_fp32 or args.precision == "fp64") else "bf16",
                    "residual_recurrence": "fp64" if (args.residual64 or args.precision == "fp64") else "fp32",
-                   "programmatic_dependent_launch": args.pdl and not args.no_graph},
+                   "programmatic_dependent_launch": args.pdl and not args.no_graph,
+                   "fused_fine_launches": args.precision == "mixed" and not args.no_fuse},
         "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_cube/_pk/_tma + fused epilogues)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
@@ -376,6 +419,9 @@ def run_ours(args, cfg_name):
         "clocks": m["clocks"],
     }
     if fp64 is not None:
+        line["trajectory_vs_fp64"] = fp64.pop("trajectory")
+        if "oracle" in fp64:
+            line["trajectory_vs_fp64_oracle"] = fp64.pop("oracle")
         line["fp64_path"] = fp64
         line["mixed_over_fp64"] = value / fp64["value"]
         line["compliance_rel_err_vs_fp64"] = abs(m["compliance"] - fp64["compliance_last"]) / abs(
@@ -386,9 +432,10 @@ def run_ours(args, cfg_name):
                                                       "rtol 1e-10: relative errors (displacement 2-norm, dc max-norm)")
     if bd is not None:
         line["breakdown_ms_per_step"] = bd
-    if ws == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, pcg_iters=float(np.mean(m["pcg"])) if m["pcg"] else
-                                            PCG_ITERS_FP64_CFG5, reps=2)
+    if cpu_job is not None:
+        line["cpu_baseline"] = cpu_reference_line(finish_cpu_reference(cpu_job, 900.0))
+        line["cpu_baseline"]["note"] = ("run in a spawned process beside the GPU measurement on all host threads "
+                                        "but two")
     return line
 
 
@@ -410,22 +457,57 @@ def breakdown(opt, rho, dr, it):
     return {CATS[i]: {"ms": round(ms[i], 3), "launches": nn[i]} for i in range(len(CATS))}
 
 
-def cpu_baseline(cfg, pcg_iters, reps=2):
-    """Reference CPU algorithm (multi-threaded port of its matvec) timed on this host."""
-    import numpy as np
-    from oracle import cpu_matvec, elements
-    K0 = elements.hex8_stiffness(1, 1, 1, 1.0, 0.3)
-    t, _ = cpu_matvec.time_matvec(cfg["nel"], K0, reps=reps)
-    mv_per_iter = 8 * pcg_iters + 1
+def _cpu_reference_worker(cfg_name, samples, threads, q):
+    """Child process: the reference's CPU SIMP iteration (oracle/cpu_simp.py) timed on
+    `threads` host threads; puts its measurement dict on q."""
+    os.environ["NUMBA_NUM_THREADS"] = str(threads)
     try:
-        import numba
-        threads = numba.get_num_threads()
-    except Exception:
-        threads = os.cpu_count()
-    return {"value": 1.0 / (t * mv_per_iter), "unit": "iter/s", "cores": threads, "kind": "port",
-            "sample": f"{reps} fine matvecs at full size ({t:.3f} s each, Numba prange on {threads} threads); "
-                      f"iter/s = 1/(t_matvec * (8*{pcg_iters:.1f} PCG iters + 1)), matvec-only lower bound "
-                      "on the reference CPU loop time"}
+        from oracle import cpu_simp
+        cfg = CONFIGS[cfg_name]
+        q.put(cpu_simp.measure(cfg["nel"], cfg["vf"], cfg["rmin"], cfg["n_level"], cfg["tol"], samples=samples))
+    except Exception as e:  # reported, not raised: the GPU measurement stands on its own
+        q.put({"error": repr(e)})
+
+
+def start_cpu_reference(cfg_name, samples, threads):
+    """Starts the CPU reference measurement in a spawned process (before any GPU call, so
+    the child holds no CUDA state), to run beside the GPU measurement."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    proc = ctx.Process(target=_cpu_reference_worker, args=(cfg_name, samples, threads, q), daemon=True)
+    proc.start()
+    return proc, q
+
+
+def finish_cpu_reference(handle, timeout_s):
+    proc, q = handle
+    import queue
+    try:
+        m = q.get(timeout=timeout_s)
+    except queue.Empty:
+        m = {"error": f"no result within {timeout_s:.0f} s"}
+    proc.join(timeout=10)
+    if proc.is_alive():
+        proc.kill()
+    return m
+
+
+def cpu_reference_line(m):
+    """cpu_baseline object of the JSON line from a cpu_simp.measure result."""
+    if "error" in m:
+        return {"value": None, "unit": "iter/s", "cores": None, "kind": "port", "sample": m["error"]}
+    return {"value": 1.0 / m["seconds_per_iteration"], "unit": "iter/s", "cores": m["threads"], "kind": "port",
+            "sample": (f"the reference's CPU SIMP iteration (oracle/cpu_simp.py) on {m['threads']} threads: first "
+                       f"analysis solved to rtol ({m['first_solve_pcg_iters']} PCG iterations, the CPU solver's own "
+                       f"count; {m['first_solve_pcg_s']:.1f} s) with set-up {m['setup_s']:.2f} s, post "
+                       f"{m['post_s']:.2f} s, OC {m['oc_s']:.2f} s, then {len(m['pcg_iteration_samples_s'])} more "
+                       f"PCG iterations timed one by one (median {m['pcg_iteration_s']:.3f} s); iteration = set-up "
+                       f"+ post + OC + {m['first_solve_pcg_iters']} x median = {m['seconds_per_iteration']:.1f} s. "
+                       "Later SIMP iterations need more PCG iterations than this cold first solve, so the CPU "
+                       f"rate is an upper bound. Fine product {m['matvec_s']:.3f} s (index arithmetic; "
+                       f"{m['matvec_list_indexing_s']:.3f} s with the reference's element-list lookups)"),
+            "detail": m}
 
 
 def run_matvec(args, cfg_name):
@@ -579,30 +661,21 @@ def run_batch(args):
 
 
 def run_reference(args, cfg_name):
+    """The reference's CPU path on this host's cores (oracle/cpu_simp.py), rank 0 only."""
     ws, rank, local = dist_env()
     if rank != 0:
         return None
-    import numpy as np
-    from oracle import cpu_matvec, elements
-    cfg = CONFIGS[cfg_name]
-    K0 = elements.hex8_stiffness(1, 1, 1, 1.0, 0.3)
-    # warm-up = JIT + cache warming; each timed step is one full-size matvec sample
-    cpu_matvec.time_matvec((4, 4, 4), K0, reps=max(1, args.warmup))
-    t, _ = cpu_matvec.time_matvec(cfg["nel"], K0, reps=max(1, args.steps))
-    mv_per_iter = 8 * PCG_ITERS_FP64_CFG5 + 1
-    v = 1.0 / (t * mv_per_iter)
-    try:
-        import numba
-        threads = numba.get_num_threads()
-    except Exception:
-        threads = os.cpu_count()
-    sample = (f"{args.steps} full-size fine matvecs, {t:.3f} s median; iter/s = 1/(t_matvec*(8*{PCG_ITERS_FP64_CFG5}"
-              f"+1)) with the FP64 PCG iteration count of this workload")
+    cores = os.cpu_count() or 1
+    m = finish_cpu_reference(start_cpu_reference(cfg_name, min(max(1, args.steps), CPU_PCG_SAMPLES), cores), 1800.0)
+    cb = cpu_reference_line(m)
+    v = cb["value"]
+    t = m.get("seconds_per_iteration")
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t * mv_per_iter * 1e3, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": t * 1e3 if t else None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg_name, "precision": "fp64", "parallelism": "host cores"},
-            "cpu_baseline": {"value": v, "unit": "iter/s", "cores": threads, "kind": "port", "sample": sample},
+            "config": {"workload": cfg_name, "precision": "fp64", "parallelism": f"host cores ({cores})",
+                       "pcg_samples": len(m.get("pcg_iteration_samples_s", []))},
+            "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -617,6 +690,10 @@ def main():
                     help="skip timing the plain FP64 path beside the mixed-precision one")
     ap.add_argument("--config", default="cantilever_256x128x128", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle-trajectory", action="store_true",
+                    help="skip the FP64 trajectory at rtol 1e-10 the timed paths are compared with")
+    ap.add_argument("--no-fuse", action="store_true",
+                    help="mixed path: the fine level's sweeps and search direction as separate launches")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles"])
     ap.add_argument("--tile", type=int, default=None, help="matvec/tiles mode: fine-kernel tile variant (0-14)")
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")

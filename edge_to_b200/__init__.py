@@ -2,7 +2,8 @@
 
 Drop-in names (EDGETO/__init__.py, TopOpt/__init__.py, solvers/__init__.py,
 kernels/__init__.py, geom/__init__.py): CuStructuredMesh2D/3D, CuStructuredStiffnessKernel,
-CuStructuredFilter2D/3D, CuMultiGrid, CuCG, CuTopOpt, SingleMaterial, PenalizedMultiMaterial,
+CuStructuredFilter2D/3D, CuMultiGrid, MultiGrid (the CPU solver's smoother-weight semantics),
+CuCG, CuTopOpt, SingleMaterial, PenalizedMultiMaterial,
 auto_stiffness; beyond the
 reference, SIMPObjective (differentiable compliance / mechanism objectives, autograd.py).
 Arrays are torch CUDA tensors; the compute runs in libedge_b200.so (sm_100a).
@@ -14,12 +15,12 @@ from .kernels import CuStructuredStiffnessKernel, StiffnessKernel
 from .material import MaterialModel, PenalizedMultiMaterial, SingleMaterial
 from .mesh import CuGeneralMesh, CuStructuredMesh2D, CuStructuredMesh3D, GeneralMesh, StructuredMesh
 from .physics import auto_stiffness, hexahedron_element_stiffness, quadrilateral_element_stiffness
-from .solvers import CuMultiGrid, CuCG
+from .solvers import CuCG, CuMultiGrid, MultiGrid
 from .topopt import CuTopOpt
 
 __all__ = [
     "CuStructuredMesh2D", "CuStructuredMesh3D", "StructuredMesh", "CuGeneralMesh", "GeneralMesh", "CuStructuredStiffnessKernel", "StiffnessKernel",
-    "CuStructuredFilter2D", "CuStructuredFilter3D", "FilterKernel", "CuMultiGrid", "CuCG", "CuTopOpt", "SingleMaterial",
+    "CuStructuredFilter2D", "CuStructuredFilter3D", "FilterKernel", "CuMultiGrid", "MultiGrid", "CuCG", "CuTopOpt", "SingleMaterial",
     "PenalizedMultiMaterial", "MaterialModel", "auto_stiffness", "hexahedron_element_stiffness", "quadrilateral_element_stiffness",
     "SIMPObjective",
 ]

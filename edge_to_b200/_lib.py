@@ -47,6 +47,8 @@ _SIGS = {
     "edge_set_stencil_pair": (ctypes.c_int, [vp, ctypes.c_longlong]),
     "edge_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_mg_set_sweeps": (ctypes.c_int, [vp, c_int_p, ctypes.c_int]),
+    "edge_mg_set_omega_carry": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_set_fuse": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_fea_integrals": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp]),
     "edge_cg_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_double_p, c_int_p]),
     "edge_launch_count": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),

@@ -32,6 +32,14 @@
 //    A stage is refilled at the barrier of the layer after the one that used it, so the
 //    epilogue reads its inputs after the barrier and holds no registers across it.
 //
+//  * The operator's input u may be computed from one or two staged arrays as the tile is
+//    read (IN): u itself (InU); the first damped-Jacobi sweep from zero, u = w Dinv b
+//    (InWDB: b FP32 and the BF16 Dinv, so a V-cycle's first fine sweep is never stored);
+//    or the PCG search direction u = z + beta p_old (InPDir), the new p written out by the
+//    epilogue into the other buffer of a ping-pong pair (blocks read p_old in their halos,
+//    so it cannot be overwritten in place).  The epilogue recomputes each output node's
+//    input value from the stage it was read from (no registers held across the layer).
+//
 // TMA boxes, strides and alignments are those of k_fine3_pk, plus the staged arrays: FP32
 // and FP64 boxes start at z0-1 rounded down to 4 nodes (16 / 32 bytes), BF16 boxes at z0-1
 // rounded down to 8 nodes (16 bytes; the 3-D fine level pads z to a multiple of 8 so that
@@ -39,6 +47,7 @@
 // the clocked wait of fine_tma.cuh).  No multicast.
 #pragma once
 #include "fine_pk.cuh"
+#include "misc.cuh"  // PcgState (the search-direction input reads beta from it)
 
 namespace edge {
 
@@ -117,7 +126,7 @@ struct SEStore {  // out = A u
   EDGE_HD static constexpr int kT(int i) { return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 0 : 0; }
   struct In {};
   EDGE_D void init() {}
-  EDGE_D In load(const unsigned char* const*, int, int) const { return {}; }
+  EDGE_D In load(const unsigned char* const*, int, int, const float*, int) const { return {}; }
   EDGE_D void apply(long long s, const float*, const float* Au, const In&, double&) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c * n + s] = Au[c];
@@ -132,7 +141,7 @@ struct SEStoreDot {  // out = A u, acc += u . A u
   EDGE_HD static constexpr int kT(int i) { return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 0 : 0; }
   struct In {};
   EDGE_D void init() {}
-  EDGE_D In load(const unsigned char* const*, int, int) const { return {}; }
+  EDGE_D In load(const unsigned char* const*, int, int, const float*, int) const { return {}; }
   EDGE_D void apply(long long s, const float* own, const float* Au, const In&, double& acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -152,7 +161,7 @@ struct SEResid {  // r = b - A u
     float b[3];
   };
   EDGE_D void init() {}
-  EDGE_D In load(const unsigned char* const* sp, int cs4, int) const {
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
@@ -177,7 +186,7 @@ struct SEJacobi {  // xo = u + w Dinv (b - A u)
     float b[3], d[3];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
-  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2) const {
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -209,7 +218,7 @@ template <bool DOT> struct SEJacobiAdd {
     float dv[DOT ? 3 : 1];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
-  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2) const {
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -230,43 +239,181 @@ template <bool DOT> struct SEJacobiAdd {
   }
 };
 
-// Stage layout of the cube kernel: the k_fine3_pk stage followed by the staged arrays.
-template <int BX, class SE> struct CubeTile {
+
+// r = b - A u with b the operator's input array 0 (the V-cycle's first fine step: u = w Dinv
+// b computed from the staged b and Dinv, so b is already in the stage)
+struct SEResidIn {
+  float* r;
+  long long n;
+  static constexpr int kN = 0;
+  static constexpr bool kDot = false;
+  EDGE_HD static constexpr int kT(int) { return 0; }
+  struct In {
+    float b[3];
+  };
+  EDGE_D void init() {}
+  EDGE_D In load(const unsigned char* const*, int, int, const float* in0, int uc4) const {
+    In v;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v.b[c] = in0[c * uc4];
+    return v;
+  }
+  EDGE_D void apply(long long s, const float*, const float* Au, const In& v, double&) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r[c * n + s] = v.b[c] - Au[c];
+  }
+};
+
+// Last post-smoothing sweep of a one-sweep fine level with the correction, where the
+// pre-smoothed iterate was never stored: xo = w Dinv b + (e + w Dinv (b - A e)), e = u; with
+// DOT, acc += b . xo (the PCG's r.z: b is the FP32 residual).  The same arithmetic, in the same
+// order, as the stored-iterate path (k_jacobi0 followed by SEJacobiAdd).
+template <bool DOT> struct SEJacobiAdd0 {
+  float* xo;
+  const double* omega;
+  double wscale;
+  long long n;
+  float w;
+  static constexpr int kN = 2;
+  static constexpr bool kDot = DOT;
+  EDGE_HD static constexpr int kT(int i) { return i == 1 ? ST_BF16 : ST_F32; }
+  struct In {
+    float b[3], d[3];
+  };
+  EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, int) const {
+    In v;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
+      v.d[c] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(sp[1])[c * cs2]);
+    }
+    return v;
+  }
+  EDGE_D void apply(long long s, const float* own, const float* Au, const In& v, double& acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float xb = (w * v.d[c]) * v.b[c];
+      const float x = xb + (own[c] + w * v.d[c] * (v.b[c] - Au[c]));
+      xo[c * n + s] = x;
+      if constexpr (DOT) acc += (double)v.b[c] * (double)x;
+    }
+  }
+};
+
+// q = A p, p written out, acc += p . A p, with p = z + beta p_old computed by the input
+// transform (InPDir); p_new goes to the buffer the iteration's parity selects.
+struct SEStorePDot {
+  float* q;
+  float* pa;  // p buffers: iteration parity 0 reads pa and writes pb, parity 1 the reverse
+  float* pb;
+  const PcgState* st;
+  long long n;
+  float* pout;
+  static constexpr int kN = 0;
+  static constexpr bool kDot = true;
+  EDGE_HD static constexpr int kT(int) { return 0; }
+  struct In {};
+  EDGE_D void init() { pout = (st->iter & 1) ? pa : pb; }
+  EDGE_D In load(const unsigned char* const*, int, int, const float*, int) const { return {}; }
+  EDGE_D void apply(long long s, const float* own, const float* Au, const In&, double& acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      q[c * n + s] = Au[c];
+      pout[c * n + s] = own[c];
+      acc += (double)own[c] * (double)Au[c];
+    }
+  }
+};
+
+// ------------------------------------------------------------------ operator inputs
+// value(a0, a1, i4, i2): the input at one node and component of the stage, from array 0
+// (FP32, element index i4) and array 1 (kT1: FP32 index i4 or BF16 index i2).
+struct InU {  // u itself
+  static constexpr int kN = 1;
+  static constexpr int kT1 = ST_F32;
+  EDGE_D void init() {}
+  EDGE_D int parity() const { return 0; }
+  EDGE_D float value(const float* a0, const void*, int i4, int) const { return a0[i4]; }
+};
+struct InWDB {  // u = (w Dinv) b: the first damped-Jacobi sweep from zero (k_jacobi0)
+  const double* omega;
+  double wscale;
+  float w;
+  static constexpr int kN = 2;
+  static constexpr int kT1 = ST_BF16;
+  EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
+  EDGE_D int parity() const { return 0; }
+  EDGE_D float value(const float* a0, const void* a1, int i4, int i2) const {
+    return (w * __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(a1)[i2])) * a0[i4];
+  }
+};
+struct InPDir {  // u = z + beta p_old (the first PCG iteration: u = z)
+  const PcgState* st;
+  float beta;
+  int par;
+  bool first;
+  static constexpr int kN = 2;
+  static constexpr int kT1 = ST_F32;
+  EDGE_D void init() {
+    first = st->iter == 0;
+    par = st->iter & 1;
+    beta = first ? 0.f : (float)(st->rz_new / st->rz);
+  }
+  EDGE_D int parity() const { return par; }
+  EDGE_D float value(const float* a0, const void* a1, int i4, int) const {
+    return first ? a0[i4] : fmaf(beta, reinterpret_cast<const float*>(a1)[i4], a0[i4]);
+  }
+};
+
+// Stage layout of the cube kernel: the operator's input array(s) with the k_fine3_pk u-box
+// geometry (array 1, when there is one, right after array 0), the element flags and E, then
+// the epilogue's staged arrays.
+template <int BX, class SE, class IN = InU> struct CubeTile {
   using B = PkTile<BX>;
   static constexpr int ROWS = 4 * BX;  // staged rows: the block's output node rows
+  static constexpr int NR = B::NR;     // input rows (with the halo row)
   static constexpr int up(int b) { return (b + 127) & ~127; }
   static constexpr int sbytes(int t) { return 3 * ROWS * st_width(t) * st_esize(t); }
+  static constexpr int U0_BYTES = B::U_BYTES;
+  static constexpr int U1_BYTES = IN::kN == 2 ? 3 * NR * st_width(IN::kT1) * st_esize(IN::kT1) : 0;
+  static constexpr int U1_OFF = up(U0_BYTES);
+  static constexpr int F_OFF = U1_OFF + up(U1_BYTES);
+  static constexpr int E_OFF = F_OFF + up(B::F_BYTES);
+  static constexpr int BASE = E_OFF + up(B::E_BYTES);
   static constexpr int s_off(int i) {
-    int o = B::STAGE;
+    int o = BASE;
     for (int j = 0; j < i; ++j) o += up(sbytes(SE::kT(j)));
     return o;
   }
   static constexpr int tx_bytes() {
-    int t = B::TX_BYTES;
+    int t = B::TX_BYTES + U1_BYTES;
     for (int j = 0; j < SE::kN; ++j) t += sbytes(SE::kT(j));
     return t;
   }
   static constexpr int STAGE = s_off(SE::kN);
   static constexpr int TX_BYTES = tx_bytes();
   static constexpr int X_BYTES = B::X_BYTES;
+  static constexpr int UC4 = NR * PK_ZB;               // component stride of an FP32 input array
+  static constexpr int UC2 = NR * st_width(ST_BF16);   // ... of a BF16 input array
 };
 
-template <int BX, int NS, class SE>
+template <int BX, int NS, class SE, class IN = InU>
 constexpr int cube_smem_bytes() {
-  return NS * CubeTile<BX, SE>::STAGE + CubeTile<BX, SE>::X_BYTES + 128 + 16 * NS;
+  return NS * CubeTile<BX, SE, IN>::STAGE + CubeTile<BX, SE, IN>::X_BYTES + 128 + 16 * NS;
 }
 
-template <class SE, int BX, int NS, int MINB>
+template <class SE, int BX, int NS, int MINB, class IN = InU>
 __global__ void __launch_bounds__(32 * BX, MINB)
-k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_constant__ CUtensorMap mapF,
-             const __grid_constant__ CUtensorMap mapE, const float* __restrict__ u, const uint8_t* __restrict__ mask,
+k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_constant__ CUtensorMap mapU1,
+             const __grid_constant__ CUtensorMap mapU1b, const __grid_constant__ CUtensorMap mapF,
+             const __grid_constant__ CUtensorMap mapE, const uint8_t* __restrict__ mask,
              const __grid_constant__ CUtensorMap mapS0, const __grid_constant__ CUtensorMap mapS1,
              const __grid_constant__ CUtensorMap mapS2, const __grid_constant__ CUtensorMap mapS3, const KCube KC,
-             const int ly, SE epi, double* part, unsigned* ticket, double* dot_dst, int* err) {
+             const int ly, IN in, SE epi, double* part, unsigned* ticket, double* dot_dst, int* err) {
   EDGE_PDL_ENTRY();
   static_assert(NS >= 3, "a stage is refilled one layer after its last use");
-  using Tile = CubeTile<BX, SE>;
-  using PT = PkTile<BX>;
+  using Tile = CubeTile<BX, SE, IN>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
   typedef float XArr[2][BX][16][3];
@@ -286,13 +433,15 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
   const int zo16 = (z0 - 1) - zs16;
   const int zs8 = (z0 >= 1) ? ((z0 - 1) & ~7) : -8;
   const int zo8 = (z0 - 1) - zs8;
-  const long long n = g.n;
   const int p0 = y0 - 1;
   const int np = y1 - p0 + 1;
   const bool zok = (zl >= 1) && (ez < g.nz);
   const bool writerA = zok && (c0 >= 1) && (exa < g.nx);
   const bool writerB = zok && (exa + 1 < g.nx);
+  in.init();
   epi.init();
+  // the array 1 map: the second buffer of a ping-pong pair on odd iterations (InPDir)
+  const CUtensorMap* map1 = in.parity() ? &mapU1b : &mapU1;
   bool ok = true;
   P2 kc[8];
   kc[0] = pk(KC.nd, KC.nd);
@@ -314,9 +463,11 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
     unsigned char* st = smem + s * Tile::STAGE;
     const int p = p0 + k;
     mbar_expect_tx(&bar[s], Tile::TX_BYTES);
-    tma_load_4d(st + PT::U_OFF, &mapU, zs4, x0 - 1, p, 0, &bar[s]);
-    tma_load_3d(st + PT::F_OFF, &mapF, zs16, x0 - 1, p, &bar[s]);
-    tma_load_3d(st + PT::E_OFF, &mapE, zs4, x0 - 1, p, &bar[s]);
+    tma_load_4d(st, &mapU, zs4, x0 - 1, p, 0, &bar[s]);
+    if constexpr (IN::kN == 2)
+      tma_load_4d(st + Tile::U1_OFF, map1, IN::kT1 == ST_BF16 ? zs8 : zs4, x0 - 1, p, 0, &bar[s]);
+    tma_load_3d(st + Tile::F_OFF, &mapF, zs16, x0 - 1, p, &bar[s]);
+    tma_load_3d(st + Tile::E_OFF, &mapE, zs4, x0 - 1, p, &bar[s]);
     const CUtensorMap* ms[4] = {&mapS0, &mapS1, &mapS2, &mapS3};
 #pragma unroll
     for (int i = 0; i < SE::kN; ++i)
@@ -325,22 +476,30 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
   if (tid == 0)
     for (int k = 0; k < NS && k < np; ++k) issue(k);
 
-  constexpr int UC = PT::NR * PK_ZB;  // component stride in a stage (words)
-  const int uoff = c0 * PK_ZB + zo4 + zl;
+  constexpr int UC4 = Tile::UC4, UC2 = Tile::UC2;
+  const int i4 = c0 * PK_ZB + zo4 + zl;                 // this thread's (row c0, z) in an FP32 input array
+  const int i2 = c0 * st_width(ST_BF16) + zo8 + zl;     // ... in a BF16 input array
   const int foff = c0 * PK_FB + zo16 + zl;
+  auto a0_of = [&](int k) { return reinterpret_cast<const float*>(smem + (k % NS) * Tile::STAGE); };
+  auto a1_of = [&](int k) { return (const void*)(smem + (k % NS) * Tile::STAGE + Tile::U1_OFF); };
+  // input value of component c at row offset r (0..2) and z offset dz (0, 1) of plane k
+  auto input = [&](int k, int c, int r, int dz) {
+    constexpr int W1 = IN::kT1 == ST_BF16 ? 32 : PK_ZB;
+    constexpr int C1 = IN::kT1 == ST_BF16 ? UC2 : UC4;
+    return in.value(a0_of(k), a1_of(k), c * UC4 + r * PK_ZB + dz + i4,
+                    IN::kT1 == ST_BF16 ? c * C1 + r * W1 + dz + i2 : c * C1 + r * W1 + dz + i4);
+  };
 
   // The 3 node rows x 2 z of plane p (stage k), masked on constrained DOFs when `fl` says
-  // some corner of the pair may be constrained; x-z transformed into t, and the thread's
-  // two own nodes (rows c0, c0+1 at z = ez) returned raw.
-  auto load_plane = [&](int k, int p, uint8_t fl, P2 t[2][2][3], float ownA[3], float ownB[3]) {
-    const float* su = reinterpret_cast<const float*>(smem + (k % NS) * Tile::STAGE + PT::U_OFF) + uoff;
+  // some corner of the pair may be constrained; x-z transformed into t.
+  auto load_plane = [&](int k, int p, uint8_t fl, P2 t[2][2][3]) {
     float s[3][2][3];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) s[r][dz][c] = su[c * UC + r * PK_ZB + dz];
+        for (int c = 0; c < 3; ++c) s[r][dz][c] = input(k, c, r, dz);
     if (__any_sync(0xffffffffu, fl != 0)) {
       if (fl) {
 #pragma unroll
@@ -356,11 +515,6 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
             }
           }
       }
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      ownA[c] = s[0][0][c];
-      ownB[c] = s[1][0][c];
     }
     // x stage (scalar, written straight into the pair registers), then z stage (packed)
 #pragma unroll
@@ -380,19 +534,18 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
       }
   };
   auto flags_of = [&](int k, uint8_t& fa, uint8_t& fb) {
-    const uint8_t* sf = smem + (k % NS) * Tile::STAGE + PT::F_OFF + foff;
+    const uint8_t* sf = smem + (k % NS) * Tile::STAGE + Tile::F_OFF + foff;
     fa = sf[0];
     fb = sf[PK_FB];
   };
 
   P2 pa[2][2][3], pb[2][2][3];  // x-z transforms of two consecutive planes (roles alternate)
   P2 car[2][2][3];              // carry to the next plane; car[0][0] holds the negated value
-  float oAa[3], oBa[3], oAb[3], oBb[3];
   if (ok) ok = mbar_wait_fast(&bar[0], 0);
   {
     uint8_t fa, fb;
     flags_of(0, fa, fb);
-    load_plane(0, p0, fa | fb, pa, oAa, oBa);
+    load_plane(0, p0, fa | fb, pa);
   }
 #pragma unroll
   for (int a = 0; a < 2; ++a)
@@ -406,8 +559,7 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
 
   // One layer: element row ey = p0 + k between plane k (lo, already transformed) and plane
   // k+1 (loaded into hi); writes the outputs of plane ey.
-  auto layer = [&](int k, P2 (&lo)[2][2][3], P2 (&hi)[2][2][3], float (&oA)[3], float (&oB)[3], float (&oAn)[3],
-                   float (&oBn)[3]) {
+  auto layer = [&](int k, P2 (&lo)[2][2][3], P2 (&hi)[2][2][3]) {
     const int ey = p0 + k;
     const long long sA = sA_base + (long long)ey * g.plane;
     const long long sB = sB_base + (long long)ey * g.plane;
@@ -416,9 +568,9 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
     uint8_t fa, fb, fa1, fb1;
     flags_of(k, fa, fb);
     flags_of(k + 1, fa1, fb1);
-    const float* sE = reinterpret_cast<const float*>(smem + (k % NS) * Tile::STAGE + PT::E_OFF) + uoff;
+    const float* sE = reinterpret_cast<const float*>(smem + (k % NS) * Tile::STAGE + Tile::E_OFF) + i4;
     const P2 Ee = pk(sE[0], sE[PK_ZB]);
-    load_plane(k + 1, ey + 1, fa | fb | fa1 | fb1, hi, oAn, oBn);
+    load_plane(k + 1, ey + 1, fa | fb | fa1 | fb1, hi);
     P2 uh[8][3];
 #pragma unroll
     for (int hx = 0; hx < 2; ++hx)
@@ -489,8 +641,9 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
         spB[i] = spA[i] + st_width(t) * st_esize(t);
       }
       constexpr int cs4 = Tile::ROWS * st_width(ST_F32), cs2 = Tile::ROWS * st_width(ST_BF16);
-      if (wrA) inA = epi.load(spA, cs4, cs2);
-      if (wrB) inB = epi.load(spB, cs4, cs2);
+      const float* in0 = a0_of(k) + i4;
+      if (wrA) inA = epi.load(spA, cs4, cs2, in0, UC4);
+      if (wrB) inB = epi.load(spB, cs4, cs2, in0 + PK_ZB, UC4);
     }
     if (xh == 0) {
 #pragma unroll
@@ -498,50 +651,40 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) AuA[c] = gx[0][c].v.x + fromL[c];
+    // each output node's input value, again from stage k (rows c0 and c0 + 1, z = ez);
+    // on a constrained DOF the row is the identity: (A u)_c = u_c
     if (wrA) {
-      float own[3], Au[3];
+      float own[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        own[c] = oA[c];
-        Au[c] = AuA[c];
-      }
+      for (int c = 0; c < 3; ++c) own[c] = input(k, c, 0, 0);
       if (fa) {
         const uint8_t m = __ldg(mask + sA);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          if ((m >> c) & 1) {
-            own[c] = __ldg(u + c * n + sA);
-            Au[c] = own[c];
-          }
+          if ((m >> c) & 1) AuA[c] = own[c];
       }
-      epi.apply(sA, own, Au, inA, dacc);
+      epi.apply(sA, own, AuA, inA, dacc);
     }
     if (wrB) {
-      float own[3], Au[3];
+      float own[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        own[c] = oB[c];
-        Au[c] = AuB[c];
-      }
+      for (int c = 0; c < 3; ++c) own[c] = input(k, c, 1, 0);
       if (fb) {
         const uint8_t m = __ldg(mask + sB);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          if ((m >> c) & 1) {
-            own[c] = __ldg(u + c * n + sB);
-            Au[c] = own[c];
-          }
+          if ((m >> c) & 1) AuB[c] = own[c];
       }
-      epi.apply(sB, own, Au, inB, dacc);
+      epi.apply(sB, own, AuB, inB, dacc);
     }
   };
 
   int k = 0;
   for (; k + 2 < np; k += 2) {
-    layer(k, pa, pb, oAa, oBa, oAb, oBb);
-    layer(k + 1, pb, pa, oAb, oBb, oAa, oBa);
+    layer(k, pa, pb);
+    layer(k + 1, pb, pa);
   }
-  if (k + 1 < np) layer(k, pa, pb, oAa, oBa, oAb, oBb);
+  if (k + 1 < np) layer(k, pa, pb);
   if (!ok) atomicOr(err, 1);
   finish_dot(epi, dacc, part, ticket, dot_dst);
 }

@@ -466,10 +466,14 @@ __global__ void k_pcg_xr_lag(long long n, float* __restrict__ x32, const float* 
 // replacement, which is at most 100 times the current one): x32 += alpha p, r32 -= alpha q
 // as FP32 fused multiply-adds with alpha rounded to FP32, 16-byte accesses, r.r summed per
 // four values in FP32 and accumulated in FP64.
-__global__ void k_pcg_xr32(long long n, float* __restrict__ x32, const float* __restrict__ p,
-                           float* __restrict__ r32, const float* __restrict__ q, PcgState* st, double* part,
-                           unsigned* ticket) {
+//
+// p1 != null: p is one of a ping-pong pair, the one the fused product of this iteration wrote
+// (iteration parity 0: p1, parity 1: p0).
+__global__ void k_pcg_xr32(long long n, float* __restrict__ x32, const float* __restrict__ p0,
+                           const float* __restrict__ p1, float* __restrict__ r32, const float* __restrict__ q,
+                           PcgState* st, double* part, unsigned* ticket) {
   EDGE_PDL_ENTRY();
+  const float* __restrict__ p = (p1 != nullptr && (st->iter & 1) == 0) ? p1 : p0;
   const double alpha = st->rz_new / st->pq;
   const float af = (float)alpha;
   double acc = 0.0;

@@ -257,6 +257,12 @@ struct Prob {
   std::vector<int> level_sweeps;  // per-level sweep counts (pre = post); levels past its end use n_smooth
   int sweeps(int l) const { return l < (int)level_sweeps.size() ? level_sweeps[l] : n_smooth; }
   double omega = 0.5, min_omega = 0.4;
+  // smoother weight across solves: false = reset every solve (the GPU solver), true = carried
+  // over from the previous solve (the CPU solver); omega_started: a solve has run since set
+  bool omega_carry = false, omega_started = false;
+  // mixed path: fused fine launches (first sweep + residual in one launch, the last sweep
+  // without a stored pre-smoothed iterate, the search direction formed inside the product)
+  bool fuse = true;
   bool cycle_w = false;
   std::vector<int> w_levels;
   std::vector<Level> lv;
@@ -690,30 +696,84 @@ static const CUtensorMap& stage_map(Prob& P, const void* base, int t) {
   return P.tmaps.emplace(key, encode_map(base, dt, 4, dims, str, box)).first->second;
 }
 
+// Map of an operator-input array of the cube kernel (u-box geometry, with the halo row):
+// FP32 24 x (4BX+1) x 1 x 3 (the packed-pair u map), BF16 32 x (4BX+1) x 1 x 3.
+template <int BX>
+static const CUtensorMap& in_map(Prob& P, const void* base, int t) {
+  if (t != ST_BF16) return pk_map<BX>(P, (const float*)base, 0);
+  auto key = std::make_pair(base, 5000 + BX);
+  auto it = P.tmaps.find(key);
+  if (it != P.tmaps.end()) return it->second;
+  const Geo& g = P.g0;
+  uint64_t dims[4] = {(uint64_t)g.pz, (uint64_t)g.nx, (uint64_t)g.ny, 3};
+  uint64_t str[3] = {(uint64_t)g.pz * 2, (uint64_t)g.plane * 2, (uint64_t)g.n * 2};
+  uint32_t box[4] = {(uint32_t)st_width(ST_BF16), 4 * BX + 1, 1, 3};
+  return P.tmaps.emplace(key, encode_map(base, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, dims, str, box)).first->second;
+}
+
+// One launch of the cube kernel: input transform IN over arrays in0 (FP32) and in1 (IN::kT1;
+// in1b its second ping-pong buffer, or null), staged epilogue arrays arr[0..SE::kN).
+template <class SE, class IN, int BX, int NS, int MINB>
+static void fine3_cube_go(Prob& P, const float* in0, const void* in1, const void* in1b, const float* E, IN in,
+                          SE epi, const void* const* arr, double* dot_dst) {
+  const Geo& g = P.g0;
+  constexpr int smem = cube_smem_bytes<BX, NS, SE, IN>();
+  static_assert(smem <= 227 * 1024, "cube kernel stage ring exceeds shared memory");
+  static std::atomic<bool> attr{false};  // setting the attribute twice is harmless
+  if (!attr.load()) {
+    CK(cudaFuncSetAttribute(k_fine3_cube<SE, BX, NS, MINB, IN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  const CUtensorMap& m0 = pk_map<BX>(P, in0, 0);
+  const CUtensorMap& m1 = IN::kN == 2 ? in_map<BX>(P, in1, IN::kT1) : m0;
+  const CUtensorMap& m1b = (IN::kN == 2 && in1b) ? in_map<BX>(P, in1b, IN::kT1) : m1;
+  const CUtensorMap* ms[4];
+  for (int i = 0; i < 4; ++i) ms[i] = i < SE::kN ? &stage_map<BX>(P, arr[i], SE::kT(i)) : &m0;
+  const unsigned tz = cdiv(g.nz, 15), tx = cdiv(g.nx, 4 * BX - 1);
+  const long long want = 148LL * P.blocks_per_sm;
+  long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
+  chunks = std::min<long long>(chunks, g.ny);
+  const int ly = (int)cdiv(g.ny, chunks);
+  launch(P, k_fine3_cube<SE, BX, NS, MINB, IN>, dim3(tz, tx, cdiv(g.ny, ly)), dim3(32, BX), smem, g, m0, m1, m1b,
+         pk_flag_map<BX>(P), pk_map<BX>(P, E, 1), (const uint8_t*)P.mask, *ms[0], *ms[1], *ms[2], *ms[3],
+         P.kcube, ly, in, epi, P.part, P.ticket, dot_dst, P.err);
+}
+
 template <class Epi, int BX, int NS, int MINB>
 static void fine3_cube_launch(Prob& P, const float* u, const float* E, Epi epi0, double* dot_dst) {
   using ST = StagedOf<Epi>;
   using SE = typename ST::SE;
   const void* arr[4] = {nullptr, nullptr, nullptr, nullptr};
   SE epi = ST::make(epi0, arr);
-  const Geo& g = P.g0;
-  constexpr int smem = cube_smem_bytes<BX, NS, SE>();
-  static std::atomic<bool> attr{false};  // setting the attribute twice is harmless
-  if (!attr.load()) {
-    CK(cudaFuncSetAttribute(k_fine3_cube<SE, BX, NS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
+  fine3_cube_go<SE, InU, BX, NS, MINB>(P, u, nullptr, nullptr, E, InU{}, epi, arr, dot_dst);
+}
+
+// Whether the fused cube launches (operator input computed from staged arrays) can run.
+static bool cube_fusable(const Prob& P) {
+  return P.fuse && P.dim == 3 && P.use_tma && P.tile_variant >= 9 && P.cube && P.ei.wht;
+}
+
+// A cube-kernel launch with an input transform, on the problem's tile variant; profiled like
+// fine_apply with io_bytes algorithmic bytes per DOF besides E.
+template <class SE, class IN>
+static void fine3_cube_fused(Prob& P, const float* in0, const void* in1, const void* in1b, IN in, SE epi,
+                             const void* const* arr, double* dot_dst, double io_bytes) {
+  CatScope cat(P, CAT_FINE);
+  const bool rec = P.prof && P.pev_used + 2 <= P.pev.size();
+  if (rec) CK(cudaEventRecord(P.pev[P.pev_used], P.stream));
+  switch (P.tile_variant) {
+    case 9: fine3_cube_go<SE, IN, 4, 3, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
+    case 10: fine3_cube_go<SE, IN, 4, 4, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
+    case 11: fine3_cube_go<SE, IN, 2, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
+    case 12: fine3_cube_go<SE, IN, 8, 3, 1>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
+    case 13: fine3_cube_go<SE, IN, 4, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
+    default: fine3_cube_go<SE, IN, 4, 4, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
   }
-  const CUtensorMap& mu = pk_map<BX>(P, u, 0);
-  const CUtensorMap* ms[4];
-  for (int i = 0; i < 4; ++i) ms[i] = i < SE::kN ? &stage_map<BX>(P, arr[i], SE::kT(i)) : &mu;
-  const unsigned tz = cdiv(g.nz, 15), tx = cdiv(g.nx, 4 * BX - 1);
-  const long long want = 148LL * P.blocks_per_sm;
-  long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
-  chunks = std::min<long long>(chunks, g.ny);
-  const int ly = (int)cdiv(g.ny, chunks);
-  launch(P, k_fine3_cube<SE, BX, NS, MINB>, dim3(tz, tx, cdiv(g.ny, ly)), dim3(32, BX), smem, g, mu,
-         pk_flag_map<BX>(P), pk_map<BX>(P, E, 1), u, (const uint8_t*)P.mask, *ms[0], *ms[1], *ms[2], *ms[3],
-         P.kcube, ly, epi, P.part, P.ticket, dot_dst, P.err);
+  if (rec) {
+    CK(cudaEventRecord(P.pev[P.pev_used + 1], P.stream));
+    P.pev_used += 2;
+    P.pbytes.push_back((double)P.n_dof * io_bytes + (double)P.n_el * sizeof(float));
+  }
 }
 
 // Fine-level operator with epilogue.  u, E in type T.  When profiling is on, each launch is
@@ -866,13 +926,18 @@ __global__ void k_copy(long long n, const TI* __restrict__ a, TO* __restrict__ o
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     o[i] = Conv<TO>::from(a[i]);
 }
-__global__ void k_pcg_init(PcgState* st, double tol, int maxiter, double min_omega, double d_omega) {
+// Start of a solve.  keep_omega = 0: the smoother weight starts at omega0 (the GPU solver
+// resets it to min_omega every solve, solvers/_multigrid_cuda.py:210; the CPU solver starts
+// its first solve at the constructor's omega); 1: it keeps the value the previous solve
+// ended with (the CPU solver never resets it, solvers/_multigrid.py:178-225).
+__global__ void k_pcg_init(PcgState* st, double tol, int maxiter, double min_omega, double d_omega, double omega0,
+                           int keep_omega) {
   EDGE_PDL_ENTRY();
   st->tol = tol;
   st->maxiter = maxiter;
   st->min_omega = min_omega;
   st->d_omega = d_omega;
-  st->omega = min_omega;
+  if (!keep_omega) st->omega = omega0;
   st->iter = 0;
   st->done = 0;
   st->rz = st->rz_new = st->pq = st->rr = st->alpha = st->beta = 0.0;
@@ -980,6 +1045,42 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
   T* y = (T*)Lv.xb;
   T* r = (T*)Lv.r;
   const int nsm = P.sweeps(l);
+  const int visits0 =
+      (P.cycle_w && std::find(P.w_levels.begin(), P.w_levels.end(), l) != P.w_levels.end()) ? 2 : 1;
+  if constexpr (std::is_same<T, float>::value && std::is_same<TD0, __nv_bfloat16>::value) {
+    // one sweep on the fine level of the mixed path: the pre-smoothed iterate w Dinv b is
+    // computed inside the two fine launches that need it instead of being stored
+    if (l == 0 && nsm == 1 && visits0 == 1 && cube_fusable(P) && (!dot_dst || (const void*)dotv == (const void*)b)) {
+      {  // r = b - A (w Dinv b)
+        InWDB in{om, ws, 0.f};
+        SEResidIn e{r, g.n};
+        fine3_cube_fused(P, b, Lv.dinv, nullptr, in, e, nullptr, nullptr, 4 + 2 + 4);
+      }
+      Level& Lc = P.lv[1];
+      P.cur_cat = CAT_TRANSFER;
+      launch(P, k_restrict3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g, r,
+             (T*)Lc.b);
+      KCHECK();
+      P.cur_cat = CAT_VECTOR;
+      vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr);
+      T* e1 = (T*)Lv.ea;
+      P.cur_cat = CAT_TRANSFER;
+      launch(P, k_prolong3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g,
+             (const T*)Lc.res, e1);
+      KCHECK();
+      P.cur_cat = CAT_VECTOR;
+      const void* arr[2] = {b, Lv.dinv};  // out = w Dinv b + (e + w Dinv (b - A e)) [, b . out]
+      if (dot_dst) {
+        SEJacobiAdd0<true> e{out, om, ws, g.n, 0.f};
+        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, dot_dst, 4 + 4 + 2 + 4);
+      } else {
+        SEJacobiAdd0<false> e{out, om, ws, g.n, 0.f};
+        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, nullptr, 4 + 4 + 2 + 4);
+      }
+      KCHECK();
+      return;
+    }
+  }
   auto sweep = [&](const T* bb, T* in, T* outv) {
     if (l == 0) {
       EpiJacobi<T, T, TD0> e{bb, (const TD0*)Lv.dinv, outv, om, ws, g.n};
@@ -1114,12 +1215,21 @@ static void mg_allocate(Prob& P) {
 // iteration) or inside one CUDA graph (solve_graph below) whose while node repeats the body
 // and whose if node runs the replacement, so the two drivers execute the same launches.
 //
+// PCG state at the start of a multigrid solve, with the smoother weight of the GPU solver
+// (reset to min_omega) or, with omega_carry, of the CPU solver (omega at the first solve,
+// then whatever the previous solve ended with).
+static void pcg_init(Prob& P, double tol, int maxiter) {
+  const int keep = (P.omega_carry && P.omega_started) ? 1 : 0;
+  const double omega0 = P.omega_carry ? P.omega : P.min_omega;
+  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega, omega0, keep);
+}
+
 // FP64: every level, vector and operator in FP64 (solvers/_multigrid_cuda.py:188-241).
 static void pcg64_prologue(Prob& P, double tol, int maxiter) {
   CatScope cat(P, CAT_VECTOR);
   const Geo& g = P.g0;
   const long long nv = (long long)g.dof * g.n;
-  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
+  pcg_init(P, tol, maxiter);
   {  // r = b - A x
     EpiResid<double, double, double> e{P.b64, P.r64, g.n};
     fine_apply<double>(P, (const double*)P.x64, e, nullptr);
@@ -1154,7 +1264,7 @@ static void cg_prologue(Prob& P, double tol, int maxiter) {
   const Geo& g = P.g0;
   const long long nv = (long long)g.dof * g.n;
   const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
-  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, 0.0, 0.0);
+  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, 0.0, 0.0, 0.0, 0);
   {
     EpiResid<double, double, double> e{P.b64, P.r64, g.n};
     fine_apply<double>(P, (const double*)P.x64, e, nullptr);
@@ -1219,7 +1329,7 @@ static void pcgmx_prologue(Prob& P, double tol, int maxiter) {
   const Geo& g = P.g0;
   const long long nv = (long long)g.dof * g.n;
   const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
-  launch(P, k_pcg_init, 1, 1, 0, P.st, tol, maxiter, P.min_omega, P.omega - P.min_omega);
+  pcg_init(P, tol, maxiter);
   CK(cudaMemsetAsync(P.x32, 0, nv * sizeof(float), P.stream));
   launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.b64, (const double*)P.b64, P.part, P.ticket,
          &P.st->bb);
@@ -1236,6 +1346,18 @@ static void pcgmx_body(Prob& P) {
   float* z = (float*)P.lv[0].res;
   // r.z with the FP32 copy of the residual (the V-cycle's right-hand side), FP64 accumulation
   vcycle<float, __nv_bfloat16, float>(P, 0, P.r32, z, P.r32, &P.st->rz_new);
+  if (P.res32 && P.n_springs == 0 && cube_fusable(P)) {
+    // p = z + beta p_old inside the product (q = A p, p.q); p ping-pongs between the two
+    // FP32 halves of the FP64-sized p buffer by iteration parity, and the x/r update reads
+    // the half the product wrote
+    float* p1 = p + nv;
+    InPDir in{(const PcgState*)P.st, 0.f, 0, false};
+    SEStorePDot e{q, p, p1, (const PcgState*)P.st, g.n, nullptr};
+    fine3_cube_fused(P, (const float*)z, p, p1, in, e, nullptr, &P.st->pq, 4 + 4 + 4 + 4);
+    launch(P, k_pcg_xr32, nb, 256, 0, nv, P.x32, (const float*)p, (const float*)p1, P.r32, (const float*)q, P.st,
+           P.part, P.ticket);
+    return;
+  }
   launch(P, k_pcg_p<float>, ew_blocks(nv), 256, 0, nv, p, (const float*)z, (const PcgState*)P.st);
   {
     EpiStoreDot<float> e{q, g.n};
@@ -1243,7 +1365,8 @@ static void pcgmx_body(Prob& P) {
     springs_apply(P, (const float*)p, q, 1.0, &P.st->pq);
   }
   if (P.res32)  // x32 += alpha p, r32 -= alpha q in FP32
-    launch(P, k_pcg_xr32, nb, 256, 0, nv, P.x32, (const float*)p, P.r32, (const float*)q, P.st, P.part, P.ticket);
+    launch(P, k_pcg_xr32, nb, 256, 0, nv, P.x32, (const float*)p, (const float*)nullptr, P.r32, (const float*)q,
+           P.st, P.part, P.ticket);
   else
     launch(P, k_pcg_xr_lag, nb, 256, 0, nv, P.x32, (const float*)p, P.r64, (const float*)q, P.st, P.part, P.ticket,
            P.r32);
@@ -1320,7 +1443,7 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, boo
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons,
                            (double)P.st_bf16, (double)P.st_pair, (double)P.st_pair_min, (double)P.res32,
-                           (double)P.pdl};
+                           (double)P.pdl, (double)P.fuse, (double)P.omega_carry, (double)(P.omega_carry && P.omega_started)};
   for (int l : P.w_levels) k.push_back((double)l);
   k.push_back(-1.0);
   for (int v : P.level_sweeps) k.push_back((double)v);
@@ -1470,6 +1593,7 @@ static void solve_internal(Prob& P, double tol, int maxiter) {
   if (!P.has_rho) fail(EDGE_ESTATE, "Solver requires a density vector to be passed or set on the kernel.");
   if (P.use_graph && !P.prof && !P.bd) {
     solve_graph(P, tol, maxiter);
+    P.omega_started = true;
     check_err(P);
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, P.ev[0], P.ev[2]));
@@ -1486,6 +1610,7 @@ static void solve_internal(Prob& P, double tol, int maxiter) {
   CK(cudaStreamSynchronize(P.stream));
   if (status) fail(EDGE_ENOTPD, "coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
   pcg_host(P, tol, maxiter);
+  P.omega_started = true;
   CK(cudaEventRecord(P.ev[2], P.stream));
   CK(cudaEventSynchronize(P.ev[2]));
   check_err(P);
@@ -1528,23 +1653,25 @@ struct OcStaticScratch {
 };
 static __device__ __align__(256) OcStaticScratch g_oc_scratch;
 
-// Device address of g_oc_scratch for the current device, looked up once per device (the
-// lookup is the only set-up; the first call on a device performs it).
-static OcStaticScratch* oc_static_scratch() {
-  static std::mutex mu;
-  static OcStaticScratch* addr[128] = {};
+// Device address of g_oc_scratch on the current device, looked up on every call: the lookup
+// is a cheap runtime query that allocates nothing, and an address kept from an earlier call
+// would be stale after a device reset (the module, and with it the array, is loaded again).
+// `stream` must belong to the current device, since the address is that device's.
+static OcStaticScratch* oc_static_scratch(cudaStream_t stream) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 128) fail(EDGE_EINVAL, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_oc_scratch);
-    if (e != cudaSuccess || !ptr)
-      fail(EDGE_ECUDA, std::string("cudaGetSymbolAddress(OC workspace): ") + cudaGetErrorString(e));
-    addr[dev] = static_cast<OcStaticScratch*>(ptr);
+  if (stream != nullptr && stream != cudaStreamLegacy && stream != cudaStreamPerThread) {
+    int sdev = -1;
+    CK(cudaStreamGetDevice(stream, &sdev));
+    if (sdev != dev)
+      fail(EDGE_EINVAL, "stream belongs to device " + std::to_string(sdev) + ", the current device is " +
+                            std::to_string(dev));
   }
-  return addr[dev];
+  void* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_oc_scratch);
+  if (e != cudaSuccess || !ptr)
+    fail(EDGE_ECUDA, std::string("cudaGetSymbolAddress(OC workspace): ") + cudaGetErrorString(e));
+  return static_cast<OcStaticScratch*>(ptr);
 }
 
 // Start state of one OC update: bracket [1e-9, 1e9] (TopOpt/_cuda.py:260-261), counter zero.
@@ -1705,6 +1832,14 @@ int edge_mg_set_sweeps(edge_problem* p, const int* sweeps, int n) {
   API_END
 }
 
+int edge_mg_set_omega_carry(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.omega_carry = enable != 0;
+  p->P.omega_started = false;
+  API_END
+}
+
 int edge_launch_count(const edge_problem* p, long long* n) {
   API_BEGIN
   if (!p || !n) fail(EDGE_EINVAL, "null argument");
@@ -1738,6 +1873,13 @@ int edge_set_pdl(edge_problem* p, int enable) {
   API_BEGIN
   if (!p) fail(EDGE_EINVAL, "null handle");
   p->P.pdl = enable != 0;
+  API_END
+}
+
+int edge_set_fuse(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.fuse = enable != 0;
   API_END
 }
 
@@ -2454,8 +2596,8 @@ int edge_oc_update_static(long long n, const double* rho_dev, const double* dr_d
   if (n > OC_STATIC_MAX_EL)
     fail(EDGE_EINVAL, "n = " + std::to_string(n) + " elements exceeds the fixed OC workspace (at most " +
                           std::to_string(OC_STATIC_MAX_EL) + " elements); use edge_oc_update");
-  OcStaticScratch* s = oc_static_scratch();
   cudaStream_t st = (cudaStream_t)stream;
+  OcStaticScratch* s = oc_static_scratch(st);
   const unsigned nb = std::min<unsigned>(ew_blocks(n), OC_STATIC_MAX_BLOCKS);
   k_oc_static_init<<<1, 1, 0, st>>>(s, vf, vol);
   k_oc_prep<<<nb, 256, 0, st>>>(n, rho_dev, dr_dev, A, s->ocp, s->part, &s->ticket, &s->scal[0]);

@@ -109,7 +109,7 @@ class _PaddedGrid:
         return v[self.dof_map]
 
 
-def pick_sweep_pattern(runs, retime, margin):
+def pick_sweep_pattern(runs, retime, margin, fallback=None):
     """Choice of the sweep autotuner among converged runs [ms, pattern, pcg_iters].
 
     The fastest pattern and the cheapest one (fewest sweeps) are timed again with
@@ -117,7 +117,9 @@ def pick_sweep_pattern(runs, retime, margin):
     pattern with more sweeps must beat the cheapest by ``margin`` (best < margin * cheapest):
     the iterations that extra sweeps save shrink as the SIMP design sharpens (at 12.8M DOF:
     17 % fewer PCG iterations in the first timed SIMP step, 5 % in the fifth), so near-ties on
-    the early tuning solve go to fewer sweeps.  Returns (ms summed, pattern, iters)."""
+    the early tuning solve go to fewer sweeps.  When no contender converges again on its
+    retime, returns ``(0.0, fallback, 0)`` (the reference's sweeps), as when nothing converged
+    at all.  Returns (ms summed, pattern, iters)."""
     runs = sorted(([float(r[0]), list(r[1]), r[2]] for r in runs), key=lambda r: r[0])
     cheap = min(runs, key=lambda r: (sum(r[1]), r[1]))
     contenders = [runs[0]] if runs[0] is cheap else [runs[0], cheap]
@@ -127,15 +129,24 @@ def pick_sweep_pattern(runs, retime, margin):
     best = contenders[0]
     if len(contenders) == 2 and not best[0] < margin * cheap[0]:
         best = cheap
+    if best[0] == float("inf") and fallback is not None:
+        return (0.0, list(fallback), 0)
     return tuple(best)
 
 
 class CuMultiGrid(Solver):
+    OMEGA_CARRY = False
+
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="splu", matrix_free=False, low_level_tol=1e-8, low_level_maxiter=5000,
-                 min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True, graph=True, tune_sweeps=None):
+                 min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True, graph=True, tune_sweeps=None,
+                 omega_carry=None):
         if not isinstance(kernel, CuStructuredStiffnessKernel):
             raise TypeError("CuMultiGrid needs the package's CuStructuredStiffnessKernel")
+        # smoother weight across solves: reset to min_omega every solve (the GPU solver,
+        # solvers/_multigrid_cuda.py:210) or carried over from the last solve (the CPU solver,
+        # solvers/_multigrid.py:178-225; the MultiGrid class below)
+        self.omega_carry = self.OMEGA_CARRY if omega_carry is None else bool(omega_carry)
         self.kernel = kernel
         self.mesh = mesh
         self.last_x0 = None
@@ -184,7 +195,8 @@ class CuMultiGrid(Solver):
             self._inner = CuMultiGrid(self._pad.kernel.mesh, self._pad.kernel, maxiter=maxiter, tol=tol,
                                       n_smooth=n_smooth, omega=omega, n_level=n_level, cycle=cycle, w_level=w_level,
                                       min_omega=min_omega, omega_boost=omega_boost, precision=precision,
-                                      autotune=autotune, graph=graph, tune_sweeps=tune_sweeps)
+                                      autotune=autotune, graph=graph, tune_sweeps=tune_sweeps,
+                                      omega_carry=self.omega_carry)
 
     def reset(self):
         self.last_x0 = None
@@ -201,6 +213,8 @@ class CuMultiGrid(Solver):
         _lib.call("edge_mg_config", self.kernel.handle, int(self.n_level), int(self.n_smooth), float(self.max_omega),
                   float(self.min_omega), 1 if self.cycle == "w" else 0, w, len(self.w_level), prec)
         _lib.call("edge_set_graph", self.kernel.handle, 1 if self.graph else 0)
+        if self._configured is None:
+            _lib.call("edge_mg_set_omega_carry", self.kernel.handle, 1 if self.omega_carry else 0)
         self._configured = key
 
     def tune(self):
@@ -263,7 +277,7 @@ class CuMultiGrid(Solver):
         if not runs:  # nothing converged within maxiter: keep the reference's sweeps
             best = (0.0, [self.n_smooth] * self.n_level, 0)
         else:
-            best = pick_sweep_pattern(runs, timed_solve, self.SWEEP_MARGIN)
+            best = pick_sweep_pattern(runs, timed_solve, self.SWEEP_MARGIN, fallback=[self.n_smooth] * self.n_level)
         _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(best[1]), len(best[1]))
         self.sweeps = {"per_level": best[1], "solve_ms": best[0] / (2 if runs else 1), "pcg_iters": best[2],
                        "tune_tol": tol, "candidates": candidates}
@@ -322,7 +336,14 @@ class CuMultiGrid(Solver):
         return {"setup_ms": a.value, "solve_ms": b.value, "pcg_iters": i.value, "true_residuals": t.value}
 
 
-MultiGrid = CuMultiGrid
+class MultiGrid(CuMultiGrid):
+    """The reference's CPU multigrid solver (solvers/_multigrid.py:11-230) on the GPU: the same
+    algorithm as CuMultiGrid except for the smoother weight, which the CPU solver starts at
+    ``omega`` and never resets between solves (CuMultiGrid resets it to ``min_omega`` at
+    every solve, as the CuPy solver does), so its PCG iterates are those of the CPU solver.
+    In 3-D the two reference solvers' transfers are the same; in 2-D the CPU restriction
+    differs from the GPU one (core/_mgm.py:159-160) and this class keeps the GPU one."""
+    OMEGA_CARRY = True
 
 
 class CuCG(Solver):

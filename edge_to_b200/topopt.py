@@ -139,9 +139,11 @@ class CuTopOpt:
         return self._update_design_generic(rho, df)
 
     def _update_design_generic(self, rho, df):
-        """OC with one bisection multiplier per design column (TopOpt/_cuda.py:242-280): every
-        column keeps bisecting until its own (l2 - l1) / (l2 + l1) <= 1e-4, on the material
-        model's ocP and constraint test.  Multi-material designs are (n_el, n_sets)."""
+        """OC with one bisection multiplier per design column (TopOpt/_cuda.py:242-280): all
+        columns are bisected together until every column satisfies (l2 - l1) / (l2 + l1) <= 1e-4
+        (the reference's np.any test, TopOpt/_cuda.py:270), so a column that has converged keeps
+        bisecting while another has not; on the material model's ocP and constraint test.
+        Multi-material designs are (n_el, n_sets)."""
         size = self.n_sets
         rho = rho.reshape(-1, size)
         df = df.reshape(-1, size)

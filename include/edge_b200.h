@@ -102,6 +102,19 @@ int edge_cg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_l
  * reference smooths every level n_smooth times (solvers/_multigrid_cuda.py:133-186); this
  * is the knob the sweep autotuner of the mixed-precision solver turns. */
 int edge_mg_set_sweeps(edge_problem* p, const int* sweeps, int n);
+/* Smoother weight across solves.  enable = 0 (default): every solve starts at min_omega, as
+ * the GPU solver does (CuMultiGrid.solve, solvers/_multigrid_cuda.py:210).  enable = 1: the
+ * first solve after this call starts at edge_mg_config's omega and every later solve keeps
+ * the weight the previous one ended with, as the CPU solver does (MultiGrid.__init__ and
+ * MultiGrid.solve, solvers/_multigrid.py:11-30, 178-225), so the iterates are the CPU
+ * solver's. */
+int edge_mg_set_omega_carry(edge_problem* p, int enable);
+/* Mixed precision, 3-D cube elements: 1 (default) fuses the fine level's work into fewer
+ * launches when the level smooths once - the first damped-Jacobi sweep from zero is computed
+ * inside the residual launch and again inside the last sweep instead of being stored, and the
+ * PCG search direction p = z + beta p is formed inside the product q = A p; 0 runs the same
+ * arithmetic as separate launches.  No counterpart in the reference. */
+int edge_set_fuse(edge_problem* p, int enable);
 /* Kernel launches made through this problem so far (a launch inside a graph counts once per
  * execution; edge_profile_begin resets the tally). */
 int edge_launch_count(const edge_problem* p, long long* n);
@@ -194,9 +207,10 @@ int edge_oc_update(edge_problem* p, const double* rho_dev, const double* dr_dev,
  * creating an edge_problem (which allocates the multigrid workspaces) is not wanted.
  * No counterpart in the reference.  n elements of uniform measure A, on `stream`.
  * It allocates nothing: its workspace is a fixed 8.1 MiB device array inside the library,
- * so n is limited to 1,048,576 elements (larger n: EDGE_EINVAL; use edge_oc_update).  The
- * first call on a device looks up that array's address; make that first call before any
- * stream capture.  The call zeroes the workspace's reduction counter itself; nothing has to
+ * so n is limited to 1,048,576 elements (larger n: EDGE_EINVAL; use edge_oc_update).  Every
+ * call looks up that array's address on the current device (a runtime query, no
+ * allocation); `stream` must belong to the current device (otherwise EDGE_EINVAL).  The call
+ * waits for `stream` before it returns.  It zeroes the workspace's reduction counter itself; nothing has to
  * be initialised by the caller.  There is one workspace per device: calls whose work
  * overlaps on the same device (different streams or host threads) race and give wrong
  * results, so order them on one stream or synchronise between them.  Results equal

@@ -11,7 +11,8 @@ reference is copied or modified; only its CPU classes are exercised:
 (core/_mgm.py), ``SingleMaterial`` (MaterialModels.py:31-99) and ``TopOpt``
 (TopOpt/_solver.py:17-417).
 
-Run from the repository root with the reference checked out at REFERENCE_ROOT:
+Run from the repository root with the reference checked out at REFERENCE_ROOT (the
+EDGETO_REFERENCE environment variable, else a folder "reference" beside the repository):
 
     NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py [--only NAME]
 
@@ -22,6 +23,9 @@ Outputs (all small .npz files, committed):
                       Galerkin level-1 and level-2 operators, OC update
   loop_mbb2d.npz      120x40 MBB half-beam, 100 SIMP iterations, MG-PCG rtol 1e-8
   loop_cant3d.npz     64x32x32 cantilever, first SIMP iterations, 4-level MG rtol 1e-6
+  loop_cant3d_50.npz  the same cantilever, 50 SIMP iterations, 4-level MG rtol 1e-6
+  loop_cant3d_50t.npz the same 50 iterations with the solves at rtol 1e-10 (the trajectory of
+                      (nearly) exact solves)
   grad_cant3d.npz     32x16x16 cantilever, random rho, compliance and filtered dr
   fea.npz             FEA_integrals, op level and the whole call
   multimaterial.npz   PenalizedMultiMaterial law: forward, plain, backward, constraint, ocP
@@ -37,8 +41,10 @@ from unittest import mock
 
 import numpy as np
 
-REFERENCE_ROOT = os.environ.get("EDGETO_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference checkout: EDGETO_REFERENCE, else a sibling "reference" folder of the repository
+REFERENCE_ROOT = os.environ.get("EDGETO_REFERENCE",
+                                os.path.normpath(os.path.join(HERE, "..", "..", "..", "reference")))
 
 
 def _import_reference():
@@ -216,7 +222,7 @@ class _Recorder:
         solver.solve = recording_solve
 
 
-def _run_loop(mesh, vf, rmin, rho0, n_iter, mg_kwargs, bc_fn, f_fn):
+def _run_loop(mesh, vf, rmin, rho0, n_iter, mg_kwargs, bc_fn, f_fn, keep_rho=None):
     ref = _REF
     mat = ref.SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=vf)
     mat.init_desvars = lambda nel, **kw: np.full(nel, rho0, dtype=np.float64)
@@ -233,6 +239,21 @@ def _run_loop(mesh, vf, rmin, rho0, n_iter, mg_kwargs, bc_fn, f_fn):
     t0 = time.time()
     rho, flag, hist = opt.optimize(save_comp_history=True, save_change_history=True, save_rho_history=True)
     dt = time.time() - t0
+    if keep_rho is not None:  # a few designs only: the whole history would be tens of MB
+        out = {
+            "rho_final": rho,
+            "comp_history": np.array(hist["comp_history"]),
+            "change_history": np.array(hist["change_history"]),
+            "residuals": np.array(rec.residuals),
+            "matvecs_per_solve": np.array(rec.matvecs),
+            "f_idx": np.nonzero(opt.f)[0],
+            "f_val": opt.f[np.nonzero(opt.f)[0]],
+            "constraints": np.where(k.constraints)[0],
+            "wall_s": np.array(dt),
+        }
+        for i in keep_rho:
+            out[f"rho_{i}"] = hist["rho_history"][i - 1]
+        return out
     out = {
         "rho_final": rho,
         "comp_history": np.array(hist["comp_history"]),
@@ -292,6 +313,26 @@ def make_loop_cant3d():
     out = _run_loop(mesh, 0.12, 1.5, 0.12, 4, dict(tol=1e-6, n_level=4, maxiter=1000), bc, force)
     np.savez_compressed(os.path.join(HERE, "loop_cant3d.npz"), **out)
     print("cant3d: comp", out["comp_history"], "wall", out["wall_s"])
+
+
+def _loop_cant3d_50(tol, name):
+    """64x32x32 cantilever, 50 SIMP iterations (TopOpt/_solver.py:336-417), 4-level MG at the
+    given rtol; keeps the compliance history, the final design, the design after 10 and 25
+    iterations and the per-solve matvec counts (a few hundred KB)."""
+    ref = _REF
+    mesh = ref.StructuredMesh3D(64, 32, 32, 64.0, 32.0, 32.0, stiffness=_stiff(0.3))
+    bc, force = _cant_bc_force(64.0)
+    out = _run_loop(mesh, 0.12, 1.5, 0.12, 50, dict(tol=tol, n_level=4, maxiter=4000), bc, force, keep_rho=(10, 25))
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, "comp", out["comp_history"][[0, 9, 24, 49]], "wall", out["wall_s"])
+
+
+def make_loop_cant3d_50():
+    _loop_cant3d_50(1e-6, "loop_cant3d_50.npz")
+
+
+def make_loop_cant3d_50t():
+    _loop_cant3d_50(1e-10, "loop_cant3d_50t.npz")
 
 
 def make_grad():
@@ -501,7 +542,8 @@ if __name__ == "__main__":
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
     _REF = _import_reference()
-    jobs = {"kat": make_kat, "ops": make_ops, "mbb": make_loop_mbb, "cant": make_loop_cant3d, "grad": make_grad,
+    jobs = {"kat": make_kat, "ops": make_ops, "mbb": make_loop_mbb, "cant": make_loop_cant3d,
+            "cant50": make_loop_cant3d_50, "cant50t": make_loop_cant3d_50t, "grad": make_grad,
             "fea": make_fea, "mm": make_multimaterial, "general": make_general}
     for name, fn in jobs.items():
         if args.only and name not in args.only.split(","):

@@ -408,6 +408,46 @@ def test_graph_and_host_loop_agree(precision):
     assert r2 < 1e-6 and s.last_iters < it1
 
 
+def test_fused_fine_launches_agree():
+    """Mixed precision with the cube kernel and one sweep per level: the fused fine launches
+    (the first Jacobi sweep computed inside the residual launch and the last-sweep launch, the
+    search direction formed inside the product with p ping-ponging between two buffers by
+    iteration parity) against the same arithmetic as separate launches: iteration counts
+    within 2, both solutions within the tolerance of the FP64 solve; the fused graph solve
+    and the fused host-driven loop are the same launches (identical iterates)."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(13)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    mesh = _mesh(3, (32, 16, 16), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    f = torch.as_tensor(p.f, device="cuda")
+    s64 = eb.CuMultiGrid(mesh, k, tol=1e-11, n_level=3, maxiter=2000, precision="fp64", autotune=False)
+    x64 = s64.solve(f, use_last=False)[0].cpu().numpy().copy()
+    out = {}
+    for fuse, graph in ((0, True), (1, True), (1, False)):
+        s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision="mixed", autotune=False,
+                           tune_sweeps=False, graph=graph)
+        s._configure()
+        _lib.call("edge_set_fine_tile", k.handle, 10, 8)
+        _lib.call("edge_mg_set_sweeps", k.handle, _lib.int_array([1, 1, 1]), 3)
+        _lib.call("edge_set_fuse", k.handle, fuse)
+        x, r = s.solve(f, use_last=False)
+        out[(fuse, graph)] = (x.cpu().numpy().copy(), s.last_iters, r)
+    _lib.call("edge_set_fuse", k.handle, 1)
+    (xu, iu, ru), (xf, i_f, rf), (xh, ih, rh) = out[(0, True)], out[(1, True)], out[(1, False)]
+    print("iterations unfused / fused / fused host loop", iu, i_f, ih)
+    assert ru < 1e-8 and rf < 1e-8 and rh < 1e-8
+    assert abs(iu - i_f) <= 2 and i_f > 3
+    assert rel(xu, x64) < 1e-6 and rel(xf, x64) < 1e-6
+    assert ih == i_f and rel(xh, xf) < 1e-12
+
+
 def test_residual_recurrence_precisions_agree():
     """Mixed precision with the residual recurrence stored in FP32 (default) and in FP64: both
     meet the tolerance on the FP64 true residual, take about the same iterations and give the

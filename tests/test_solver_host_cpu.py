@@ -29,3 +29,17 @@ def test_sweep_choice_tie_goes_to_fewer_sweeps():
     assert best[1] == [1, 1, 1]
     # the input list is not modified
     assert runs[0][0] == 100.0
+
+
+def test_sweep_choice_falls_back_when_no_contender_converges_again():
+    m = CuMultiGrid.SWEEP_MARGIN
+    fallback = [3, 3, 3]
+    # the only contender (fastest = cheapest) fails on its retime
+    runs = [[100.0, [1, 1, 1], 10], [120.0, [2, 2, 2], 8]]
+    best = pick_sweep_pattern(runs, _retime({(1, 1, 1): 100.0}, fail={(1, 1, 1)}), m, fallback=fallback)
+    assert best == (0.0, [3, 3, 3], 0)
+    # both contenders fail on their retimes
+    runs = [[100.0, [1, 1, 1], 10], [60.0, [2, 2, 2], 8]]
+    best = pick_sweep_pattern(runs, _retime({(1, 1, 1): 100.0, (2, 2, 2): 60.0}, fail={(1, 1, 1), (2, 2, 2)}), m,
+                              fallback=fallback)
+    assert best == (0.0, [3, 3, 3], 0)
