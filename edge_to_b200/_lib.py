@@ -49,6 +49,21 @@ _SIGS = {
     "edge_mg_set_sweeps": (ctypes.c_int, [vp, c_int_p, ctypes.c_int]),
     "edge_mg_set_omega_carry": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_fuse": (ctypes.c_int, [vp, ctypes.c_int]),
+    "edge_gen_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, c_int_p, c_int_p, c_double_p,
+                                       ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(vp)]),
+    "edge_gen_destroy": (ctypes.c_int, [vp]),
+    "edge_gen_set_stream": (ctypes.c_int, [vp, vp]),
+    "edge_gen_set_rho": (ctypes.c_int, [vp, vp]),
+    "edge_gen_set_constraints": (ctypes.c_int, [vp, vp]),
+    "edge_gen_matvec": (ctypes.c_int, [vp, vp, vp]),
+    "edge_gen_diagonal": (ctypes.c_int, [vp, vp]),
+    "edge_gen_process_grad": (ctypes.c_int, [vp, vp, vp]),
+    "edge_gen_cg_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_double_p,
+                                         c_int_p]),
+    "edge_csr_create": (ctypes.c_int, [ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong), c_int_p, c_double_p,
+                                       ctypes.POINTER(vp)]),
+    "edge_csr_destroy": (ctypes.c_int, [vp]),
+    "edge_csr_apply": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
     "edge_fea_integrals": (ctypes.c_int, [vp, vp, vp, vp, vp, ctypes.c_int, vp, vp, vp]),
     "edge_cg_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_double_p, c_int_p]),
     "edge_launch_count": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
@@ -74,6 +89,10 @@ _SIGS = {
     "edge_simp_solve_and_process": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_double, vp, vp, ctypes.c_int,
                                                    ctypes.c_double, ctypes.c_int, c_double_p, vp, vp, c_double_p,
                                                    c_int_p]),
+    "edge_simp_iteration": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int, vp, vp, vp, c_double_p, c_double_p, c_int_p,
+                                           c_double_p, c_int_p, c_double_p]),
     "edge_last_solve_stats": (ctypes.c_int, [vp, c_double_p, c_double_p, c_int_p, c_int_p]),
     "edge_profile_begin": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_breakdown_begin": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -265,28 +265,30 @@ struct SEResidIn {
 };
 
 // Last post-smoothing sweep of a one-sweep fine level with the correction, where the
-// pre-smoothed iterate was never stored: xo = w Dinv b + (e + w Dinv (b - A e)), e = u; with
-// DOT, acc += b . xo (the PCG's r.z: b is the FP32 residual).  The same arithmetic, in the same
-// order, as the stored-iterate path (k_jacobi0 followed by SEJacobiAdd).
+// pre-smoothed iterate was never stored: xo = w Dinv b + (e + w Dinv (r - A e)), e = u, r the
+// level's residual (the correction equation's right-hand side) and b the V-cycle's right-hand
+// side; with DOT, acc += b . xo (the PCG's r.z: b is the FP32 residual).  The same arithmetic,
+// in the same order, as the stored-iterate path (k_jacobi0 followed by SEJacobiAdd).
 template <bool DOT> struct SEJacobiAdd0 {
   float* xo;
   const double* omega;
   double wscale;
   long long n;
   float w;
-  static constexpr int kN = 2;
+  static constexpr int kN = 3;
   static constexpr bool kDot = DOT;
-  EDGE_HD static constexpr int kT(int i) { return i == 1 ? ST_BF16 : ST_F32; }
+  EDGE_HD static constexpr int kT(int i) { return i == 1 ? ST_BF16 : ST_F32; }  // r, Dinv, b
   struct In {
-    float b[3], d[3];
+    float r[3], d[3], b[3];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
   EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
+      v.r[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
       v.d[c] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(sp[1])[c * cs2]);
+      v.b[c] = reinterpret_cast<const float*>(sp[2])[c * cs4];
     }
     return v;
   }
@@ -294,7 +296,7 @@ template <bool DOT> struct SEJacobiAdd0 {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float xb = (w * v.d[c]) * v.b[c];
-      const float x = xb + (own[c] + w * v.d[c] * (v.b[c] - Au[c]));
+      const float x = xb + (own[c] + w * v.d[c] * (v.r[c] - Au[c]));
       xo[c * n + s] = x;
       if constexpr (DOT) acc += (double)v.b[c] * (double)x;
     }

@@ -867,6 +867,24 @@ __global__ void k_oc_final(long long n, const double* __restrict__ rho, const do
   grid_reduce_finish(bt, part, ticket, DotSink{chg_dst});
 }
 
+// Start state of one OC bisection on the device: bracket [1e-9, 1e9] (TopOpt/_cuda.py:260-261).
+__global__ void k_oc_state_init(OcState* st, double vf, double vol) {
+  EDGE_PDL_ENTRY();
+  OcState init{};
+  init.l1 = 1e-9;
+  init.l2 = 1e9;
+  init.last = 0.5 * (init.l1 + init.l2);
+  init.vf = vf;
+  init.vol = vol;
+  *st = init;
+}
+// Condition of the OC loop inside a graph: bisect again while the bracket is open and fewer
+// than max_steps bisection steps ran (the bound of the host loop).
+__global__ void k_cond_oc(cudaGraphConditionalHandle h, const OcState* st, int max_steps) {
+  EDGE_PDL_ENTRY();
+  cudaGraphSetConditional(h, (st->done == 0 && st->steps < max_steps) ? 1u : 0u);
+}
+
 // Multi-material SIMP law (PenalizedMultiMaterial, MaterialModels.py:102-205).  rho is the
 // n_el x n_mat row-major design of the reference.  With c_m = clip(rho_m, void, 1),
 // a_m = c_m^p and b_m = 1 - a_m:

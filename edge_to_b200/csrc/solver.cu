@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <atomic>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <cmath>
 #include <cstring>
@@ -27,6 +28,7 @@
 #include "fine_tma.cuh"
 #include "fine_pk.cuh"
 #include "fine_cube.cuh"
+#include "general.cuh"
 #include "misc.cuh"
 
 namespace edge {
@@ -238,6 +240,12 @@ struct Prob {
   bool use_graph = true;
   cudaGraph_t sg_graph = nullptr;
   cudaGraphExec_t sg_exec = nullptr;
+  // one SIMP iteration (OC update + analysis) as one graph over owned buffers
+  cudaGraph_t it_graph = nullptr;
+  cudaGraphExec_t it_exec = nullptr;
+  std::vector<double> it_key;
+  long long it_fixed = 0, it_oc_body = 0, it_body = 0, it_rep = 0;
+  double *it_rho = nullptr, *it_dr = nullptr, *it_rho_new = nullptr, *it_dr_new = nullptr;
   std::vector<double> sg_key;
   long long sg_pro = 0, sg_body = 0, sg_if = 0;  // launches per section, for the launch tally
   cudaStream_t cap[3] = {nullptr, nullptr, nullptr};
@@ -315,6 +323,8 @@ struct Prob {
   ~Prob() {
     if (sg_exec) cudaGraphExecDestroy(sg_exec);
     if (sg_graph) cudaGraphDestroy(sg_graph);
+    if (it_exec) cudaGraphExecDestroy(it_exec);
+    if (it_graph) cudaGraphDestroy(it_graph);
     for (int i = 0; i < 3; ++i)
       if (cap[i]) cudaStreamDestroy(cap[i]);
     for (void* a : allocs) cudaFree(a);
@@ -1069,13 +1079,13 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
              (const T*)Lc.res, e1);
       KCHECK();
       P.cur_cat = CAT_VECTOR;
-      const void* arr[2] = {b, Lv.dinv};  // out = w Dinv b + (e + w Dinv (b - A e)) [, b . out]
+      const void* arr[3] = {r, Lv.dinv, b};  // out = w Dinv b + (e + w Dinv (r - A e)) [, b . out]
       if (dot_dst) {
         SEJacobiAdd0<true> e{out, om, ws, g.n, 0.f};
-        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, dot_dst, 4 + 4 + 2 + 4);
+        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, dot_dst, 4 + 4 + 2 + 4 + 4);
       } else {
         SEJacobiAdd0<false> e{out, om, ws, g.n, 0.f};
-        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, nullptr, 4 + 4 + 2 + 4);
+        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, nullptr, 4 + 4 + 2 + 4 + 4);
       }
       KCHECK();
       return;
@@ -1454,100 +1464,121 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, boo
 // whose body holds, for mixed precision, the replacement as an if node) into P.sg_exec.
 // Captured on the library's own streams so that the caller's stream may be the legacy
 // default stream; touches only buffers the problem owns.
-static void capture_solve(Prob& P, double tol, int maxiter, bool cg = false) {
+// Launch counts of one captured solve, for the launch tally of a graph execution: prologue
+// and epilogue once, the loop body per iteration, the replacement per true residual.
+struct SolveCounts {
+  long long pro = 0, body = 0, rep = 0;
+};
+
+// Appends one solve (hierarchy set-up, PCG prologue, the iteration loop as a while node whose
+// body holds, for mixed precision, the replacement as an if node, the epilogue) to the
+// capture open on P.cap[0] (P.stream == P.cap[0]).  `depth` tracks the captures open (for
+// the caller's clean-up on error).
+static SolveCounts capture_solve_into(Prob& P, double tol, int maxiter, bool cg, int& depth) {
   const bool mixed = !cg && P.prec != EDGE_FP64;
-  for (int i = 0; i < 3; ++i)
-    if (!P.cap[i]) CK(cudaStreamCreateWithFlags(&P.cap[i], cudaStreamNonBlocking));
-  if (P.sg_exec) {
-    CK(cudaGraphExecDestroy(P.sg_exec));
-    P.sg_exec = nullptr;
-  }
-  if (P.sg_graph) {
-    CK(cudaGraphDestroy(P.sg_graph));
-    P.sg_graph = nullptr;
-  }
-  cudaStream_t user = P.stream;
   const long long n0 = P.nlaunch;
   long long n1 = 0, n2 = 0, n3 = 0, n4e = 0;
-  int depth = 0;  // captures open
+  if (cg)
+    cg_prologue(P, tol, maxiter);
+  else {
+    mg_setup_prec(P);
+    if (mixed)
+      pcgmx_prologue(P, tol, maxiter);
+    else
+      pcg64_prologue(P, tol, maxiter);
+  }
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g;
+  const cudaGraphNode_t* deps;
+  size_t nd;
+  CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &g, &deps, &nd));
+  cudaGraphConditionalHandle hw;
+  CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
+  launch(P, k_cond_while, 1, 1, 0, hw, (const PcgState*)P.st);
+  n1 = P.nlaunch;
+  CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hw;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  CK(cudaGraphAddNode(&wnode, g, deps, nd, &wp));
+  CK(cudaStreamUpdateCaptureDependencies(P.cap[0], &wnode, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  P.stream = P.cap[1];
+  CK(cudaStreamBeginCaptureToGraph(P.cap[1], body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  depth = 2;
+  if (mixed) {
+    pcgmx_body(P);
+    cudaGraph_t gb;
+    CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
+    cudaGraphConditionalHandle hr;
+    CK(cudaGraphConditionalHandleCreate(&hr, gb, 0, cudaGraphCondAssignDefault));
+    launch(P, k_cond_replace, 1, 1, 0, hr, (const PcgState*)P.st, REPLACE_DROP);
+    CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = hr;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    CK(cudaGraphAddNode(&inode, gb, deps, nd, &ip));
+    CK(cudaStreamUpdateCaptureDependencies(P.cap[1], &inode, 1, cudaStreamSetCaptureDependencies));
+    n2 = P.nlaunch;
+    P.stream = P.cap[2];
+    CK(cudaStreamBeginCaptureToGraph(P.cap[2], ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    depth = 3;
+    pcgmx_replace(P);
+    CK(cudaStreamEndCapture(P.cap[2], nullptr));
+    depth = 2;
+    n3 = P.nlaunch;
+    P.stream = P.cap[1];
+  } else if (cg) {
+    cg_body(P);
+  } else {
+    pcg64_body(P);
+  }
+  launch(P, k_cond_while, 1, 1, 0, hw, (const PcgState*)P.st);
+  CK(cudaStreamEndCapture(P.cap[1], nullptr));
+  depth = 1;
+  P.stream = P.cap[0];
+  n4e = P.nlaunch;
+  if (cg) cg_epilogue(P);
+  if (mixed) pcgmx_fold(P);
+  const long long n5 = P.nlaunch;
+  SolveCounts c;
+  c.pro = (n1 - n0) + (n5 - n4e);
+  if (mixed) {
+    c.rep = n3 - n2;
+    c.body = (n2 - n1) + (n4e - n3);
+  } else {
+    c.body = n4e - n1;
+  }
+  return c;
+}
+
+// Runs `record` inside a capture of the library's own streams (the caller's stream may be the
+// legacy default stream) into a new graph; on any error every capture still open is ended
+// and the state restored before the error propagates.
+template <class F>
+static cudaGraph_t capture_graph(Prob& P, F record) {
+  for (int i = 0; i < 3; ++i)
+    if (!P.cap[i]) CK(cudaStreamCreateWithFlags(&P.cap[i], cudaStreamNonBlocking));
+  cudaStream_t user = P.stream;
+  const long long n0 = P.nlaunch;
+  int depth = 0;
+  cudaGraph_t graph = nullptr;
   try {
     P.stream = P.cap[0];
     P.capturing = true;
     CK(cudaStreamBeginCapture(P.cap[0], cudaStreamCaptureModeThreadLocal));
     depth = 1;
-    if (cg)
-      cg_prologue(P, tol, maxiter);
-    else {
-      mg_setup_prec(P);
-      if (mixed)
-        pcgmx_prologue(P, tol, maxiter);
-      else
-        pcg64_prologue(P, tol, maxiter);
-    }
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t g;
-    const cudaGraphNode_t* deps;
-    size_t nd;
-    CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &g, &deps, &nd));
-    cudaGraphConditionalHandle hw;
-    CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
-    launch(P, k_cond_while, 1, 1, 0, hw, (const PcgState*)P.st);
-    n1 = P.nlaunch;
-    CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &g, &deps, &nd));
-    cudaGraphNodeParams wp = {};
-    wp.type = cudaGraphNodeTypeConditional;
-    wp.conditional.handle = hw;
-    wp.conditional.type = cudaGraphCondTypeWhile;
-    wp.conditional.size = 1;
-    cudaGraphNode_t wnode;
-    CK(cudaGraphAddNode(&wnode, g, deps, nd, &wp));
-    CK(cudaStreamUpdateCaptureDependencies(P.cap[0], &wnode, 1, cudaStreamSetCaptureDependencies));
-    cudaGraph_t body = wp.conditional.phGraph_out[0];
-    P.stream = P.cap[1];
-    CK(cudaStreamBeginCaptureToGraph(P.cap[1], body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    depth = 2;
-    if (mixed) {
-      pcgmx_body(P);
-      cudaGraph_t gb;
-      CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
-      cudaGraphConditionalHandle hr;
-      CK(cudaGraphConditionalHandleCreate(&hr, gb, 0, cudaGraphCondAssignDefault));
-      launch(P, k_cond_replace, 1, 1, 0, hr, (const PcgState*)P.st, REPLACE_DROP);
-      CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
-      cudaGraphNodeParams ip = {};
-      ip.type = cudaGraphNodeTypeConditional;
-      ip.conditional.handle = hr;
-      ip.conditional.type = cudaGraphCondTypeIf;
-      ip.conditional.size = 1;
-      cudaGraphNode_t inode;
-      CK(cudaGraphAddNode(&inode, gb, deps, nd, &ip));
-      CK(cudaStreamUpdateCaptureDependencies(P.cap[1], &inode, 1, cudaStreamSetCaptureDependencies));
-      n2 = P.nlaunch;
-      P.stream = P.cap[2];
-      CK(cudaStreamBeginCaptureToGraph(P.cap[2], ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                       cudaStreamCaptureModeThreadLocal));
-      depth = 3;
-      pcgmx_replace(P);
-      CK(cudaStreamEndCapture(P.cap[2], nullptr));
-      depth = 2;
-      n3 = P.nlaunch;
-      P.stream = P.cap[1];
-    } else if (cg) {
-      cg_body(P);
-    } else {
-      pcg64_body(P);
-    }
-    launch(P, k_cond_while, 1, 1, 0, hw, (const PcgState*)P.st);
-    CK(cudaStreamEndCapture(P.cap[1], nullptr));
-    depth = 1;
-    P.stream = P.cap[0];
-    n4e = P.nlaunch;
-    if (cg) cg_epilogue(P);
-    if (mixed) pcgmx_fold(P);
-    CK(cudaStreamEndCapture(P.cap[0], &P.sg_graph));
+    record(depth);
+    CK(cudaStreamEndCapture(P.cap[0], &graph));
     depth = 0;
     P.capturing = false;
-    CK(cudaGraphInstantiate(&P.sg_exec, P.sg_graph, 0));
   } catch (...) {
     P.capturing = false;
     for (int d = depth; d >= 1; --d) {
@@ -1561,16 +1592,25 @@ static void capture_solve(Prob& P, double tol, int maxiter, bool cg = false) {
     throw;
   }
   P.stream = user;
-  const long long n4 = n4e, n5 = P.nlaunch;
-  P.sg_pro = (n1 - n0) + (n5 - n4);  // prologue and epilogue run once
-  if (mixed) {
-    P.sg_if = n3 - n2;
-    P.sg_body = (n2 - n1) + (n4 - n3);
-  } else {
-    P.sg_if = 0;
-    P.sg_body = n4 - n1;
-  }
   P.nlaunch = n0;
+  return graph;
+}
+
+static void capture_solve(Prob& P, double tol, int maxiter, bool cg = false) {
+  if (P.sg_exec) {
+    CK(cudaGraphExecDestroy(P.sg_exec));
+    P.sg_exec = nullptr;
+  }
+  if (P.sg_graph) {
+    CK(cudaGraphDestroy(P.sg_graph));
+    P.sg_graph = nullptr;
+  }
+  SolveCounts c;
+  P.sg_graph = capture_graph(P, [&](int& depth) { c = capture_solve_into(P, tol, maxiter, cg, depth); });
+  CK(cudaGraphInstantiate(&P.sg_exec, P.sg_graph, 0));
+  P.sg_pro = c.pro;
+  P.sg_body = c.body;
+  P.sg_if = c.rep;
   P.sg_key = graph_key(P, tol, maxiter, cg);
 }
 
@@ -1621,6 +1661,7 @@ static void solve_internal(Prob& P, double tol, int maxiter) {
   P.last_solve_ms = b;
 }
 
+
 }  // namespace edge
 
 using namespace edge;
@@ -1637,6 +1678,148 @@ struct edge_filter {
     if (N) cudaFree(N);
   }
 };
+
+// One SIMP iteration as one CUDA graph: the OC update of (it_rho, it_dr) into it_rho_new
+// (prep, floor, bracket init, the bisection passes as a while node whose condition a kernel
+// sets from the device-side state, the final design), then the analysis of it_rho_new:
+// filter + SIMP law, the solve (hierarchy set-up and PCG loop as in capture_solve),
+// compliance, sensitivities and the filter transpose into it_dr_new.  Every buffer is the
+// problem's own; the caller copies the user's arrays in and out around the launch.
+static const int OC_MAX_STEPS = 200;  // the host loop's bound (edge_oc_update)
+static void capture_iteration(Prob& P, const edge_filter& F, double A, double vol, double vf, double move,
+                              double penalty, double void_, double tol, int maxiter) {
+  if (P.it_exec) {
+    CK(cudaGraphExecDestroy(P.it_exec));
+    P.it_exec = nullptr;
+  }
+  if (P.it_graph) {
+    CK(cudaGraphDestroy(P.it_graph));
+    P.it_graph = nullptr;
+  }
+  const Geo& g = P.g0;
+  const long long n = P.n_el;
+  const unsigned nb = std::min<unsigned>(ew_blocks(n), 1024);
+  const unsigned nbp = std::min<unsigned>(nb, (unsigned)(P.part_cap / OC_NODES));
+  const unsigned nbe = cdiv(P.n_el, 256);
+  const long long nv = (long long)g.dof * g.n;
+  long long n_fixed0 = 0, n_fixed1 = 0, n_fixed2 = 0, n_ocb = 0;
+  SolveCounts sc;
+  P.it_graph = capture_graph(P, [&](int& depth) {
+    const long long a0 = P.nlaunch;
+    {
+      CatScope cat(P, CAT_OC);
+      launch(P, k_oc_prep, nb, 256, 0, n, (const double*)P.it_rho, (const double*)P.it_dr, A, P.ocp, P.part,
+             P.ticket, P.scal);
+      launch(P, k_oc_floor, nb, 256, 0, n, P.ocp, (const double*)P.scal);
+      launch(P, k_oc_state_init, 1, 1, 0, P.oc, vf, vol);
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t gg;
+      const cudaGraphNode_t* deps;
+      size_t nd;
+      CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &gg, &deps, &nd));
+      cudaGraphConditionalHandle ho;
+      CK(cudaGraphConditionalHandleCreate(&ho, gg, 0, cudaGraphCondAssignDefault));
+      launch(P, k_cond_oc, 1, 1, 0, ho, (const OcState*)P.oc, OC_MAX_STEPS);
+      CK(cudaStreamGetCaptureInfo(P.cap[0], &cs, nullptr, &gg, &deps, &nd));
+      cudaGraphNodeParams wp = {};
+      wp.type = cudaGraphNodeTypeConditional;
+      wp.conditional.handle = ho;
+      wp.conditional.type = cudaGraphCondTypeWhile;
+      wp.conditional.size = 1;
+      cudaGraphNode_t wnode;
+      CK(cudaGraphAddNode(&wnode, gg, deps, nd, &wp));
+      CK(cudaStreamUpdateCaptureDependencies(P.cap[0], &wnode, 1, cudaStreamSetCaptureDependencies));
+      P.stream = P.cap[1];
+      CK(cudaStreamBeginCaptureToGraph(P.cap[1], wp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal));
+      depth = 2;
+      const long long b0 = P.nlaunch;
+      launch(P, k_oc_pass, nbp, 256, 0, n, (const double*)P.it_rho, (const double*)P.ocp, A, move, P.oc, P.part,
+             P.ticket);
+      launch(P, k_cond_oc, 1, 1, 0, ho, (const OcState*)P.oc, OC_MAX_STEPS);
+      n_ocb = P.nlaunch - b0;
+      CK(cudaStreamEndCapture(P.cap[1], nullptr));
+      depth = 1;
+      P.stream = P.cap[0];
+      launch(P, k_oc_final, nb, 256, 0, n, (const double*)P.it_rho, (const double*)P.ocp, move, (const OcState*)P.oc,
+             P.it_rho_new, P.part, P.ticket, P.scal + 1);
+    }
+    {
+      CatScope cat(P, CAT_SENS);
+      launch(P, k_filter_material<double, float>, nbe, 256, 0, g, F.taps, (const double*)P.it_rho_new, P.rho_f,
+             P.E64, P.E32, penalty, void_, 0);
+    }
+    n_fixed0 = P.nlaunch - a0 - n_ocb;
+    sc = capture_solve_into(P, tol, maxiter, false, depth);
+    const long long c0 = P.nlaunch;
+    {
+      CatScope cat(P, CAT_SENS);
+      launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, (const double*)P.b64,
+             (const double*)P.x64, P.part, P.ticket, P.scal + 2);
+      launch(P, k_dk<double>, nbe, 256, 0, g, (const double*)P.x64, P.ei.k3, P.ei.k2, (const double*)P.dK0b,
+             P.ei.wht ? 1 : 0, (double*)nullptr, (const double*)P.rho_f, P.gsens, penalty, void_);
+      launch(P, k_filter_T, nbe, 256, 0, F.g, F.taps, (const double*)F.N, (const double*)P.gsens, P.it_dr_new);
+    }
+    n_fixed1 = P.nlaunch - c0;
+  });
+  CK(cudaGraphInstantiate(&P.it_exec, P.it_graph, 0));
+  (void)n_fixed2;
+  P.it_fixed = n_fixed0 + n_fixed1 + sc.pro;
+  P.it_oc_body = n_ocb;
+  P.it_body = sc.body;
+  P.it_rep = sc.rep;
+}
+
+
+
+
+// ------------------------------------------------------------------ unstructured meshes
+// One general mesh with its element matrices, the node adjacency, the density, the BC mask
+// and the CG workspace (all allocated at creation).
+struct edge_gen {
+  GenGeo G{};
+  long long n_dof = 0;
+  double* rho = nullptr;
+  uint8_t* cons = nullptr;
+  double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *b = nullptr;
+  PcgState* st = nullptr;
+  PcgState* st_h = nullptr;
+  double* part = nullptr;
+  unsigned* ticket = nullptr;
+  int* zero = nullptr;  // a device zero (the CG's "coarse factorisation ok" status)
+  cudaStream_t stream = nullptr;
+  bool has_rho = false;
+  int last_iters = 0;
+  std::vector<void*> allocs;
+  template <typename T> T* alloc(size_t n) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)));
+    allocs.push_back(q);
+    return (T*)q;
+  }
+  template <typename T> T* upload(const T* h, size_t n) {
+    T* d = alloc<T>(n);
+    CK(cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+  }
+  ~edge_gen() {
+    for (void* q : allocs) cudaFree(q);
+    if (st_h) cudaFreeHost(st_h);
+  }
+};
+
+static unsigned gen_blocks(long long n) { return (unsigned)std::min<long long>(cdiv(n, 256), 148LL * 8); }
+
+template <typename... KArgs, typename... Args>
+static void glaunch(edge_gen& M, void (*kern)(KArgs...), unsigned grid, unsigned block, Args... args) {
+  kern<<<grid, block, 0, M.stream>>>(static_cast<KArgs>(args)...);
+  KCHECK();
+}
+
+static void gen_matvec(edge_gen& M, const double* u, double* out, double* dot) {
+  glaunch(M, k_gen_matvec, std::min<unsigned>(gen_blocks(M.n_dof), 1024), 256, M.G, (const double*)M.rho,
+          (const uint8_t*)M.cons, u, out, M.part, M.ticket, dot);
+}
 
 // ------------------------------------------------------------------ OC update without a workspace
 // edge_oc_update_static runs the OC kernels of edge_oc_update on a fixed workspace that is a
@@ -1914,6 +2097,23 @@ int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm) {
 static double time_fine(Prob& P, int precision, bool sweep, int reps, bool mix = false) {
   const Geo& g = P.g0;
   auto run = [&]() {
+    if (mix && cube_fusable(P)) {
+      // the same three launches fused as the solver runs them on this tile: first sweep +
+      // residual, last sweep + correction + r.z, search direction + product + p.q
+      Level& L0 = P.lv[0];
+      InWDB i1{&P.st->omega, 1.0, 0.f};
+      SEResidIn e1{(float*)L0.r, g.n};
+      fine3_cube_fused(P, P.r32, L0.dinv, nullptr, i1, e1, nullptr, nullptr, 4 + 2 + 4);
+      const void* arr[3] = {L0.r, L0.dinv, P.r32};
+      SEJacobiAdd0<true> e2{(float*)L0.res, &P.st->omega, 1.0, g.n, 0.f};
+      fine3_cube_fused(P, (const float*)L0.ea, nullptr, nullptr, InU{}, e2, arr, &P.st->rz, 4 + 4 + 2 + 4 + 4);
+      const long long nv = (long long)g.dof * g.n;
+      float* p0 = (float*)P.p;
+      InPDir i3{(const PcgState*)P.st, 0.f, 0, false};
+      SEStorePDot e3{(float*)P.q, p0, p0 + nv, (const PcgState*)P.st, g.n, nullptr};
+      fine3_cube_fused(P, (const float*)L0.res, p0, p0 + nv, i3, e3, nullptr, &P.st->pq, 4 + 4 + 4 + 4);
+      return;
+    }
     if (mix) {
       // the fine-level launches of one mixed-precision PCG iteration with one sweep per level:
       // residual, last sweep + correction + r.z, product + p.q
@@ -2575,6 +2775,230 @@ static void oc_run(Prob& P, long long n, const double* rho, const double* dr, do
   CK(cudaStreamSynchronize(P.stream));
 }
 
+
+// ---- unstructured meshes (kernels/_cuda.py:305-815, solvers/_gpu.py:11-58, geom/_filters.py:278-298)
+int edge_gen_create(int dof, long long n_nodes, long long n_el, const int* elem_ptr, const int* elem_flat,
+                    const double* K, const long long* K_ptr, edge_gen** out) {
+  API_BEGIN
+  if (!out || !elem_ptr || !elem_flat || !K || !K_ptr) fail(EDGE_EINVAL, "null argument");
+  if (dof < 1 || dof > 3 || n_nodes < 1 || n_el < 1) fail(EDGE_EINVAL, "bad mesh sizes");
+  const long long nflat = elem_ptr[n_el];
+  for (long long e = 0; e < n_el; ++e) {
+    const int sz = elem_ptr[e + 1] - elem_ptr[e];
+    if (sz < 1 || sz > 27) fail(EDGE_EINVAL, "element " + std::to_string(e) + " has " + std::to_string(sz) + " nodes");
+    const long long nk = (long long)sz * dof;
+    if (K_ptr[e + 1] - K_ptr[e] != nk * nk)
+      fail(EDGE_EINVAL, "element " + std::to_string(e) + ": matrix size does not match its node count");
+  }
+  for (long long a = 0; a < nflat; ++a)
+    if (elem_flat[a] < 0 || elem_flat[a] >= n_nodes) fail(EDGE_EINVAL, "connectivity refers to a missing node");
+  // node -> (element, local corner), sorted by node, then element (counting sort)
+  std::vector<long long> adj_ptr(n_nodes + 1, 0);
+  for (long long a = 0; a < nflat; ++a) ++adj_ptr[elem_flat[a] + 1];
+  for (long long i = 0; i < n_nodes; ++i) adj_ptr[i + 1] += adj_ptr[i];
+  std::vector<long long> fill(adj_ptr.begin(), adj_ptr.end() - 1);
+  std::vector<int> adj_el(nflat);
+  std::vector<unsigned char> adj_loc(nflat);
+  for (long long e = 0; e < n_el; ++e)
+    for (int c = elem_ptr[e]; c < elem_ptr[e + 1]; ++c) {
+      const long long slot = fill[elem_flat[c]]++;
+      adj_el[slot] = (int)e;
+      adj_loc[slot] = (unsigned char)(c - elem_ptr[e]);
+    }
+  std::unique_ptr<edge_gen> M(new edge_gen());
+  M->G.dof = dof;
+  M->G.n_nodes = n_nodes;
+  M->G.n_el = n_el;
+  M->n_dof = n_nodes * dof;
+  M->G.elem_ptr = M->upload(elem_ptr, n_el + 1);
+  M->G.elem_flat = M->upload(elem_flat, nflat);
+  M->G.K_ptr = M->upload(K_ptr, n_el + 1);
+  M->G.K = M->upload(K, (size_t)K_ptr[n_el]);
+  M->G.adj_ptr = M->upload(adj_ptr.data(), n_nodes + 1);
+  M->G.adj_el = M->upload(adj_el.data(), nflat);
+  M->G.adj_loc = M->upload(adj_loc.data(), nflat);
+  M->rho = M->alloc<double>(n_el);
+  M->cons = M->alloc<uint8_t>(M->n_dof);
+  CK(cudaMemset(M->cons, 0, M->n_dof));
+  for (double** v : {&M->x, &M->r, &M->p, &M->q, &M->b}) *v = M->alloc<double>(M->n_dof);
+  M->st = M->alloc<PcgState>(1);
+  CK(cudaMallocHost(&M->st_h, sizeof(PcgState)));
+  M->part = M->alloc<double>(1024);
+  M->ticket = M->alloc<unsigned>(1);
+  CK(cudaMemset(M->ticket, 0, sizeof(unsigned)));
+  M->zero = M->alloc<int>(1);
+  CK(cudaMemset(M->zero, 0, sizeof(int)));
+  *out = M.release();
+  API_END
+}
+
+int edge_gen_destroy(edge_gen* m) {
+  API_BEGIN
+  delete m;
+  API_END
+}
+
+int edge_gen_set_stream(edge_gen* m, void* stream) {
+  API_BEGIN
+  if (!m) fail(EDGE_EINVAL, "null handle");
+  m->stream = (cudaStream_t)stream;
+  API_END
+}
+
+int edge_gen_set_rho(edge_gen* m, const double* rho_dev) {
+  API_BEGIN
+  if (!m || !rho_dev) fail(EDGE_EINVAL, "null argument");
+  CK(cudaMemcpyAsync(m->rho, rho_dev, m->G.n_el * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+  m->has_rho = true;
+  API_END
+}
+
+int edge_gen_set_constraints(edge_gen* m, const uint8_t* cons_dev) {
+  API_BEGIN
+  if (!m || !cons_dev) fail(EDGE_EINVAL, "null argument");
+  CK(cudaMemcpyAsync(m->cons, cons_dev, m->n_dof, cudaMemcpyDeviceToDevice, m->stream));
+  API_END
+}
+
+int edge_gen_matvec(edge_gen* m, const double* u_dev, double* out_dev) {
+  API_BEGIN
+  if (!m || !u_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  if (!m->has_rho) fail(EDGE_ESTATE, "Rho has not been set. dot works only after setting rho.");
+  gen_matvec(*m, u_dev, out_dev, nullptr);
+  API_END
+}
+
+int edge_gen_diagonal(edge_gen* m, double* diag_dev) {
+  API_BEGIN
+  if (!m || !diag_dev) fail(EDGE_EINVAL, "null argument");
+  if (!m->has_rho) fail(EDGE_ESTATE, "Rho has not been set. diagonal works only after setting rho or if rho is provided.");
+  glaunch(*m, k_gen_diagonal, gen_blocks(m->n_dof), 256, m->G, (const double*)m->rho, (const uint8_t*)m->cons,
+          diag_dev);
+  API_END
+}
+
+int edge_gen_process_grad(edge_gen* m, const double* U_dev, double* dk_dev) {
+  API_BEGIN
+  if (!m || !U_dev || !dk_dev) fail(EDGE_EINVAL, "null argument");
+  glaunch(*m, k_gen_dk, gen_blocks(m->G.n_el), 256, m->G, U_dev, dk_dev);
+  API_END
+}
+
+// CG without a preconditioner (cupyx.scipy.sparse.linalg.cg with M = None, as the reference's
+// CG solver runs on general meshes), FP64, the structured solver's CG kernels on these
+// vectors; one state read per iteration decides convergence (where cupyx's loop checks it).
+int edge_gen_cg_solve(edge_gen* m, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
+                      double* residual_out, int* iters_out) {
+  API_BEGIN
+  if (!m || !f_dev || !x_dev) fail(EDGE_EINVAL, "null argument");
+  if (!m->has_rho) fail(EDGE_ESTATE, "Solver requires a density vector to be passed or set on the kernel.");
+  edge_gen& M = *m;
+  const long long nv = M.n_dof;
+  const unsigned nb = std::min<unsigned>(gen_blocks(nv), 1024);
+  CK(cudaMemcpyAsync(M.b, f_dev, nv * sizeof(double), cudaMemcpyDeviceToDevice, M.stream));
+  if (use_last)
+    CK(cudaMemcpyAsync(M.x, x_dev, nv * sizeof(double), cudaMemcpyDeviceToDevice, M.stream));
+  else
+    CK(cudaMemsetAsync(M.x, 0, nv * sizeof(double), M.stream));
+  glaunch(M, k_pcg_init, 1, 1, M.st, tol, maxiter, 0.0, 0.0, 0.0, 0);
+  gen_matvec(M, M.x, M.r, nullptr);  // r = b - A x
+  glaunch(M, k_axpby, gen_blocks(nv), 256, nv, 1.0, (const double*)M.b, -1.0, M.r);
+  glaunch(M, k_dot<double, double>, nb, 256, nv, (const double*)M.b, (const double*)M.b, M.part, M.ticket, &M.st->bb);
+  glaunch(M, k_dot<double, double>, nb, 256, nv, (const double*)M.r, (const double*)M.r, M.part, M.ticket, &M.st->rr);
+  glaunch(M, k_pcg_check_bb, 1, 1, M.st, (const int*)M.zero);
+  auto read = [&]() {
+    CK(cudaMemcpyAsync(M.st_h, M.st, sizeof(PcgState), cudaMemcpyDeviceToHost, M.stream));
+    CK(cudaStreamSynchronize(M.stream));
+  };
+  read();
+  while (!M.st_h->done) {
+    glaunch(M, k_cg_rz, 1, 1, M.st);
+    glaunch(M, k_pcg_p<double>, gen_blocks(nv), 256, nv, M.p, (const double*)M.r, (const PcgState*)M.st);
+    gen_matvec(M, M.p, M.q, &M.st->pq);
+    glaunch(M, k_pcg_xr<double, double>, nb, 256, nv, M.x, (const double*)M.p, M.r, (const double*)M.q, M.st, M.part,
+            M.ticket, (float*)nullptr);
+    read();
+  }
+  M.last_iters = M.st_h->iter;
+  // true residual ||f - K x|| / ||f||, as the reference reports it
+  gen_matvec(M, M.x, M.r, nullptr);
+  glaunch(M, k_axpby, gen_blocks(nv), 256, nv, 1.0, (const double*)M.b, -1.0, M.r);
+  glaunch(M, k_dot<double, double>, nb, 256, nv, (const double*)M.r, (const double*)M.r, M.part, M.ticket, &M.st->rr);
+  glaunch(M, k_final_res, 1, 1, M.st);
+  CK(cudaMemcpyAsync(x_dev, M.x, nv * sizeof(double), cudaMemcpyDeviceToDevice, M.stream));
+  read();
+  if (residual_out) *residual_out = M.st_h->res;
+  if (iters_out) *iters_out = M.last_iters;
+  API_END
+}
+
+// CSR density filter of a general mesh: H and its transpose both stored as CSR (the
+// transpose built on the host), applied by gather SpMVs in stored order.
+struct edge_csr {
+  long long n = 0;
+  long long *ptr = nullptr, *ptrT = nullptr;
+  int *idx = nullptr, *idxT = nullptr;
+  double *val = nullptr, *valT = nullptr;
+  ~edge_csr() {
+    for (void* q : {(void*)ptr, (void*)ptrT, (void*)idx, (void*)idxT, (void*)val, (void*)valT})
+      if (q) cudaFree(q);
+  }
+};
+
+int edge_csr_create(long long n, const long long* indptr, const int* indices, const double* data, edge_csr** out) {
+  API_BEGIN
+  if (!out || !indptr || !indices || !data) fail(EDGE_EINVAL, "null argument");
+  if (n < 1) fail(EDGE_EINVAL, "empty matrix");
+  const long long nnz = indptr[n];
+  for (long long a = 0; a < nnz; ++a)
+    if (indices[a] < 0 || indices[a] >= n) fail(EDGE_EINVAL, "column index out of range");
+  std::vector<long long> pT(n + 1, 0);
+  for (long long a = 0; a < nnz; ++a) ++pT[indices[a] + 1];
+  for (long long i = 0; i < n; ++i) pT[i + 1] += pT[i];
+  std::vector<long long> fill(pT.begin(), pT.end() - 1);
+  std::vector<int> iT(nnz);
+  std::vector<double> vT(nnz);
+  for (long long i = 0; i < n; ++i)
+    for (long long a = indptr[i]; a < indptr[i + 1]; ++a) {
+      const long long s = fill[indices[a]]++;
+      iT[s] = (int)i;
+      vT[s] = data[a];
+    }
+  std::unique_ptr<edge_csr> F(new edge_csr());
+  F->n = n;
+  auto up = [](auto*& d, const auto* h, size_t k) {
+    CK(cudaMalloc((void**)&d, std::max<size_t>(k, 1) * sizeof(*h)));
+    CK(cudaMemcpy(d, h, k * sizeof(*h), cudaMemcpyHostToDevice));
+  };
+  up(F->ptr, indptr, n + 1);
+  up(F->idx, indices, nnz);
+  up(F->val, data, nnz);
+  up(F->ptrT, pT.data(), n + 1);
+  up(F->idxT, iT.data(), nnz);
+  up(F->valT, vT.data(), nnz);
+  *out = F.release();
+  API_END
+}
+
+int edge_csr_destroy(edge_csr* f) {
+  API_BEGIN
+  delete f;
+  API_END
+}
+
+int edge_csr_apply(edge_csr* f, const double* in_dev, double* out_dev, int transpose, void* stream) {
+  API_BEGIN
+  if (!f || !in_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  const long long n = f->n;
+  const unsigned nb = (unsigned)std::min<long long>(cdiv(n, 256), 148LL * 8);
+  if (transpose)
+    k_csr_spmv<<<nb, 256, 0, (cudaStream_t)stream>>>(n, f->ptrT, f->idxT, f->valT, in_dev, out_dev);
+  else
+    k_csr_spmv<<<nb, 256, 0, (cudaStream_t)stream>>>(n, f->ptr, f->idx, f->val, in_dev, out_dev);
+  KCHECK();
+  API_END
+}
+
 int edge_oc_update(edge_problem* p, const double* rho_dev, const double* dr_dev, double A, double vol, double vf,
                    double move, double* rho_new_dev, double* lambda_out, int* steps_out, double* sqchange_out) {
   API_BEGIN
@@ -2623,6 +3047,76 @@ int edge_oc_update_static(long long n, const double* rho_dev, const double* dr_d
   if (lambda_out) *lambda_out = h.last;
   if (steps_out) *steps_out = h.steps;
   if (sqchange_out) *sqchange_out = chg;
+  API_END
+}
+
+// One SIMP iteration, OC update then analysis, as one graph launch and one host read
+// (TopOpt/_cuda.py:242-302: update_design followed by solve_and_process).
+int edge_simp_iteration(edge_problem* p, edge_filter* f, const double* rho_dev, const double* dr_dev, double A,
+                        double vol, double vf, double move, double penalty, double void_, const double* f_dev,
+                        double* U_dev, int use_last, double tol, int maxiter, double* rho_new_dev, double* dr_new_dev,
+                        double* rho_f_dev, double* compliance_out, double* residual_out, int* iters_out,
+                        double* lambda_out, int* oc_steps_out, double* sqchange_out) {
+  API_BEGIN
+  if (!p || !f || !rho_dev || !dr_dev || !f_dev || !U_dev || !rho_new_dev || !dr_new_dev)
+    fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  if (f->n_el != P.n_el) fail(EDGE_EINVAL, "filter and mesh sizes differ");
+  if (!P.use_graph || P.prof || P.bd)
+    fail(EDGE_ESTATE, "edge_simp_iteration needs the graph solve (no profiling or breakdown in progress)");
+  ensure_mg(P);
+  const Geo& g = P.g0;
+  const size_t eb = (size_t)P.n_el * sizeof(double);
+  if (!P.it_rho) {  // once per problem
+    P.it_rho = P.alloc<double>(P.n_el);
+    P.it_dr = P.alloc<double>(P.n_el);
+    P.it_rho_new = P.alloc<double>(P.n_el);
+    P.it_dr_new = P.alloc<double>(P.n_el);
+  }
+  std::vector<double> key = graph_key(P, tol, maxiter);
+  for (double v : {(double)(uintptr_t)f, A, vol, vf, move, penalty, void_}) key.push_back(v);
+  if (!P.it_exec || key != P.it_key) {
+    capture_iteration(P, *f, A, vol, vf, move, penalty, void_, tol, maxiter);
+    P.it_key = key;
+  }
+  CK(cudaMemcpyAsync(P.it_rho, rho_dev, eb, cudaMemcpyDeviceToDevice, P.stream));
+  CK(cudaMemcpyAsync(P.it_dr, dr_dev, eb, cudaMemcpyDeviceToDevice, P.stream));
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, f_dev, P.b64);
+  if (use_last)
+    launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, (const double*)U_dev, P.x64);
+  else
+    CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
+  CK(cudaEventRecord(P.ev[0], P.stream));
+  CK(cudaGraphLaunch(P.it_exec, P.stream));
+  CK(cudaEventRecord(P.ev[2], P.stream));
+  P.has_rho = true;
+  P.omega_started = true;
+  CK(cudaMemcpyAsync(rho_new_dev, P.it_rho_new, eb, cudaMemcpyDeviceToDevice, P.stream));
+  CK(cudaMemcpyAsync(dr_new_dev, P.it_dr_new, eb, cudaMemcpyDeviceToDevice, P.stream));
+  if (rho_f_dev) CK(cudaMemcpyAsync(rho_f_dev, P.rho_f, eb, cudaMemcpyDeviceToDevice, P.stream));
+  launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, (const double*)P.x64, U_dev);
+  int status = 0;
+  CK(cudaMemcpyAsync(&status, P.chol_status, sizeof(int), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaMemcpyAsync(P.oc_h, P.oc, sizeof(OcState), cudaMemcpyDeviceToHost, P.stream));
+  CK(cudaMemcpyAsync(P.scal_h, P.scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, P.stream));
+  read_state(P);  // synchronises the stream: the one host read of the iteration
+  if (status) fail(EDGE_ENOTPD, "coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
+  check_err(P);
+  P.last_iters = P.st_h->iter;
+  P.last_true_res = (P.prec != EDGE_FP64) ? 1 + P.st_h->n_true : 0;
+  const long long passes = (P.oc_h->steps + OC_DEPTH - 1) / OC_DEPTH;
+  P.nlaunch += P.it_fixed + P.it_body * (long long)P.st_h->iter + P.it_rep * (long long)P.st_h->n_true +
+               P.it_oc_body * passes;
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, P.ev[0], P.ev[2]));
+  P.last_setup_ms = 0.0;
+  P.last_solve_ms = ms;
+  if (compliance_out) *compliance_out = P.scal_h[2];
+  if (residual_out) *residual_out = P.st_h->res;
+  if (iters_out) *iters_out = P.st_h->iter;
+  if (lambda_out) *lambda_out = P.oc_h->last;
+  if (oc_steps_out) *oc_steps_out = P.oc_h->steps;
+  if (sqchange_out) *sqchange_out = P.scal_h[1];
   API_END
 }
 

@@ -151,3 +151,72 @@ class CuStructuredFilter2D(_CuStructuredFilter):
 
 StructuredFilter2D = CuStructuredFilter2D
 StructuredFilter3D = CuStructuredFilter3D
+
+
+class CuGeneralFilter(FilterKernel):
+    """Cone density filter of an unstructured mesh, drop-in for CuGeneralFilter
+    (geom/_filters.py:278-298 with filter_kernel_{2D,3D}_general, core/_filter.py:126-182):
+    for every element the element centroids within r_min (a KD-tree ball query, closed
+    ball), weights (r_min - d) / r_min normalised to sum 1 per row.  The matrix is built on
+    the host once; H and H^T are applied on the device (edge_csr_apply, a transpose stored
+    beside H so both products are gathers in a fixed order)."""
+
+    def __init__(self, mesh, r_min):
+        super().__init__()
+        from scipy.spatial import cKDTree
+        self.dtype = mesh.dtype
+        self.nd = int(np.asarray(mesh.nodes).shape[1])
+        cent = np.asarray(mesh.centeroids, dtype=np.float64)
+        n = cent.shape[0]
+        tree = cKDTree(cent)
+        rows = tree.query_ball_point(cent, r_min)
+        indptr = np.zeros(n + 1, dtype=np.int64)
+        idx, val = [], []
+        for i, nb in enumerate(rows):
+            nb = np.asarray(sorted(nb), dtype=np.int64)
+            w = (r_min - np.linalg.norm(cent[nb] - cent[i], axis=-1)) / r_min
+            idx.append(nb)
+            val.append(w / w.sum())
+            indptr[i + 1] = indptr[i] + nb.size
+        self._indptr = indptr
+        self._indices = np.ascontiguousarray(np.concatenate(idx).astype(np.int32))
+        self._data = np.ascontiguousarray(np.concatenate(val))
+        self.shape = (n, n)
+        self.weights = torch.as_tensor(self._data, device="cuda")
+        h = ctypes.c_void_p()
+        _lib.call("edge_csr_create", n, indptr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                  self._indices.ctypes.data_as(_lib.c_int_p), self._data.ctypes.data_as(_lib.c_double_p),
+                  ctypes.byref(h))
+        self._h = h
+
+    @property
+    def kernel(self):
+        """H as a torch sparse CSR matrix on the device (the reference keeps a cupy CSR)."""
+        return torch.sparse_csr_tensor(torch.as_tensor(self._indptr), torch.as_tensor(self._indices.astype(np.int64)),
+                                       torch.as_tensor(self._data), size=self.shape).to("cuda")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().edge_csr_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def _apply(self, rho, transpose):
+        if isinstance(rho, np.ndarray):
+            rho = torch.from_numpy(rho)
+        x = rho.to(device="cuda", dtype=torch.float64).contiguous().reshape(-1)
+        out = torch.empty_like(x)
+        _lib.call("edge_csr_apply", self._h, _lib.ptr(x), _lib.ptr(out), 1 if transpose else 0, _lib.stream_ptr())
+        return out.reshape(rho.shape)
+
+    def _matvec(self, rho):
+        return self._apply(rho, False)
+
+    def _rmatvec(self, rho):
+        return self._apply(rho, True)
+
+
+GeneralFilter = CuGeneralFilter

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .kernels import CuStructuredStiffnessKernel, _as_dev_f64
+from .kernels import CuStructuredStiffnessKernel, _CuGeneralKernel, _as_dev_f64
 
 
 class Solver:
@@ -350,13 +350,15 @@ class CuCG(Solver):
     """Conjugate gradients without a preconditioner on the matrix-free stiffness operator:
     the reference's CG solver (solvers/_gpu.py:11-58, cupyx cg with M = None; the returned
     residual is recomputed as ||f - K x|| / ||f||).  Works on any grid extent (the multigrid
-    needs element counts divisible by 2**n_level).  The iteration runs on the device as one
+    needs element counts divisible by 2**n_level) and on unstructured meshes
+    (CuUniformStiffnessKernel / CuGeneralStiffnessKernel, the reference's pairing of general
+    meshes with CG; there it runs as a host loop with one state read per iteration).  The iteration runs on the device as one
     CUDA graph launch.  matrix_free=False in the reference assembles K first; the product
     and hence the iterates are the same, so here it only records the choice."""
 
     def __init__(self, kernel, maxiter=1000, tol=1e-5, matrix_free=None):
-        if not isinstance(kernel, CuStructuredStiffnessKernel):
-            raise TypeError("CuCG needs the package's CuStructuredStiffnessKernel")
+        if not isinstance(kernel, (CuStructuredStiffnessKernel, _CuGeneralKernel)):
+            raise TypeError("CuCG needs one of the package's stiffness kernels")
         self.kernel = kernel
         self.last_x0 = None
         self.tol = tol
@@ -381,7 +383,8 @@ class CuCG(Solver):
             warm = 0
         res, its = ctypes.c_double(), ctypes.c_int()
         self.kernel._bind_stream()
-        _lib.call("edge_cg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
+        fn = "edge_gen_cg_solve" if isinstance(self.kernel, _CuGeneralKernel) else "edge_cg_solve"
+        _lib.call(fn, self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
                   int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
         if use_last:  # the reference keeps the warm start only on this branch
             self.last_x0 = x

@@ -4,8 +4,10 @@ Same constructor, BC/load API, ``optimize`` loop, history and termination test. 
 the objects handed in are this package's (CuStructuredStiffnessKernel, CuMultiGrid,
 CuStructuredFilter2D/3D, SingleMaterial) one SIMP analysis runs as a single library call
 (edge_simp_solve_and_process: filter + SIMP law + GMG-PCG + compliance + sensitivity +
-filter transpose) and the OC bisection runs on the GPU (edge_oc_update).  Other duck-typed
-objects go through the reference's object-by-object call order.
+filter transpose) and the OC bisection runs on the GPU (edge_oc_update); ``iterate`` (used by
+``optimize``) runs a whole SIMP iteration, OC update and analysis, as one CUDA graph launch
+(edge_simp_iteration).  Other duck-typed objects go through the reference's object-by-object
+call order.
 
 Differences from the reference, on purpose: ``rho_init`` works (the reference raises
 UnboundLocalError, TopOpt/_cuda.py:322), and arrays are torch CUDA tensors instead of cupy.
@@ -254,6 +256,45 @@ class CuTopOpt:
         self.last_stats.update(pcg_iters=its.value, residual=res.value)
         return torch.tensor(c.value, dtype=torch.float64), dr.reshape(-1, 1), res.value
 
+    def iterate(self, rho, df, iteration):
+        """One SIMP iteration: ``update_design(rho, df)`` followed by
+        ``solve_and_process(rho_new, iteration)``, returning (rho_new, compliance, dr, residual).
+        With this package's objects (and once the solver's autotuners have run, on the first
+        analyses) the two run as one CUDA graph launch with one host read
+        (edge_simp_iteration: the OC bisection loop is a device-side conditional node);
+        otherwise as the two calls."""
+        sv = self.solver
+        ready = (self.fused and self.n_sets == 1 and self.reuse_sol and sv.graph and sv.last_x0 is not None
+                 and (not sv.autotune or sv.tuned is not None) and (not sv.tune_sweeps or sv.sweeps is not None))
+        if not ready:
+            rho_new = self.update_design(rho, df)
+            comp, dr, res = self.solve_and_process(rho_new, iteration)
+            return rho_new, comp, dr, res
+        sv._configure()
+        rho = _as_dev_f64(rho).reshape(-1)
+        df = _as_dev_f64(df).reshape(-1)
+        rho_new = torch.empty_like(rho)
+        dr = torch.empty_like(rho)
+        rho_f = torch.empty_like(rho)
+        U = sv.last_x0
+        c, res, its = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        lam, steps, sq = ctypes.c_double(), ctypes.c_int(), ctypes.c_double()
+        A = float(np.asarray(self.mesh.As).reshape(-1)[0])
+        pen = float(self.material_model.current_penalty(iteration))
+        self.kernel._bind_stream()
+        _lib.call("edge_simp_iteration", self.kernel.handle, self.filter_kernel.handle, _lib.ptr(rho), _lib.ptr(df), A,
+                  float(self.mesh.volume), float(self.material_model.volume_fraction), float(self.move), pen,
+                  float(self.material_model.void), _lib.ptr(self.f), _lib.ptr(U), 1, float(sv.tol), int(sv.maxiter),
+                  _lib.ptr(rho_new), _lib.ptr(dr), _lib.ptr(rho_f), ctypes.byref(c), ctypes.byref(res),
+                  ctypes.byref(its), ctypes.byref(lam), ctypes.byref(steps), ctypes.byref(sq))
+        self.kernel.has_rho = True
+        sv.last_iters = its.value
+        self._U = U
+        self.last_stats.update(sv.stats())
+        self.last_stats.update(pcg_iters=its.value, residual=res.value, oc_lambda=lam.value, oc_steps=steps.value,
+                               oc_sqchange=sq.value, graph_iteration=True)
+        return rho_new, torch.tensor(c.value, dtype=torch.float64), dr.reshape(-1, 1), res.value
+
     # ----------------------------------------------------------------- loop (TopOpt/_cuda.py:304-382)
     def optimize(self, save_comp_history=False, save_change_history=False, save_rho_history=False, rho_init=None,
                  callback=None):
@@ -272,8 +313,7 @@ class CuTopOpt:
         for i in prog:
             rho_old = rho.clone()
             comp_old = float(comp)
-            rho = self.update_design(rho, df)
-            comp, df, res = self.solve_and_process(rho, i)
+            rho, comp, df, res = self.iterate(rho, df, i)
             change = float(torch.sqrt(torch.square(rho - rho_old).mean()))
             compf = float(comp)
             change_f = abs(compf - comp_old) / compf

@@ -30,6 +30,8 @@ extern "C" {
 
 typedef struct edge_problem edge_problem;
 typedef struct edge_filter edge_filter;
+typedef struct edge_gen edge_gen;
+typedef struct edge_csr edge_csr;
 
 const char* edge_last_error(void);
 int edge_version(void);
@@ -195,6 +197,34 @@ int edge_filter_destroy(edge_filter* f);
 int edge_filter_apply(edge_filter* f, const double* in_dev, double* out_dev, void* stream);
 int edge_filter_apply_T(edge_filter* f, const double* in_dev, double* out_dev, void* stream);
 
+/* ---- unstructured meshes (any mix of element kinds, dof 2 or 3).  Replaces the reference's
+ * UniformStiffnessKernel / GeneralStiffnessKernel (kernels/_cuda.py:305-815: node-basis
+ * product, diagonal, process_grad) on CuGeneralMesh (geom/_mesh.py:146-251).  Host arrays at
+ * creation: elem_ptr[n_el+1] offsets into elem_flat (node ids), K the element matrices
+ * row-major back to back with K_ptr[n_el+1] offsets (element e: (size*dof)^2 entries).  The
+ * product: out = K(rho) u with constrained rows/columns -> identity; the diagonal has 1 on
+ * constrained DOFs; dk_e = -u_e^T K_e u_e.  Device vectors use the reference's interleaved
+ * DOF layout; cons is one byte per DOF. */
+int edge_gen_create(int dof, long long n_nodes, long long n_el, const int* elem_ptr, const int* elem_flat,
+                    const double* K, const long long* K_ptr, edge_gen** out);
+int edge_gen_destroy(edge_gen* m);
+int edge_gen_set_stream(edge_gen* m, void* stream);
+int edge_gen_set_rho(edge_gen* m, const double* rho_dev);
+int edge_gen_set_constraints(edge_gen* m, const uint8_t* cons_dev);
+int edge_gen_matvec(edge_gen* m, const double* u_dev, double* out_dev);
+int edge_gen_diagonal(edge_gen* m, double* diag_dev);
+int edge_gen_process_grad(edge_gen* m, const double* U_dev, double* dk_dev);
+/* The reference's CG on a general mesh (solvers/_gpu.py:11-58: cupyx cg, M = None, stop at
+ * ||r|| <= tol ||f||, residual reported as ||f - K x|| / ||f||), FP64, matrix-free; use_last:
+ * start from x_dev.  Does not fail on non-convergence. */
+int edge_gen_cg_solve(edge_gen* m, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
+                      double* residual_out, int* iters_out);
+/* Density filter of a general mesh as a CSR matrix H (host arrays: the KD-tree cone weights
+ * of CuGeneralFilter, geom/_filters.py:278-298): out = H in, or H^T in with transpose != 0. */
+int edge_csr_create(long long n, const long long* indptr, const int* indices, const double* data, edge_csr** out);
+int edge_csr_destroy(edge_csr* f);
+int edge_csr_apply(edge_csr* f, const double* in_dev, double* out_dev, int transpose, void* stream);
+
 /* ---- OC update.  Replaces TopOpt.update_design (TopOpt/_cuda.py:242-280) with
  * SingleMaterial.ocP / evaluate_constraint (MaterialModels.py:75-90).  Also returns
  * sum((rho_new - rho)^2) for the RMS design change. */
@@ -226,6 +256,21 @@ int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* r
                                 double void_, const double* f_dev, double* U_dev, int use_last, double tol,
                                 int maxiter, double* compliance_out, double* dr_dev, double* rho_f_dev,
                                 double* residual_out, int* iters_out);
+
+/* ---- one whole SIMP iteration as one CUDA graph launch.  Replaces TopOpt.update_design
+ * followed by TopOpt.solve_and_process (TopOpt/_cuda.py:242-302) for SingleMaterial: the OC
+ * update of rho_dev with the sensitivities dr_dev (the bisection loop runs on the device as a
+ * conditional node: no host read inside it) into rho_new_dev, then the analysis of rho_new_dev
+ * exactly as edge_simp_solve_and_process (new sensitivities into dr_new_dev, U_dev updated,
+ * the filtered density into rho_f_dev when given).  The host reads the results once.  The
+ * graph is captured on the first call and again when a setting baked into it changes; the
+ * first call allocates the four element-sized buffers the graph works on.  Not available
+ * while profiling (edge_profile_begin / edge_breakdown_begin): EDGE_ESTATE. */
+int edge_simp_iteration(edge_problem* p, edge_filter* f, const double* rho_dev, const double* dr_dev, double A,
+                        double vol, double vf, double move, double penalty, double void_, const double* f_dev,
+                        double* U_dev, int use_last, double tol, int maxiter, double* rho_new_dev, double* dr_new_dev,
+                        double* rho_f_dev, double* compliance_out, double* residual_out, int* iters_out,
+                        double* lambda_out, int* oc_steps_out, double* sqchange_out);
 
 /* Benchmark instrumentation: between begin and end, every fine-level operator launch
  * (the dominant kernel) is bracketed by CUDA events on the problem's stream and its

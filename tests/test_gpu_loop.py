@@ -181,3 +181,37 @@ def test_cantilever_50_iterations_against_exact_solve_trajectory(golden, precisi
     z = golden("loop_cant3d_50t.npz")
     opt = _cant((64, 32, 32), 0.12, 1.5, dict(tol=tol, n_level=4, maxiter=4000), precision)
     _check_trajectory(f"{precision} rtol {tol:g}", z, *_trajectory(opt, 50))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_iteration_graph_matches_separate_calls(precision):
+    """A whole SIMP iteration as one CUDA graph launch (CuTopOpt.iterate: the OC bisection as a
+    device-side while node, then the analysis) against update_design + solve_and_process
+    (the host-driven OC loop and the solve graph): the same kernels with the same arguments,
+    so five iterations give bit-identical designs, compliances and sensitivities."""
+    import torch
+    from edge_to_b200 import _lib
+    runs = []
+    for graph_iteration in (False, True):
+        opt = _cant((32, 16, 16), 0.3, 1.5, dict(tol=1e-8, n_level=3, maxiter=1000, autotune=False,
+                                                 tune_sweeps=False), precision)
+        if precision == "mixed":
+            opt.solver._configure()
+            _lib.call("edge_set_fine_tile", opt.kernel.handle, 10, 8)
+            _lib.call("edge_mg_set_sweeps", opt.kernel.handle, _lib.int_array([1, 1, 1]), 3)
+        rho = torch.full((32 * 16 * 16,), 0.3, dtype=torch.float64, device="cuda")
+        c, dr, _ = opt.solve_and_process(rho, 0)
+        hist = []
+        for i in range(5):
+            if graph_iteration:
+                rho, c, dr, _ = opt.iterate(rho, dr, i)
+                assert opt.last_stats.get("graph_iteration")
+            else:
+                rho = opt.update_design(rho, dr)
+                c, dr, _ = opt.solve_and_process(rho, i)
+            hist.append(float(c))
+        runs.append((hist, rho.clone(), dr.clone()))
+    (h0, r0, d0), (h1, r1, d1) = runs
+    print(precision, "compliances", h0, h1)
+    assert h0 == h1
+    assert torch.equal(r0, r1) and torch.equal(d0, d1)
