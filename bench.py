@@ -285,14 +285,8 @@ def run_ours(args, cfg_name):
     rho, dr, it, t_ms = m["rho"], m["dr"], m["it"], m["t_ms"]
     traj += m["comps"]
     rho_traj = rho.detach().clone()
-    # ---------------- one more step with CUDA events around every fine-operator launch (the
-    # host-driven loop, same launches) for the live roofline of the dominant kernel
-    pm = timed_steps(opt, rho, dr, it, 1, ws, local, profile=True)
-    rho, dr, it, prof = pm["rho"], pm["dr"], pm["it"], pm["prof"]
-    # checked against a tight FP64 solve below: compliance, displacement and sensitivities
-    rho_chk, c_chk = rho.detach().clone(), pm["compliance"]
-    u_chk, dr_chk = opt.solver.last_x0.detach().clone(), dr.detach().clone().reshape(-1)
-
+    # the state after the timed steps (the profiled step below continues from it)
+    after = (rho.clone(), dr.clone(), it, opt.solver.last_x0.clone())
     # ---------------- end-to-end: design on the host, copies inside the timed region, from the
     # timed steps' starting state
     stream = torch.cuda.current_stream()
@@ -319,6 +313,17 @@ def run_ours(args, cfg_name):
     s1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = _max_over_ranks(s0.elapsed_time(s1), ws)
+    # ---------------- back to the state after the timed steps
+    rho, dr, it = after[0], after[1], after[2]
+    opt.solver.last_x0.copy_(after[3])
+    # ---------------- one more step with CUDA events around every fine-operator launch (the
+    # host-driven loop, same launches) for the live roofline of the dominant kernel
+    pm = timed_steps(opt, rho, dr, it, 1, ws, local, profile=True)
+    rho, dr, it, prof = pm["rho"], pm["dr"], pm["it"], pm["prof"]
+    # checked against a tight FP64 solve below: compliance, displacement and sensitivities
+    rho_chk, c_chk = rho.detach().clone(), pm["compliance"]
+    u_chk, dr_chk = opt.solver.last_x0.detach().clone(), dr.detach().clone().reshape(-1)
+
     bd = breakdown(opt, rho, dr, it) if args.breakdown else None
     tuned = opt.solver.tuned
     sweeps = opt.solver.sweeps

@@ -443,6 +443,52 @@ __global__ void k_restrict3(const Geo gf, const Geo gc, const TI* __restrict__ i
   for (int c = 0; c < 3; ++c) out[c * gc.n + sc] = Conv<TO>::from(v[c] * iw);
 }
 
+// The same restriction fused with the coarse level's first damped-Jacobi sweep from zero
+// (k_jacobi0): out = R in and x = (w Dinv) out at every coarse node, w = omega * wscale; the
+// padding slots of x are not written (they hold zero from allocation and are never read).
+template <typename T>
+__global__ void k_restrict3_j0(const Geo gf, const Geo gc, const T* __restrict__ in, T* __restrict__ out,
+                               const T* __restrict__ dinv, T* __restrict__ x, const double* omega, double wscale) {
+  EDGE_PDL_ENTRY();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int J = blockIdx.y;
+  if (t >= gc.nz * gc.nx) return;
+  const int K = t % gc.nz, I = t / gc.nz;
+  using TT = typename TransferT<T>::type;
+  using T2 = typename V2<T>::type;
+  const int nb = is_bnd(I, gc.nx) + is_bnd(J, gc.ny) + is_bnd(K, gc.nz);
+  const bool zm = K >= 1, zp = 2 * K + 1 < gf.nz;
+  TT v[3] = {0, 0, 0};
+#pragma unroll
+  for (int di = -1; di <= 1; ++di) {
+    const int fi = 2 * I + di;
+    if (fi < 0 || fi >= gf.nx) continue;
+#pragma unroll
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int fj = 2 * J + dj;
+      if (fj < 0 || fj >= gf.ny) continue;
+      const TT w0 = (TT)dist_w(abs(di) + abs(dj)), w1 = (TT)dist_w(abs(di) + abs(dj) + 1);
+      const long long sf = gf.slot3(fi, fj, 2 * K);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T* a = in + c * gf.n + sf;
+        const T2 pr = __ldg(reinterpret_cast<const T2*>(a));
+        if (zm) v[c] += w1 * Conv<TT>::from(__ldg(a - 1));
+        v[c] += w0 * Conv<TT>::from(pr.x);
+        if (zp) v[c] += w1 * Conv<TT>::from(pr.y);
+      }
+    }
+  }
+  const TT iw = inv_bnd_total3<TT>(nb);
+  const long long sc = gc.slot3(I, J, K);
+  const T wt = Conv<T>::from((*omega) * wscale);
+  for (int c = 0; c < 3; ++c) {
+    const T bv = Conv<T>::from(v[c] * iw);
+    out[c * gc.n + sc] = bv;
+    x[c * gc.n + sc] = wt * Conv<T>::from(__ldg(dinv + c * gc.n + sc)) * bv;
+  }
+}
+
 template <typename TI, typename TO>
 __global__ void k_restrict2(const Geo gf, const Geo gc, const TI* __restrict__ in, TO* __restrict__ out) {
   EDGE_PDL_ENTRY();

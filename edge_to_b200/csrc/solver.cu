@@ -30,6 +30,7 @@
 #include "fine_cube.cuh"
 #include "general.cuh"
 #include "misc.cuh"
+#include "tail.cuh"
 
 namespace edge {
 
@@ -271,6 +272,12 @@ struct Prob {
   // mixed path: fused fine launches (first sweep + residual in one launch, the last sweep
   // without a stored pre-smoothed iterate, the search direction formed inside the product)
   bool fuse = true;
+  // mixed path, 3-D: the V-cycle from level tail_l0 down (sweeps, residuals, transfers and
+  // the coarsest solve) as one persistent cooperative launch; 0 = off (the default: at 12.8M
+  // DOF the launch took longer than the per-step launches it replaces)
+  int tail_l0 = 0;
+  unsigned* tail_bar = nullptr;  // grid barrier of that launch (count, generation)
+  int tail_blocks = 0;
   bool cycle_w = false;
   std::vector<int> w_levels;
   std::vector<Level> lv;
@@ -1035,10 +1042,102 @@ static void mg_setup(Prob& P) {
 }
 
 // ------------------------------------------------------------------ V-cycle
+// Whether the mixed path runs the V-cycle from level l down as one persistent launch.
+static bool tail_usable(const Prob& P, int l) {
+  if (P.tail_l0 < 1 || l != P.tail_l0 || P.dim != 3 || P.prec == EDGE_FP64 || l >= P.n_level) return false;
+  if (P.n_level - l + 1 > TAIL_MAX) return false;
+  if (P.cycle_w)
+    for (int w : P.w_levels)
+      if (w >= l) return false;
+  return true;
+}
+
+template <typename TS>
+static void launch_tail(Prob& P, int l0) {
+  TailParams<TS> T{};
+  T.L0 = l0;
+  T.L = P.n_level;
+  for (int l = l0; l <= P.n_level; ++l) {
+    Level& Lv = P.lv[l];
+    TailLevel<TS>& V = T.lv[l - l0];
+    V.g = Lv.g;
+    V.S = (l < P.n_level) ? (const TS*)((std::is_same<TS, __nv_bfloat16>::value) ? Lv.S16 : Lv.S) : nullptr;
+    V.dinv = (const float*)Lv.dinv;
+    V.b = (float*)Lv.b;
+    V.xa = (float*)Lv.xa;
+    V.xb = (float*)Lv.xb;
+    V.r = (float*)Lv.r;
+    V.ea = (float*)Lv.ea;
+    V.eb = (float*)Lv.eb;
+    V.res = (float*)Lv.res;
+    V.ws = std::pow(1.06, l);
+    V.nsm = std::max(1, P.sweeps(l));
+  }
+  T.Ainv = P.Ainv;
+  T.nd = P.nd;
+  T.omega = &P.st->omega;
+  T.bar = P.tail_bar;
+  T.err = P.err;
+  if (P.tail_blocks == 0) {
+    int dev = 0, sms = 0, per = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_vcycle_tail<TS>, 256, 0));
+    if (per < 1) fail(EDGE_ECUDA, "persistent V-cycle kernel cannot be resident");
+    P.tail_blocks = sms * std::min(per, 2);
+  }
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.tail_blocks);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = P.stream;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const bool rec = P.bd && P.bev_used + 2 <= P.bev.size();
+  if (rec) CK(cudaEventRecord(P.bev[P.bev_used], P.stream));
+  CK(cudaLaunchKernelEx(&cfg, k_vcycle_tail<TS>, T));
+  ++P.nlaunch;
+  KCHECK();
+  if (rec) {
+    CK(cudaEventRecord(P.bev[P.bev_used + 1], P.stream));
+    P.bev_used += 2;
+    P.bcat.push_back(CAT_STENCIL);
+  }
+}
+
 // Result in `out`; b and out have type T.  With dot_dst, the last fine sweep also
 // computes dotv . out (FP64 accumulation).
+// Whether the restriction from level l also runs level l+1's first sweep (mixed path, 3-D,
+// level l+1 smoothed with the per-launch kernels).
+static bool restrict_j0(const Prob& P, int l) {
+  const int c = l + 1;
+  return P.fuse && P.prec != EDGE_FP64 && P.dim == 3 && c < P.n_level && P.sweeps(c) >= 1 && !tail_usable(P, c);
+}
+
+// Restriction of level l's residual r into level l+1's right-hand side (with level l+1's
+// first Jacobi sweep when restrict_j0).
+template <typename T>
+static void restrict_to(Prob& P, int l, const T* r) {
+  Level& Lc = P.lv[l + 1];
+  const Geo& g = P.lv[l].g;
+  P.cur_cat = CAT_TRANSFER;
+  if (P.dim == 3 && restrict_j0(P, l))
+    launch(P, k_restrict3_j0<T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g, r,
+           (T*)Lc.b, (const T*)Lc.dinv, (T*)Lc.xa, (const double*)&P.st->omega, std::pow(1.06, l + 1));
+  else if (P.dim == 3)
+    launch(P, k_restrict3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g, r,
+           (T*)Lc.b);
+  else
+    launch(P, k_restrict2<T, T>, dim3(cdiv(Lc.g.nx, 64), Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
+  KCHECK();
+  P.cur_cat = CAT_VECTOR;
+}
+
 template <typename T, typename TD0, typename TV>
-static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* dot_dst) {
+static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* dot_dst, bool pre_done = false) {
   Level& Lv = P.lv[l];
   const Geo& g = Lv.g;
   const long long nv = (long long)g.dof * g.n;
@@ -1055,6 +1154,15 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
   T* y = (T*)Lv.xb;
   T* r = (T*)Lv.r;
   const int nsm = P.sweeps(l);
+  if constexpr (std::is_same<T, float>::value) {
+    if (tail_usable(P, l) && (const void*)b == Lv.b && (const void*)out == Lv.res) {
+      if (P.st_bf16 && P.lv[l].S16)
+        launch_tail<__nv_bfloat16>(P, l);
+      else
+        launch_tail<float>(P, l);
+      return;
+    }
+  }
   const int visits0 =
       (P.cycle_w && std::find(P.w_levels.begin(), P.w_levels.end(), l) != P.w_levels.end()) ? 2 : 1;
   if constexpr (std::is_same<T, float>::value && std::is_same<TD0, __nv_bfloat16>::value) {
@@ -1067,12 +1175,8 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
         fine3_cube_fused(P, b, Lv.dinv, nullptr, in, e, nullptr, nullptr, 4 + 2 + 4);
       }
       Level& Lc = P.lv[1];
-      P.cur_cat = CAT_TRANSFER;
-      launch(P, k_restrict3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g, r,
-             (T*)Lc.b);
-      KCHECK();
-      P.cur_cat = CAT_VECTOR;
-      vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr);
+      restrict_to<T>(P, l, r);
+      vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr, restrict_j0(P, l));
       T* e1 = (T*)Lv.ea;
       P.cur_cat = CAT_TRANSFER;
       launch(P, k_prolong3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g,
@@ -1100,9 +1204,10 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
       level_apply<T>(P, l, in, e);
     }
   };
-  // pre-smoothing from x = 0
+  // pre-smoothing from x = 0 (the first sweep already done by the restriction when pre_done)
   if (nsm >= 1) {
-    if (l == 0)
+    if (pre_done) {
+    } else if (l == 0)
       launch(P, k_jacobi0<T, TD0, T>, ew_blocks(nv), 256, 0, nv, b, (const TD0*)Lv.dinv, x, om, ws);
     else
       launch(P, k_jacobi0<T, T, T>, ew_blocks(nv), 256, 0, nv, b, (const T*)Lv.dinv, x, om, ws);
@@ -1124,15 +1229,8 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     }
     const T* xcur = first ? x : out;
     Level& Lc = P.lv[l + 1];
-    P.cur_cat = CAT_TRANSFER;
-    if (P.dim == 3)
-      launch(P, k_restrict3<T, T>, dim3(cdiv((long long)Lc.g.nz * Lc.g.nx, 256), Lc.g.ny), 256, 0, g, Lc.g, r,
-             (T*)Lc.b);
-    else
-      launch(P, k_restrict2<T, T>, dim3(cdiv(Lc.g.nx, 64), Lc.g.ny), 64, 0, g, Lc.g, r, (T*)Lc.b);
-    KCHECK();
-    P.cur_cat = CAT_VECTOR;
-    vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr);
+    restrict_to<T>(P, l, r);
+    vcycle<T, TD0, T>(P, l + 1, (const T*)Lc.b, (T*)Lc.res, (const T*)nullptr, nullptr, restrict_j0(P, l));
     T* e1 = (T*)Lv.ea;
     T* e2 = (T*)Lv.eb;
     P.cur_cat = CAT_TRANSFER;
@@ -1214,6 +1312,10 @@ static void mg_allocate(Prob& P) {
                           8192 * (int)sizeof(double)));
   CK(cudaFuncSetAttribute(k_coarse_solve<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           8192 * (int)sizeof(double)));
+  if (!P.tail_bar) {
+    P.tail_bar = P.alloc<unsigned>(2);
+    CK(cudaMemset(P.tail_bar, 0, 2 * sizeof(unsigned)));
+  }
   P.Adense = P.alloc<double>((size_t)P.nd * P.nd);
   P.Ainv = P.alloc<double>((size_t)P.nd * P.nd);
   P.Ut = P.alloc<double>((size_t)P.nd * P.nd);
@@ -1453,7 +1555,7 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, boo
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons,
                            (double)P.st_bf16, (double)P.st_pair, (double)P.st_pair_min, (double)P.res32,
-                           (double)P.pdl, (double)P.fuse, (double)P.omega_carry, (double)(P.omega_carry && P.omega_started)};
+                           (double)P.pdl, (double)P.fuse, (double)P.tail_l0, (double)P.omega_carry, (double)(P.omega_carry && P.omega_started)};
   for (int l : P.w_levels) k.push_back((double)l);
   k.push_back(-1.0);
   for (int v : P.level_sweeps) k.push_back((double)v);
@@ -2056,6 +2158,14 @@ int edge_set_pdl(edge_problem* p, int enable) {
   API_BEGIN
   if (!p) fail(EDGE_EINVAL, "null handle");
   p->P.pdl = enable != 0;
+  API_END
+}
+
+int edge_set_tail(edge_problem* p, int level) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  if (level < 0) fail(EDGE_EINVAL, "level must be >= 0");
+  p->P.tail_l0 = level;
   API_END
 }
 

@@ -117,6 +117,12 @@ int edge_mg_set_omega_carry(edge_problem* p, int enable);
  * PCG search direction p = z + beta p is formed inside the product q = A p; 0 runs the same
  * arithmetic as separate launches.  No counterpart in the reference. */
 int edge_set_fuse(edge_problem* p, int enable);
+/* Mixed precision, 3-D: the V-cycle from `level` down to the coarsest solve (smoothing
+ * sweeps, residuals, transfers, the dense coarsest solve) as one persistent cooperative
+ * launch with bounded grid barriers between its stages, instead of one launch per step;
+ * 0 (default) = every step its own launch.  The same arithmetic per node.  No counterpart
+ * in the reference. */
+int edge_set_tail(edge_problem* p, int level);
 /* Kernel launches made through this problem so far (a launch inside a graph counts once per
  * execution; edge_profile_begin resets the tally). */
 int edge_launch_count(const edge_problem* p, long long* n);

@@ -448,6 +448,43 @@ def test_fused_fine_launches_agree():
     assert ih == i_f and rel(xh, xf) < 1e-12
 
 
+@pytest.mark.parametrize("sweeps", [(1, 1, 1, 1), (1, 2, 3, 1)])
+def test_persistent_vcycle_tail_agrees(sweeps):
+    """Mixed precision: the V-cycle below level 1 as one persistent cooperative launch
+    (edge_set_tail 2) against one launch per step (edge_set_tail 0, the default), with one and
+    with several sweeps per level: the same arithmetic per node except for the summation order
+    of the small levels' stencils, so iteration counts within 1 and solutions within 1e-7;
+    graph and host-driven loops agree exactly."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    p = topopt.cantilever_problem(64, 32, 32, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=4, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(17)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    mesh = _mesh(3, (64, 32, 32), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    f = torch.as_tensor(p.f, device="cuda")
+    out = {}
+    for tail, graph in ((0, True), (2, True), (2, False)):
+        s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=4, maxiter=500, precision="mixed", autotune=False,
+                           tune_sweeps=False, graph=graph)
+        s._configure()
+        _lib.call("edge_mg_set_sweeps", k.handle, _lib.int_array(list(sweeps)), 4)
+        _lib.call("edge_set_tail", k.handle, tail)
+        x, r = s.solve(f, use_last=False)
+        out[(tail, graph)] = (x.cpu().numpy().copy(), s.last_iters, r)
+    _lib.call("edge_set_tail", k.handle, 0)
+    (x0, i0, r0), (x1, i1, r1), (xh, ih, rh) = out[(0, True)], out[(2, True)], out[(2, False)]
+    print("iterations per-launch / persistent / persistent host loop", i0, i1, ih)
+    assert r0 < 1e-8 and r1 < 1e-8 and rh < 1e-8
+    assert abs(i0 - i1) <= 1
+    assert rel(x1, x0) < 1e-7
+    assert ih == i1 and rel(xh, x1) < 1e-12
+
+
 def test_residual_recurrence_precisions_agree():
     """Mixed precision with the residual recurrence stored in FP32 (default) and in FP64: both
     meet the tolerance on the FP64 true residual, take about the same iterations and give the
