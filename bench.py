@@ -574,7 +574,7 @@ def run_tiles(args, cfg_name):
         _lib.call("edge_mg_setup", h)
     torch.cuda.synchronize()
     prec = 1 if args.precision == "mixed" else 0
-    nvar = 5 if args.precision == "fp64" else (15 if _lib.lib().edge_uses_cube_form(h) else 9)
+    nvar = 5 if args.precision == "fp64" else (16 if _lib.lib().edge_uses_cube_form(h) else 9)
     k = opt.kernel
     n_dof, n_el = k.shape[0], k.n_elements
     w = 8 if args.precision == "fp64" else 4
@@ -701,7 +701,7 @@ def main():
     ap.add_argument("--no-fuse", action="store_true",
                     help="mixed path: the fine level's sweeps and search direction as separate launches")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles"])
-    ap.add_argument("--tile", type=int, default=None, help="matvec/tiles mode: fine-kernel tile variant (0-14)")
+    ap.add_argument("--tile", type=int, default=None, help="matvec/tiles mode: fine-kernel tile variant (0-15)")
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--n-smooth", type=int, default=3,
                     help="default smoothing sweeps of the timed path (the FP64 path keeps the reference's 3)")

@@ -784,6 +784,7 @@ static void fine3_cube_fused(Prob& P, const float* in0, const void* in1, const v
     case 11: fine3_cube_go<SE, IN, 2, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
     case 12: fine3_cube_go<SE, IN, 8, 3, 1>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
     case 13: fine3_cube_go<SE, IN, 4, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
+    case 15: fine3_cube_go<SE, IN, 4, 3, 3>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
     default: fine3_cube_go<SE, IN, 4, 4, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
   }
   if (rec) {
@@ -814,6 +815,7 @@ static void fine_apply(Prob& P, const T* u, Epi epi, double* dot_dst) {
             case 11: fine3_cube_launch<Epi, 2, 3, 4>(P, u, E, epi, dot_dst); break;
             case 12: fine3_cube_launch<Epi, 8, 3, 1>(P, u, E, epi, dot_dst); break;
             case 13: fine3_cube_launch<Epi, 4, 3, 4>(P, u, E, epi, dot_dst); break;
+            case 15: fine3_cube_launch<Epi, 4, 3, 3>(P, u, E, epi, dot_dst); break;
             default: fine3_cube_launch<Epi, 4, 4, 4>(P, u, E, epi, dot_dst); break;
           }
           packed = true;
@@ -2297,7 +2299,7 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
   int bv = P.tile_variant, bb = P.blocks_per_sm;
   const int bps_list[4] = {2, 4, 8, 16};
   // variants 5..8: packed-pair FP32 kernel; 9..12: its cube-element form
-  const int nvar = precision == EDGE_FP64 ? 5 : (P.cube ? 15 : 9);
+  const int nvar = precision == EDGE_FP64 ? 5 : (P.cube ? 16 : 9);
   const bool sweep = can_time_sweep(P, precision);
   const bool mix = sweep && precision != EDGE_FP64;  // time the whole per-iteration mix
   for (int v = 0; v < nvar; ++v)

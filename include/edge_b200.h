@@ -70,8 +70,8 @@ int edge_matvec_dense(edge_problem* p, const double* u_dev, double* out_dev);
  * cooperative-load version of the same kernel. */
 int edge_set_tma(edge_problem* p, int enable);
 /* Fine-kernel tile: variant 0..4 = k_fine3_tma (warps, TMA stages) (8,4) (8,3) (8,2) (4,4)
- * (4,3); FP32 only: 5..8 = packed-pair k_fine3_pk, 9..14 = its cube-element block form
- * k_fine3_cube (used when edge_uses_cube_form is 1, else 9..14 run k_fine3_pk); and the
+ * (4,3); FP32 only: 5..8 = packed-pair k_fine3_pk, 9..15 = its cube-element block form
+ * k_fine3_cube (used when edge_uses_cube_form is 1, else 9..15 run k_fine3_pk); and the
  * target of resident blocks per SM that sets the y-chunking of the grid. */
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm);
 /* Autotuner: times every tile variant and y-chunking on the current density with the plain
