@@ -408,8 +408,8 @@ def run_ours(args, cfg_name):
         "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_cube/_pk/_tma + fused epilogues)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                     "traffic": traffic, "traffic_case": "ncu DRAM bytes of one plain-product launch"
-                     if traffic else None, "launches": prof["kernel_launches"], "kernel_ms": kms,
+                     "traffic": traffic, "traffic_case": "ncu DRAM bytes per launch, mean over the three fused "
+                     "fine launches of one PCG iteration (profiles/fine_operator_traffic.json)" if traffic else None, "launches": prof["kernel_launches"], "kernel_ms": kms,
                      "algorithmic_bytes_per_launch": kby / max(1, prof["kernel_launches"]),
                      "share_of_step": kms / pm["t_ms"] if pm["t_ms"] else None,
                      "timing": "CUDA events around every fine-operator launch of one SIMP step run right "
@@ -616,6 +616,35 @@ def run_tiles(args, cfg_name):
             "stencil_levels": levels}
 
 
+def run_analysis(args, cfg_name):
+    """Profiling helper: one SIMP analysis (filter, SIMP law, solve, sensitivities) of the
+    workload at rho = vf with the fine tile, the per-level sweeps, the persistent-tail level
+    and maxiter pinned (--tile/--tile-bps, --sweeps, --tail, --maxiter) and no autotuning, so a
+    profiler sees a fixed, short sequence of launches (--no-graph: every kernel its own launch).
+    Prints its own JSON line."""
+    import torch
+    from edge_to_b200 import _lib
+    cfg = CONFIGS[cfg_name]
+    opt, rho = build_problem(cfg, args.precision, args.n_smooth, graph=not args.no_graph)
+    sv = opt.solver
+    sv.autotune = False
+    sv.tune_sweeps = False
+    sv._configure()
+    h = opt.kernel.handle
+    _lib.call("edge_set_fine_tile", h, 10 if args.tile is None else args.tile, args.tile_bps)
+    if args.sweeps:
+        pat = [int(v) for v in args.sweeps.split(",")]
+        _lib.call("edge_mg_set_sweeps", h, _lib.int_array(pat), len(pat))
+    _lib.call("edge_set_tail", h, args.tail)
+    if args.no_fuse:
+        _lib.call("edge_set_fuse", h, 0)
+    sv.maxiter = args.maxiter
+    c, dr, res = opt.solve_and_process(rho, 0)
+    torch.cuda.synchronize()
+    return {"mode": "analysis", "workload": cfg_name, "precision": args.precision, "pcg_iters":
+            opt.last_stats.get("pcg_iters"), "residual": res, "compliance": float(c)}
+
+
 def run_batch(args):
     """Batching configuration: randomized 2-D problems of uneven size (edge_to_b200.batch),
     spread over host threads with one CUDA stream each; value = problem-iterations per second
@@ -700,7 +729,10 @@ def main():
                     help="skip the FP64 trajectory at rtol 1e-10 the timed paths are compared with")
     ap.add_argument("--no-fuse", action="store_true",
                     help="mixed path: the fine level's sweeps and search direction as separate launches")
-    ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles"])
+    ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles", "analysis"])
+    ap.add_argument("--maxiter", type=int, default=12, help="analysis mode: PCG iteration limit")
+    ap.add_argument("--tail", type=int, default=0,
+                    help="analysis mode: level from which the V-cycle is one persistent launch (0 = off)")
     ap.add_argument("--tile", type=int, default=None, help="matvec/tiles mode: fine-kernel tile variant (0-15)")
     ap.add_argument("--tile-bps", type=int, default=8, help="matvec mode: y-chunking target (blocks per SM)")
     ap.add_argument("--n-smooth", type=int, default=3,
@@ -730,6 +762,8 @@ def main():
         line = run_matvec(args, args.config)
     elif args.mode == "tiles":
         line = run_tiles(args, args.config)
+    elif args.mode == "analysis":
+        line = run_analysis(args, args.config)
     else:
         line = run_ours(args, args.config)
     if line is not None:
