@@ -273,6 +273,8 @@ def run_ours(args, cfg_name):
     if args.no_fuse:
         from edge_to_b200 import _lib as _l
         _l.call("edge_set_fuse", opt.kernel.handle, 0)
+    if args.omega_schedule:
+        opt.solver.mixed_omega = None
     traj = []
     rho, dr, it = warm(opt, rho, args.warmup, traj)
     # the state the timed steps start from; the end-to-end steps restart from it, so both
@@ -327,6 +329,7 @@ def run_ours(args, cfg_name):
     bd = breakdown(opt, rho, dr, it) if args.breakdown else None
     tuned = opt.solver.tuned
     sweeps = opt.solver.sweeps
+    fixed_omega = opt.solver.fixed_omega
     del opt, rho, dr, rho_h, out_h
 
     # ---------------- the plain FP64 path on the same workload, same steps (the metric's
@@ -404,7 +407,9 @@ def run_ours(args, cfg_name):
                    "coarse_stencils": "fp32" if (args.coarse_fp32 or args.precision == "fp64") else "bf16",
                    "residual_recurrence": "fp64" if (args.residual64 or args.precision == "fp64") else "fp32",
                    "programmatic_dependent_launch": args.pdl and not args.no_graph,
-                   "fused_fine_launches": args.precision == "mixed" and not args.no_fuse},
+                   "fused_fine_launches": args.precision == "mixed" and not args.no_fuse,
+                   "smoother_omega": (f"fixed at {fixed_omega}" if fixed_omega is not None
+                                      else "reference schedule (0.40-0.45 on the fine level)")},
         "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_cube/_pk/_tma + fused epilogues)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
@@ -729,6 +734,8 @@ def main():
                     help="skip the FP64 trajectory at rtol 1e-10 the timed paths are compared with")
     ap.add_argument("--no-fuse", action="store_true",
                     help="mixed path: the fine level's sweeps and search direction as separate launches")
+    ap.add_argument("--omega-schedule", action="store_true",
+                    help="mixed path: the reference's residual-driven smoother weight (default: fixed at omega)")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles", "analysis"])
     ap.add_argument("--maxiter", type=int, default=12, help="analysis mode: PCG iteration limit")
     ap.add_argument("--tail", type=int, default=0,

@@ -140,13 +140,29 @@ class CuMultiGrid(Solver):
     def __init__(self, mesh, kernel, maxiter=1000, tol=1e-5, n_smooth=3, omega=0.5, n_level=3, cycle="W",
                  w_level=1, coarse_solver="splu", matrix_free=False, low_level_tol=1e-8, low_level_maxiter=5000,
                  min_omega=0.4, omega_boost=1.06, precision="fp64", autotune=True, graph=True, tune_sweeps=None,
-                 omega_carry=None):
+                 omega_carry=None, mixed_omega="auto"):
         if not isinstance(kernel, CuStructuredStiffnessKernel):
             raise TypeError("CuMultiGrid needs the package's CuStructuredStiffnessKernel")
         # smoother weight across solves: reset to min_omega every solve (the GPU solver,
         # solvers/_multigrid_cuda.py:210) or carried over from the last solve (the CPU solver,
         # solvers/_multigrid.py:178-225; the MultiGrid class below)
         self.omega_carry = self.OMEGA_CARRY if omega_carry is None else bool(omega_carry)
+        # the mixed-precision preconditioner's smoother weight.  The reference's schedule moves
+        # between min_omega and (min_omega + omega) / 2 with the residual
+        # (solvers/_multigrid_cuda.py:227); "max" holds it fixed at omega, the schedule's upper
+        # bound, and a number holds it there; None keeps the schedule; "auto" (the default)
+        # starts on the schedule and lets the sweep autotuner time the weight fixed at omega
+        # against it on its tuning solve, keeping the faster.  A solve that does not converge
+        # with a fixed weight runs again from the same start on the schedule, which is kept from
+        # then on.  Coarser levels scale the weight by omega_boost**level either way, and the
+        # FP64 path always keeps the schedule.
+        if not (mixed_omega is None or mixed_omega in ("auto", "max")
+                or (isinstance(mixed_omega, (int, float)) and mixed_omega > 0)):
+            raise ValueError("mixed_omega must be None, 'auto', 'max' or a positive number")
+        self.mixed_omega = mixed_omega
+        self._omega_mode = "fixed" if mixed_omega not in (None, "auto") else "schedule"
+        self._omega_failed = False
+        self._x_keep = None
         self.kernel = kernel
         self.mesh = mesh
         self.last_x0 = None
@@ -196,22 +212,62 @@ class CuMultiGrid(Solver):
                                       n_smooth=n_smooth, omega=omega, n_level=n_level, cycle=cycle, w_level=w_level,
                                       min_omega=min_omega, omega_boost=omega_boost, precision=precision,
                                       autotune=autotune, graph=graph, tune_sweeps=tune_sweeps,
-                                      omega_carry=self.omega_carry)
+                                      omega_carry=self.omega_carry, mixed_omega=mixed_omega)
 
     def reset(self):
         self.last_x0 = None
         if self._inner is not None:
             self._inner.reset()
 
+    def _omega_value(self):
+        """The weight a fixed mode would hold (None: this solver only runs the schedule)."""
+        if self.precision != "mixed" or self.mixed_omega is None:
+            return None
+        return float(self.max_omega) if self.mixed_omega in ("auto", "max") else float(self.mixed_omega)
+
+    @property
+    def fixed_omega(self):
+        """The smoother weight the mixed path holds fixed now, or None (the reference's schedule)."""
+        return self._omega_value() if self._omega_mode == "fixed" else None
+
+    def _set_omega_mode(self, mode):
+        self._omega_mode = mode
+        if self._inner is not None:
+            self._inner._set_omega_mode(mode)
+        self._configure()
+
+    def use_omega_schedule(self):
+        """Move the mixed path from a fixed smoother weight to the reference's schedule for good
+        (after a solve the fixed weight did not converge); returns False when it already runs
+        the schedule."""
+        if self.fixed_omega is None:
+            return False
+        self._omega_failed = True
+        self._set_omega_mode("schedule")
+        return True
+
+    def keep_start(self, x):
+        """Copy of a warm start, for the rerun of a solve that the fixed weight did not converge."""
+        if self.fixed_omega is None:
+            return None
+        if self._x_keep is None or self._x_keep.shape != x.shape:
+            self._x_keep = torch.empty_like(x)
+        self._x_keep.copy_(x)
+        return self._x_keep
+
     def _configure(self):
+        fixed = self.fixed_omega
         key = (self.n_level, self.n_smooth, self.max_omega, self.min_omega, self.cycle, tuple(self.w_level),
-               self.precision, bool(self.graph))
+               self.precision, bool(self.graph), fixed)
         if self._configured == key:
             return
         w = _lib.int_array(self.w_level) if self.w_level else None
         prec = _lib.EDGE_FP64 if self.precision == "fp64" else _lib.EDGE_MIXED
-        _lib.call("edge_mg_config", self.kernel.handle, int(self.n_level), int(self.n_smooth), float(self.max_omega),
-                  float(self.min_omega), 1 if self.cycle == "w" else 0, w, len(self.w_level), prec)
+        om, om_min = float(self.max_omega), float(self.min_omega)
+        if fixed is not None:
+            om = om_min = fixed
+        _lib.call("edge_mg_config", self.kernel.handle, int(self.n_level), int(self.n_smooth), om, om_min,
+                  1 if self.cycle == "w" else 0, w, len(self.w_level), prec)
         _lib.call("edge_set_graph", self.kernel.handle, 1 if self.graph else 0)
         if self._configured is None:
             _lib.call("edge_mg_set_omega_carry", self.kernel.handle, 1 if self.omega_carry else 0)
@@ -278,9 +334,26 @@ class CuMultiGrid(Solver):
             best = (0.0, [self.n_smooth] * self.n_level, 0)
         else:
             best = pick_sweep_pattern(runs, timed_solve, self.SWEEP_MARGIN, fallback=[self.n_smooth] * self.n_level)
+        found = bool(runs) and best[0] > 0.0
+        best_ms = best[0] / 2 if found else None
+        omega = None
+        if self._omega_value() is not None and not self._omega_failed:
+            # the chosen pattern once more with the other smoother weight (fixed at omega, or the
+            # reference's schedule): keep the faster of the two that converged
+            mode = self._omega_mode
+            other = "schedule" if mode == "fixed" else "fixed"
+            self._set_omega_mode(other)
+            ms_o, ok_o, it_o = timed_solve(best[1])
+            switch = ok_o and (not found or ms_o < best_ms)
+            omega = {"fixed": self._omega_value(), mode + "_ms": round(best_ms, 3) if found else None,
+                     other + "_ms": round(ms_o, 3) if ok_o else None, "chosen": other if switch else mode}
+            if switch:
+                best, best_ms = (ms_o, best[1], it_o), ms_o
+            else:
+                self._set_omega_mode(mode)
         _lib.call("edge_mg_set_sweeps", self.kernel.handle, _lib.int_array(best[1]), len(best[1]))
-        self.sweeps = {"per_level": best[1], "solve_ms": best[0] / (2 if runs else 1), "pcg_iters": best[2],
-                       "tune_tol": tol, "candidates": candidates}
+        self.sweeps = {"per_level": best[1], "solve_ms": best_ms or 0.0, "pcg_iters": best[2],
+                       "tune_tol": tol, "candidates": candidates, "omega": omega}
         return self.sweeps
 
     @property
@@ -320,8 +393,15 @@ class CuMultiGrid(Solver):
         res = ctypes.c_double()
         its = ctypes.c_int()
         self.kernel._bind_stream()
+        keep = self.keep_start(x) if warm else None
         _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
                   int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
+        if not res.value < self.tol and self.use_omega_schedule():
+            # the fixed smoother weight did not converge: the same solve with the schedule
+            if keep is not None:
+                x.copy_(keep)
+            _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
+                      int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
         self.last_x0 = x
         self.last_iters = its.value
         return x, res.value

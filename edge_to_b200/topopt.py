@@ -245,10 +245,17 @@ class CuTopOpt:
         rho_f = torch.empty_like(dr)
         c, res, its = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
         self.kernel._bind_stream()
-        _lib.call("edge_simp_solve_and_process", self.kernel.handle, self.filter_kernel.handle, _lib.ptr(rho), pen,
-                  float(self.material_model.void), _lib.ptr(self.f), _lib.ptr(U), 1 if use_last else 0,
-                  float(sv.tol), int(sv.maxiter), ctypes.byref(c), _lib.ptr(dr), _lib.ptr(rho_f), ctypes.byref(res),
-                  ctypes.byref(its))
+        keep = sv.keep_start(U) if use_last else None
+        for attempt in range(2):
+            _lib.call("edge_simp_solve_and_process", self.kernel.handle, self.filter_kernel.handle, _lib.ptr(rho),
+                      pen, float(self.material_model.void), _lib.ptr(self.f), _lib.ptr(U), 1 if use_last else 0,
+                      float(sv.tol), int(sv.maxiter), ctypes.byref(c), _lib.ptr(dr), _lib.ptr(rho_f),
+                      ctypes.byref(res), ctypes.byref(its))
+            # the fixed smoother weight did not converge: once more with the reference's schedule
+            if attempt or res.value < sv.tol or not sv.use_omega_schedule():
+                break
+            if keep is not None:
+                U.copy_(keep)
         self.kernel.has_rho = True
         sv.last_iters = its.value
         self._U = U
@@ -282,11 +289,19 @@ class CuTopOpt:
         A = float(np.asarray(self.mesh.As).reshape(-1)[0])
         pen = float(self.material_model.current_penalty(iteration))
         self.kernel._bind_stream()
-        _lib.call("edge_simp_iteration", self.kernel.handle, self.filter_kernel.handle, _lib.ptr(rho), _lib.ptr(df), A,
-                  float(self.mesh.volume), float(self.material_model.volume_fraction), float(self.move), pen,
-                  float(self.material_model.void), _lib.ptr(self.f), _lib.ptr(U), 1, float(sv.tol), int(sv.maxiter),
-                  _lib.ptr(rho_new), _lib.ptr(dr), _lib.ptr(rho_f), ctypes.byref(c), ctypes.byref(res),
-                  ctypes.byref(its), ctypes.byref(lam), ctypes.byref(steps), ctypes.byref(sq))
+        keep = sv.keep_start(U)
+        for attempt in range(2):
+            _lib.call("edge_simp_iteration", self.kernel.handle, self.filter_kernel.handle, _lib.ptr(rho),
+                      _lib.ptr(df), A, float(self.mesh.volume), float(self.material_model.volume_fraction),
+                      float(self.move), pen, float(self.material_model.void), _lib.ptr(self.f), _lib.ptr(U), 1,
+                      float(sv.tol), int(sv.maxiter), _lib.ptr(rho_new), _lib.ptr(dr), _lib.ptr(rho_f),
+                      ctypes.byref(c), ctypes.byref(res), ctypes.byref(its), ctypes.byref(lam), ctypes.byref(steps),
+                      ctypes.byref(sq))
+            # the fixed smoother weight did not converge: once more with the reference's schedule
+            if attempt or res.value < sv.tol or not sv.use_omega_schedule():
+                break
+            if keep is not None:
+                U.copy_(keep)
         self.kernel.has_rho = True
         sv.last_iters = its.value
         self._U = U

@@ -324,8 +324,10 @@ def test_packed_kernel_in_mixed_solve():
         _lib.call("edge_set_fine_tile", k.handle, v, 8)
         x, r = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
         res.append((x.cpu().numpy().copy(), s.last_iters, r))
+    # the variants sum the element products in different FP32 orders: the PCG iteration count at
+    # rtol 1e-8 moves by a few (42-45 here), the converged solutions agree
     for x, it, r in res[1:]:
-        assert abs(it - res[0][1]) <= 2 and r < 1e-8
+        assert abs(it - res[0][1]) <= max(2, res[0][1] // 10) and r < 1e-8
         assert rel(x, res[0][0]) < 1e-6
 
 
