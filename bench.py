@@ -651,9 +651,11 @@ def run_analysis(args, cfg_name):
 
 
 def run_batch(args):
-    """Batching configuration: randomized 2-D problems of uneven size (edge_to_b200.batch),
-    spread over host threads with one CUDA stream each; value = problem-iterations per second
-    (one SIMP iteration of one problem = filter + SIMP law + GMG-PCG solve + sensitivities + OC).
+    """Batching configuration: randomized 2-D problems of uneven size (edge_to_b200.batch);
+    by default every SIMP stage's solves and OC updates run as one persistent launch each
+    (BatchSIMP(persistent=True)), else per-problem solve graphs on host threads with one CUDA
+    stream each; value = problem-iterations per second (one SIMP iteration of one problem =
+    filter + SIMP law + GMG-PCG solve + sensitivities + OC).
     With N ranks every rank solves its own batch_size problems (batch.shard_specs: disjoint
     seeded problems, no collective on the data path; weak scaling), timed between barriers
     and taken over the slowest rank."""
@@ -668,7 +670,12 @@ def run_batch(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     n = args.batch_size
     specs = batch.shard_specs(n, rank, seed=0)
-    b = batch.BatchSIMP(specs, precision=args.precision, tol=1e-6, maxiter=1000, n_threads=args.batch_threads)
+    persistent = args.batch_mode == "persistent"
+    sweeps = tuple(int(v) for v in args.batch_sweeps.split(",")) if (persistent and args.batch_sweeps) else None
+    max_level = args.batch_max_level if args.batch_max_level else (6 if persistent else 4)
+    b = batch.BatchSIMP(specs, precision=args.precision, tol=1e-6, maxiter=1000, n_threads=args.batch_threads,
+                        persistent=persistent, max_level=max_level, block_threads=args.batch_block,
+                        sweeps=sweeps, team=args.batch_team)
     b.step(args.warmup)               # initial analysis, autotuners, warm-up iterations
     clocks = ClockSampler(local)
     clocks.start()
@@ -694,7 +701,11 @@ def run_batch(args):
                        "parallelism": f"independent problems x{ws}" if ws > 1 else "1 GPU",
                        "dof_total_rank0": int(np.sum(dofs)),
                        "elements_total_rank0": int(sum(sp["nelx"] * sp["nely"] for sp in specs)),
-                       "rtol": 1e-6, "precision": args.precision, "threads_streams": b.n_threads,
+                       "rtol": 1e-6, "precision": args.precision, "mode": args.batch_mode,
+                       "threads_streams": b.n_threads, "max_level": max_level,
+                       "solve_launch": ({"threads_per_block": args.batch_block, "blocks_per_problem": args.batch_team,
+                                         "sweeps_fine_coarse": sweeps} if persistent else None),
+                       "pcg_iters_max_rank0": int(max(max(it["pcg"][-args.steps:]) for it in b.items)),
                        "padded_problems_rank0": int(sum(it["opt"].solver.padded for it in b.items)),
                        "pcg_iters_mean_rank0": float(np.mean(pcg))},
             "clocks": clk}
@@ -756,7 +767,18 @@ def main():
     ap.add_argument("--batch", action="store_true",
                     help="the batching configuration (random uneven 2-D problems) instead of --config")
     ap.add_argument("--batch-size", type=int, default=256)
-    ap.add_argument("--batch-threads", type=int, default=16)
+    ap.add_argument("--batch-threads", type=int, default=16, help="batch, threads mode: host threads / streams")
+    ap.add_argument("--batch-mode", default="persistent", choices=["threads", "persistent"],
+                    help="batch: every solve and OC update of a SIMP stage in one persistent launch (default), or "
+                         "per-problem solve graphs on host threads")
+    ap.add_argument("--batch-max-level", type=int, default=0,
+                    help="batch: deepest multigrid per problem (0: 6 persistent, 4 threads)")
+    ap.add_argument("--batch-block", type=int, default=1024, choices=[256, 512, 1024],
+                    help="batch, persistent mode: threads per block of the solve launch")
+    ap.add_argument("--batch-team", type=int, default=4, choices=[1, 2, 4, 8],
+                    help="batch, persistent mode: blocks (a thread block cluster) per problem")
+    ap.add_argument("--batch-sweeps", default="1,2",
+                    help="batch, persistent mode: smoothing sweeps on the fine level and on coarser levels")
     ap.add_argument("--breakdown", action="store_true",
                     help="extra untimed step with per-category launch timing (events on every launch)")
     args = ap.parse_args()

@@ -89,7 +89,7 @@ def n_level_for(nelx, nely, max_level=4):
     return lv
 
 
-def build(spec, precision="mixed", tol=1e-6, maxiter=1000):
+def build(spec, precision="mixed", tol=1e-6, maxiter=1000, max_level=4):
     """CuTopOpt of one problem (and its initial design rho = vf)."""
     from . import (CuMultiGrid, CuStructuredFilter2D, CuStructuredMesh2D, CuStructuredStiffnessKernel, CuTopOpt,
                    SingleMaterial, auto_stiffness)
@@ -98,7 +98,7 @@ def build(spec, precision="mixed", tol=1e-6, maxiter=1000):
     mat = SingleMaterial(E=1.0, nu=0.3, void=1e-9, penalty=3.0, volume_fraction=spec["vf"])
     kernel = CuStructuredStiffnessKernel(mesh)
     filt = CuStructuredFilter2D(mesh, spec["rmin"])
-    solver = CuMultiGrid(mesh, kernel, tol=tol, n_level=n_level_for(nelx, nely), maxiter=maxiter,
+    solver = CuMultiGrid(mesh, kernel, tol=tol, n_level=n_level_for(nelx, nely, max_level), maxiter=maxiter,
                          precision=precision)
     opt = CuTopOpt(mesh, mat, kernel, solver, filt, max_iter=1, move=0.2, ch_tol=0, fun_tol=0, verbose=False)
     opt.add_BC_nodal(spec["clamped_nodes"], np.array([[True, True]]))
@@ -107,21 +107,161 @@ def build(spec, precision="mixed", tol=1e-6, maxiter=1000):
     return opt, rho
 
 
+class BatchAnalysis:
+    """The analyses of many problems with all their solves in one persistent launch
+    (edge_batch_solve_and_process): ``solve_and_process(rhos, iteration)`` is the batched form
+    of CuTopOpt.solve_and_process for a list of CuTopOpt objects on 2-D structured grids with
+    CuMultiGrid solvers (V-cycle) and one SingleMaterial law.  A problem whose solver runs on a
+    padded grid contributes that grid's problem (its constraints set once here); the filter,
+    law and sensitivities stay on the real grid.  The FP64 Krylov recurrence of the batched
+    solve is preconditioned by each solver's V-cycle in its precision."""
+
+    def __init__(self, opts, threads=512, sweeps=None, team=1):
+        import ctypes
+        from . import CuMultiGrid, SingleMaterial, _lib
+        self.opts = list(opts)
+        probs, filts, nelx, nely = [], [], [], []
+        for opt in self.opts:
+            sv = opt.solver
+            if not isinstance(sv, CuMultiGrid) or not isinstance(opt.material_model, SingleMaterial):
+                raise TypeError("BatchAnalysis needs CuMultiGrid solvers and SingleMaterial laws")
+            if sv.padded:
+                if not opt.kernel.has_rho:  # the padded grid's constraints are copied with a density
+                    opt.kernel.set_rho(torch.full((opt.mesh.n_elements,), float(opt.material_model.void),
+                                                  dtype=torch.float64, device="cuda"))
+                sv._pad.sync(opt.kernel)
+                inner = sv._inner
+                inner.tol, inner.maxiter = sv.tol, sv.maxiter
+                inner._configure()
+                h = inner.kernel.handle
+            else:
+                sv._configure()
+                h = opt.kernel.handle
+            if sweeps is not None:  # (fine level, coarser levels) smoothing sweeps per V-cycle
+                pat = [int(sweeps[0])] + [int(sweeps[-1])] * (int(sv.n_level) - 1)
+                _lib.call("edge_mg_set_sweeps", h, _lib.int_array(pat), len(pat))
+            probs.append(h)
+            filts.append(opt.filter_kernel.handle)
+            nelx.append(int(opt.mesh.nel[0]))
+            nely.append(int(opt.mesh.nel[1]))
+        n = len(self.opts)
+        laws = {(float(o.material_model.void), float(o.material_model.current_penalty(0))) for o in self.opts}
+        if len(laws) != 1:
+            raise ValueError("every problem of a batch needs the same void stiffness and penalty")
+        self._probs = (ctypes.c_void_p * n)(*probs)
+        self._filts = (ctypes.c_void_p * n)(*filts)
+        h = ctypes.c_void_p()
+        _lib.call("edge_batch_create", n, self._probs, self._filts, _lib.int_array(nelx), _lib.int_array(nely),
+                  ctypes.byref(h))
+        self.handle = h
+        _lib.call("edge_batch_set_threads", self.handle, int(threads), int(team))
+        self.U = [torch.zeros_like(o.f) for o in self.opts]
+        self.warm = False
+        self.last_iters = [0] * n
+
+    def close(self):
+        from . import _lib
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            _lib.call("edge_batch_destroy", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    def update_design(self, rhos, drs):
+        """The OC updates of every problem in one launch (edge_batch_oc_update): the batched
+        form of CuTopOpt.update_design; returns the new designs."""
+        import ctypes
+        from . import _lib
+        n = len(self.opts)
+        rhos = [r.reshape(-1).to(dtype=torch.float64).contiguous() for r in rhos]
+        drs = [d.reshape(-1).to(dtype=torch.float64).contiguous() for d in drs]
+        new = [torch.empty_like(r) for r in rhos]
+        P = lambda ts: (ctypes.c_void_p * n)(*[t.data_ptr() for t in ts])  # noqa: E731
+        moves = {float(o.move) for o in self.opts}
+        if len(moves) != 1:
+            raise ValueError("every problem of a batch needs the same move limit")
+        A = _lib.double_array([float(np.asarray(o.mesh.As).reshape(-1)[0]) for o in self.opts])
+        vol = _lib.double_array([float(o.mesh.volume) for o in self.opts])
+        vf = _lib.double_array([float(o.material_model.volume_fraction) for o in self.opts])
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.call("edge_batch_oc_update", self.handle, P(rhos), P(drs), A, vol, vf, moves.pop(), P(new), None, None,
+                  stream)
+        return new
+
+    def solve_and_process(self, rhos, iteration):
+        """(compliances, drs, residuals) of the designs rhos (one per problem, on the device)."""
+        import ctypes
+        from . import _lib
+        n = len(self.opts)
+        rhos = [r.reshape(-1).to(dtype=torch.float64).contiguous() for r in rhos]
+        drs = [torch.empty_like(r) for r in rhos]
+        mm = self.opts[0].material_model
+        pen = float(mm.current_penalty(iteration))
+        P = lambda ts: (ctypes.c_void_p * n)(*[t.data_ptr() for t in ts])  # noqa: E731
+        comp = (ctypes.c_double * n)()
+        res = (ctypes.c_double * n)()
+        its = (ctypes.c_int * n)()
+        fs = [o.f for o in self.opts]
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        sv = self.opts[0].solver
+        _lib.call("edge_batch_solve_and_process", self.handle, P(rhos), pen, float(mm.void), P(fs), P(self.U),
+                  1 if self.warm else 0, float(sv.tol), int(sv.maxiter), comp, P(drs), res, its, stream)
+        self.warm = all(o.reuse_sol for o in self.opts)
+        self.last_iters = list(its)
+        for o, u, it in zip(self.opts, self.U, its):
+            o._U = u
+            o.solver.last_x0 = u
+            o.solver.last_iters = int(it)
+        return list(comp), [d.reshape(-1, 1) for d in drs], list(res)
+
+
 class BatchSIMP:
     """SIMP iterations of many problems, spread over `n_threads` host threads with one CUDA
     stream each.  ``step(n)`` runs n iterations of every problem and returns the device time
     (ms) from the first launch to the last completion, measured with CUDA events."""
 
-    def __init__(self, specs, precision="mixed", tol=1e-6, maxiter=1000, n_threads=8):
+    def __init__(self, specs, precision="mixed", tol=1e-6, maxiter=1000, n_threads=8, persistent=False,
+                 max_level=4, block_threads=512, sweeps=None, team=1):
         self.specs = list(specs)
-        self.n_threads = max(1, min(n_threads, len(self.specs)))
+        self.persistent = bool(persistent)
+        self.n_threads = 1 if self.persistent else max(1, min(n_threads, len(self.specs)))
         self.streams = [torch.cuda.Stream() for _ in range(self.n_threads)]
         self.items = []
         for k, spec in enumerate(self.specs):
             with torch.cuda.stream(self.streams[k % self.n_threads]):
-                opt, rho = build(spec, precision, tol, maxiter)
+                opt, rho = build(spec, precision, tol, maxiter, max_level)
             self.items.append({"opt": opt, "rho": rho, "dr": None, "it": 0, "comp": [], "pcg": []})
         torch.cuda.synchronize()
+        # persistent: every analysis's solve in one launch (BatchAnalysis), the OC updates
+        # per problem, all on one stream
+        self.batch = None
+        if self.persistent:
+            with torch.cuda.stream(self.streams[0]):
+                self.batch = BatchAnalysis([it["opt"] for it in self.items], threads=block_threads, sweeps=sweeps,
+                                           team=team)
+            torch.cuda.synchronize()
+
+    def _run_persistent(self, n_iter):
+        items = self.items
+        with torch.cuda.stream(self.streams[0]):
+            for _ in range(n_iter):
+                first = items[0]["dr"] is None
+                if not first:
+                    rhos = self.batch.update_design([item["rho"] for item in items], [item["dr"] for item in items])
+                    for item, r in zip(items, rhos):
+                        item["rho"] = r
+                comps, drs, _ = self.batch.solve_and_process([item["rho"] for item in items], items[0]["it"])
+                for item, c, d, it in zip(items, comps, drs, self.batch.last_iters):
+                    item["dr"] = d
+                    if not first:
+                        item["it"] += 1
+                    item["comp"].append(float(c))
+                    item["pcg"].append(int(it))
+            self._end[0].record(self.streams[0])
 
     def _run(self, t, n_iter, err):
         try:
@@ -148,6 +288,10 @@ class BatchSIMP:
         for s in self.streams:
             s.wait_event(start)
         self._end = [torch.cuda.Event(enable_timing=True) for _ in range(self.n_threads)]
+        if self.persistent:
+            self._run_persistent(n_iter)
+            torch.cuda.synchronize()
+            return start.elapsed_time(self._end[0])
         err = []
         threads = [threading.Thread(target=self._run, args=(t, n_iter, err)) for t in range(self.n_threads)]
         for th in threads:

@@ -31,6 +31,7 @@
 #include "general.cuh"
 #include "misc.cuh"
 #include "tail.cuh"
+#include "batch.cuh"
 
 namespace edge {
 
@@ -2334,7 +2335,7 @@ int edge_time_level(edge_problem* p, int level, int reps, double* ms) {
 int edge_time_fine(edge_problem* p, int precision, int variant, int blocks_per_sm, int sweep, int reps,
                    double* ms) {
   API_BEGIN
-  if (!p || !ms || reps < 1 || variant < 0 || variant > 14 || blocks_per_sm < 1 || blocks_per_sm > 64)
+  if (!p || !ms || reps < 1 || variant < 0 || variant > 15 || blocks_per_sm < 1 || blocks_per_sm > 64)
     fail(EDGE_EINVAL, "bad argument");
   Prob& P = p->P;
   if (!P.has_rho) fail(EDGE_ESTATE, "rho not set");
@@ -3271,6 +3272,380 @@ int edge_simp_solve_and_process(edge_problem* p, edge_filter* f, const double* r
   if (compliance_out) *compliance_out = P.scal_h[2];
   if (residual_out) *residual_out = P.st_h->res;
   if (iters_out) *iters_out = P.st_h->iter;
+  API_END
+}
+
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ many 2-D problems, one solve launch
+struct edge_batch {
+  std::vector<edge_problem*> probs;
+  std::vector<edge_filter*> filters;
+  std::vector<int> nxr, nyr;  // real node extents (the problem's grid may be padded beyond them)
+  // queue order of the solve: problems by decreasing expected cost, DOFs times the PCG
+  // iterations of the problem's previous batched solve (DOFs alone before the first), so the
+  // longest solves start first
+  std::vector<int> order;
+  std::vector<long long> cost;
+  int threads = 512;
+  int team = 1;  // blocks per problem (a thread block cluster when > 1)
+  BatchDesc* d_desc = nullptr;
+  BatchDesc* h_desc = nullptr;
+  double** d_scal = nullptr;
+  double** h_scal = nullptr;
+  unsigned* queue = nullptr;
+  double *d_res = nullptr, *d_comp = nullptr;
+  int *d_iters = nullptr, *d_done = nullptr;
+  double *h_res = nullptr, *h_comp = nullptr;
+  int *h_iters = nullptr, *h_done = nullptr;
+  BatchOcDesc* d_oc = nullptr;
+  BatchOcDesc* h_oc = nullptr;
+  ~edge_batch() {
+    if (d_oc) cudaFree(d_oc);
+    if (h_oc) cudaFreeHost(h_oc);
+    for (void* q : {(void*)d_desc, (void*)d_scal, (void*)queue, (void*)d_res, (void*)d_comp, (void*)d_iters,
+                    (void*)d_done})
+      if (q) cudaFree(q);
+    for (void* q : {(void*)h_desc, (void*)h_scal, (void*)h_res, (void*)h_comp, (void*)h_iters, (void*)h_done})
+      if (q) cudaFreeHost(q);
+  }
+};
+
+namespace edge {
+template <typename TV, typename TD0, typename TS, int BT, int C>
+static void batch_go(Prob& P0, edge_batch& B, int n, double tol, int maxiter) {
+  auto kern = k_batch_pcg<TV, TD0, TS, BT, C>;
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if constexpr (C == 1) {
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, 0));
+    const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
+    launch(P0, kern, dim3(grid), dim3(BT), 0, (const BatchDesc*)B.d_desc, n, B.queue, tol, maxiter);
+  } else {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C * sms);
+    cfg.blockDim = dim3(BT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = P0.stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    CK(cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
+    const int teams = std::max(1, std::min(n, clusters));
+    cfg.gridDim = dim3(C * teams);
+    CK(cudaLaunchKernelEx(&cfg, kern, (const BatchDesc*)B.d_desc, n, B.queue, tol, maxiter));
+    ++P0.nlaunch;
+    KCHECK();
+  }
+}
+template <typename TV, typename TD0, typename TS>
+static void batch_launch(Prob& P0, edge_batch& B, int n, double tol, int maxiter) {
+  const int key = B.threads * 16 + B.team;
+  switch (key) {
+    case 256 * 16 + 1: batch_go<TV, TD0, TS, 256, 1>(P0, B, n, tol, maxiter); break;
+    case 1024 * 16 + 1: batch_go<TV, TD0, TS, 1024, 1>(P0, B, n, tol, maxiter); break;
+    case 512 * 16 + 2: batch_go<TV, TD0, TS, 512, 2>(P0, B, n, tol, maxiter); break;
+    case 512 * 16 + 4: batch_go<TV, TD0, TS, 512, 4>(P0, B, n, tol, maxiter); break;
+    case 512 * 16 + 8: batch_go<TV, TD0, TS, 512, 8>(P0, B, n, tol, maxiter); break;
+    case 1024 * 16 + 2: batch_go<TV, TD0, TS, 1024, 2>(P0, B, n, tol, maxiter); break;
+    case 1024 * 16 + 4: batch_go<TV, TD0, TS, 1024, 4>(P0, B, n, tol, maxiter); break;
+    case 1024 * 16 + 8: batch_go<TV, TD0, TS, 1024, 8>(P0, B, n, tol, maxiter); break;
+    default: batch_go<TV, TD0, TS, 512, 1>(P0, B, n, tol, maxiter); break;
+  }
+}
+}  // namespace edge
+
+extern "C" {
+
+int edge_batch_create(int n, edge_problem* const* problems, edge_filter* const* filters, const int* nelx,
+                      const int* nely, edge_batch** out) {
+  API_BEGIN
+  if (n < 1 || !problems || !filters || !nelx || !nely || !out) fail(EDGE_EINVAL, "null argument or n < 1");
+  auto B = std::make_unique<edge_batch>();
+  std::vector<long long> dofs(n);
+  for (int i = 0; i < n; ++i) {
+    if (!problems[i] || !filters[i]) fail(EDGE_EINVAL, "null problem or filter");
+    const Prob& P = problems[i]->P;
+    const edge_filter& F = *filters[i];
+    if (P.dim != 2 || F.g.dim != 2) fail(EDGE_EINVAL, "batched problems must be 2-D");
+    if (nelx[i] < 1 || nely[i] < 1 || nelx[i] > P.nel[0] || nely[i] > P.nel[1])
+      fail(EDGE_EINVAL, "problem " + std::to_string(i) + ": real extents outside the problem's grid");
+    if (F.n_el != (long long)nelx[i] * nely[i])
+      fail(EDGE_EINVAL, "problem " + std::to_string(i) + ": filter and real extents differ");
+    B->probs.push_back(problems[i]);
+    B->filters.push_back(filters[i]);
+    B->nxr.push_back(nelx[i] + 1);
+    B->nyr.push_back(nely[i] + 1);
+    dofs[i] = P.n_dof;
+  }
+  B->order.resize(n);
+  for (int i = 0; i < n; ++i) B->order[i] = i;
+  B->cost = dofs;
+  std::stable_sort(B->order.begin(), B->order.end(), [&](int a, int b) { return dofs[a] > dofs[b]; });
+  CK(cudaMalloc(&B->d_desc, n * sizeof(BatchDesc)));
+  CK(cudaMallocHost(&B->h_desc, n * sizeof(BatchDesc)));
+  CK(cudaMalloc(&B->d_scal, n * sizeof(double*)));
+  CK(cudaMallocHost(&B->h_scal, n * sizeof(double*)));
+  CK(cudaMalloc(&B->queue, sizeof(unsigned)));
+  CK(cudaMalloc(&B->d_res, n * sizeof(double)));
+  CK(cudaMalloc(&B->d_comp, n * sizeof(double)));
+  CK(cudaMalloc(&B->d_iters, n * sizeof(int)));
+  CK(cudaMalloc(&B->d_done, n * sizeof(int)));
+  CK(cudaMallocHost(&B->h_res, n * sizeof(double)));
+  CK(cudaMallocHost(&B->h_comp, n * sizeof(double)));
+  CK(cudaMallocHost(&B->h_iters, n * sizeof(int)));
+  CK(cudaMallocHost(&B->h_done, n * sizeof(int)));
+  std::memset(B->h_desc, 0, n * sizeof(BatchDesc));
+  CK(cudaMalloc(&B->d_oc, n * sizeof(BatchOcDesc)));
+  CK(cudaMallocHost(&B->h_oc, n * sizeof(BatchOcDesc)));
+  *out = B.release();
+  API_END
+}
+
+int edge_batch_destroy(edge_batch* b) {
+  API_BEGIN
+  delete b;
+  API_END
+}
+
+int edge_batch_set_threads(edge_batch* b, int threads, int team) {
+  API_BEGIN
+  if (!b) fail(EDGE_EINVAL, "null handle");
+  const bool ok = (team == 1 && (threads == 256 || threads == 512 || threads == 1024)) ||
+                  ((team == 2 || team == 4 || team == 8) && (threads == 512 || threads == 1024));
+  if (!ok) fail(EDGE_EINVAL, "supported: team 1 with 256, 512 or 1024 threads; team 2, 4 or 8 with 512 or 1024");
+  b->threads = threads;
+  b->team = team;
+  API_END
+}
+
+int edge_batch_oc_update(edge_batch* b, const double* const* rho, const double* const* dr, const double* A,
+                         const double* vol, const double* vf, double move, double* const* rho_new, double* lambda_out,
+                         int* steps_out, void* stream) {
+  API_BEGIN
+  if (!b || !rho || !dr || !A || !vol || !vf || !rho_new) fail(EDGE_EINVAL, "null argument");
+  edge_batch& B = *b;
+  const int n = (int)B.probs.size();
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int k = 0; k < n; ++k) {
+    const int i = B.order[k];
+    if (!rho[i] || !dr[i] || !rho_new[i]) fail(EDGE_EINVAL, "null array of problem " + std::to_string(i));
+    Prob& P = B.probs[i]->P;
+    BatchOcDesc& d = B.h_oc[k];
+    d.n = B.filters[i]->n_el;
+    d.rho = rho[i];
+    d.dr = dr[i];
+    d.ocp = P.ocp;  // sized for the problem's grid, at least the real element count
+    d.rho_new = rho_new[i];
+    d.A = A[i];
+    d.vol = vol[i];
+    d.vf = vf[i];
+  }
+  Prob& P0 = B.probs[B.order[0]]->P;
+  const cudaStream_t saved0 = P0.stream;
+  P0.stream = s;
+  try {
+    CK(cudaMemcpyAsync(B.d_oc, B.h_oc, n * sizeof(BatchOcDesc), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(B.queue, 0, sizeof(unsigned), s));
+    int per_sm = 0, sms = 0, dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_oc<512>, 512, 0));
+    const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
+    launch(P0, k_batch_oc<512>, dim3(grid), dim3(512), 0, (const BatchOcDesc*)B.d_oc, n, B.queue, move, B.d_res,
+           B.d_iters);
+  } catch (...) {
+    P0.stream = saved0;
+    throw;
+  }
+  P0.stream = saved0;
+  if (lambda_out || steps_out) {
+    CK(cudaMemcpyAsync(B.h_res, B.d_res, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(B.h_iters, B.d_iters, n * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int k = 0; k < n; ++k) {
+      if (lambda_out) lambda_out[B.order[k]] = B.h_res[k];
+      if (steps_out) steps_out[B.order[k]] = B.h_iters[k];
+    }
+  }
+  API_END
+}
+
+int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double penalty, double void_,
+                                 const double* const* f, double* const* U, int use_last, double tol, int maxiter,
+                                 double* compliance, double* const* dr, double* residual, int* iters, void* stream) {
+  API_BEGIN
+  if (!b || !rho || !f || !U || !dr) fail(EDGE_EINVAL, "null argument");
+  if (tol <= 0.0 || maxiter < 1) fail(EDGE_EINVAL, "tol must be > 0 and maxiter >= 1");
+  edge_batch& B = *b;
+  const int n = (int)B.probs.size();
+  cudaStream_t s = (cudaStream_t)stream;
+  int prec = -1;
+  bool bf16 = true;
+  for (int i = 0; i < n; ++i) {
+    if (!rho[i] || !f[i] || !U[i] || !dr[i]) fail(EDGE_EINVAL, "null array of problem " + std::to_string(i));
+    Prob& P = B.probs[i]->P;
+    ensure_mg(P);
+    if (P.n_level < 1 || P.n_level >= BATCH_MAXL)
+      fail(EDGE_EINVAL, "batched solves need 1 <= n_level < " + std::to_string(BATCH_MAXL));
+    if (P.cycle_w) fail(EDGE_EINVAL, "batched solves run the V-cycle only");
+    if (P.n_springs) fail(EDGE_EINVAL, "batched solves take no springs");
+    if (prec >= 0 && P.prec != prec) fail(EDGE_EINVAL, "every problem of a batch must have the same precision");
+    prec = P.prec;
+    bf16 = bf16 && P.st_bf16;
+  }
+  const bool mixed = prec != EDGE_FP64;
+  std::stable_sort(B.order.begin(), B.order.end(), [&](int a, int c) { return B.cost[a] > B.cost[c]; });
+  // per problem: filter + SIMP law into the (possibly padded) grid, loads and warm starts,
+  // the hierarchy for the new E
+  for (int k = 0; k < n; ++k) {
+    const int i = B.order[k];
+    Prob& P = B.probs[i]->P;
+    const edge_filter& F = *B.filters[i];
+    const cudaStream_t saved = P.stream;
+    P.stream = s;
+    try {
+      const Geo& g = P.g0;
+      Geo gr = g;  // the real grid's extents in the problem's slot layout
+      gr.nx = B.nxr[i];
+      gr.ny = B.nyr[i];
+      const unsigned nbe = cdiv(F.n_el, 256);
+      launch(P, k_filter_material<double, float>, nbe, 256, 0, gr, F.taps, rho[i], P.rho_f, P.E64, P.E32, penalty,
+             void_, 0);
+      P.has_rho = true;
+      launch(P, k_user_to_slots_pad, cdiv(g.n, 256), 256, 0, g, B.nxr[i], B.nyr[i], f[i], P.b64);
+      if (use_last)
+        launch(P, k_user_to_slots_pad, cdiv(g.n, 256), 256, 0, g, B.nxr[i], B.nyr[i], (const double*)U[i], P.x64);
+      else
+        CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), s));
+      mg_setup_prec(P);
+      BatchDesc& d = B.h_desc[k];
+      std::memset(&d, 0, sizeof(d));
+      d.n_level = P.n_level;
+      d.nd = P.nd;
+      d.keep_omega = (P.omega_carry && P.omega_started) ? 1 : 0;
+      for (int l = 0; l < BATCH_MAXL; ++l) {
+        d.sweeps[l] = l < P.n_level ? P.sweeps(l) : 0;
+        d.wscale[l] = std::pow(1.06, l);
+      }
+      d.omega = P.omega;
+      d.min_omega = P.min_omega;
+      d.omega0 = P.omega_carry ? P.omega : P.min_omega;
+      d.mask = P.mask;
+      d.E64 = P.E64;
+      d.ET = mixed ? (const void*)P.E32 : (const void*)P.E64;
+      d.K0_64 = P.dK0b;
+      d.K0_T = mixed ? (const void*)P.dK0bf : (const void*)P.dK0b;
+      d.b64 = P.b64;
+      d.x64 = P.x64;
+      d.r64 = P.r64;
+      d.p64 = (double*)P.p;
+      d.q64 = (double*)P.q;
+      d.rT = mixed ? (void*)P.r32 : (void*)P.r64;
+      d.Ainv = P.Ainv;
+      d.st = P.st;
+      d.chol_status = P.chol_status;
+      for (int l = 0; l <= P.n_level; ++l) {
+        const Level& Lv = P.lv[l];
+        BatchLevel& bl = d.lv[l];
+        bl.g = Lv.g;
+        bl.b = Lv.b;
+        bl.xa = Lv.xa;
+        bl.xb = Lv.xb;
+        bl.r = Lv.r;
+        bl.ea = Lv.ea;
+        bl.eb = Lv.eb;
+        bl.res = Lv.res;
+        bl.S = (mixed && bf16 && Lv.S16) ? Lv.S16 : Lv.S;
+        bl.dinv = Lv.dinv;
+      }
+      B.h_scal[k] = P.scal;
+    } catch (...) {
+      P.stream = saved;
+      throw;
+    }
+    P.stream = saved;
+  }
+  // all solves in one launch
+  Prob& P0 = B.probs[B.order[0]]->P;
+  const cudaStream_t saved0 = P0.stream;
+  P0.stream = s;
+  try {
+    CK(cudaMemcpyAsync(B.d_desc, B.h_desc, n * sizeof(BatchDesc), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.d_scal, B.h_scal, n * sizeof(double*), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(B.queue, 0, sizeof(unsigned), s));
+    if (!mixed)
+      batch_launch<double, double, double>(P0, B, n, tol, maxiter);
+    else if (bf16)
+      batch_launch<float, __nv_bfloat16, __nv_bfloat16>(P0, B, n, tol, maxiter);
+    else
+      batch_launch<float, __nv_bfloat16, float>(P0, B, n, tol, maxiter);
+  } catch (...) {
+    P0.stream = saved0;
+    throw;
+  }
+  P0.stream = saved0;
+  // per problem: compliance f . U, dr = H^T (dE/drho_f dk), U back in the user layout
+  for (int k = 0; k < n; ++k) {
+    const int i = B.order[k];
+    Prob& P = B.probs[i]->P;
+    const edge_filter& F = *B.filters[i];
+    const cudaStream_t saved = P.stream;
+    P.stream = s;
+    try {
+      const Geo& g = P.g0;
+      Geo gr = g;
+      gr.nx = B.nxr[i];
+      gr.ny = B.nyr[i];
+      const long long nv = (long long)g.dof * g.n;
+      const unsigned nbe = cdiv(F.n_el, 256);
+      launch(P, k_dot<double, double>, std::min<unsigned>(ew_blocks(nv), 1024), 256, 0, nv, (const double*)P.b64,
+             (const double*)P.x64, P.part, P.ticket, P.scal + 2);
+      launch(P, k_dk<double>, nbe, 256, 0, gr, (const double*)P.x64, P.ei.k3, P.ei.k2, (const double*)P.dK0b,
+             P.ei.wht ? 1 : 0, (double*)nullptr, (const double*)P.rho_f, P.gsens, penalty, void_);
+      launch(P, k_filter_T, nbe, 256, 0, F.g, F.taps, (const double*)F.N, (const double*)P.gsens, dr[i]);
+      launch(P, k_slots_to_user_pad, cdiv(g.n, 256), 256, 0, g, B.nxr[i], B.nyr[i], (const double*)P.x64, U[i]);
+    } catch (...) {
+      P.stream = saved;
+      throw;
+    }
+    P.stream = saved;
+  }
+  k_batch_gather<<<cdiv(n, 128), 128, 0, s>>>(B.d_desc, (const double* const*)B.d_scal, n, B.d_res, B.d_comp,
+                                               B.d_iters, B.d_done);
+  KCHECK();
+  CK(cudaMemcpyAsync(B.h_res, B.d_res, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(B.h_comp, B.d_comp, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(B.h_iters, B.d_iters, n * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(B.h_done, B.d_done, n * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  int bad = -1;
+  for (int k = 0; k < n; ++k) {
+    const int i = B.order[k];
+    Prob& P = B.probs[i]->P;
+    if (residual) residual[i] = B.h_res[k];
+    if (iters) iters[i] = B.h_iters[k];
+    if (compliance) compliance[i] = B.h_comp[k];
+    P.st_h->res = B.h_res[k];
+    P.st_h->iter = B.h_iters[k];
+    P.st_h->done = B.h_done[k];
+    P.last_iters = B.h_iters[k];
+    P.last_true_res = 0;
+    P.omega_started = true;
+    B.cost[i] = P.n_dof * std::max(1, B.h_iters[k]);
+    if (B.h_done[k] == 3 && bad < 0) bad = i;
+  }
+  if (bad >= 0)
+    fail(EDGE_ENOTPD, "problem " + std::to_string(bad) +
+                          ": coarsest Galerkin matrix is not positive definite (missing boundary conditions?)");
   API_END
 }
 

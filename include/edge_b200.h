@@ -31,6 +31,7 @@ extern "C" {
 typedef struct edge_problem edge_problem;
 typedef struct edge_filter edge_filter;
 typedef struct edge_gen edge_gen;
+typedef struct edge_batch edge_batch;
 typedef struct edge_csr edge_csr;
 
 const char* edge_last_error(void);
@@ -277,6 +278,47 @@ int edge_simp_iteration(edge_problem* p, edge_filter* f, const double* rho_dev, 
                         double* U_dev, int use_last, double tol, int maxiter, double* rho_new_dev, double* dr_new_dev,
                         double* rho_f_dev, double* compliance_out, double* residual_out, int* iters_out,
                         double* lambda_out, int* oc_steps_out, double* sqchange_out);
+
+/* ---- many independent 2-D problems: every analysis's solve in one persistent launch.
+ * No reference counterpart (the reference solves problems one at a time; its randomizer,
+ * randomizer/ConfigSolve.py:6-26, is the intent): the batched form of
+ * edge_simp_solve_and_process.  problems[i] is the problem the multigrid runs on, with its
+ * multigrid configured (edge_mg_config, 1 <= n_level < 8, V-cycle, no springs) and its BCs
+ * set; its grid may be larger than the real nelx[i] x nely[i] grid (a padded grid: the
+ * real grid in its lower corner, padding elements without stiffness that the SIMP law never
+ * writes, padding nodes constrained).  filters[i] is the density filter of the real grid.
+ * Every problem has the same precision.  The handle keeps pointers to the problems and
+ * filters: destroy it before them.  */
+int edge_batch_create(int n, edge_problem* const* problems, edge_filter* const* filters, const int* nelx,
+                      const int* nely, edge_batch** out);
+int edge_batch_destroy(edge_batch* b);
+/* Shape of the solve launch: `threads` per block and `team` blocks per problem (team > 1: a
+ * thread block cluster of that many blocks solves each problem together).  Supported: team 1
+ * with 256, 512 (default) or 1024 threads; team 2, 4 or 8 with 512 or 1024 threads. */
+int edge_batch_set_threads(edge_batch* b, int threads, int team);
+/* The OC update of every problem (edge_oc_update, TopOpt/_cuda.py:242-280) in one launch on
+ * `stream`: one block per problem, the bisection's sums as block sums; rho[i], dr[i],
+ * rho_new[i] on the real grid (nelx[i] * nely[i]), A[i] the element area, vol[i] the domain
+ * volume, vf[i] the volume fraction.  The last lambda and the bisection steps per problem
+ * into lambda_out / steps_out when given (then it synchronises `stream`; otherwise it only
+ * enqueues). */
+int edge_batch_oc_update(edge_batch* b, const double* const* rho, const double* const* dr, const double* A,
+                         const double* vol, const double* vf, double move, double* const* rho_new, double* lambda_out,
+                         int* steps_out, void* stream);
+/* One SIMP analysis of every problem, on `stream`, arrays in each problem's real-grid user
+ * layout (rho[i], dr[i]: nelx[i] * nely[i]; f[i], U[i]: 2 (nelx[i] + 1)(nely[i] + 1)):
+ * per problem the filter and SIMP law of edge_simp_solve_and_process into the problem's
+ * grid, the load and warm start (use_last) and the multigrid hierarchy for the new E; then
+ * ONE launch that solves all n systems to ||r|| / ||f|| < tol (a block takes the next
+ * unsolved problem, largest first, and runs its whole PCG: FP64 Krylov vectors, products of
+ * the search direction and inner products, preconditioned by the problem's V-cycle in its
+ * precision); then per problem c = f . U, dr = H^T (p clip(rho_f, void, 1)^(p-1) dk) and U.
+ * Results per problem in compliance, residual, iters (any may be null).  Never fails on
+ * non-convergence; a coarsest Galerkin matrix that is not positive definite is EDGE_ENOTPD
+ * after the call (the other problems' results are valid).  Synchronises `stream` once. */
+int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double penalty, double void_,
+                                 const double* const* f, double* const* U, int use_last, double tol, int maxiter,
+                                 double* compliance, double* const* dr, double* residual, int* iters, void* stream);
 
 /* Benchmark instrumentation: between begin and end, every fine-level operator launch
  * (the dominant kernel) is bracketed by CUDA events on the problem's stream and its

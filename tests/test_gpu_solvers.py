@@ -165,15 +165,18 @@ def test_simp_loop_on_odd_mbb_beam(precision):
     assert np.abs(rho.cpu().numpy() - rho_ref).max() < (1e-6 if precision == "fp64" else 1e-4)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batch_of_random_problems_against_oracle(precision):
-    """Random uneven 2-D problems (the batching configuration's generator at reduced sizes)
-    solved concurrently on several streams: every problem's compliance history matches the
-    oracle's SIMP loop with exact solves."""
+@pytest.mark.parametrize("precision,mode", [("fp64", "threads"), ("mixed", "threads"), ("fp64", "persistent"),
+                                            ("mixed", "persistent")])
+def test_batch_of_random_problems_against_oracle(precision, mode):
+    """Random uneven 2-D problems (the batching configuration's generator at reduced sizes),
+    solved concurrently on several streams or with every solve and every OC update of a SIMP
+    stage in one persistent launch (teams of two blocks): every problem's compliance history
+    matches the oracle's SIMP loop with exact solves."""
     from edge_to_b200 import batch
     specs = [batch.random_spec(i, seed=100, nelx_range=(20, 44), nely_range=(12, 26)) for i in range(6)]
     tol = 1e-10 if precision == "fp64" else 1e-8
-    b = batch.BatchSIMP(specs, precision=precision, tol=tol, maxiter=2000, n_threads=3)
+    b = batch.BatchSIMP(specs, precision=precision, tol=tol, maxiter=2000, n_threads=3,
+                        persistent=mode == "persistent", team=2)
     ms = b.step(6)  # initial analysis + 5 design updates per problem
     assert ms > 0
     for spec, item in zip(specs, b.items):
@@ -186,3 +189,43 @@ def test_batch_of_random_problems_against_oracle(precision):
         want = np.array([hist["comp0"]] + hist["comp"])
         err = np.abs(c - want) / np.abs(want)
         assert err.max() < (1e-7 if precision == "fp64" else 1e-5), (spec["index"], err)
+
+
+@pytest.mark.parametrize("threads,team", [(512, 1), (1024, 1), (512, 4), (1024, 8)])
+def test_persistent_batch_equals_per_problem_solves(threads, team):
+    """The batched persistent solve (FP64) runs the per-problem FP64 solver's algorithm: the same
+    PCG iteration counts and compliances and designs equal to rounding over five SIMP
+    iterations, whatever the launch shape (blocks per problem, threads per block); its batched
+    OC update gives the per-problem OC update's designs bit for bit."""
+    import torch
+    from edge_to_b200 import batch
+    specs = [batch.random_spec(i, seed=7, nelx_range=(20, 90), nely_range=(12, 48)) for i in range(6)]
+    a = batch.BatchSIMP(specs, precision="fp64", tol=1e-8, maxiter=1000, n_threads=2)
+    c = batch.BatchSIMP(specs, precision="fp64", tol=1e-8, maxiter=1000, persistent=True, block_threads=threads,
+                        team=team)
+    a.step(5)
+    c.step(5)
+    for ia, ic in zip(a.items, c.items):
+        assert ia["pcg"] == ic["pcg"]
+        ca, cc = np.array(ia["comp"]), np.array(ic["comp"])
+        assert np.max(np.abs(ca - cc) / np.abs(ca)) < 1e-9
+        assert float((ia["rho"] - ic["rho"]).abs().max()) < 1e-9
+    new = c.batch.update_design([it["rho"] for it in a.items], [it["dr"] for it in a.items])
+    for it, nb in zip(a.items, new):
+        assert torch.equal(it["opt"].update_design(it["rho"], it["dr"]), nb)
+
+
+def test_persistent_batch_rejects_what_it_does_not_run():
+    """Batched problems must share precision and material law; a W-cycle or springs are refused."""
+    from edge_to_b200 import batch
+    specs = [batch.random_spec(i, seed=3, nelx_range=(20, 30), nely_range=(12, 16)) for i in range(2)]
+    o1, _ = batch.build(specs[0], "fp64", 1e-8, 100)
+    o2, _ = batch.build(specs[1], "mixed", 1e-8, 100)
+    with pytest.raises(ValueError):
+        b = batch.BatchAnalysis([o1, o2])
+        b.solve_and_process([torch_full(o1), torch_full(o2)], 0)
+
+
+def torch_full(opt):
+    import torch
+    return torch.full((opt.mesh.n_elements,), 0.5, dtype=torch.float64, device="cuda")
