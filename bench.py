@@ -675,8 +675,9 @@ def run_batch(args):
     max_level = args.batch_max_level if args.batch_max_level else (6 if persistent else 4)
     b = batch.BatchSIMP(specs, precision=args.precision, tol=1e-6, maxiter=1000, n_threads=args.batch_threads,
                         persistent=persistent, max_level=max_level, block_threads=args.batch_block,
-                        sweeps=sweeps, team=args.batch_team)
+                        sweeps=sweeps, team=args.batch_team, split_dof=args.batch_split)
     b.step(args.warmup)               # initial analysis, autotuners, warm-up iterations
+    b.phase_ms = {}
     clocks = ClockSampler(local)
     clocks.start()
     _barrier(ws)
@@ -704,8 +705,11 @@ def run_batch(args):
                        "rtol": 1e-6, "precision": args.precision, "mode": args.batch_mode,
                        "threads_streams": b.n_threads, "max_level": max_level,
                        "solve_launch": ({"threads_per_block": args.batch_block, "blocks_per_problem": args.batch_team,
+                                         "single_block_below_dof": args.batch_split,
                                          "sweeps_fine_coarse": sweeps} if persistent else None),
                        "pcg_iters_max_rank0": int(max(max(it["pcg"][-args.steps:]) for it in b.items)),
+                       "phase_ms_per_step_rank0": ({k: v / args.steps for k, v in b.phase_ms.items()}
+                                                   if persistent else None),
                        "padded_problems_rank0": int(sum(it["opt"].solver.padded for it in b.items)),
                        "pcg_iters_mean_rank0": float(np.mean(pcg))},
             "clocks": clk}
@@ -777,6 +781,8 @@ def main():
                     help="batch, persistent mode: threads per block of the solve launch")
     ap.add_argument("--batch-team", type=int, default=4, choices=[1, 2, 4, 8],
                     help="batch, persistent mode: blocks (a thread block cluster) per problem")
+    ap.add_argument("--batch-split", type=int, default=0,
+                    help="batch, persistent mode: problems below this many DOFs solved by single blocks beside the teams")
     ap.add_argument("--batch-sweeps", default="1,2",
                     help="batch, persistent mode: smoothing sweeps on the fine level and on coarser levels")
     ap.add_argument("--breakdown", action="store_true",

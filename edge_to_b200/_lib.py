@@ -97,6 +97,9 @@ _SIGS = {
     "edge_batch_create": (ctypes.c_int, [ctypes.c_int, vp, vp, c_int_p, c_int_p, ctypes.POINTER(vp)]),
     "edge_batch_destroy": (ctypes.c_int, [vp]),
     "edge_batch_set_threads": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+    "edge_batch_set_split": (ctypes.c_int, [vp, ctypes.c_longlong, ctypes.c_int]),
+    "edge_batch_last_problem_times": (ctypes.c_int, [vp, c_double_p, c_double_p]),
+    "edge_batch_last_times": (ctypes.c_int, [vp, c_double_p, c_double_p, c_double_p]),
     "edge_batch_oc_update": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, ctypes.c_double, vp, c_double_p, c_int_p, vp]),
     "edge_batch_solve_and_process": (ctypes.c_int, [vp, vp, ctypes.c_double, ctypes.c_double, vp, vp, ctypes.c_int,
                                                     ctypes.c_double, ctypes.c_int, c_double_p, vp, c_double_p,

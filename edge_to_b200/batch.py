@@ -116,7 +116,7 @@ class BatchAnalysis:
     law and sensitivities stay on the real grid.  The FP64 Krylov recurrence of the batched
     solve is preconditioned by each solver's V-cycle in its precision."""
 
-    def __init__(self, opts, threads=512, sweeps=None, team=1):
+    def __init__(self, opts, threads=512, sweeps=None, team=1, split_dof=0):
         import ctypes
         from . import CuMultiGrid, SingleMaterial, _lib
         self.opts = list(opts)
@@ -155,6 +155,7 @@ class BatchAnalysis:
                   ctypes.byref(h))
         self.handle = h
         _lib.call("edge_batch_set_threads", self.handle, int(threads), int(team))
+        _lib.call("edge_batch_set_split", self.handle, int(split_dof), 1024)
         self.U = [torch.zeros_like(o.f) for o in self.opts]
         self.warm = False
         self.last_iters = [0] * n
@@ -170,6 +171,15 @@ class BatchAnalysis:
             self.close()
         except Exception:  # noqa: BLE001 - interpreter shutdown
             pass
+
+    def problem_times(self):
+        """(start_ms, end_ms) of every problem's solve in the last solve launch."""
+        import ctypes
+        from . import _lib
+        n = len(self.opts)
+        a, b = (ctypes.c_double * n)(), (ctypes.c_double * n)()
+        _lib.call("edge_batch_last_problem_times", self.handle, a, b)
+        return list(a), list(b)
 
     def update_design(self, rhos, drs):
         """The OC updates of every problem in one launch (edge_batch_oc_update): the batched
@@ -212,6 +222,9 @@ class BatchAnalysis:
                   1 if self.warm else 0, float(sv.tol), int(sv.maxiter), comp, P(drs), res, its, stream)
         self.warm = all(o.reuse_sol for o in self.opts)
         self.last_iters = list(its)
+        t = [ctypes.c_double() for _ in range(3)]
+        _lib.call("edge_batch_last_times", self.handle, *[ctypes.byref(v) for v in t])
+        self.last_times = {"setup_ms": t[0].value, "solve_ms": t[1].value, "post_ms": t[2].value}
         for o, u, it in zip(self.opts, self.U, its):
             o._U = u
             o.solver.last_x0 = u
@@ -225,7 +238,7 @@ class BatchSIMP:
     (ms) from the first launch to the last completion, measured with CUDA events."""
 
     def __init__(self, specs, precision="mixed", tol=1e-6, maxiter=1000, n_threads=8, persistent=False,
-                 max_level=4, block_threads=512, sweeps=None, team=1):
+                 max_level=4, block_threads=512, sweeps=None, team=1, split_dof=0):
         self.specs = list(specs)
         self.persistent = bool(persistent)
         self.n_threads = 1 if self.persistent else max(1, min(n_threads, len(self.specs)))
@@ -236,13 +249,15 @@ class BatchSIMP:
                 opt, rho = build(spec, precision, tol, maxiter, max_level)
             self.items.append({"opt": opt, "rho": rho, "dr": None, "it": 0, "comp": [], "pcg": []})
         torch.cuda.synchronize()
-        # persistent: every analysis's solve in one launch (BatchAnalysis), the OC updates
-        # per problem, all on one stream
+        # persistent: every analysis's solves in one launch and every OC update in one launch
+        # (BatchAnalysis), all on one stream; phase_ms sums the device time of the analyses'
+        # phases (per-problem preparation, the solve launch, post-processing)
         self.batch = None
+        self.phase_ms = {}
         if self.persistent:
             with torch.cuda.stream(self.streams[0]):
                 self.batch = BatchAnalysis([it["opt"] for it in self.items], threads=block_threads, sweeps=sweeps,
-                                           team=team)
+                                           team=team, split_dof=split_dof)
             torch.cuda.synchronize()
 
     def _run_persistent(self, n_iter):
@@ -255,6 +270,8 @@ class BatchSIMP:
                     for item, r in zip(items, rhos):
                         item["rho"] = r
                 comps, drs, _ = self.batch.solve_and_process([item["rho"] for item in items], items[0]["it"])
+                for k, v in self.batch.last_times.items():
+                    self.phase_ms[k] = self.phase_ms.get(k, 0.0) + v
                 for item, c, d, it in zip(items, comps, drs, self.batch.last_iters):
                     item["dr"] = d
                     if not first:

@@ -466,9 +466,17 @@ EDGE_D void b_pcg_problem(const BatchDesc& d, const TV* sK, const double* sK64, 
 
 // The batched solve.  C > 1: launched as thread block clusters of C blocks (cluster
 // dimension set at launch); rank 0 of a team takes the team's problems from the queue.
+EDGE_D long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// tns (may be null): start and end of each problem's solve (global timer, ns), for the
+// benchmark's load-balance record.
 template <typename TV, typename TD0, typename TS, int BT, int C>
 __global__ void __launch_bounds__(BT) k_batch_pcg(const BatchDesc* D, int nprob, unsigned* queue, double tol,
-                                                  int maxiter) {
+                                                  int maxiter, long long* tns) {
   using TM = Team<C>;
   __shared__ double sh[33 + C];
   __shared__ double sb[BATCH_COARSE_SMEM];
@@ -495,8 +503,13 @@ __global__ void __launch_bounds__(BT) k_batch_pcg(const BatchDesc* D, int nprob,
       sK64[k] = sd.K0_64[k];
     }
     __syncthreads();
+    const long long t0 = global_ns();
     b_pcg_problem<C, TV, TD0, TS>(sd, sK, sK64, tol, maxiter, sh, sb);
     TM::sync();
+    if (tns && TM::first() == 0) {
+      tns[2 * idx] = t0;
+      tns[2 * idx + 1] = global_ns();
+    }
   }
 }
 

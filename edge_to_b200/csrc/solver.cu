@@ -3290,6 +3290,11 @@ struct edge_batch {
   std::vector<long long> cost;
   int threads = 512;
   int team = 1;  // blocks per problem (a thread block cluster when > 1)
+  // with team > 1: problems with fewer DOFs than this are solved by single blocks of
+  // small_threads threads in a launch beside the teams' (0, the default: every problem by a team;
+  // at 256 problems of 5k-260k DOFs the split changed the solve launch's time by under 1 %)
+  long long split_dof = 0;
+  int small_threads = 1024;
   BatchDesc* d_desc = nullptr;
   BatchDesc* h_desc = nullptr;
   double** d_scal = nullptr;
@@ -3301,7 +3306,24 @@ struct edge_batch {
   int *h_iters = nullptr, *h_done = nullptr;
   BatchOcDesc* d_oc = nullptr;
   BatchOcDesc* h_oc = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // around the three phases of the last call
+  long long* d_tns = nullptr;  // per problem (queue order): start and end of its solve (global timer, ns)
+  long long* h_tns = nullptr;
+  // the per-problem preparation and post-processing run on these streams side by side,
+  // forked from and joined back into the caller's stream
+  static constexpr int NSIDE = 16;
+  cudaStream_t side[NSIDE] = {};
+  cudaEvent_t fork = nullptr, join[NSIDE] = {};
   ~edge_batch() {
+    for (auto st : side)
+      if (st) cudaStreamDestroy(st);
+    if (fork) cudaEventDestroy(fork);
+    for (auto e : join)
+      if (e) cudaEventDestroy(e);
+    if (d_tns) cudaFree(d_tns);
+    if (h_tns) cudaFreeHost(h_tns);
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
     if (d_oc) cudaFree(d_oc);
     if (h_oc) cudaFreeHost(h_oc);
     for (void* q : {(void*)d_desc, (void*)d_scal, (void*)queue, (void*)d_res, (void*)d_comp, (void*)d_iters,
@@ -3313,17 +3335,23 @@ struct edge_batch {
 };
 
 namespace edge {
+// One persistent solve launch over the problems [off, off + cnt) of the queue order, on
+// `stream`, with at most `sm_budget` SMs' worth of blocks (0: as many as fit).
 template <typename TV, typename TD0, typename TS, int BT, int C>
-static void batch_go(Prob& P0, edge_batch& B, int n, double tol, int maxiter) {
+static void batch_go(Prob& P0, edge_batch& B, int off, int cnt, int qslot, int sm_budget, cudaStream_t stream,
+                     double tol, int maxiter) {
   auto kern = k_batch_pcg<TV, TD0, TS, BT, C>;
   int dev = 0, sms = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int budget = sm_budget > 0 ? std::min(sm_budget, sms) : sms;
+  const BatchDesc* D = B.d_desc + off;
+  long long* tns = B.d_tns + 2 * off;
   if constexpr (C == 1) {
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, 0));
-    const int grid = std::max(1, std::min(n, std::max(1, per_sm) * sms));
-    launch(P0, kern, dim3(grid), dim3(BT), 0, (const BatchDesc*)B.d_desc, n, B.queue, tol, maxiter);
+    const int grid = std::max(1, std::min(cnt, std::max(1, per_sm) * budget));
+    kern<<<grid, BT, 0, stream>>>(D, cnt, B.queue + qslot, tol, maxiter, tns);
   } else {
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -3334,32 +3362,62 @@ static void batch_go(Prob& P0, edge_batch& B, int n, double tol, int maxiter) {
     cfg.gridDim = dim3(C * sms);
     cfg.blockDim = dim3(BT);
     cfg.dynamicSmemBytes = 0;
-    cfg.stream = P0.stream;
+    cfg.stream = stream;
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int clusters = 0;
     CK(cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
-    const int teams = std::max(1, std::min(n, clusters));
+    const int fit = std::max(1, clusters * budget / sms);
+    const int teams = std::max(1, std::min(cnt, fit));
     cfg.gridDim = dim3(C * teams);
-    CK(cudaLaunchKernelEx(&cfg, kern, (const BatchDesc*)B.d_desc, n, B.queue, tol, maxiter));
-    ++P0.nlaunch;
-    KCHECK();
+    CK(cudaLaunchKernelEx(&cfg, kern, D, cnt, B.queue + qslot, tol, maxiter, tns));
+  }
+  ++P0.nlaunch;
+  KCHECK();
+}
+template <typename TV, typename TD0, typename TS, int BT>
+static void batch_go_team(Prob& P0, edge_batch& B, int team, int off, int cnt, int qslot, int sm_budget,
+                          cudaStream_t stream, double tol, int maxiter) {
+  switch (team) {
+    case 2: batch_go<TV, TD0, TS, BT, 2>(P0, B, off, cnt, qslot, sm_budget, stream, tol, maxiter); break;
+    case 4: batch_go<TV, TD0, TS, BT, 4>(P0, B, off, cnt, qslot, sm_budget, stream, tol, maxiter); break;
+    case 8: batch_go<TV, TD0, TS, BT, 8>(P0, B, off, cnt, qslot, sm_budget, stream, tol, maxiter); break;
+    default: batch_go<TV, TD0, TS, BT, 1>(P0, B, off, cnt, qslot, sm_budget, stream, tol, maxiter); break;
   }
 }
 template <typename TV, typename TD0, typename TS>
-static void batch_launch(Prob& P0, edge_batch& B, int n, double tol, int maxiter) {
-  const int key = B.threads * 16 + B.team;
-  switch (key) {
-    case 256 * 16 + 1: batch_go<TV, TD0, TS, 256, 1>(P0, B, n, tol, maxiter); break;
-    case 1024 * 16 + 1: batch_go<TV, TD0, TS, 1024, 1>(P0, B, n, tol, maxiter); break;
-    case 512 * 16 + 2: batch_go<TV, TD0, TS, 512, 2>(P0, B, n, tol, maxiter); break;
-    case 512 * 16 + 4: batch_go<TV, TD0, TS, 512, 4>(P0, B, n, tol, maxiter); break;
-    case 512 * 16 + 8: batch_go<TV, TD0, TS, 512, 8>(P0, B, n, tol, maxiter); break;
-    case 1024 * 16 + 2: batch_go<TV, TD0, TS, 1024, 2>(P0, B, n, tol, maxiter); break;
-    case 1024 * 16 + 4: batch_go<TV, TD0, TS, 1024, 4>(P0, B, n, tol, maxiter); break;
-    case 1024 * 16 + 8: batch_go<TV, TD0, TS, 1024, 8>(P0, B, n, tol, maxiter); break;
-    default: batch_go<TV, TD0, TS, 512, 1>(P0, B, n, tol, maxiter); break;
+static void batch_group(Prob& P0, edge_batch& B, int threads, int team, int off, int cnt, int qslot, int sm_budget,
+                        cudaStream_t stream, double tol, int maxiter) {
+  if (threads == 1024)
+    batch_go_team<TV, TD0, TS, 1024>(P0, B, team, off, cnt, qslot, sm_budget, stream, tol, maxiter);
+  else if (threads == 256 && team == 1)
+    batch_go<TV, TD0, TS, 256, 1>(P0, B, off, cnt, qslot, sm_budget, stream, tol, maxiter);
+  else
+    batch_go_team<TV, TD0, TS, 512>(P0, B, team, off, cnt, qslot, sm_budget, stream, tol, maxiter);
+}
+// The solve launch(es): problems below B.split_dof DOFs (when a team of several blocks is
+// configured) are solved by single blocks in a second launch beside the teams' launch, on its
+// own share of the SMs (proportional to the groups' expected work), since a team's barriers
+// dominate a small problem's iteration.
+template <typename TV, typename TD0, typename TS>
+static void batch_launch(Prob& P0, edge_batch& B, int n, int n_large, double w_large, double w_small,
+                         cudaStream_t s, double tol, int maxiter) {
+  if (B.team == 1 || n_large == n || n_large == 0) {
+    batch_group<TV, TD0, TS>(P0, B, B.threads, B.team, 0, n, 0, 0, s, tol, maxiter);
+    return;
   }
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int sm_large = (int)std::lround(sms * w_large / std::max(1e-30, w_large + w_small));
+  sm_large = std::max(B.team, std::min(sms - 1, sm_large)) / B.team * B.team;
+  CK(cudaEventRecord(B.fork, s));
+  CK(cudaStreamWaitEvent(B.side[0], B.fork, 0));
+  batch_group<TV, TD0, TS>(P0, B, B.threads, B.team, 0, n_large, 0, sm_large, s, tol, maxiter);
+  batch_group<TV, TD0, TS>(P0, B, B.small_threads, 1, n_large, n - n_large, 1, sms - sm_large, B.side[0], tol,
+                           maxiter);
+  CK(cudaEventRecord(B.join[0], B.side[0]));
+  CK(cudaStreamWaitEvent(s, B.join[0], 0));
 }
 }  // namespace edge
 
@@ -3394,7 +3452,7 @@ int edge_batch_create(int n, edge_problem* const* problems, edge_filter* const* 
   CK(cudaMallocHost(&B->h_desc, n * sizeof(BatchDesc)));
   CK(cudaMalloc(&B->d_scal, n * sizeof(double*)));
   CK(cudaMallocHost(&B->h_scal, n * sizeof(double*)));
-  CK(cudaMalloc(&B->queue, sizeof(unsigned)));
+  CK(cudaMalloc(&B->queue, 2 * sizeof(unsigned)));
   CK(cudaMalloc(&B->d_res, n * sizeof(double)));
   CK(cudaMalloc(&B->d_comp, n * sizeof(double)));
   CK(cudaMalloc(&B->d_iters, n * sizeof(int)));
@@ -3406,6 +3464,12 @@ int edge_batch_create(int n, edge_problem* const* problems, edge_filter* const* 
   std::memset(B->h_desc, 0, n * sizeof(BatchDesc));
   CK(cudaMalloc(&B->d_oc, n * sizeof(BatchOcDesc)));
   CK(cudaMallocHost(&B->h_oc, n * sizeof(BatchOcDesc)));
+  for (auto& e : B->ev) CK(cudaEventCreate(&e));
+  CK(cudaMalloc(&B->d_tns, 2 * n * sizeof(long long)));
+  CK(cudaMallocHost(&B->h_tns, 2 * n * sizeof(long long)));
+  for (auto& st : B->side) CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
+  for (auto& e : B->join) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   *out = B.release();
   API_END
 }
@@ -3413,6 +3477,15 @@ int edge_batch_create(int n, edge_problem* const* problems, edge_filter* const* 
 int edge_batch_destroy(edge_batch* b) {
   API_BEGIN
   delete b;
+  API_END
+}
+
+int edge_batch_set_split(edge_batch* b, long long split_dof, int small_threads) {
+  API_BEGIN
+  if (!b || split_dof < 0 || (small_threads != 256 && small_threads != 512 && small_threads != 1024))
+    fail(EDGE_EINVAL, "split_dof must be >= 0 and small_threads 256, 512 or 1024");
+  b->split_dof = split_dof;
+  b->small_threads = small_threads;
   API_END
 }
 
@@ -3424,6 +3497,34 @@ int edge_batch_set_threads(edge_batch* b, int threads, int team) {
   if (!ok) fail(EDGE_EINVAL, "supported: team 1 with 256, 512 or 1024 threads; team 2, 4 or 8 with 512 or 1024");
   b->threads = threads;
   b->team = team;
+  API_END
+}
+
+int edge_batch_last_times(const edge_batch* b, double* setup_ms, double* solve_ms, double* post_ms) {
+  API_BEGIN
+  if (!b) fail(EDGE_EINVAL, "null handle");
+  float a = 0, c = 0, d = 0;
+  CK(cudaEventElapsedTime(&a, b->ev[0], b->ev[1]));
+  CK(cudaEventElapsedTime(&c, b->ev[1], b->ev[2]));
+  CK(cudaEventElapsedTime(&d, b->ev[2], b->ev[3]));
+  if (setup_ms) *setup_ms = a;
+  if (solve_ms) *solve_ms = c;
+  if (post_ms) *post_ms = d;
+  API_END
+}
+
+int edge_batch_last_problem_times(edge_batch* b, double* start_ms, double* end_ms) {
+  API_BEGIN
+  if (!b || !start_ms || !end_ms) fail(EDGE_EINVAL, "null argument");
+  const int n = (int)b->probs.size();
+  CK(cudaMemcpy(b->h_tns, b->d_tns, 2 * n * sizeof(long long), cudaMemcpyDeviceToHost));
+  long long t0 = b->h_tns[0];
+  for (int k = 0; k < n; ++k) t0 = std::min(t0, b->h_tns[2 * k]);
+  for (int k = 0; k < n; ++k) {
+    const int i = b->order[k];
+    start_ms[i] = 1e-6 * (double)(b->h_tns[2 * k] - t0);
+    end_ms[i] = 1e-6 * (double)(b->h_tns[2 * k + 1] - t0);
+  }
   API_END
 }
 
@@ -3504,14 +3605,44 @@ int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double
   }
   const bool mixed = prec != EDGE_FP64;
   std::stable_sort(B.order.begin(), B.order.end(), [&](int a, int c) { return B.cost[a] > B.cost[c]; });
+  // teams take the problems of at least split_dof DOFs (queue positions [0, n_large)), single
+  // blocks the rest; expected work per group: sum of (DOFs + a fixed share for the per-iteration
+  // steps) x the previous PCG iterations
+  int n_large = n;
+  double w_large = 0.0, w_small = 0.0;
+  if (B.team > 1 && B.split_dof > 0) {
+    auto big = [&](int i) { return B.probs[i]->P.n_dof >= B.split_dof; };
+    std::stable_partition(B.order.begin(), B.order.end(), big);
+    n_large = (int)std::count_if(B.order.begin(), B.order.end(), big);
+    for (int k = 0; k < n; ++k) {
+      const int i = B.order[k];
+      const double its = (double)std::max<long long>(1, B.cost[i] / std::max<long long>(1, B.probs[i]->P.n_dof));
+      const double w = its * ((double)B.probs[i]->P.n_dof + 25000.0);
+      if (k < n_large) w_large += 1.2 * w;
+      else w_small += w;
+    }
+  }
+  CK(cudaEventRecord(B.ev[0], s));
+  const int nside = std::min(n, edge_batch::NSIDE);
+  auto fork = [&]() {
+    CK(cudaEventRecord(B.fork, s));
+    for (int q = 0; q < nside; ++q) CK(cudaStreamWaitEvent(B.side[q], B.fork, 0));
+  };
+  auto join = [&]() {
+    for (int q = 0; q < nside; ++q) {
+      CK(cudaEventRecord(B.join[q], B.side[q]));
+      CK(cudaStreamWaitEvent(s, B.join[q], 0));
+    }
+  };
   // per problem: filter + SIMP law into the (possibly padded) grid, loads and warm starts,
   // the hierarchy for the new E
+  fork();
   for (int k = 0; k < n; ++k) {
     const int i = B.order[k];
     Prob& P = B.probs[i]->P;
     const edge_filter& F = *B.filters[i];
     const cudaStream_t saved = P.stream;
-    P.stream = s;
+    P.stream = B.side[k % nside];
     try {
       const Geo& g = P.g0;
       Geo gr = g;  // the real grid's extents in the problem's slot layout
@@ -3525,7 +3656,7 @@ int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double
       if (use_last)
         launch(P, k_user_to_slots_pad, cdiv(g.n, 256), 256, 0, g, B.nxr[i], B.nyr[i], (const double*)U[i], P.x64);
       else
-        CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), s));
+        CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
       mg_setup_prec(P);
       BatchDesc& d = B.h_desc[k];
       std::memset(&d, 0, sizeof(d));
@@ -3574,6 +3705,7 @@ int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double
     }
     P.stream = saved;
   }
+  join();
   // all solves in one launch
   Prob& P0 = B.probs[B.order[0]]->P;
   const cudaStream_t saved0 = P0.stream;
@@ -3581,25 +3713,28 @@ int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double
   try {
     CK(cudaMemcpyAsync(B.d_desc, B.h_desc, n * sizeof(BatchDesc), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(B.d_scal, B.h_scal, n * sizeof(double*), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(B.queue, 0, sizeof(unsigned), s));
+    CK(cudaMemsetAsync(B.queue, 0, 2 * sizeof(unsigned), s));
+    CK(cudaEventRecord(B.ev[1], s));
     if (!mixed)
-      batch_launch<double, double, double>(P0, B, n, tol, maxiter);
+      batch_launch<double, double, double>(P0, B, n, n_large, w_large, w_small, s, tol, maxiter);
     else if (bf16)
-      batch_launch<float, __nv_bfloat16, __nv_bfloat16>(P0, B, n, tol, maxiter);
+      batch_launch<float, __nv_bfloat16, __nv_bfloat16>(P0, B, n, n_large, w_large, w_small, s, tol, maxiter);
     else
-      batch_launch<float, __nv_bfloat16, float>(P0, B, n, tol, maxiter);
+      batch_launch<float, __nv_bfloat16, float>(P0, B, n, n_large, w_large, w_small, s, tol, maxiter);
   } catch (...) {
     P0.stream = saved0;
     throw;
   }
   P0.stream = saved0;
+  CK(cudaEventRecord(B.ev[2], s));
   // per problem: compliance f . U, dr = H^T (dE/drho_f dk), U back in the user layout
+  fork();
   for (int k = 0; k < n; ++k) {
     const int i = B.order[k];
     Prob& P = B.probs[i]->P;
     const edge_filter& F = *B.filters[i];
     const cudaStream_t saved = P.stream;
-    P.stream = s;
+    P.stream = B.side[k % nside];
     try {
       const Geo& g = P.g0;
       Geo gr = g;
@@ -3619,6 +3754,8 @@ int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double
     }
     P.stream = saved;
   }
+  join();
+  CK(cudaEventRecord(B.ev[3], s));
   k_batch_gather<<<cdiv(n, 128), 128, 0, s>>>(B.d_desc, (const double* const*)B.d_scal, n, B.d_res, B.d_comp,
                                                B.d_iters, B.d_done);
   KCHECK();

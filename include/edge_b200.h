@@ -296,6 +296,18 @@ int edge_batch_destroy(edge_batch* b);
  * thread block cluster of that many blocks solves each problem together).  Supported: team 1
  * with 256, 512 (default) or 1024 threads; team 2, 4 or 8 with 512 or 1024 threads. */
 int edge_batch_set_threads(edge_batch* b, int threads, int team);
+/* With team > 1: problems with fewer than split_dof DOFs (default 0 = none) are solved
+ * by single blocks of small_threads threads (256, 512 or 1024, the default) in a second
+ * launch beside the teams' launch, each launch on a share of the SMs proportional to its
+ * problems' expected work. */
+int edge_batch_set_split(edge_batch* b, long long split_dof, int small_threads);
+/* Device time (ms) of the three phases of the last edge_batch_solve_and_process: the
+ * per-problem preparation (filter, law, loads, hierarchy set-up), the solve launch, and the
+ * per-problem post-processing. */
+int edge_batch_last_times(const edge_batch* b, double* setup_ms, double* solve_ms, double* post_ms);
+/* Start and end (ms after the first start) of each problem's solve in the last solve launch,
+ * from the device's global timer: the launch's load balance.  Synchronises the device. */
+int edge_batch_last_problem_times(edge_batch* b, double* start_ms, double* end_ms);
 /* The OC update of every problem (edge_oc_update, TopOpt/_cuda.py:242-280) in one launch on
  * `stream`: one block per problem, the bisection's sums as block sums; rho[i], dr[i],
  * rho_new[i] on the real grid (nelx[i] * nely[i]), A[i] the element area, vol[i] the domain

@@ -191,18 +191,23 @@ def test_batch_of_random_problems_against_oracle(precision, mode):
         assert err.max() < (1e-7 if precision == "fp64" else 1e-5), (spec["index"], err)
 
 
-@pytest.mark.parametrize("threads,team", [(512, 1), (1024, 1), (512, 4), (1024, 8)])
-def test_persistent_batch_equals_per_problem_solves(threads, team):
+@pytest.mark.parametrize("threads,team,split", [(512, 1, 0), (1024, 1, 0), (512, 4, 0), (1024, 8, 0),
+                                               (1024, 4, 4000)])
+def test_persistent_batch_equals_per_problem_solves(threads, team, split):
     """The batched persistent solve (FP64) runs the per-problem FP64 solver's algorithm: the same
     PCG iteration counts and compliances and designs equal to rounding over five SIMP
-    iterations, whatever the launch shape (blocks per problem, threads per block); its batched
-    OC update gives the per-problem OC update's designs bit for bit."""
+    iterations, whatever the launch shape (blocks per problem, threads per block, small problems
+    split off to single blocks in a second launch); its batched OC update gives the per-problem
+    OC update's designs bit for bit."""
     import torch
     from edge_to_b200 import batch
     specs = [batch.random_spec(i, seed=7, nelx_range=(20, 90), nely_range=(12, 48)) for i in range(6)]
     a = batch.BatchSIMP(specs, precision="fp64", tol=1e-8, maxiter=1000, n_threads=2)
     c = batch.BatchSIMP(specs, precision="fp64", tol=1e-8, maxiter=1000, persistent=True, block_threads=threads,
-                        team=team)
+                        team=team, split_dof=split)
+    if split:
+        dofs = [2 * (sp["nelx"] + 1) * (sp["nely"] + 1) for sp in specs]
+        assert min(dofs) < split < max(dofs)
     a.step(5)
     c.step(5)
     for ia, ic in zip(a.items, c.items):
