@@ -275,6 +275,9 @@ def run_ours(args, cfg_name):
         _l.call("edge_set_fuse", opt.kernel.handle, 0)
     if args.omega_schedule:
         opt.solver.mixed_omega = None
+    if args.fuse_xr:
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_fuse_xr", opt.kernel.handle, 1)
     traj = []
     rho, dr, it = warm(opt, rho, args.warmup, traj)
     # the state the timed steps start from; the end-to-end steps restart from it, so both
@@ -408,6 +411,8 @@ def run_ours(args, cfg_name):
                    "residual_recurrence": "fp64" if (args.residual64 or args.precision == "fp64") else "fp32",
                    "programmatic_dependent_launch": args.pdl and not args.no_graph,
                    "fused_fine_launches": args.precision == "mixed" and not args.no_fuse,
+                   "fused_xr_update": (args.precision == "mixed" and not args.no_fuse and args.fuse_xr
+                                       and fixed_omega is not None),
                    "smoother_omega": (f"fixed at {fixed_omega}" if fixed_omega is not None
                                       else "reference schedule (0.40-0.45 on the fine level)")},
         "roofline": {"bound": "hbm", "kernel": "fine-level operator (k_fine3_cube/_pk/_tma + fused epilogues)",
@@ -634,9 +639,14 @@ def run_analysis(args, cfg_name):
     sv = opt.solver
     sv.autotune = False
     sv.tune_sweeps = False
+    if args.fixed_omega and args.precision == "mixed":
+        sv.mixed_omega = "max"
+        sv._omega_mode = "fixed"
     sv._configure()
     h = opt.kernel.handle
     _lib.call("edge_set_fine_tile", h, 10 if args.tile is None else args.tile, args.tile_bps)
+    if args.fuse_xr:
+        _lib.call("edge_set_fuse_xr", h, 1)
     if args.sweeps:
         pat = [int(v) for v in args.sweeps.split(",")]
         _lib.call("edge_mg_set_sweeps", h, _lib.int_array(pat), len(pat))
@@ -749,6 +759,11 @@ def main():
                     help="skip the FP64 trajectory at rtol 1e-10 the timed paths are compared with")
     ap.add_argument("--no-fuse", action="store_true",
                     help="mixed path: the fine level's sweeps and search direction as separate launches")
+    ap.add_argument("--fuse-xr", action="store_true",
+                    help="mixed path: the PCG's x/r update folded into the next iteration's fine launches when "
+                         "the smoother weight is fixed (default: its own launch, faster at 12.8M DOF)")
+    ap.add_argument("--fixed-omega", action="store_true",
+                    help="analysis mode: the mixed path's smoother weight fixed at omega (the autotuner's other choice)")
     ap.add_argument("--omega-schedule", action="store_true",
                     help="mixed path: the reference's residual-driven smoother weight (default: fixed at omega)")
     ap.add_argument("--mode", default="simp", choices=["simp", "matvec", "tiles", "analysis"])

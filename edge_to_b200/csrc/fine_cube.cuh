@@ -67,6 +67,25 @@ EDGE_D bool mbar_wait_fast(uint64_t* bar, uint32_t parity) {
   return mbar_wait(bar, parity);
 }
 
+// Optional members of the input transforms (IN) and epilogues (SE), detected at compile time:
+// IN::parity0() selects the alternative map of input array 0 (a ping-pong pair), IN::kT2 the
+// type of a third input array; SE::kParS names the staged array with an alternative map
+// (chosen by SE::parity()), SE::fin() a custom finisher of the launch's reduction.
+template <class T, class = void> struct HasPar0 : std::false_type {};
+template <class T> struct HasPar0<T, std::void_t<decltype(std::declval<const T&>().parity0())>> : std::true_type {};
+template <class T, class = void> struct HasParS : std::false_type {};
+template <class T> struct HasParS<T, std::void_t<decltype(T::kParS)>> : std::true_type {};
+template <class T, class = void> struct HasFin : std::false_type {};
+template <class T> struct HasFin<T, std::void_t<decltype(std::declval<const T&>().fin())>> : std::true_type {};
+template <class IN> EDGE_HD constexpr int in_t2() {
+  if constexpr (IN::kN == 3) return IN::kT2;
+  else return 0;
+}
+template <class SE> EDGE_HD constexpr int se_pars() {
+  if constexpr (HasParS<SE>::value) return SE::kParS;
+  else return -1;
+}
+
 // v = E * Khat u in block form; uh / vh indexed [h][c], h = hx | hy<<1 | hz<<2; h = 0 is
 // neither read nor written.
 EDGE_D void khat_cube(const P2 kc[8], P2 E, const P2 uh[8][3], P2 vh[8][3]) {
@@ -126,7 +145,7 @@ struct SEStore {  // out = A u
   EDGE_HD static constexpr int kT(int i) { return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 0 : 0; }
   struct In {};
   EDGE_D void init() {}
-  EDGE_D In load(const unsigned char* const*, int, int, const float*, int) const { return {}; }
+  EDGE_D In load(const unsigned char* const*, int, int, const float*, const float*, int) const { return {}; }
   EDGE_D void apply(long long s, const float*, const float* Au, const In&, double&) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) out[c * n + s] = Au[c];
@@ -141,7 +160,7 @@ struct SEStoreDot {  // out = A u, acc += u . A u
   EDGE_HD static constexpr int kT(int i) { return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 0 : 0; }
   struct In {};
   EDGE_D void init() {}
-  EDGE_D In load(const unsigned char* const*, int, int, const float*, int) const { return {}; }
+  EDGE_D In load(const unsigned char* const*, int, int, const float*, const float*, int) const { return {}; }
   EDGE_D void apply(long long s, const float* own, const float* Au, const In&, double& acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -161,7 +180,7 @@ struct SEResid {  // r = b - A u
     float b[3];
   };
   EDGE_D void init() {}
-  EDGE_D In load(const unsigned char* const* sp, int cs4, int, const float*, int) const {
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int, const float*, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) v.b[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
@@ -186,7 +205,7 @@ struct SEJacobi {  // xo = u + w Dinv (b - A u)
     float b[3], d[3];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
-  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, int) const {
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -218,7 +237,7 @@ template <bool DOT> struct SEJacobiAdd {
     float dv[DOT ? 3 : 1];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
-  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, int) const {
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -252,7 +271,7 @@ struct SEResidIn {
     float b[3];
   };
   EDGE_D void init() {}
-  EDGE_D In load(const unsigned char* const*, int, int, const float* in0, int uc4) const {
+  EDGE_D In load(const unsigned char* const*, int, int, const float* in0, const float*, int uc4) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) v.b[c] = in0[c * uc4];
@@ -275,14 +294,19 @@ template <bool DOT> struct SEJacobiAdd0 {
   double wscale;
   long long n;
   float w;
+  // with st: b is the residual of a ping-pong pair, in the buffer of the iteration's parity
+  // (staged array 2 from the alternative map when st->iter is odd)
+  const PcgState* st;
   static constexpr int kN = 3;
   static constexpr bool kDot = DOT;
+  static constexpr int kParS = 2;
+  EDGE_D int parity() const { return st ? (st->iter & 1) : 0; }
   EDGE_HD static constexpr int kT(int i) { return i == 1 ? ST_BF16 : ST_F32; }  // r, Dinv, b
   struct In {
     float r[3], d[3], b[3];
   };
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
-  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, int) const {
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int cs2, const float*, const float*, int) const {
     In v;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -317,7 +341,7 @@ struct SEStorePDot {
   EDGE_HD static constexpr int kT(int) { return 0; }
   struct In {};
   EDGE_D void init() { pout = (st->iter & 1) ? pa : pb; }
-  EDGE_D In load(const unsigned char* const*, int, int, const float*, int) const { return {}; }
+  EDGE_D In load(const unsigned char* const*, int, int, const float*, const float*, int) const { return {}; }
   EDGE_D void apply(long long s, const float* own, const float* Au, const In&, double& acc) const {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -328,6 +352,116 @@ struct SEStorePDot {
   }
 };
 
+// Finisher of the residual-update launch: the state of k_pcg_xr32's finisher (alpha, rz,
+// rr, residual, iteration count, stop reason, next omega), and the pending solution update
+// x32 += alpha p that the next search-direction launch applies (st->xa).
+struct PcgXrFinX {
+  PcgState* st;
+  bool upd;
+  double alpha;
+  EDGE_D void operator()(double t) const {
+    if (!upd) return;
+    PcgXrFin{st, alpha}(t);
+    st->xa = alpha;
+  }
+};
+
+// Epilogue of the fused first launch (InWDBQ): r = b - A u into the level-0 residual, and,
+// with an update pending, the updated PCG residual b into the other buffer of the ping-pong
+// pair and r.r (FP64 sum of the FP32 squares) for the finisher.
+struct SEResidInX {
+  float* r;
+  float* R0;
+  float* R1;
+  PcgState* st;
+  long long n;
+  float af;
+  bool upd;
+  double alpha;
+  float* rout;
+  static constexpr int kN = 0;
+  static constexpr bool kDot = true;
+  EDGE_HD static constexpr int kT(int) { return 0; }
+  struct In {
+    float b[3];
+  };
+  EDGE_D void init() {
+    upd = st->pend != 0;
+    alpha = upd ? st->rz_new / st->pq : 0.0;
+    af = (float)alpha;
+    rout = (st->iter & 1) ? R0 : R1;
+  }
+  EDGE_D In load(const unsigned char* const*, int, int, const float* in0, const float* in1, int uc4) const {
+    In v;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v.b[c] = upd ? fmaf(-af, in1[c * uc4], in0[c * uc4]) : in0[c * uc4];
+    return v;
+  }
+  EDGE_D void apply(long long s, const float*, const float* Au, const In& v, double& acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      r[c * n + s] = v.b[c] - Au[c];
+      if (upd) {
+        rout[c * n + s] = v.b[c];
+        acc += (double)(v.b[c] * v.b[c]);
+      }
+    }
+  }
+  EDGE_D PcgXrFinX fin() const { return PcgXrFinX{st, upd, alpha}; }
+};
+
+// Finisher of the search-direction launch: p.q, and from now on a residual update is pending.
+struct PqFin {
+  PcgState* st;
+  EDGE_D void operator()(double t) const {
+    st->pq = t;
+    st->pend = 1;
+  }
+};
+
+// SEStorePDot with the pending solution update: x32 += xa p_old at the owner nodes (FP32,
+// k_pcg_xr32's arithmetic; p_old is the input transform's array 1, x32 staged), xa the alpha
+// of the previous iteration (0: nothing pending).
+struct SEStorePDotX {
+  float* q;
+  float* pa;
+  float* pb;
+  PcgState* st;
+  long long n;
+  float* x32;
+  float* pout;
+  float xa;
+  static constexpr int kN = 1;
+  static constexpr bool kDot = true;
+  EDGE_HD static constexpr int kT(int) { return ST_F32; }
+  struct In {
+    float x[3], po[3];
+  };
+  EDGE_D void init() {
+    pout = (st->iter & 1) ? pa : pb;
+    xa = (float)st->xa;
+  }
+  EDGE_D In load(const unsigned char* const* sp, int cs4, int, const float*, const float* in1, int uc4) const {
+    In v;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      v.x[c] = reinterpret_cast<const float*>(sp[0])[c * cs4];
+      v.po[c] = in1[c * uc4];
+    }
+    return v;
+  }
+  EDGE_D void apply(long long s, const float* own, const float* Au, const In& v, double& acc) const {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      q[c * n + s] = Au[c];
+      pout[c * n + s] = own[c];
+      acc += (double)own[c] * (double)Au[c];
+      if (xa != 0.f) x32[c * n + s] = fmaf(xa, v.po[c], v.x[c]);
+    }
+  }
+  EDGE_D PqFin fin() const { return PqFin{st}; }
+};
+
 // ------------------------------------------------------------------ operator inputs
 // value(a0, a1, i4, i2): the input at one node and component of the stage, from array 0
 // (FP32, element index i4) and array 1 (kT1: FP32 index i4 or BF16 index i2).
@@ -336,7 +470,7 @@ struct InU {  // u itself
   static constexpr int kT1 = ST_F32;
   EDGE_D void init() {}
   EDGE_D int parity() const { return 0; }
-  EDGE_D float value(const float* a0, const void*, int i4, int) const { return a0[i4]; }
+  EDGE_D float value(const float* a0, const void*, const void*, int i4, int) const { return a0[i4]; }
 };
 struct InWDB {  // u = (w Dinv) b: the first damped-Jacobi sweep from zero (k_jacobi0)
   const double* omega;
@@ -346,7 +480,7 @@ struct InWDB {  // u = (w Dinv) b: the first damped-Jacobi sweep from zero (k_ja
   static constexpr int kT1 = ST_BF16;
   EDGE_D void init() { w = (float)(__ldg(omega) * wscale); }
   EDGE_D int parity() const { return 0; }
-  EDGE_D float value(const float* a0, const void* a1, int i4, int i2) const {
+  EDGE_D float value(const float* a0, const void* a1, const void*, int i4, int i2) const {
     return (w * __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(a1)[i2])) * a0[i4];
   }
 };
@@ -363,8 +497,39 @@ struct InPDir {  // u = z + beta p_old (the first PCG iteration: u = z)
     beta = first ? 0.f : (float)(st->rz_new / st->rz);
   }
   EDGE_D int parity() const { return par; }
-  EDGE_D float value(const float* a0, const void* a1, int i4, int) const {
+  EDGE_D float value(const float* a0, const void* a1, const void*, int i4, int) const {
     return first ? a0[i4] : fmaf(beta, reinterpret_cast<const float*>(a1)[i4], a0[i4]);
+  }
+};
+
+// The PCG's residual update folded into the V-cycle's first fine launch: b = r_old - alpha q
+// (alpha = rz / pq of the previous iteration; FP32 arithmetic of k_pcg_xr32), then
+// u = (w Dinv) b, the first damped-Jacobi sweep from zero.  r_old is the residual of a
+// ping-pong pair (array 0: the map of the buffer of st->iter's parity), q FP32 (array 1),
+// Dinv BF16 (array 2).  No update is pending before the first product (st->pend == 0) or with
+// `plain` (the residual was just replaced): b = r_old.
+struct InWDBQ {
+  const PcgState* st;
+  const double* omega;
+  double wscale;
+  bool plain;
+  float w, af;
+  bool upd;
+  int par;
+  static constexpr int kN = 3;
+  static constexpr int kT1 = ST_F32;
+  static constexpr int kT2 = ST_BF16;
+  EDGE_D void init() {
+    w = (float)(__ldg(omega) * wscale);
+    upd = !plain && st->pend;
+    af = upd ? (float)(st->rz_new / st->pq) : 0.f;
+    par = st->iter & 1;
+  }
+  EDGE_D int parity() const { return 0; }
+  EDGE_D int parity0() const { return par; }
+  EDGE_D float value(const float* a0, const void* a1, const void* a2, int i4, int i2) const {
+    const float b = upd ? fmaf(-af, reinterpret_cast<const float*>(a1)[i4], a0[i4]) : a0[i4];
+    return (w * __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(a2)[i2])) * b;
   }
 };
 
@@ -378,9 +543,11 @@ template <int BX, class SE, class IN = InU> struct CubeTile {
   static constexpr int up(int b) { return (b + 127) & ~127; }
   static constexpr int sbytes(int t) { return 3 * ROWS * st_width(t) * st_esize(t); }
   static constexpr int U0_BYTES = B::U_BYTES;
-  static constexpr int U1_BYTES = IN::kN == 2 ? 3 * NR * st_width(IN::kT1) * st_esize(IN::kT1) : 0;
+  static constexpr int U1_BYTES = IN::kN >= 2 ? 3 * NR * st_width(IN::kT1) * st_esize(IN::kT1) : 0;
+  static constexpr int U2_BYTES = IN::kN == 3 ? 3 * NR * st_width(in_t2<IN>()) * st_esize(in_t2<IN>()) : 0;
   static constexpr int U1_OFF = up(U0_BYTES);
-  static constexpr int F_OFF = U1_OFF + up(U1_BYTES);
+  static constexpr int U2_OFF = U1_OFF + up(U1_BYTES);
+  static constexpr int F_OFF = U2_OFF + up(U2_BYTES);
   static constexpr int E_OFF = F_OFF + up(B::F_BYTES);
   static constexpr int BASE = E_OFF + up(B::E_BYTES);
   static constexpr int s_off(int i) {
@@ -389,7 +556,7 @@ template <int BX, class SE, class IN = InU> struct CubeTile {
     return o;
   }
   static constexpr int tx_bytes() {
-    int t = B::TX_BYTES + U1_BYTES;
+    int t = B::TX_BYTES + U1_BYTES + U2_BYTES;
     for (int j = 0; j < SE::kN; ++j) t += sbytes(SE::kT(j));
     return t;
   }
@@ -407,12 +574,14 @@ constexpr int cube_smem_bytes() {
 
 template <class SE, int BX, int NS, int MINB, class IN = InU>
 __global__ void __launch_bounds__(32 * BX, MINB)
-k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_constant__ CUtensorMap mapU1,
-             const __grid_constant__ CUtensorMap mapU1b, const __grid_constant__ CUtensorMap mapF,
+k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid_constant__ CUtensorMap mapUb,
+             const __grid_constant__ CUtensorMap mapU1, const __grid_constant__ CUtensorMap mapU1b,
+             const __grid_constant__ CUtensorMap mapU2, const __grid_constant__ CUtensorMap mapF,
              const __grid_constant__ CUtensorMap mapE, const uint8_t* __restrict__ mask,
              const __grid_constant__ CUtensorMap mapS0, const __grid_constant__ CUtensorMap mapS1,
-             const __grid_constant__ CUtensorMap mapS2, const __grid_constant__ CUtensorMap mapS3, const KCube KC,
-             const int ly, IN in, SE epi, double* part, unsigned* ticket, double* dot_dst, int* err) {
+             const __grid_constant__ CUtensorMap mapS2, const __grid_constant__ CUtensorMap mapS3,
+             const __grid_constant__ CUtensorMap mapSb, const KCube KC, const int ly, IN in, SE epi, double* part,
+             unsigned* ticket, double* dot_dst, int* err) {
   EDGE_PDL_ENTRY();
   static_assert(NS >= 3, "a stage is refilled one layer after its last use");
   using Tile = CubeTile<BX, SE, IN>;
@@ -442,8 +611,13 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
   const bool writerB = zok && (exa + 1 < g.nx);
   in.init();
   epi.init();
-  // the array 1 map: the second buffer of a ping-pong pair on odd iterations (InPDir)
+  // the array 1 map: the second buffer of a ping-pong pair on odd iterations (InPDir); array 0
+  // and the staged array SE::kParS likewise when the input transform / epilogue says so
   const CUtensorMap* map1 = in.parity() ? &mapU1b : &mapU1;
+  const CUtensorMap* map0 = &mapU;
+  if constexpr (HasPar0<IN>::value) map0 = in.parity0() ? &mapUb : &mapU;
+  int spar = 0;
+  if constexpr (se_pars<SE>() >= 0) spar = epi.parity();
   bool ok = true;
   P2 kc[8];
   kc[0] = pk(KC.nd, KC.nd);
@@ -465,15 +639,18 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
     unsigned char* st = smem + s * Tile::STAGE;
     const int p = p0 + k;
     mbar_expect_tx(&bar[s], Tile::TX_BYTES);
-    tma_load_4d(st, &mapU, zs4, x0 - 1, p, 0, &bar[s]);
-    if constexpr (IN::kN == 2)
+    tma_load_4d(st, map0, zs4, x0 - 1, p, 0, &bar[s]);
+    if constexpr (IN::kN >= 2)
       tma_load_4d(st + Tile::U1_OFF, map1, IN::kT1 == ST_BF16 ? zs8 : zs4, x0 - 1, p, 0, &bar[s]);
+    if constexpr (IN::kN == 3)
+      tma_load_4d(st + Tile::U2_OFF, &mapU2, in_t2<IN>() == ST_BF16 ? zs8 : zs4, x0 - 1, p, 0, &bar[s]);
     tma_load_3d(st + Tile::F_OFF, &mapF, zs16, x0 - 1, p, &bar[s]);
     tma_load_3d(st + Tile::E_OFF, &mapE, zs4, x0 - 1, p, &bar[s]);
     const CUtensorMap* ms[4] = {&mapS0, &mapS1, &mapS2, &mapS3};
 #pragma unroll
     for (int i = 0; i < SE::kN; ++i)
-      tma_load_4d(st + Tile::s_off(i), ms[i], SE::kT(i) == ST_BF16 ? zs8 : zs4, x0 - 1, p, 0, &bar[s]);
+      tma_load_4d(st + Tile::s_off(i), (i == se_pars<SE>() && spar) ? &mapSb : ms[i],
+                  SE::kT(i) == ST_BF16 ? zs8 : zs4, x0 - 1, p, 0, &bar[s]);
   };
   if (tid == 0)
     for (int k = 0; k < NS && k < np; ++k) issue(k);
@@ -484,12 +661,12 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
   const int foff = c0 * PK_FB + zo16 + zl;
   auto a0_of = [&](int k) { return reinterpret_cast<const float*>(smem + (k % NS) * Tile::STAGE); };
   auto a1_of = [&](int k) { return (const void*)(smem + (k % NS) * Tile::STAGE + Tile::U1_OFF); };
-  // input value of component c at row offset r (0..2) and z offset dz (0, 1) of plane k
+  auto a2_of = [&](int k) { return (const void*)(smem + (k % NS) * Tile::STAGE + Tile::U2_OFF); };
+  // input value of component c at row offset r (0..2) and z offset dz (0, 1) of plane k; the
+  // transform indexes FP32 arrays with the first index and BF16 arrays with the second
   auto input = [&](int k, int c, int r, int dz) {
-    constexpr int W1 = IN::kT1 == ST_BF16 ? 32 : PK_ZB;
-    constexpr int C1 = IN::kT1 == ST_BF16 ? UC2 : UC4;
-    return in.value(a0_of(k), a1_of(k), c * UC4 + r * PK_ZB + dz + i4,
-                    IN::kT1 == ST_BF16 ? c * C1 + r * W1 + dz + i2 : c * C1 + r * W1 + dz + i4);
+    return in.value(a0_of(k), a1_of(k), a2_of(k), c * UC4 + r * PK_ZB + dz + i4,
+                    c * UC2 + r * st_width(ST_BF16) + dz + i2);
   };
 
   // The 3 node rows x 2 z of plane p (stage k), masked on constrained DOFs when `fl` says
@@ -644,8 +821,10 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
       }
       constexpr int cs4 = Tile::ROWS * st_width(ST_F32), cs2 = Tile::ROWS * st_width(ST_BF16);
       const float* in0 = a0_of(k) + i4;
-      if (wrA) inA = epi.load(spA, cs4, cs2, in0, UC4);
-      if (wrB) inB = epi.load(spB, cs4, cs2, in0 + PK_ZB, UC4);
+      // array 1 at the node when it is FP32 (the previous search direction, the product q)
+      const float* in1 = reinterpret_cast<const float*>(a1_of(k)) + i4;
+      if (wrA) inA = epi.load(spA, cs4, cs2, in0, in1, UC4);
+      if (wrB) inB = epi.load(spB, cs4, cs2, in0 + PK_ZB, in1 + PK_ZB, UC4);
     }
     if (xh == 0) {
 #pragma unroll
@@ -688,7 +867,13 @@ k_fine3_cube(const Geo g, const __grid_constant__ CUtensorMap mapU, const __grid
   }
   if (k + 1 < np) layer(k, pa, pb);
   if (!ok) atomicOr(err, 1);
-  finish_dot(epi, dacc, part, ticket, dot_dst);
+  if constexpr (HasFin<SE>::value) {
+    __shared__ double shf[32];
+    const double bt = block_sum(dacc, shf);
+    grid_reduce_finish(bt, part, ticket, epi.fin());
+  } else {
+    finish_dot(epi, dacc, part, ticket, dot_dst);
+  }
 }
 
 }  // namespace edge

@@ -351,6 +351,11 @@ struct PcgState {
   double last_replace;      // ||r||/||f|| at the last true-residual replacement (mixed precision)
   int iter, maxiter, done;  // done: 1 converged, 2 maxiter
   int n_true;               // replacements made inside the iteration loop
+  // residual update folded into the next iteration's first fine launch (mixed path): pend =
+  // a search direction's product exists whose update is still to be applied; xa = the alpha
+  // of the solution update x32 += alpha p still to be applied (0: none)
+  int pend;
+  double xa;
 };
 
 // x += alpha p ; r -= alpha q ; rr = r.r with alpha = rz_new / pq.  The finisher
@@ -508,6 +513,44 @@ __global__ void k_pcg_xr32(long long n, float* __restrict__ x32, const float* __
   grid_reduce_finish(bt, part, ticket, PcgXrFin{st, alpha});
 }
 
+// The pending solution update of the fused residual update (st->xa != 0): x32 += xa p with the
+// search direction of the previous iteration (the p buffer k_pcg_xr32 would have read then),
+// applied before the solution is folded into FP64 or the solve ends; FP32, k_pcg_xr32's
+// arithmetic.
+__global__ void k_x32_pend(long long n, float* __restrict__ x32, const float* __restrict__ p0,
+                           const float* __restrict__ p1, const PcgState* st) {
+  EDGE_PDL_ENTRY();
+  const float af = (float)st->xa;
+  if (af == 0.f) return;
+  const float* __restrict__ p = (st->iter & 1) ? p1 : p0;
+  const long long n4 = n >> 2;
+  float4* __restrict__ x4 = reinterpret_cast<float4*>(x32);
+  const float4* __restrict__ p4 = reinterpret_cast<const float4*>(p);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 pv = p4[i];
+    float4 xv = x4[i];
+    xv.x = fmaf(af, pv.x, xv.x);
+    xv.y = fmaf(af, pv.y, xv.y);
+    xv.z = fmaf(af, pv.z, xv.z);
+    xv.w = fmaf(af, pv.w, xv.w);
+    x4[i] = xv;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
+    const long long i = 4 * n4 + threadIdx.x;
+    x32[i] = fmaf(af, p[i], x32[i]);
+  }
+}
+
+// FP32 copy of the replaced residual into the buffer of the ping-pong pair that holds the
+// current residual (st->iter's parity).
+__global__ void k_r32_par(long long n, const double* __restrict__ r, float* __restrict__ R0, float* __restrict__ R1,
+                          const PcgState* st) {
+  EDGE_PDL_ENTRY();
+  float* __restrict__ o = (st->iter & 1) ? R1 : R0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    o[i] = (float)r[i];
+}
+
 // x64 += x32, x32 = 0
 __global__ void k_fold_x(long long n, double* __restrict__ x, float* __restrict__ x32) {
   EDGE_PDL_ENTRY();
@@ -525,6 +568,7 @@ __global__ void k_pcg_true_res(PcgState* st) {
   st->res = R;
   st->last_replace = R;
   st->n_true += 1;
+  st->xa = 0.0;  // a pending solution update was applied before the replacement
   if (R < st->tol) {
     st->done = 1;
   } else {
@@ -635,6 +679,22 @@ __global__ void k_cond_while(cudaGraphConditionalHandle h, const PcgState* st) {
 __global__ void k_cond_replace(cudaGraphConditionalHandle h, const PcgState* st, double drop) {
   EDGE_PDL_ENTRY();
   cudaGraphSetConditional(h, (st->done == 1 || st->res < drop * st->last_replace) ? 1u : 0u);
+}
+// The same test with the residual update fused into the iteration's first launch: only once a
+// residual update has been applied (not in the first iteration, whose residual is the
+// prologue's true residual).
+EDGE_HD bool replace_due_xr(const PcgState* st, double drop) {
+  return st->pend && (st->done == 1 || st->res < drop * st->last_replace);
+}
+__global__ void k_cond_replace_xr(cudaGraphConditionalHandle h, const PcgState* st, double drop) {
+  EDGE_PDL_ENTRY();
+  cudaGraphSetConditional(h, replace_due_xr(st, drop) ? 1u : 0u);
+}
+// The rest of the iteration (V-cycle below the first launch, the search direction's product)
+// runs while the solve is not done.
+__global__ void k_cond_rest(cudaGraphConditionalHandle h, const PcgState* st) {
+  EDGE_PDL_ENTRY();
+  cudaGraphSetConditional(h, st->done == 0 ? 1u : 0u);
 }
 
 // ------------------------------------------------------------------ point springs and adjoint sensitivity

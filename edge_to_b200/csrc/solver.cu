@@ -273,6 +273,13 @@ struct Prob {
   // mixed path: fused fine launches (first sweep + residual in one launch, the last sweep
   // without a stored pre-smoothed iterate, the search direction formed inside the product)
   bool fuse = true;
+  // mixed path with a fixed smoother weight and the fused fine launches: the PCG's x/r update
+  // folded into the next iteration's first fine launch (residual) and search-direction launch
+  // (solution); r32b is the second buffer of the FP32 residual's ping-pong pair.  Off by
+  // default: at 12.8M DOF the two launches grew by 50 and 31 us (their third staged array and
+  // the extra registers cost occupancy), more than the 50 us update launch they replace.
+  bool fuse_xr = false;
+  float* r32b = nullptr;
   // mixed path, 3-D: the V-cycle from level tail_l0 down (sweeps, residuals, transfers and
   // the coarsest solve) as one persistent cooperative launch; 0 = off (the default: at 12.8M
   // DOF the launch took longer than the per-step launches it replaces)
@@ -731,9 +738,18 @@ static const CUtensorMap& in_map(Prob& P, const void* base, int t) {
 
 // One launch of the cube kernel: input transform IN over arrays in0 (FP32) and in1 (IN::kT1;
 // in1b its second ping-pong buffer, or null), staged epilogue arrays arr[0..SE::kN).
+// Alternative and third arrays of a cube launch: in0b, the other buffer of input array 0's
+// ping-pong pair (IN::parity0); in2, input array 2 (IN::kN == 3); sb, the other buffer of the
+// staged array SE::kParS.
+struct CubeExtra {
+  const float* in0b = nullptr;
+  const void* in2 = nullptr;
+  const void* sb = nullptr;
+};
+
 template <class SE, class IN, int BX, int NS, int MINB>
 static void fine3_cube_go(Prob& P, const float* in0, const void* in1, const void* in1b, const float* E, IN in,
-                          SE epi, const void* const* arr, double* dot_dst) {
+                          SE epi, const void* const* arr, double* dot_dst, const CubeExtra& xa = {}) {
   const Geo& g = P.g0;
   constexpr int smem = cube_smem_bytes<BX, NS, SE, IN>();
   static_assert(smem <= 227 * 1024, "cube kernel stage ring exceeds shared memory");
@@ -743,18 +759,23 @@ static void fine3_cube_go(Prob& P, const float* in0, const void* in1, const void
     attr = true;
   }
   const CUtensorMap& m0 = pk_map<BX>(P, in0, 0);
-  const CUtensorMap& m1 = IN::kN == 2 ? in_map<BX>(P, in1, IN::kT1) : m0;
-  const CUtensorMap& m1b = (IN::kN == 2 && in1b) ? in_map<BX>(P, in1b, IN::kT1) : m1;
+  const CUtensorMap& m0b = xa.in0b ? pk_map<BX>(P, xa.in0b, 0) : m0;
+  const CUtensorMap& m1 = IN::kN >= 2 ? in_map<BX>(P, in1, IN::kT1) : m0;
+  const CUtensorMap& m1b = (IN::kN >= 2 && in1b) ? in_map<BX>(P, in1b, IN::kT1) : m1;
+  const CUtensorMap& m2 = IN::kN == 3 ? in_map<BX>(P, xa.in2, in_t2<IN>()) : m0;
   const CUtensorMap* ms[4];
   for (int i = 0; i < 4; ++i) ms[i] = i < SE::kN ? &stage_map<BX>(P, arr[i], SE::kT(i)) : &m0;
+  constexpr int ps = se_pars<SE>();
+  const CUtensorMap* msb = &m0;
+  if constexpr (ps >= 0 && ps < SE::kN) msb = xa.sb ? &stage_map<BX>(P, xa.sb, SE::kT(ps)) : ms[ps];
   const unsigned tz = cdiv(g.nz, 15), tx = cdiv(g.nx, 4 * BX - 1);
   const long long want = 148LL * P.blocks_per_sm;
   long long chunks = std::max<long long>(1, (want + (long long)tz * tx - 1) / ((long long)tz * tx));
   chunks = std::min<long long>(chunks, g.ny);
   const int ly = (int)cdiv(g.ny, chunks);
-  launch(P, k_fine3_cube<SE, BX, NS, MINB, IN>, dim3(tz, tx, cdiv(g.ny, ly)), dim3(32, BX), smem, g, m0, m1, m1b,
-         pk_flag_map<BX>(P), pk_map<BX>(P, E, 1), (const uint8_t*)P.mask, *ms[0], *ms[1], *ms[2], *ms[3],
-         P.kcube, ly, in, epi, P.part, P.ticket, dot_dst, P.err);
+  launch(P, k_fine3_cube<SE, BX, NS, MINB, IN>, dim3(tz, tx, cdiv(g.ny, ly)), dim3(32, BX), smem, g, m0, m0b, m1,
+         m1b, m2, pk_flag_map<BX>(P), pk_map<BX>(P, E, 1), (const uint8_t*)P.mask, *ms[0], *ms[1], *ms[2], *ms[3],
+         *msb, P.kcube, ly, in, epi, P.part, P.ticket, dot_dst, P.err);
 }
 
 template <class Epi, int BX, int NS, int MINB>
@@ -775,18 +796,18 @@ static bool cube_fusable(const Prob& P) {
 // fine_apply with io_bytes algorithmic bytes per DOF besides E.
 template <class SE, class IN>
 static void fine3_cube_fused(Prob& P, const float* in0, const void* in1, const void* in1b, IN in, SE epi,
-                             const void* const* arr, double* dot_dst, double io_bytes) {
+                             const void* const* arr, double* dot_dst, double io_bytes, const CubeExtra& xa = {}) {
   CatScope cat(P, CAT_FINE);
   const bool rec = P.prof && P.pev_used + 2 <= P.pev.size();
   if (rec) CK(cudaEventRecord(P.pev[P.pev_used], P.stream));
   switch (P.tile_variant) {
-    case 9: fine3_cube_go<SE, IN, 4, 3, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
-    case 10: fine3_cube_go<SE, IN, 4, 4, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
-    case 11: fine3_cube_go<SE, IN, 2, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
-    case 12: fine3_cube_go<SE, IN, 8, 3, 1>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
-    case 13: fine3_cube_go<SE, IN, 4, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
-    case 15: fine3_cube_go<SE, IN, 4, 3, 3>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
-    default: fine3_cube_go<SE, IN, 4, 4, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst); break;
+    case 9: fine3_cube_go<SE, IN, 4, 3, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
+    case 10: fine3_cube_go<SE, IN, 4, 4, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
+    case 11: fine3_cube_go<SE, IN, 2, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
+    case 12: fine3_cube_go<SE, IN, 8, 3, 1>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
+    case 13: fine3_cube_go<SE, IN, 4, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
+    case 15: fine3_cube_go<SE, IN, 4, 3, 3>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
+    default: fine3_cube_go<SE, IN, 4, 4, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
   }
   if (rec) {
     CK(cudaEventRecord(P.pev[P.pev_used + 1], P.stream));
@@ -964,6 +985,8 @@ __global__ void k_pcg_init(PcgState* st, double tol, int maxiter, double min_ome
   st->res = 0.0;
   st->last_replace = 1.0;
   st->n_true = 0;
+  st->pend = 0;
+  st->xa = 0.0;
 }
 __global__ void k_pcg_check_bb(PcgState* st, const int* chol_status) {
   EDGE_PDL_ENTRY();
@@ -1139,8 +1162,11 @@ static void restrict_to(Prob& P, int l, const T* r) {
   P.cur_cat = CAT_VECTOR;
 }
 
+// xr (level 0 of the fused x/r path): the first fine launch already ran (pcgmx_l1x) and b is
+// the FP32 residual of the ping-pong pair (P.r32 / P.r32b by the iteration's parity).
 template <typename T, typename TD0, typename TV>
-static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* dot_dst, bool pre_done = false) {
+static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* dot_dst, bool pre_done = false,
+                   bool xr = false) {
   Level& Lv = P.lv[l];
   const Geo& g = Lv.g;
   const long long nv = (long long)g.dof * g.n;
@@ -1172,7 +1198,7 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
     // one sweep on the fine level of the mixed path: the pre-smoothed iterate w Dinv b is
     // computed inside the two fine launches that need it instead of being stored
     if (l == 0 && nsm == 1 && visits0 == 1 && cube_fusable(P) && (!dot_dst || (const void*)dotv == (const void*)b)) {
-      {  // r = b - A (w Dinv b)
+      if (!xr) {  // r = b - A (w Dinv b)
         InWDB in{om, ws, 0.f};
         SEResidIn e{r, g.n};
         fine3_cube_fused(P, b, Lv.dinv, nullptr, in, e, nullptr, nullptr, 4 + 2 + 4);
@@ -1187,12 +1213,15 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
       KCHECK();
       P.cur_cat = CAT_VECTOR;
       const void* arr[3] = {r, Lv.dinv, b};  // out = w Dinv b + (e + w Dinv (r - A e)) [, b . out]
+      CubeExtra xb;
+      if (xr) xb.sb = P.r32b;
+      const PcgState* pst = xr ? (const PcgState*)P.st : nullptr;
       if (dot_dst) {
-        SEJacobiAdd0<true> e{out, om, ws, g.n, 0.f};
-        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, dot_dst, 4 + 4 + 2 + 4 + 4);
+        SEJacobiAdd0<true> e{out, om, ws, g.n, 0.f, pst};
+        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, dot_dst, 4 + 4 + 2 + 4 + 4, xb);
       } else {
-        SEJacobiAdd0<false> e{out, om, ws, g.n, 0.f};
-        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, nullptr, 4 + 4 + 2 + 4 + 4);
+        SEJacobiAdd0<false> e{out, om, ws, g.n, 0.f, pst};
+        fine3_cube_fused(P, e1, nullptr, nullptr, InU{}, e, arr, nullptr, 4 + 4 + 2 + 4 + 4, xb);
       }
       KCHECK();
       return;
@@ -1486,6 +1515,74 @@ static void pcgmx_body(Prob& P) {
     launch(P, k_pcg_xr_lag, nb, 256, 0, nv, P.x32, (const float*)p, P.r64, (const float*)q, P.st, P.part, P.ticket,
            P.r32);
 }
+// ---- mixed path, x/r update fused (xr_usable).  One iteration:
+//   head: the first fine launch applies the previous iteration's residual update
+//         r = r_old - alpha q on the fly (InWDBQ), writes it into the other buffer of the
+//         residual's ping-pong pair with r.r for the convergence test (SEResidInX), and starts
+//         the V-cycle from it (u = w Dinv r, level-0 residual r - A u);
+//   replace (when due): the pending solution update, fold into FP64, true residual, and the
+//         head's V-cycle start again from the replaced residual;
+//   rest (while not done): the V-cycle below the head, p = z + beta p_old with q = A p and the
+//         previous iteration's solution update x32 += alpha p_old (SEStorePDotX).
+// The smoother weight must not depend on the residual of the same iteration (it is fixed):
+// the head's V-cycle start runs before that residual's norm is known.
+static bool xr_usable(const Prob& P) {
+  if (P.prec == EDGE_FP64 || !P.fuse || !P.fuse_xr || !P.res32 || P.n_springs || !cube_fusable(P)) return false;
+  if (P.omega != P.min_omega || P.sweeps(0) != 1 || P.n_level < 1) return false;
+  return !(P.cycle_w && std::find(P.w_levels.begin(), P.w_levels.end(), 0) != P.w_levels.end());
+}
+static void pcgmx_l1x(Prob& P, bool plain) {
+  const Level& L0 = P.lv[0];
+  const Geo& g = P.g0;
+  InWDBQ in{(const PcgState*)P.st, &P.st->omega, 1.0, plain, 0.f, 0.f, false, 0};
+  CubeExtra xa;
+  xa.in0b = P.r32b;
+  xa.in2 = L0.dinv;
+  const float* q = (const float*)P.q;
+  if (plain) {
+    SEResidIn e{(float*)L0.r, g.n};
+    fine3_cube_fused(P, P.r32, q, q, in, e, nullptr, nullptr, 4 + 4 + 2 + 4, xa);
+  } else {
+    SEResidInX e{(float*)L0.r, P.r32, P.r32b, P.st, g.n, 0.f, false, 0.0, nullptr};
+    fine3_cube_fused(P, P.r32, q, q, in, e, nullptr, nullptr, 4 + 4 + 2 + 4 + 4, xa);
+  }
+}
+static void pcgmx_pending_x(Prob& P) {
+  const long long nv = (long long)P.g0.dof * P.g0.n;
+  float* p = (float*)P.p;
+  launch(P, k_x32_pend, ew_blocks(nv), 256, 0, nv, P.x32, (const float*)p, (const float*)(p + nv),
+         (const PcgState*)P.st);
+}
+static void pcgmx_replace_xr(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  const unsigned nb = std::min<unsigned>(ew_blocks(nv), 1024);
+  pcgmx_pending_x(P);
+  launch(P, k_fold_x, ew_blocks(nv), 256, 0, nv, P.x64, P.x32);
+  EpiResid<double, double, double> e{P.b64, P.r64, g.n};
+  fine_apply<double>(P, (const double*)P.x64, e, nullptr);
+  launch(P, k_dot<double, double>, nb, 256, 0, nv, (const double*)P.r64, (const double*)P.r64, P.part, P.ticket,
+         &P.st->rr);
+  launch(P, k_r32_par, ew_blocks(nv), 256, 0, nv, (const double*)P.r64, P.r32, P.r32b, (const PcgState*)P.st);
+  launch(P, k_pcg_true_res, 1, 1, 0, P.st);
+  pcgmx_l1x(P, true);
+}
+static void pcgmx_rest_xr(Prob& P) {
+  CatScope cat(P, CAT_VECTOR);
+  const Geo& g = P.g0;
+  const long long nv = (long long)g.dof * g.n;
+  float* p = (float*)P.p;
+  float* q = (float*)P.q;
+  float* z = (float*)P.lv[0].res;
+  vcycle<float, __nv_bfloat16, float>(P, 0, P.r32, z, P.r32, &P.st->rz_new, false, true);
+  float* p1 = p + nv;
+  InPDir in{(const PcgState*)P.st, 0.f, 0, false};
+  SEStorePDotX e{q, p, p1, P.st, g.n, P.x32, nullptr, 0.f};
+  const void* arr[1] = {P.x32};
+  fine3_cube_fused(P, (const float*)z, p, p1, in, e, arr, nullptr, 4 + 4 + 4 + 4 + 8);
+}
+
 // x64 += x32 (the FP32 increment of the solution since the last replacement), x32 = 0
 static void pcgmx_fold(Prob& P) {
   CatScope cat(P, CAT_VECTOR);
@@ -1513,6 +1610,22 @@ static void pcg_host(Prob& P, double tol, int maxiter) {
     pcg64_prologue(P, tol, maxiter);
   read_state(P);
   P.last_true_res = mixed ? 1 : 0;
+  if (mixed && xr_usable(P)) {  // the launches of the graph's fused x/r iteration
+    while (!P.st_h->done) {
+      pcgmx_l1x(P, false);
+      read_state(P);
+      if (replace_due_xr(P.st_h, REPLACE_DROP)) {
+        pcgmx_replace_xr(P);
+        read_state(P);
+        ++P.last_true_res;
+      }
+      if (!P.st_h->done) pcgmx_rest_xr(P);
+    }
+    pcgmx_pending_x(P);
+    pcgmx_fold(P);
+    P.last_iters = P.st_h->iter;
+    return;
+  }
   while (!P.st_h->done) {
     if (mixed) {
       pcgmx_body(P);
@@ -1558,7 +1671,8 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, boo
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons,
                            (double)P.st_bf16, (double)P.st_pair, (double)P.st_pair_min, (double)P.res32,
-                           (double)P.pdl, (double)P.fuse, (double)P.tail_l0, (double)P.omega_carry, (double)(P.omega_carry && P.omega_started)};
+                           (double)P.pdl, (double)P.fuse, (double)P.tail_l0, (double)P.omega_carry, (double)(P.omega_carry && P.omega_started),
+                           (double)P.fuse_xr};
   for (int l : P.w_levels) k.push_back((double)l);
   k.push_back(-1.0);
   for (int v : P.level_sweeps) k.push_back((double)v);
@@ -1614,7 +1728,42 @@ static SolveCounts capture_solve_into(Prob& P, double tol, int maxiter, bool cg,
   P.stream = P.cap[1];
   CK(cudaStreamBeginCaptureToGraph(P.cap[1], body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   depth = 2;
-  if (mixed) {
+  // an if node inside the body whose graph `rec` records (on P.cap[2]); h is set by `cond`
+  auto if_node = [&](auto cond, auto rec) {
+    cudaGraph_t gb;
+    CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, gb, 0, cudaGraphCondAssignDefault));
+    cond(h);
+    CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = h;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    CK(cudaGraphAddNode(&inode, gb, deps, nd, &ip));
+    CK(cudaStreamUpdateCaptureDependencies(P.cap[1], &inode, 1, cudaStreamSetCaptureDependencies));
+    P.stream = P.cap[2];
+    CK(cudaStreamBeginCaptureToGraph(P.cap[2], ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    depth = 3;
+    rec();
+    CK(cudaStreamEndCapture(P.cap[2], nullptr));
+    depth = 2;
+    P.stream = P.cap[1];
+  };
+  const bool xr = mixed && xr_usable(P);
+  if (xr) {
+    pcgmx_l1x(P, false);
+    n2 = P.nlaunch;
+    if_node([&](cudaGraphConditionalHandle h) {
+      launch(P, k_cond_replace_xr, 1, 1, 0, h, (const PcgState*)P.st, REPLACE_DROP);
+    }, [&]() { pcgmx_replace_xr(P); });
+    n3 = P.nlaunch;
+    if_node([&](cudaGraphConditionalHandle h) { launch(P, k_cond_rest, 1, 1, 0, h, (const PcgState*)P.st); },
+            [&]() { pcgmx_rest_xr(P); });
+  } else if (mixed) {
     pcgmx_body(P);
     cudaGraph_t gb;
     CK(cudaStreamGetCaptureInfo(P.cap[1], &cs, nullptr, &gb, &deps, &nd));
@@ -1651,6 +1800,7 @@ static SolveCounts capture_solve_into(Prob& P, double tol, int maxiter, bool cg,
   P.stream = P.cap[0];
   n4e = P.nlaunch;
   if (cg) cg_epilogue(P);
+  if (xr) pcgmx_pending_x(P);
   if (mixed) pcgmx_fold(P);
   const long long n5 = P.nlaunch;
   SolveCounts c;
@@ -2071,6 +2221,7 @@ int edge_problem_create(int dim, const int* nel, const double* K0, int precision
     P.p = P.alloc<double>(nv);  // sized for FP64; the mixed path uses the first half as FP32
     P.q = P.alloc<double>(nv);
     P.r32 = P.alloc<float>(nv);
+    P.r32b = P.alloc<float>(nv);
     P.x32 = P.alloc<float>(nv);
     P.rho_f = P.alloc<double>(P.n_el);
     P.gsens = P.alloc<double>(P.n_el);
@@ -2176,6 +2327,13 @@ int edge_set_fuse(edge_problem* p, int enable) {
   API_BEGIN
   if (!p) fail(EDGE_EINVAL, "null handle");
   p->P.fuse = enable != 0;
+  API_END
+}
+
+int edge_set_fuse_xr(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.fuse_xr = enable != 0;
   API_END
 }
 

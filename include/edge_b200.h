@@ -118,6 +118,14 @@ int edge_mg_set_omega_carry(edge_problem* p, int enable);
  * PCG search direction p = z + beta p is formed inside the product q = A p; 0 runs the same
  * arithmetic as separate launches.  No counterpart in the reference. */
 int edge_set_fuse(edge_problem* p, int enable);
+/* With the fused launches and a fixed smoother weight (omega == min_omega): 1 folds the PCG's
+ * x/r update into the next iteration's launches - the residual update r = r - alpha q into
+ * the first fine launch (which writes it into the other buffer of a ping-pong pair with r.r)
+ * and the solution update x += alpha p into the search direction's product; 0 (default) keeps
+ * the separate update launch (at 12.8M DOF it is faster: the two fused launches grow by more
+ * than the update launch costs).  Same arithmetic either way (r.r summed in another order).
+ * No counterpart in the reference. */
+int edge_set_fuse_xr(edge_problem* p, int enable);
 /* Mixed precision, 3-D: the V-cycle from `level` down to the coarsest solve (smoothing
  * sweeps, residuals, transfers, the dense coarsest solve) as one persistent cooperative
  * launch with bounded grid barriers between its stages, instead of one launch per step;

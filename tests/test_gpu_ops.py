@@ -450,6 +450,54 @@ def test_fused_fine_launches_agree():
     assert ih == i_f and rel(xh, xf) < 1e-12
 
 
+def test_fused_xr_update_agrees():
+    """Mixed precision, fixed smoother weight: the PCG's x/r update folded into the next
+    iteration's first fine launch (residual, written into a ping-pong pair, with r.r) and
+    search-direction launch (solution) against the separate update launch: the same
+    arithmetic except the order of the r.r sum, so iteration counts within 1 and solutions
+    within the tolerance of the FP64 solve; the graph solve and the host-driven loop are the
+    same launches (identical iterates); warm-started solves (a pending update from the
+    previous solve must not leak into the next) agree as well."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    p = topopt.cantilever_problem(32, 16, 16, vf=0.3, mg_kwargs=dict(tol=1e-8, n_level=3, maxiter=500,
+                                                                       variant="gpu"))
+    rng = np.random.default_rng(17)
+    E = np.clip(rng.uniform(0.05, 1.0, p.grid.n_el) ** 3, 1e-9, 1)
+    mesh = _mesh(3, (32, 16, 16), None)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    k.add_constraints(np.asarray(p.cons))
+    k.set_rho(torch.as_tensor(E, device="cuda"))
+    f = torch.as_tensor(p.f, device="cuda")
+    s64 = eb.CuMultiGrid(mesh, k, tol=1e-11, n_level=3, maxiter=2000, precision="fp64", autotune=False)
+    x64 = s64.solve(f, use_last=False)[0].cpu().numpy().copy()
+    out = {}
+    for xr, graph in ((0, True), (1, True), (1, False)):
+        s = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=3, maxiter=500, precision="mixed", autotune=False,
+                           tune_sweeps=False, graph=graph, mixed_omega="max")
+        s._configure()
+        _lib.call("edge_set_fine_tile", k.handle, 10, 8)
+        _lib.call("edge_mg_set_sweeps", k.handle, _lib.int_array([1, 1, 1]), 3)
+        _lib.call("edge_set_fuse_xr", k.handle, xr)
+        x, r = s.solve(f, use_last=False)
+        it0 = s.last_iters
+        x0 = x.cpu().numpy().copy()
+        # a second solve warm-started from a perturbed solution
+        s.last_x0 = x * (1.0 + 1e-3 * torch.cos(torch.arange(x.numel(), device="cuda", dtype=torch.float64)))
+        x2, r2 = s.solve(f, use_last=True)
+        out[(xr, graph)] = (x0, it0, r, x2.cpu().numpy().copy(), s.last_iters, r2)
+    _lib.call("edge_set_fuse_xr", k.handle, 1)
+    a, b, c = out[(0, True)], out[(1, True)], out[(1, False)]
+    print("iterations separate / fused / fused host loop", a[1], b[1], c[1], "warm", a[4], b[4], c[4])
+    for o in (a, b, c):
+        assert o[2] < 1e-8 and o[5] < 1e-8
+        assert rel(o[0], x64) < 1e-6 and rel(o[3], x64) < 1e-6
+    assert abs(a[1] - b[1]) <= 1 and abs(a[4] - b[4]) <= 1 and b[1] > 3
+    assert c[1] == b[1] and c[4] == b[4]
+    assert rel(c[0], b[0]) < 1e-12 and rel(c[3], b[3]) < 1e-12
+
+
 @pytest.mark.parametrize("sweeps", [(1, 1, 1, 1), (1, 2, 3, 1)])
 def test_persistent_vcycle_tail_agrees(sweeps):
     """Mixed precision: the V-cycle below level 1 as one persistent cooperative launch
