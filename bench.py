@@ -211,6 +211,19 @@ def _max_over_ranks(v, ws):
     return float(tt.item())
 
 
+def _gather_over_ranks(v, ws):
+    """The list of every rank's value v (rank order); [v] on one rank."""
+    if ws == 1:
+        return [v]
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    mine = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    out = [torch.zeros_like(mine) for _ in range(ws)]
+    dist.all_gather(out, mine)
+    return [float(t.item()) for t in out]
+
+
 def whole_job_rate(units_per_rank, ws, t_max_ms):
     """Units processed by all ranks per second, over the slowest rank's time: every rank does
     the same amount of work (replicas or equal shards), so the job ends with the slowest."""
@@ -697,6 +710,11 @@ def run_batch(args):
     ms = _max_over_ranks(ms, ws)
     pcg = [int(np.mean(it["pcg"][-args.steps:])) for it in b.items]
     dofs = [2 * (sp["nelx"] + 1) * (sp["nely"] + 1) for sp in specs]
+    # every rank solves its own seeded problems: their sizes and PCG work differ, so the line
+    # records each rank's DOF total and DOF x PCG-iteration work beside the slowest rank's time
+    work = float(sum(d * p for d, p in zip(dofs, pcg)))
+    dof_per_rank = _gather_over_ranks(float(sum(dofs)), ws)
+    work_per_rank = _gather_over_ranks(work, ws)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -711,6 +729,8 @@ def run_batch(args):
             "config": {"workload": f"batch{n}_2d", "problems": n * ws, "problems_per_gpu": n,
                        "parallelism": f"independent problems x{ws}" if ws > 1 else "1 GPU",
                        "dof_total_rank0": int(np.sum(dofs)),
+                       "dof_total_per_rank": [int(v) for v in dof_per_rank],
+                       "dof_x_pcg_iters_per_step_per_rank": [int(v) for v in work_per_rank],
                        "elements_total_rank0": int(sum(sp["nelx"] * sp["nely"] for sp in specs)),
                        "rtol": 1e-6, "precision": args.precision, "mode": args.batch_mode,
                        "threads_streams": b.n_threads, "max_level": max_level,
