@@ -102,6 +102,52 @@ __global__ void k_elem_user_to_slots(const Geo g, const double* __restrict__ use
   v[s] = Conv<TO>::from(val);
 }
 
+// A real grid embedded in the lower corner of a larger (padded) grid g: gr holds the real
+// grid's node counts.  The user arrays are the real grid's (its own numbering); slots of g
+// outside the real grid read zero and are not written back.
+EDGE_D bool real_node_of_slot(const Geo& g, const Geo& gr, long long s, int& i, int& j, int& k, long long& node) {
+  long long np;
+  if (!node_of_slot(g, s, i, j, k, np)) return false;
+  if (i >= gr.nx || j >= gr.ny || (g.dim == 3 && k >= gr.nz)) return false;
+  node = g.dim == 3 ? ((long long)j * gr.nx + i) * gr.nz + k : (long long)j * gr.nx + i;
+  return true;
+}
+template <typename TO>
+__global__ void k_user_to_slots_emb(const Geo g, const Geo gr, const double* __restrict__ user, TO* __restrict__ v) {
+  EDGE_PDL_ENTRY();
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  const bool ok = real_node_of_slot(g, gr, s, i, j, k, node);
+  for (int c = 0; c < g.dof; ++c) v[c * g.n + s] = Conv<TO>::from(ok ? user[node * g.dof + c] : 0.0);
+}
+template <typename TI>
+__global__ void k_slots_to_user_emb(const Geo g, const Geo gr, const TI* __restrict__ v, double* __restrict__ user) {
+  EDGE_PDL_ENTRY();
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  if (!real_node_of_slot(g, gr, s, i, j, k, node)) return;
+  for (int c = 0; c < g.dof; ++c) user[node * g.dof + c] = (double)Conv<double>::from(v[c * g.n + s]);
+}
+// Element array of the real grid (the reference's element order) into g's slots; padding
+// elements (and slots without an element) get zero.
+template <typename TO>
+__global__ void k_elem_user_to_slots_emb(const Geo g, const Geo gr, const double* __restrict__ user,
+                                         TO* __restrict__ v) {
+  EDGE_PDL_ENTRY();
+  const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (s >= g.n) return;
+  int i, j, k;
+  long long node;
+  double val = 0.0;
+  if (node_of_slot(g, s, i, j, k, node) && i < gr.nx - 1 && j < gr.ny - 1 && (g.dim == 2 || k < gr.nz - 1))
+    val = user[user_elem(gr, i, j, k)];
+  v[s] = Conv<TO>::from(val);
+}
+
 // ------------------------------------------------------------------ density filter
 // Cone filter (geom/_filters.py:72-161, core/_filter.py:78-124): taps o_k with global
 // weights w_k; (H rho)_e = sum_k w_k rho_{e+o_k} / sum_{in-bounds k} w_k.

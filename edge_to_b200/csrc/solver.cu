@@ -2540,6 +2540,51 @@ int edge_set_rho(edge_problem* p, const double* E_dev) {
   API_END
 }
 
+// The real grid of nel_real elements per axis inside the problem's (padded) grid.
+static Geo real_geo(const Prob& P, const int* nel_real) {
+  for (int d = 0; d < P.dim; ++d)
+    if (nel_real[d] < 1 || nel_real[d] > P.nel[d]) fail(EDGE_EINVAL, "real extents outside the problem's grid");
+  Geo gr = P.g0;
+  gr.nx = nel_real[0] + 1;
+  gr.ny = nel_real[1] + 1;
+  if (P.dim == 3) gr.nz = nel_real[2] + 1;
+  return gr;
+}
+
+int edge_set_rho_embedded(edge_problem* p, const double* E_dev, const int* nel_real) {
+  API_BEGIN
+  if (!p || !E_dev || !nel_real) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  const Geo gr = real_geo(P, nel_real);
+  launch(P, k_elem_user_to_slots_emb<double>, cdiv(P.g0.n, 256), 256, 0, P.g0, gr, E_dev, P.E64);
+  if (P.E32) launch(P, k_elem_user_to_slots_emb<float>, cdiv(P.g0.n, 256), 256, 0, P.g0, gr, E_dev, P.E32);
+  KCHECK();
+  P.has_rho = true;
+  API_END
+}
+
+int edge_mg_solve_embedded(edge_problem* p, const int* nel_real, const double* f_dev, double* x_dev, int use_last,
+                           double tol, int maxiter, double* residual_out, int* iters_out) {
+  API_BEGIN
+  if (!p || !nel_real || !f_dev || !x_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  const Geo& g = P.g0;
+  const Geo gr = real_geo(P, nel_real);
+  launch(P, k_user_to_slots_emb<double>, cdiv(g.n, 256), 256, 0, g, gr, f_dev, P.b64);
+  if (use_last)
+    launch(P, k_user_to_slots_emb<double>, cdiv(g.n, 256), 256, 0, g, gr, (const double*)x_dev, P.x64);
+  else
+    CK(cudaMemsetAsync(P.x64, 0, (size_t)g.dof * g.n * sizeof(double), P.stream));
+  KCHECK();
+  solve_internal(P, tol, maxiter);
+  launch(P, k_slots_to_user_emb<double>, cdiv(g.n, 256), 256, 0, g, gr, P.x64, x_dev);
+  KCHECK();
+  CK(cudaStreamSynchronize(P.stream));
+  if (residual_out) *residual_out = P.st_h->res;
+  if (iters_out) *iters_out = P.st_h->iter;
+  API_END
+}
+
 int edge_matvec(edge_problem* p, const double* u_dev, double* out_dev) {
   API_BEGIN
   if (!p || !u_dev || !out_dev) fail(EDGE_EINVAL, "null argument");

@@ -80,10 +80,23 @@ class _PaddedGrid:
 
     def sync(self, kernel):
         """Copy the real kernel's density, constraints and springs onto the padded kernel."""
+        self.set_rho(kernel)
+        self.sync_bcs(kernel)
+
+    def set_rho(self, kernel):
+        """The real kernel's density onto the padded grid (padding elements zero), on the device
+        (edge_set_rho_embedded)."""
         kp = self.kernel
-        E = torch.zeros(kp.n_elements, dtype=torch.float64, device="cuda")
-        E[self.el_map] = _as_dev_f64(kernel.rho).reshape(-1)
-        kp.set_rho(E)
+        rho = _as_dev_f64(kernel.rho).reshape(-1).contiguous()
+        kp._bind_stream()
+        _lib.call("edge_set_rho_embedded", kp.handle, _lib.ptr(rho), _lib.int_array(self.nel))
+        kp.rho = None  # the padded grid's E lives in the library only
+        kp.has_rho = True
+
+    def sync_bcs(self, kernel):
+        """The real kernel's constraints (every padding-only node constrained as well) and springs
+        onto the padded kernel, when they changed."""
+        kp = self.kernel
         key = (kernel.constraints.data_ptr(), int(kernel.constraints.sum().item()), kernel.has_con)
         if key != self._cons_key:
             c = torch.zeros(kp.shape[0], dtype=torch.bool, device="cuda")
@@ -361,14 +374,50 @@ class CuMultiGrid(Solver):
         """True when this solver works on a padded copy of the grid (odd extents)."""
         return self._pad is not None
 
+    def _run_solve(self, f, x, warm):
+        """One solve of K x = f (x: the warm start when warm, overwritten with the solution), on
+        this solver's problem or, when padded, on the padded problem through the embedding
+        (edge_mg_solve_embedded: the load, warm start and solution stay in the real grid's
+        layout); a fixed smoother weight that does not converge is retried on the schedule.
+        Returns (residual, iterations)."""
+        res, its = ctypes.c_double(), ctypes.c_int()
+        target = self._inner if self._pad is not None else self
+        target.kernel._bind_stream()
+        keep = target.keep_start(x) if warm else None
+
+        def go():
+            if self._pad is not None:
+                _lib.call("edge_mg_solve_embedded", target.kernel.handle, _lib.int_array(self._pad.nel), _lib.ptr(f),
+                          _lib.ptr(x), warm, float(self.tol), int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
+            else:
+                _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
+                          int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
+
+        go()
+        if not res.value < self.tol and self.use_omega_schedule():
+            # the fixed smoother weight did not converge: the same solve with the schedule
+            if keep is not None:
+                x.copy_(keep)
+            go()
+        return res.value, its.value
+
     def _solve_padded(self, rhs, use_last):
-        inner = self._inner
+        inner, pad = self._inner, self._pad
         inner.tol, inner.maxiter = self.tol, self.maxiter
-        self._pad.sync(self.kernel)
-        xp, res = inner.solve(self._pad.embed(rhs), use_last=use_last)
-        x = self._pad.extract(xp)
+        pad.sync_bcs(self.kernel)
+        pad.set_rho(self.kernel)
+        inner._configure()
+        inner.tune()
+        f = _as_dev_f64(rhs)
+        warm = 1 if (use_last and self.last_x0 is not None) else 0
+        if warm and inner.sweeps is None and inner.tune_sweeps:
+            # the sweep autotuner times whole solves on the padded grid (once)
+            inner.tune_sweep_counts(pad.embed(f), pad.embed(self.last_x0))
+        self._omega_mode, self._omega_failed = inner._omega_mode, inner._omega_failed  # the tuner's choice
+        x = self.last_x0 if warm else torch.zeros_like(f)
+        res, its = self._run_solve(f, x, warm)
         self.last_x0 = x
-        self.last_iters = inner.last_iters
+        self.last_iters = inner.last_iters = its
         self.tuned, self.sweeps = inner.tuned, inner.sweeps
         return x, res
 
@@ -390,21 +439,10 @@ class CuMultiGrid(Solver):
         else:
             x = torch.zeros_like(f)
             warm = 0
-        res = ctypes.c_double()
-        its = ctypes.c_int()
-        self.kernel._bind_stream()
-        keep = self.keep_start(x) if warm else None
-        _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
-                  int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
-        if not res.value < self.tol and self.use_omega_schedule():
-            # the fixed smoother weight did not converge: the same solve with the schedule
-            if keep is not None:
-                x.copy_(keep)
-            _lib.call("edge_mg_solve", self.kernel.handle, _lib.ptr(f), _lib.ptr(x), warm, float(self.tol),
-                      int(self.maxiter), ctypes.byref(res), ctypes.byref(its))
+        res, its = self._run_solve(f, x, warm)
         self.last_x0 = x
-        self.last_iters = its.value
-        return x, res.value
+        self.last_iters = its
+        return x, res
 
     def stats(self):
         if self._inner is not None:

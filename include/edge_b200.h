@@ -184,6 +184,16 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
 int edge_mg_solve(edge_problem* p, const double* f_dev, double* x_dev, int use_last, double tol, int maxiter,
                   double* residual_out, int* iters_out);
 
+/* A real grid of nel_real elements per axis embedded in the lower corner of the problem's
+ * grid (a padded grid whose padding elements have no stiffness and whose padding nodes are
+ * constrained): E_dev in the real grid's element order sets E (zero on the padding), and
+ * the solve takes f_dev / x_dev in the real grid's user layout (the padding's load is zero, its
+ * solution is not returned).  The multigrid of a grid whose extents do not divide by
+ * 2^n_level runs on such a padded problem (CuMultiGrid's padded path). */
+int edge_set_rho_embedded(edge_problem* p, const double* E_dev, const int* nel_real);
+int edge_mg_solve_embedded(edge_problem* p, const int* nel_real, const double* f_dev, double* x_dev, int use_last,
+                           double tol, int maxiter, double* residual_out, int* iters_out);
+
 /* Builds the hierarchy for the current E / BCs without solving (CuMultiGrid._setup,
  * solvers/_multigrid_cuda.py:64-118), and returns level l (1..n_level) as a dense
  * row-major n x n FP64 matrix in the reference's coarse DOF order (test inspection). */
