@@ -1044,4 +1044,69 @@ __global__ void k_mm_law(long long n_el, int n_mat, const double* __restrict__ r
   }
 }
 
+// OC update of an n_el x ns design with one bisection multiplier per column (the multi-material
+// update of TopOpt/_cuda.py:242-280 with PenalizedMultiMaterial's ocP and constraint,
+// MaterialModels.py:204-225): every column is bisected while any column's gap
+// (l2 - l1) / (l2 + l1) exceeds 1e-4 (np.any); column m is feasible when
+// sum_e rho_new[e, m] A_e / vol - mass[m] <= 0, or, with a shared mass (rho_mat given), every
+// column is when sum_e sum_m rho_new[e, m] A_e rho_mat[m] / vol <= mass[0].  rho_new is the
+// design at the last multipliers tried.  One block: sums in a fixed order, the bisection
+// state held alike by every thread, at most 200 steps.
+struct MmOcCon {
+  int ns, shared;
+  double mass[MM_MAX], rm[MM_MAX];
+};
+__global__ void __launch_bounds__(1024) k_oc_multi(long long n, MmOcCon cn, const double* __restrict__ rho,
+                                                   const double* __restrict__ ocp, const double* __restrict__ A,
+                                                   int a_per_el, double move, double vol,
+                                                   double* __restrict__ rho_new, int* steps_out) {
+  EDGE_PDL_ENTRY();
+  __shared__ double sh[33];
+  const int ns = cn.ns;
+  double l1[MM_MAX], l2[MM_MAX], lm[MM_MAX];
+  for (int m = 0; m < ns; ++m) {
+    l1[m] = 1e-9;
+    l2[m] = 1e9;
+    lm[m] = 0.5 * (l1[m] + l2[m]);
+  }
+  int steps = 0;
+  for (; steps < 200; ++steps) {
+    bool open = false;
+    for (int m = 0; m < ns; ++m) open = open || ((l2[m] - l1[m]) / (l2[m] + l1[m]) > 1e-4);
+    if (!open) break;
+    for (int m = 0; m < ns; ++m) lm[m] = 0.5 * (l1[m] + l2[m]);
+    double acc[MM_MAX];
+    for (int m = 0; m < ns; ++m) acc[m] = 0.0;
+    for (long long e = threadIdx.x; e < n; e += blockDim.x) {
+      const double a = A[a_per_el ? e : 0];
+      for (int m = 0; m < ns; ++m) acc[m] += oc_rho(rho[e * ns + m], ocp[e * ns + m], lm[m], move) * a;
+    }
+    double V[MM_MAX];
+    for (int m = 0; m < ns; ++m) {
+      const double t = block_sum(acc[m], sh);
+      __syncthreads();
+      if (threadIdx.x == 0) sh[32] = t;
+      __syncthreads();
+      V[m] = sh[32];
+      __syncthreads();
+    }
+    bool valid[MM_MAX];
+    if (cn.shared) {
+      double tot = 0.0;
+      for (int m = 0; m < ns; ++m) tot += V[m] * cn.rm[m];
+      const bool ok = tot / vol <= cn.mass[0];
+      for (int m = 0; m < ns; ++m) valid[m] = ok;
+    } else {
+      for (int m = 0; m < ns; ++m) valid[m] = (V[m] / vol - cn.mass[m]) <= 0.0;
+    }
+    for (int m = 0; m < ns; ++m) {
+      if (valid[m]) l2[m] = lm[m];
+      else l1[m] = lm[m];
+    }
+  }
+  for (long long e = threadIdx.x; e < n; e += blockDim.x)
+    for (int m = 0; m < ns; ++m) rho_new[e * ns + m] = oc_rho(rho[e * ns + m], ocp[e * ns + m], lm[m], move);
+  if (steps_out && threadIdx.x == 0) *steps_out = steps;
+}
+
 }  // namespace edge

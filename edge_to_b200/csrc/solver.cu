@@ -2993,6 +2993,27 @@ int edge_mm_law(long long n_el, int n_mat, const double* rho_dev, const double* 
   API_END
 }
 
+int edge_oc_update_multi(long long n_el, int n_sets, const double* rho_dev, const double* ocp_dev, const double* A_dev,
+                         int A_per_element, double move, double vol, const double* mass, const double* rho_mat,
+                         double* rho_new_dev, void* stream) {
+  API_BEGIN
+  if (!rho_dev || !ocp_dev || !A_dev || !mass || !rho_new_dev) fail(EDGE_EINVAL, "null argument");
+  if (n_el < 1 || n_sets < 1 || n_sets > MM_MAX)
+    fail(EDGE_EINVAL, "n_sets must be in 1.." + std::to_string(MM_MAX) + " and n_el >= 1");
+  if (!(vol > 0.0)) fail(EDGE_EINVAL, "vol must be positive");
+  MmOcCon cn{};
+  cn.ns = n_sets;
+  cn.shared = rho_mat ? 1 : 0;
+  for (int m = 0; m < n_sets; ++m) {
+    cn.mass[m] = rho_mat ? mass[0] : mass[m];
+    cn.rm[m] = rho_mat ? rho_mat[m] : 0.0;
+  }
+  k_oc_multi<<<1, 1024, 0, (cudaStream_t)stream>>>(n_el, cn, rho_dev, ocp_dev, A_dev, A_per_element ? 1 : 0, move,
+                                                   vol, rho_new_dev, nullptr);
+  KCHECK();
+  API_END
+}
+
 int edge_restrict(int dim, const int* nel, const double* in_dev, double* out_dev, void* stream) {
   API_BEGIN
   if (!nel || !in_dev || !out_dev) fail(EDGE_EINVAL, "null argument");

@@ -23,7 +23,7 @@ from tqdm.auto import trange
 from . import _lib
 from .filters import _CuStructuredFilter
 from .kernels import CuStructuredStiffnessKernel, _as_dev_f64
-from .material import SingleMaterial
+from .material import PenalizedMultiMaterial, SingleMaterial
 from .solvers import CuMultiGrid
 
 logger = logging.getLogger(__name__)
@@ -149,11 +149,35 @@ class CuTopOpt:
         size = self.n_sets
         rho = rho.reshape(-1, size)
         df = df.reshape(-1, size)
-        xU = torch.clamp(rho + self.move, 0.0, 1.0)
-        xL = torch.clamp(rho - self.move, 0.0, 1.0)
         As = torch.as_tensor(np.asarray(self.mesh.As), dtype=torch.float64, device="cuda")
         ocP = self.material_model.ocP(df, As, rho)
         ocP = torch.clamp(ocP, min=1e-12)
+        mm = self.material_model
+        if isinstance(mm, PenalizedMultiMaterial) and 1 <= size <= 8:
+            # the bisection as one launch (edge_oc_update_multi): no host read per step
+            rho_c = rho.contiguous()
+            ocp_c = ocP.reshape(-1, size).contiguous()
+            A = As.reshape(-1).contiguous()
+            out = torch.empty_like(rho_c)
+            if mm.rho_mat is None:
+                mass = _lib.double_array(np.asarray(mm.mass, dtype=np.float64).reshape(-1)[:size].tolist())
+                rm = None
+            else:
+                mass = _lib.double_array([float(mm.mass)])
+                rm = _lib.double_array(np.asarray(mm.rho_mat, dtype=np.float64).reshape(-1).tolist())
+            _lib.call("edge_oc_update_multi", rho_c.shape[0], size, _lib.ptr(rho_c), _lib.ptr(ocp_c), _lib.ptr(A),
+                      1 if A.numel() == rho_c.shape[0] else 0, float(self.move), float(self.mesh.volume), mass, rm,
+                      _lib.ptr(out), _lib.stream_ptr())
+            return out.reshape(-1) if size == 1 else out
+        return self._bisect_torch(rho, ocP, As)
+
+    def _bisect_torch(self, rho, ocP, As):
+        """The bisection of _update_design_generic in torch operations, for material models other
+        than PenalizedMultiMaterial (their constraint test is theirs to define); one host read
+        per step, as the reference's loop."""
+        size = self.n_sets
+        xU = torch.clamp(rho + self.move, 0.0, 1.0)
+        xL = torch.clamp(rho - self.move, 0.0, 1.0)
         l1 = 1e-9 * torch.ones(size, dtype=torch.float64, device="cuda")
         l2 = 1e9 * torch.ones(size, dtype=torch.float64, device="cuda")
         lmid = 0.5 * (l1 + l2)

@@ -200,6 +200,18 @@ int edge_mg_solve_embedded(edge_problem* p, const int* nel_real, const double* f
 int edge_mg_setup(edge_problem* p);
 int edge_mg_level_dense(edge_problem* p, int level, double* out_dev, long long n);
 
+/* ---- multi-material OC update.  Replaces the bisection of TopOpt.update_design
+ * (TopOpt/_cuda.py:242-280) for PenalizedMultiMaterial (constraint MaterialModels.py:204-215):
+ * rho_dev and ocp_dev (the material's ocP, clipped to >= 1e-12) are n_el x n_sets row-major,
+ * A_dev the element areas (n_el values, or one value when A_per_element == 0); every column's
+ * multiplier is bisected while any column's gap exceeds 1e-4.  mass: n_sets per-column mass
+ * fractions, or with rho_mat (n_sets densities, may be NULL) the one shared mass fraction
+ * mass[0] of sum_e sum_m rho[e, m] A_e rho_mat[m].  rho_new_dev receives the design at the last
+ * multipliers.  One launch on stream, no host synchronisation; 1 <= n_sets <= 8. */
+int edge_oc_update_multi(long long n_el, int n_sets, const double* rho_dev, const double* ocp_dev, const double* A_dev,
+                         int A_per_element, double move, double vol, const double* mass, const double* rho_mat,
+                         double* rho_new_dev, void* stream);
+
 /* ---- multi-material SIMP law.  Replaces PenalizedMultiMaterial.__forward__ / __backward__
  * (MaterialModels.py:146-205): rho_dev is the n_el x n_mat row-major design (filtered),
  * E_mat the n_mat Young's moduli (host array), 1 <= n_mat <= 8.  E_dev (n_el) receives

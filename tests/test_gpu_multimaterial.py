@@ -112,3 +112,37 @@ def test_multimaterial_simp_against_oracle(shared):
         assert (r @ np.array([1.0, 0.35])).mean() <= 0.3 * (1 + 1e-4)
     else:
         assert (r.mean(axis=0) <= np.array([0.25, 0.15]) * (1 + 1e-4)).all()
+
+
+@pytest.mark.parametrize("n_mat,shared", [(2, False), (3, False), (2, True), (3, True)])
+def test_multimaterial_oc_launch_equals_torch_bisection(n_mat, shared):
+    """The multi-material OC update as one launch (edge_oc_update_multi) gives the designs of the
+    bisection written in torch operations (one host read per step, the reference's loop) on
+    random designs and sensitivities, per-material and shared mass constraints; the bisection's
+    decisions only depend on sums that the two compute in different orders."""
+    import torch
+    import edge_to_b200 as eb
+    nelx, nely = 40, 24
+    mesh = eb.CuStructuredMesh2D(nelx, nely, float(nelx), float(nely), stiffness=lambda x: eb.auto_stiffness(x, 1.0, 0.3))
+    E_mat = np.linspace(1.0, 0.3, n_mat).reshape(-1, 1)
+    if shared:
+        mat = eb.PenalizedMultiMaterial(n_material=n_mat, mass=np.array([[0.3]]), E_mat=E_mat,
+                                        rho_mat=np.linspace(1.0, 0.4, n_mat).reshape(-1, 1), void=1e-9)
+    else:
+        mat = eb.PenalizedMultiMaterial(n_material=n_mat, mass=np.full((n_mat, 1), 0.6 / n_mat), E_mat=E_mat,
+                                        void=1e-9)
+    k = eb.CuStructuredStiffnessKernel(mesh)
+    filt = eb.CuStructuredFilter2D(mesh, 1.5)
+    solver = eb.CuMultiGrid(mesh, k, tol=1e-8, n_level=2, maxiter=500, precision="fp64")
+    opt = eb.CuTopOpt(mesh, mat, k, solver, filt, max_iter=1, move=0.2, verbose=False)
+    g = torch.Generator(device="cuda").manual_seed(5 + n_mat)
+    n = nelx * nely
+    for trial in range(3):
+        rho = 0.05 + 0.9 * torch.rand(n, n_mat, generator=g, device="cuda", dtype=torch.float64)
+        df = -torch.rand(n, n_mat, generator=g, device="cuda", dtype=torch.float64) * (10.0 ** trial)
+        fast = opt.update_design(rho, df)
+        As = torch.as_tensor(np.asarray(mesh.As), dtype=torch.float64, device="cuda")
+        ocP = torch.clamp(mat.ocP(df, As, rho), min=1e-12)
+        ref = opt._bisect_torch(rho, ocP, As)
+        assert tuple(fast.shape) == (n, n_mat)
+        assert float((fast - ref).abs().max()) < 1e-12, trial
