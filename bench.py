@@ -291,6 +291,9 @@ def run_ours(args, cfg_name):
     if args.fuse_xr:
         from edge_to_b200 import _lib as _l
         _l.call("edge_set_fuse_xr", opt.kernel.handle, 1)
+    if args.no_kind_tune:
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_kind_tune", opt.kernel.handle, 0)
     traj = []
     rho, dr, it = warm(opt, rho, args.warmup, traj)
     # the state the timed steps start from; the end-to-end steps restart from it, so both
@@ -779,6 +782,9 @@ def main():
                     help="skip the FP64 trajectory at rtol 1e-10 the timed paths are compared with")
     ap.add_argument("--no-fuse", action="store_true",
                     help="mixed path: the fine level's sweeps and search direction as separate launches")
+    ap.add_argument("--no-kind-tune", action="store_true",
+                    help="mixed path: one fine tile for the three fused launch kinds (default: the autotuner may "
+                         "give each kind its own)")
     ap.add_argument("--fuse-xr", action="store_true",
                     help="mixed path: the PCG's x/r update folded into the next iteration's fine launches when "
                          "the smoother weight is fixed (default: its own launch, faster at 12.8M DOF)")

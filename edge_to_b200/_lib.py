@@ -51,6 +51,8 @@ _SIGS = {
     "edge_set_fuse": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_fuse_xr": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_rho_embedded": (ctypes.c_int, [vp, vp, c_int_p]),
+    "edge_fine_kind_tiles": (ctypes.c_int, [vp, c_int_p, c_int_p]),
+    "edge_set_kind_tune": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_oc_update_multi": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, vp, vp, vp, ctypes.c_int,
                                             ctypes.c_double, ctypes.c_double, c_double_p, c_double_p, vp, vp]),
     "edge_mg_solve_embedded": (ctypes.c_int, [vp, c_int_p, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,

@@ -224,6 +224,12 @@ struct Prob {
   KCube kcube;             // block form of the same operator (cube elements)
   bool cube = false;       // kcube reproduces every entry of the transformed operator
   int blocks_per_sm = 4;   // y-chunking target of the fine kernel
+  // per kind of fused cube launch (0: first sweep + residual, 1: last sweep + correction,
+  // 2: search direction + product), the tile variant and y-chunking target chosen for that
+  // launch alone; -1: tile_variant / blocks_per_sm
+  int kind_variant[3] = {-1, -1, -1};
+  int kind_bps[3] = {0, 0, 0};
+  bool kind_tune = true;  // edge_autotune_fine also picks the per-kind tiles
   long long st_quad_max = 40000;   // 3-D stencil levels with at most this many slots use k_st3_apply_q
   bool st_bf16 = true;             // mixed precision: apply the coarse stencils from BF16 copies
   // mixed precision: the residual recurrence between FP64 replacements is stored in FP32
@@ -794,13 +800,36 @@ static bool cube_fusable(const Prob& P) {
 
 // A cube-kernel launch with an input transform, on the problem's tile variant; profiled like
 // fine_apply with io_bytes algorithmic bytes per DOF besides E.
+// Kind of a fused cube launch for the per-kind tile choice (Prob::kind_variant), -1 for others.
+template <class SE, class IN> constexpr int cube_kind() {
+  if constexpr (std::is_same<SE, SEResidIn>::value && std::is_same<IN, InWDB>::value) return 0;
+  else if constexpr (std::is_same<SE, SEJacobiAdd0<true>>::value || std::is_same<SE, SEJacobiAdd0<false>>::value)
+    return 1;
+  else if constexpr (std::is_same<SE, SEStorePDot>::value) return 2;
+  else return -1;
+}
+
 template <class SE, class IN>
 static void fine3_cube_fused(Prob& P, const float* in0, const void* in1, const void* in1b, IN in, SE epi,
                              const void* const* arr, double* dot_dst, double io_bytes, const CubeExtra& xa = {}) {
   CatScope cat(P, CAT_FINE);
   const bool rec = P.prof && P.pev_used + 2 <= P.pev.size();
   if (rec) CK(cudaEventRecord(P.pev[P.pev_used], P.stream));
-  switch (P.tile_variant) {
+  constexpr int kind = cube_kind<SE, IN>();
+  int variant = P.tile_variant;
+  const int bps0 = P.blocks_per_sm;
+  if constexpr (kind >= 0) {
+    if (P.kind_variant[kind] >= 9) {
+      variant = P.kind_variant[kind];
+      P.blocks_per_sm = P.kind_bps[kind];
+    }
+  }
+  struct Restore {
+    Prob& P;
+    int b;
+    ~Restore() { P.blocks_per_sm = b; }
+  } restore{P, bps0};
+  switch (variant) {
     case 9: fine3_cube_go<SE, IN, 4, 3, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
     case 10: fine3_cube_go<SE, IN, 4, 4, 2>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
     case 11: fine3_cube_go<SE, IN, 2, 3, 4>(P, in0, in1, in1b, P.E32, in, epi, arr, dot_dst, xa); break;
@@ -1672,7 +1701,8 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, boo
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons,
                            (double)P.st_bf16, (double)P.st_pair, (double)P.st_pair_min, (double)P.res32,
                            (double)P.pdl, (double)P.fuse, (double)P.tail_l0, (double)P.omega_carry, (double)(P.omega_carry && P.omega_started),
-                           (double)P.fuse_xr};
+                           (double)P.fuse_xr, (double)P.kind_variant[0], (double)P.kind_variant[1],
+                           (double)P.kind_variant[2], (double)P.kind_bps[0], (double)P.kind_bps[1], (double)P.kind_bps[2]};
   for (int l : P.w_levels) k.push_back((double)l);
   k.push_back(-1.0);
   for (int v : P.level_sweeps) k.push_back((double)v);
@@ -2356,33 +2386,44 @@ int edge_uses_cube_form(const edge_problem* p) { return p && p->P.cube ? 1 : 0; 
 
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm) {
   API_BEGIN
-  if (!p || variant < 0 || variant > 14 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
+  if (!p || variant < 0 || variant > 15 || blocks_per_sm < 1 || blocks_per_sm > 64) fail(EDGE_EINVAL, "bad tile");
   p->P.tile_variant = variant;
   p->P.blocks_per_sm = blocks_per_sm;
+  for (int k = 0; k < 3; ++k) {  // one tile for every launch
+    p->P.kind_variant[k] = -1;
+    p->P.kind_bps[k] = 0;
+  }
   API_END
 }
 
 // Average device time of `reps` fine-operator launches with the current tile, the smoother
 // sweep epilogue (sweep = true; needs the multigrid allocated) or the plain product; buffer
 // contents do not matter for timing.
-static double time_fine(Prob& P, int precision, bool sweep, int reps, bool mix = false) {
+static double time_fine(Prob& P, int precision, bool sweep, int reps, bool mix = false, int only_kind = -1) {
   const Geo& g = P.g0;
   auto run = [&]() {
     if (mix && cube_fusable(P)) {
       // the same three launches fused as the solver runs them on this tile: first sweep +
-      // residual, last sweep + correction + r.z, search direction + product + p.q
+      // residual, last sweep + correction + r.z, search direction + product + p.q (or the
+      // one of kind only_kind)
       Level& L0 = P.lv[0];
-      InWDB i1{&P.st->omega, 1.0, 0.f};
-      SEResidIn e1{(float*)L0.r, g.n};
-      fine3_cube_fused(P, P.r32, L0.dinv, nullptr, i1, e1, nullptr, nullptr, 4 + 2 + 4);
-      const void* arr[3] = {L0.r, L0.dinv, P.r32};
-      SEJacobiAdd0<true> e2{(float*)L0.res, &P.st->omega, 1.0, g.n, 0.f};
-      fine3_cube_fused(P, (const float*)L0.ea, nullptr, nullptr, InU{}, e2, arr, &P.st->rz, 4 + 4 + 2 + 4 + 4);
-      const long long nv = (long long)g.dof * g.n;
-      float* p0 = (float*)P.p;
-      InPDir i3{(const PcgState*)P.st, 0.f, 0, false};
-      SEStorePDot e3{(float*)P.q, p0, p0 + nv, (const PcgState*)P.st, g.n, nullptr};
-      fine3_cube_fused(P, (const float*)L0.res, p0, p0 + nv, i3, e3, nullptr, &P.st->pq, 4 + 4 + 4 + 4);
+      if (only_kind < 0 || only_kind == 0) {
+        InWDB i1{&P.st->omega, 1.0, 0.f};
+        SEResidIn e1{(float*)L0.r, g.n};
+        fine3_cube_fused(P, P.r32, L0.dinv, nullptr, i1, e1, nullptr, nullptr, 4 + 2 + 4);
+      }
+      if (only_kind < 0 || only_kind == 1) {
+        const void* arr[3] = {L0.r, L0.dinv, P.r32};
+        SEJacobiAdd0<true> e2{(float*)L0.res, &P.st->omega, 1.0, g.n, 0.f};
+        fine3_cube_fused(P, (const float*)L0.ea, nullptr, nullptr, InU{}, e2, arr, &P.st->rz, 4 + 4 + 2 + 4 + 4);
+      }
+      if (only_kind < 0 || only_kind == 2) {
+        const long long nv = (long long)g.dof * g.n;
+        float* p0 = (float*)P.p;
+        InPDir i3{(const PcgState*)P.st, 0.f, 0, false};
+        SEStorePDot e3{(float*)P.q, p0, p0 + nv, (const PcgState*)P.st, g.n, nullptr};
+        fine3_cube_fused(P, (const float*)L0.res, p0, p0 + nv, i3, e3, nullptr, &P.st->pq, 4 + 4 + 4 + 4);
+      }
       return;
     }
     if (mix) {
@@ -2475,9 +2516,64 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
   check_err(P);
   P.tile_variant = bv;
   P.blocks_per_sm = bb;
+  for (int k = 0; k < 3; ++k) {
+    P.kind_variant[k] = -1;
+    P.kind_bps[k] = 0;
+  }
+  if (mix && P.kind_tune && cube_fusable(P)) {
+    // each fused launch kind alone: the variants of the cube kernel (their register caps and
+    // stage counts suit the three epilogues differently) at the mix's y-chunking and one
+    // either side of it; a kind keeps the mix's tile unless another is 2 % faster
+    const int cube_v[6] = {9, 10, 11, 12, 13, 15};
+    for (int k = 0; k < 3; ++k) {
+      P.kind_variant[k] = bv;
+      P.kind_bps[k] = bb;
+      const double base = time_fine(P, precision, sweep, reps, true, k);
+      double kb = base;
+      int kv = bv, kbps = bb;
+      for (int v : cube_v)
+        for (int b : {bb / 2, bb, bb * 2}) {
+          if (b < 1 || b > 64 || (v == bv && b == bb)) continue;
+          P.kind_variant[k] = v;
+          P.kind_bps[k] = b;
+          const double ms = time_fine(P, precision, sweep, reps, true, k);
+          if (ms < kb) {
+            kb = ms;
+            kv = v;
+            kbps = b;
+          }
+        }
+      const bool keep = kb < 0.98 * base;
+      P.kind_variant[k] = keep ? kv : -1;
+      P.kind_bps[k] = keep ? kbps : 0;
+    }
+    check_err(P);
+  }
   if (best_ms) *best_ms = best;
   if (best_variant) *best_variant = bv;
   if (best_bps) *best_bps = bb;
+  API_END
+}
+
+int edge_fine_kind_tiles(const edge_problem* p, int* variants, int* blocks_per_sm) {
+  API_BEGIN
+  if (!p || !variants || !blocks_per_sm) fail(EDGE_EINVAL, "null argument");
+  for (int k = 0; k < 3; ++k) {
+    variants[k] = p->P.kind_variant[k];
+    blocks_per_sm[k] = p->P.kind_bps[k];
+  }
+  API_END
+}
+
+int edge_set_kind_tune(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.kind_tune = enable != 0;
+  if (!enable)
+    for (int k = 0; k < 3; ++k) {
+      p->P.kind_variant[k] = -1;
+      p->P.kind_bps[k] = 0;
+    }
   API_END
 }
 

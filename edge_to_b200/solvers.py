@@ -296,7 +296,10 @@ class CuMultiGrid(Solver):
         self.kernel._bind_stream()
         _lib.call("edge_autotune_fine", self.kernel.handle, prec, 5, ctypes.byref(ms), ctypes.byref(v),
                   ctypes.byref(b))
-        self.tuned = {"variant": v.value, "blocks_per_sm": b.value, "ms": ms.value}
+        kv, kb = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+        _lib.call("edge_fine_kind_tiles", self.kernel.handle, kv, kb)
+        self.tuned = {"variant": v.value, "blocks_per_sm": b.value, "ms": ms.value,
+                      "per_kind": [[int(kv[i]), int(kb[i])] for i in range(3)]}
         return self.tuned
 
     SWEEP_CANDIDATES = ("1", "1,2", "2", "1,3", "n")

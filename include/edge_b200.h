@@ -75,8 +75,16 @@ int edge_set_tma(edge_problem* p, int enable);
  * k_fine3_cube (used when edge_uses_cube_form is 1, else 9..15 run k_fine3_pk); and the
  * target of resident blocks per SM that sets the y-chunking of the grid. */
 int edge_set_fine_tile(edge_problem* p, int variant, int blocks_per_sm);
+/* Tiles of the three fused launch kinds (first sweep + residual, last sweep + correction,
+ * search direction + product): variant (-1: the common tile) and y-chunking target each. */
+int edge_fine_kind_tiles(const edge_problem* p, int* variants, int* blocks_per_sm);
+int edge_set_kind_tune(edge_problem* p, int enable);
 /* Autotuner: times every tile variant and y-chunking on the current density with the plain
- * operator in `precision` (reps launches each), keeps the fastest, reports it. */
+ * operator in `precision` (reps launches each; for the mixed path with the cube kernel, the
+ * iteration's three fused fine launches together), keeps the fastest, reports it.  Then, unless
+ * edge_set_kind_tune(p, 0), it times each fused launch kind alone over the cube-kernel variants
+ * and keeps a kind's own tile where it is at least 2 % faster (edge_fine_kind_tiles reports
+ * them: variant -1 = the common tile).  edge_set_fine_tile sets one tile for every launch. */
 int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms, int* best_variant,
                        int* best_bps);
 /* Benchmark helper: average device time (ms) of `reps` fine-operator launches with the given
