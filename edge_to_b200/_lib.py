@@ -84,6 +84,7 @@ _SIGS = {
     "edge_mg_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, c_double_p, c_int_p]),
     "edge_mg_setup": (ctypes.c_int, [vp]),
     "edge_mg_level_dense": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_longlong]),
+    "edge_jacobi_sweep": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, ctypes.c_double, ctypes.c_int, vp]),
     "edge_restrict": (ctypes.c_int, [ctypes.c_int, c_int_p, vp, vp, vp]),
     "edge_prolong": (ctypes.c_int, [ctypes.c_int, c_int_p, vp, vp, vp]),
     "edge_filter_create": (ctypes.c_int, [ctypes.c_int, c_int_p, ctypes.c_int, c_int_p, c_double_p, ctypes.POINTER(vp)]),

@@ -2995,6 +2995,37 @@ int edge_mg_level_dense(edge_problem* p, int level, double* out_dev, long long n
   API_END
 }
 
+int edge_jacobi_sweep(edge_problem* p, int level, const double* x_dev, const double* b_dev, double omega, int n_step,
+                      double* out_dev) {
+  API_BEGIN
+  if (!p || !x_dev || !b_dev || !out_dev) fail(EDGE_EINVAL, "null argument");
+  Prob& P = p->P;
+  ensure_mg(P);
+  if (P.prec != EDGE_FP64) fail(EDGE_ESTATE, "the standalone smoother needs the FP64 hierarchy (precision EDGE_FP64)");
+  if (level < 0 || level >= P.n_level || (int)P.lv.size() <= level)
+    fail(EDGE_EINVAL, "level must be a smoothed level, 0 <= level < n_level");
+  if (!P.has_rho) fail(EDGE_ESTATE, "rho not set");
+  if (n_step < 0) fail(EDGE_EINVAL, "n_step must be >= 0");
+  Level& Lv = P.lv[level];
+  const Geo& g = Lv.g;
+  double* x = (double*)Lv.xa;
+  double* y = (double*)Lv.xb;
+  double* b = (double*)Lv.r;
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, x_dev, x);
+  launch(P, k_user_to_slots<double>, cdiv(g.n, 256), 256, 0, g, b_dev, b);
+  CK(cudaMemcpyAsync(P.scal + 8, &omega, sizeof(double), cudaMemcpyHostToDevice, P.stream));
+  for (int s = 0; s < n_step; ++s) {
+    EpiJacobi<double, double, double> e{b, (const double*)Lv.dinv, y, P.scal + 8, 1.0, g.n};
+    level_apply<double>(P, level, x, e);
+    std::swap(x, y);
+  }
+  launch(P, k_slots_to_user<double>, cdiv(g.n, 256), 256, 0, g, (const double*)x, out_dev);
+  KCHECK();
+  CK(cudaStreamSynchronize(P.stream));
+  check_err(P);
+  API_END
+}
+
 int edge_breakdown_begin(edge_problem* p, int max_launches) {
   API_BEGIN
   if (!p || max_launches < 1) fail(EDGE_EINVAL, "bad argument");

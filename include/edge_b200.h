@@ -207,6 +207,15 @@ int edge_mg_solve_embedded(edge_problem* p, const int* nel_real, const double* f
  * row-major n x n FP64 matrix in the reference's coarse DOF order (test inspection). */
 int edge_mg_setup(edge_problem* p);
 int edge_mg_level_dense(edge_problem* p, int level, double* out_dev, long long n);
+/* The damped-Jacobi smoother of the V-cycle on its own.  Replaces CuMultiGrid._jacobi_smoother
+ * (solvers/_multigrid_cuda.py:59-62): n_step times x <- x + omega Dinv (b - A_level x) on level
+ * 0 <= level < n_level of the hierarchy that the last edge_mg_setup or solve built (level 0:
+ * K(E) with its BC rows, Dinv = 1 / diag), FP64 (precision EDGE_FP64).  x_dev, b_dev, out_dev
+ * in the level's user layout (the reference's node numbering of that level's grid, DOFs
+ * interleaved); omega is the weight as used (the V-cycle passes omega * 1.06^level).
+ * Synchronises the problem's stream. */
+int edge_jacobi_sweep(edge_problem* p, int level, const double* x_dev, const double* b_dev, double omega, int n_step,
+                      double* out_dev);
 
 /* ---- multi-material OC update.  Replaces the bisection of TopOpt.update_design
  * (TopOpt/_cuda.py:242-280) for PenalizedMultiMaterial (constraint MaterialModels.py:204-215):

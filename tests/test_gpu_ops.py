@@ -227,6 +227,42 @@ def test_galerkin_against_oracle_ragged():
             assert rel(out.cpu(), ref) < TOL, (nel, lvl)
 
 
+def test_jacobi_sweep_entry_point_against_oracle():
+    """edge_jacobi_sweep (the V-cycle's damped-Jacobi smoother on its own) on level 0 and on a
+    Galerkin level of a ragged grid with BCs equals n_step sweeps x + omega (b - A x) / diag(A)
+    with the oracle's assembled and Galerkin matrices."""
+    import torch
+    import edge_to_b200 as eb
+    from edge_to_b200 import _lib
+    for nel in ((9, 7), (6, 5, 7)):
+        dim = len(nel)
+        g = Grid(nel)
+        rng = np.random.default_rng(23)
+        E = rng.uniform(1e-3, 1, g.n_el)
+        cons = np.where(rng.random(g.n_dof) < 0.1)[0]
+        K0 = elements.q4_stiffness(1, 1, 1, 0.3) if dim == 2 else elements.hex8_stiffness(1, 1, 1, 1, 0.3)
+        A0 = ops.assemble(g, K0, E, cons)
+        mesh = _mesh(dim, nel, None)
+        k = eb.CuStructuredStiffnessKernel(mesh)
+        k.set_rho(torch.as_tensor(E, device="cuda"))
+        k.add_constraints(cons)
+        s = eb.CuMultiGrid(mesh, k, n_level=2)
+        s._configure()
+        _lib.call("edge_mg_setup", k.handle)
+        for lvl, A in ((0, A0), (1, ops.galerkin(A0, g))):
+            A = A.toarray()
+            n = A.shape[0]
+            x = rng.standard_normal(n)
+            b = rng.standard_normal(n)
+            want = x.copy()
+            for _ in range(3):
+                want = want + 0.45 * (b - A @ want) / np.diag(A)
+            out = torch.empty(n, dtype=torch.float64, device="cuda")
+            xd, bd = torch.as_tensor(x, device="cuda"), torch.as_tensor(b, device="cuda")
+            _lib.call("edge_jacobi_sweep", k.handle, lvl, _lib.ptr(xd), _lib.ptr(bd), 0.45, 3, _lib.ptr(out))
+            assert rel(out.cpu(), want) < 1e-12, (nel, lvl)
+
+
 @pytest.mark.parametrize("nel", [(4, 4, 4), (7, 5, 3), (40, 9, 33), (9, 33, 65), (3, 3, 130), (20, 20, 47)])
 def test_fine_kernel_variants_agree(nel):
     """TMA-staged, cooperative-load and dense kernels give the same K(E) u (ragged tiles, BCs)."""
