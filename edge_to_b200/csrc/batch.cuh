@@ -89,7 +89,6 @@ struct BatchDesc {
   const double* K0_64;  // element matrix, corner-bit order, FP64
   const void* K0_T;     // the same in the V-cycle's type
   double *b64, *x64, *r64, *p64, *q64;
-  void* rT;  // the residual in the V-cycle's type (r64 itself in FP64)
   const double* Ainv;
   PcgState* st;
   const int* chol_status;
@@ -104,9 +103,16 @@ struct BatchDesc {
 // node is unconditional (a neighbour or element outside the grid reads the node's own slot
 // and is replaced by zero), so a thread's loads are in flight together: each pass is a few
 // round trips to L2 per node, not one per neighbour.
-template <int C, typename T, typename TE, class F>
-EDGE_D void b_fine2(const Geo& g, const T* u, const TE* E, const uint8_t* mask, const T* sK, F&& epi) {
-  const long long n = g.n;
+// Input of the fine operator: u itself (ArrIn) or a value computed from other arrays
+// (uin(slot, component)).
+template <typename T> struct ArrIn {
+  const T* u;
+  long long n;
+  EDGE_D T operator()(long long ss, int c) const { return u[c * n + ss]; }
+};
+
+template <int C, typename T, typename TE, class UIn, class F>
+EDGE_D void b_fine2(const Geo& g, UIn uin, const TE* E, const uint8_t* mask, const T* sK, F&& epi) {
   const int nn = g.nx * g.ny;
   for (int t = Team<C>::first(); t < nn; t += Team<C>::stride()) {
     const int i = t % g.nx, j = t / g.nx;
@@ -121,7 +127,7 @@ EDGE_D void b_fine2(const Geo& g, const T* u, const TE* E, const uint8_t* mask, 
         const long long ss = in ? s + (long long)(dy - 1) * g.pz + (dx - 1) : s;
         const uint8_t mr = __ldg(mask + ss);
         const uint8_t m = in ? mr : (uint8_t)3;
-        const T a0 = u[ss], a1 = u[n + ss];
+        const T a0 = uin(ss, 0), a1 = uin(ss, 1);
         U[dy][dx][0] = (m & 1) ? T(0) : a0;
         U[dy][dx][1] = (m & 2) ? T(0) : a1;
       }
@@ -148,7 +154,7 @@ EDGE_D void b_fine2(const Geo& g, const T* u, const TE* E, const uint8_t* mask, 
       for (int c = 0; c < 2; ++c) Au[c] += Ee * r[c];
     }
     const uint8_t m = __ldg(mask + s);
-    T own[2] = {u[s], u[n + s]};
+    T own[2] = {uin(s, 0), uin(s, 1)};
     Au[0] = (m & 1) ? own[0] : Au[0];
     Au[1] = (m & 2) ? own[1] : Au[1];
     epi(s, own, Au);
@@ -279,23 +285,30 @@ EDGE_D double b_dot(long long nv, const TA* a, const TB* b, double* sh) {
 template <int C, typename TV, typename TS, class F>
 EDGE_D void b_level_op(const BatchDesc& d, int l, const TV* u, const TV* sK, F&& epi) {
   if (l == 0)
-    b_fine2<C, TV, TV>(d.lv[0].g, u, (const TV*)d.ET, d.mask, sK, epi);
+    b_fine2<C, TV, TV>(d.lv[0].g, ArrIn<TV>{u, d.lv[0].g.n}, (const TV*)d.ET, d.mask, sK, epi);
   else
     b_st2<C, TV, TS>(d.lv[l].g, u, (const TS*)d.lv[l].S, epi);
 }
 
-// Damped-Jacobi pieces with level l's inverse diagonal (type TD).  down: x = w Dinv b
-// (k_jacobi0), ns - 1 more sweeps, r = b - A x; up (after the interpolation into e1): ns - 1
-// sweeps on the correction, then out = xb + (e + w Dinv (r - A e)).
-template <int C, typename TV, typename TS, typename TD>
-EDGE_D void b_smooth_level(const BatchDesc& d, int l, const TV* sK, TV w, const TV* b, const TV* xb, TV*& x, TV*& y,
-                           TV*& e1, TV*& e2, TV* r, TV* out, bool down) {
+// Damped-Jacobi pieces with level l's inverse diagonal (type TD); the level's right-hand side
+// b has type TB (level 0: the FP64 PCG residual, read in the V-cycle's type).  down: x = w
+// Dinv b (k_jacobi0), ns - 1 more sweeps, r = b - A x; with one sweep on level 0 the two are
+// one pass (the operator's input w Dinv b computed where it is read, x never stored: fused0).
+// up (after the interpolation into e1): ns - 1 sweeps on the correction, then
+// out = xb + (e + w Dinv (r - A e)) with xb the down pass's x (recomputed as w Dinv b when
+// fused0); with dot, acc += dotv . out (the PCG's r.z) per thread.
+template <int C, typename TV, typename TS, typename TD, typename TB>
+EDGE_D void b_smooth_level(const BatchDesc& d, int l, const TV* sK, TV w, const TB* b, const TV* xb, TV*& x, TV*& y,
+                           TV*& e1, TV*& e2, TV* r, TV* out, bool down, bool fused0, const double* dotv,
+                           double& acc) {
   using TM = Team<C>;
   const BatchLevel& Lv = d.lv[l];
   const Geo& g = Lv.g;
   const long long n = g.n, nv = 2 * n;
   const TD* D = (const TD*)Lv.dinv;
   const int ns = d.sweeps[l];
+  auto bv = [&](long long q) { return Conv<TV>::from(b[q]); };
+  auto wdb = [&](long long q) { return w * Conv<TV>::from(__ldg(D + q)) * bv(q); };
   auto sweep = [&](const TV* bb, const TV* in, TV* o) {
     b_level_op<C, TV, TS>(d, l, in, sK, [&](long long s, const TV* own, const TV* Au) {
       for (int c = 0; c < 2; ++c) {
@@ -305,12 +318,29 @@ EDGE_D void b_smooth_level(const BatchDesc& d, int l, const TV* sK, TV w, const 
     });
     TM::sync();
   };
+  auto sweep_b = [&](const TV* in, TV* o) {  // a sweep on the down pass (right-hand side b)
+    b_level_op<C, TV, TS>(d, l, in, sK, [&](long long s, const TV* own, const TV* Au) {
+      for (int c = 0; c < 2; ++c) {
+        const long long q = c * n + s;
+        o[q] = own[c] + w * Conv<TV>::from(__ldg(D + q)) * (bv(q) - Au[c]);
+      }
+    });
+    TM::sync();
+  };
   if (down) {
+    if (fused0) {
+      b_fine2<C, TV, TV>(g, [&](long long ss, int c) { return wdb(c * n + ss); }, (const TV*)d.ET, d.mask, sK,
+                         [&](long long s, const TV* own, const TV* Au) {
+                           for (int c = 0; c < 2; ++c) r[c * n + s] = bv(c * n + s) - Au[c];
+                         });
+      TM::sync();
+      return;
+    }
     if (ns >= 1) {
-      for (long long q = TM::first(); q < nv; q += TM::stride()) x[q] = w * Conv<TV>::from(__ldg(D + q)) * b[q];
+      for (long long q = TM::first(); q < nv; q += TM::stride()) x[q] = wdb(q);
       TM::sync();
       for (int s = 1; s < ns; ++s) {
-        sweep(b, x, y);
+        sweep_b(x, y);
         TV* t = x;
         x = y;
         y = t;
@@ -320,7 +350,7 @@ EDGE_D void b_smooth_level(const BatchDesc& d, int l, const TV* sK, TV w, const 
       TM::sync();
     }
     b_level_op<C, TV, TS>(d, l, x, sK, [&](long long s, const TV* own, const TV* Au) {
-      for (int c = 0; c < 2; ++c) r[c * n + s] = b[c * n + s] - Au[c];
+      for (int c = 0; c < 2; ++c) r[c * n + s] = bv(c * n + s) - Au[c];
     });
     TM::sync();
   } else {
@@ -330,40 +360,50 @@ EDGE_D void b_smooth_level(const BatchDesc& d, int l, const TV* sK, TV w, const 
       e1 = e2;
       e2 = t;
     }
+    auto xbase = [&](long long q) { return fused0 ? wdb(q) : xb[q]; };
     if (ns >= 1) {
       b_level_op<C, TV, TS>(d, l, e1, sK, [&](long long s, const TV* own, const TV* Au) {
         for (int c = 0; c < 2; ++c) {
           const long long q = c * n + s;
           const TV e = own[c] + w * Conv<TV>::from(__ldg(D + q)) * (r[q] - Au[c]);
-          out[q] = xb[q] + e;
+          const TV v = xbase(q) + e;
+          out[q] = v;
+          if (dotv) acc += dotv[q] * (double)v;
         }
       });
     } else {
-      for (long long q = TM::first(); q < nv; q += TM::stride())
-        out[q] = Conv<TV>::from((double)xb[q] + (double)e1[q]);
+      for (long long q = TM::first(); q < nv; q += TM::stride()) {
+        const TV v = Conv<TV>::from((double)xb[q] + (double)e1[q]);
+        out[q] = v;
+        if (dotv) acc += dotv[q] * (double)v;
+      }
     }
-    TM::sync();
+    if (!dotv) TM::sync();  // with dot, the team sum that follows is the barrier
   }
 }
 
-// z = V-cycle(rT) into lv[0].res.
+// z = V-cycle(r) into lv[0].res, r the FP64 PCG residual (read in the V-cycle's type); returns
+// this thread's part of r.z, which the caller sums over the team.
 template <int C, typename TV, typename TD0, typename TS>
-EDGE_D void b_vcycle(const BatchDesc& d, const TV* sK, double omega, double* sb) {
+EDGE_D double b_vcycle(const BatchDesc& d, const TV* sK, double omega, double* sb) {
   using TM = Team<C>;
   const int L = d.n_level;
   TV* xcur[BATCH_MAXL];
+  const bool fused0 = d.sweeps[0] == 1;
+  double acc = 0.0;
   for (int l = 0; l < L; ++l) {
     const BatchLevel& Lv = d.lv[l];
-    const TV* b = (const TV*)(l == 0 ? d.rT : Lv.b);
     TV* x = (TV*)Lv.xa;
     TV* y = (TV*)Lv.xb;
     TV* e1 = nullptr;
     TV* e2 = nullptr;
     const TV w = Conv<TV>::from(omega * d.wscale[l]);
     if (l == 0)
-      b_smooth_level<C, TV, TS, TD0>(d, l, sK, w, b, nullptr, x, y, e1, e2, (TV*)Lv.r, nullptr, true);
+      b_smooth_level<C, TV, TS, TD0, double>(d, l, sK, w, d.r64, nullptr, x, y, e1, e2, (TV*)Lv.r, nullptr, true,
+                                              fused0, nullptr, acc);
     else
-      b_smooth_level<C, TV, TS, TV>(d, l, sK, w, b, nullptr, x, y, e1, e2, (TV*)Lv.r, nullptr, true);
+      b_smooth_level<C, TV, TS, TV, TV>(d, l, sK, w, (const TV*)Lv.b, nullptr, x, y, e1, e2, (TV*)Lv.r, nullptr,
+                                        true, false, nullptr, acc);
     xcur[l] = x;
     b_restrict2<C, TV>(Lv.g, d.lv[l + 1].g, (const TV*)Lv.r, (TV*)d.lv[l + 1].b);
     TM::sync();
@@ -380,10 +420,13 @@ EDGE_D void b_vcycle(const BatchDesc& d, const TV* sK, double omega, double* sb)
     TM::sync();
     const TV w = Conv<TV>::from(omega * d.wscale[l]);
     if (l == 0)
-      b_smooth_level<C, TV, TS, TD0>(d, l, sK, w, nullptr, xcur[l], x, y, e1, e2, (TV*)Lv.r, (TV*)Lv.res, false);
+      b_smooth_level<C, TV, TS, TD0, double>(d, l, sK, w, d.r64, xcur[l], x, y, e1, e2, (TV*)Lv.r, (TV*)Lv.res,
+                                              false, fused0, d.r64, acc);
     else
-      b_smooth_level<C, TV, TS, TV>(d, l, sK, w, nullptr, xcur[l], x, y, e1, e2, (TV*)Lv.r, (TV*)Lv.res, false);
+      b_smooth_level<C, TV, TS, TV, TV>(d, l, sK, w, (const TV*)Lv.b, xcur[l], x, y, e1, e2, (TV*)Lv.r,
+                                        (TV*)Lv.res, false, false, nullptr, acc);
   }
+  return acc;
 }
 
 template <int C, typename TV, typename TD0, typename TS>
@@ -397,15 +440,14 @@ EDGE_D void b_pcg_problem(const BatchDesc& d, const TV* sK, const double* sK64, 
   double* p = d.p64;
   double* q = d.q64;
   const double* b = d.b64;
-  TV* rT = (TV*)d.rT;
   const TV* z = (const TV*)d.lv[0].res;
-  const bool same = (const void*)rT == (const void*)r;
   double omega = d.keep_omega ? d.st->omega : d.omega0;
   const double min_omega = d.min_omega, d_omega = d.omega - d.min_omega;
   // r = b - A x (FP64)
-  b_fine2<C, double, double>(g, x, d.E64, d.mask, sK64, [&](long long s, const double* own, const double* Au) {
-    for (int c = 0; c < 2; ++c) r[c * n + s] = b[c * n + s] - Au[c];
-  });
+  b_fine2<C, double, double>(g, ArrIn<double>{x, n}, d.E64, d.mask, sK64,
+                             [&](long long s, const double* own, const double* Au) {
+                               for (int c = 0; c < 2; ++c) r[c * n + s] = b[c * n + s] - Au[c];
+                             });
   TM::sync();
   const double bb = b_dot<C>(nv, b, b, sh);
   int done = 0, iter = 0;
@@ -413,23 +455,19 @@ EDGE_D void b_pcg_problem(const BatchDesc& d, const TV* sK, const double* sK64, 
   if (bb == 0.0) done = 1;  // nothing to solve: residual 0, like a converged solve
   if (*d.chol_status) done = 3;
   while (!done) {
-    if (!same) {
-      for (long long k = TM::first(); k < nv; k += TM::stride()) rT[k] = Conv<TV>::from(r[k]);
-      TM::sync();
-    }
-    b_vcycle<C, TV, TD0, TS>(d, sK, omega, sb);
-    const double rz_new = b_dot<C>(nv, r, z, sh);
+    const double rz_new = TM::sum(b_vcycle<C, TV, TD0, TS>(d, sK, omega, sb), sh);
     const double beta = iter == 0 ? 0.0 : rz_new / rz;
     for (long long k = TM::first(); k < nv; k += TM::stride())
       p[k] = iter == 0 ? (double)z[k] : (double)z[k] + beta * p[k];
     TM::sync();
     double acc = 0.0;
-    b_fine2<C, double, double>(g, p, d.E64, d.mask, sK64, [&](long long s, const double* own, const double* Au) {
-      for (int c = 0; c < 2; ++c) {
-        q[c * n + s] = Au[c];
-        acc += own[c] * Au[c];
-      }
-    });
+    b_fine2<C, double, double>(g, ArrIn<double>{p, n}, d.E64, d.mask, sK64,
+                               [&](long long s, const double* own, const double* Au) {
+                                 for (int c = 0; c < 2; ++c) {
+                                   q[c * n + s] = Au[c];
+                                   acc += own[c] * Au[c];
+                                 }
+                               });
     const double pq = TM::sum(acc, sh);
     const double alpha = rz_new / pq;
     double racc = 0.0;

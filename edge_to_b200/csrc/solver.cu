@@ -4031,7 +4031,6 @@ int edge_batch_solve_and_process(edge_batch* b, const double* const* rho, double
       d.r64 = P.r64;
       d.p64 = (double*)P.p;
       d.q64 = (double*)P.q;
-      d.rT = mixed ? (void*)P.r32 : (void*)P.r64;
       d.Ainv = P.Ainv;
       d.st = P.st;
       d.chol_status = P.chol_status;
