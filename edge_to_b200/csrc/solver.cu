@@ -2497,13 +2497,14 @@ int edge_autotune_fine(edge_problem* p, int precision, int reps, double* best_ms
   }
   double best = 1e30;
   int bv = P.tile_variant, bb = P.blocks_per_sm;
-  const int bps_list[4] = {2, 4, 8, 16};
+  // y-chunking targets: the grid's wave count against the resident blocks depends on them
+  const int bps_list[8] = {2, 3, 4, 6, 8, 10, 12, 16};
   // variants 5..8: packed-pair FP32 kernel; 9..12: its cube-element form
   const int nvar = precision == EDGE_FP64 ? 5 : (P.cube ? 16 : 9);
   const bool sweep = can_time_sweep(P, precision);
   const bool mix = sweep && precision != EDGE_FP64;  // time the whole per-iteration mix
   for (int v = 0; v < nvar; ++v)
-    for (int bi = 0; bi < 4; ++bi) {
+    for (int bi = 0; bi < 8; ++bi) {
       P.tile_variant = v;
       P.blocks_per_sm = bps_list[bi];
       const double ms = time_fine(P, precision, sweep, reps, mix);
