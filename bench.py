@@ -294,6 +294,9 @@ def run_ours(args, cfg_name):
     if args.no_kind_tune:
         from edge_to_b200 import _lib as _l
         _l.call("edge_set_kind_tune", opt.kernel.handle, 0)
+    if args.stencil != "default":
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_stencil_tiled", opt.kernel.handle, -1 if args.stencil == "linear" else 200000)
     traj = []
     rho, dr, it = warm(opt, rho, args.warmup, traj)
     # the state the timed steps start from; the end-to-end steps restart from it, so both
@@ -425,6 +428,7 @@ def run_ours(args, cfg_name):
                    "fine_tile": tuned, "sweeps": sweeps,
                    "coarse_stencils": "fp32" if (args.coarse_fp32 or args.precision == "fp64") else "bf16",
                    "residual_recurrence": "fp64" if (args.residual64 or args.precision == "fp64") else "fp32",
+                   "level_stencil_kernel": args.stencil,
                    "programmatic_dependent_launch": args.pdl and not args.no_graph,
                    "fused_fine_launches": args.precision == "mixed" and not args.no_fuse,
                    "fused_xr_update": (args.precision == "mixed" and not args.no_fuse and args.fuse_xr
@@ -625,16 +629,21 @@ def run_tiles(args, cfg_name):
     for lvl in range(1, cfg["n_level"]):
         ne = [v >> lvl for v in cfg["nel"]]
         nodes = (ne[0] + 1) * (ne[1] + 1) * (ne[2] + 1)
-        # stencil (123 coefficients) + u, b, Dinv, out per node
-        b = nodes * (123 * w + 4 * 3 * w)
+        # stencil (123 coefficients; BF16 copies in mixed precision) + u, b, Dinv, out per node
+        b = nodes * (123 * (2 if args.precision == "mixed" else w) + 4 * 3 * w)
         row = {"level": lvl, "nodes": nodes}
-        for name, qmax, pair in (("thread", 0, -1), ("pair", 0, 0), ("quad", 1 << 40, -1)):
+        for name, qmax, pair, tiled in (("thread", 0, -1, -1), ("pair", 0, 0, -1), ("quad", 1 << 40, -1, -1),
+                                        ("tiled", 0, 0, 0)):
             _lib.call("edge_set_stencil_quad", h, qmax)
             _lib.call("edge_set_stencil_pair", h, pair)
+            _lib.call("edge_set_stencil_tiled", h, tiled)
+            if tiled >= 0:
+                _lib.call("edge_mg_setup", h)  # fills the tile-major copies
             _lib.call("edge_time_level", h, lvl, max(1, args.steps), ctypes.byref(ms))
             row[name + "_us"] = round(ms.value * 1e3, 2)
             row[name + "_frac"] = round(b / (ms.value / 1e3) / 1e9 / peak, 3)
         _lib.call("edge_set_stencil_pair", h, 200000)
+        _lib.call("edge_set_stencil_tiled", h, 200000)
         levels.append(row)
     _lib.call("edge_set_stencil_quad", h, 40000)
     return {"mode": "tiles", "workload": cfg_name, "precision": args.precision, "peak_GBps": peak,
@@ -785,6 +794,9 @@ def main():
     ap.add_argument("--no-kind-tune", action="store_true",
                     help="mixed path: one fine tile for the three fused launch kinds (default: the autotuner may "
                          "give each kind its own)")
+    ap.add_argument("--stencil", default="default", choices=["default", "linear", "tiled"],
+                    help="mixed path, coarse levels of 200k slots and more: linear BF16 stencil copy (k_st3_apply2) "
+                         "or tile-major copy (k_st3_apply2t)")
     ap.add_argument("--fuse-xr", action="store_true",
                     help="mixed path: the PCG's x/r update folded into the next iteration's fine launches when "
                          "the smoother weight is fixed (default: its own launch, faster at 12.8M DOF)")

@@ -45,6 +45,7 @@ _SIGS = {
     "edge_mm_law": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_int, vp, c_double_p, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_int, vp, vp, vp]),
     "edge_set_stencil_pair": (ctypes.c_int, [vp, ctypes.c_longlong]),
+    "edge_set_stencil_tiled": (ctypes.c_int, [vp, ctypes.c_longlong]),
     "edge_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_mg_set_sweeps": (ctypes.c_int, [vp, c_int_p, ctypes.c_int]),
     "edge_mg_set_omega_carry": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -279,6 +279,163 @@ k_st3_apply2(const Geo g, const T* __restrict__ u, const TS* __restrict__ S, Epi
   finish_dot(epi, dacc, part, ticket, dot_dst);
 }
 
+// BF16 pair (low half: the even slot) -> two FP32 values, exactly
+EDGE_D float2 bf16x2_to_f2(uint32_t w) { return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u)); }
+
+// Tile-major BF16 pair copy of a 3-D stencil for k_st3_apply2t: word
+// (p >> 5) * STT_TILE + q * 32 + (p & 31) holds coefficient array q of the slot pair p (slots
+// 2p and 2p + 1, the low half for slot 2p).  The 32 pairs of a warp form one tile, so every
+// coefficient load of a thread is the tile base of its pair plus a constant offset (q * 128
+// bytes), with no per-load address arithmetic; a warp's loads stay 128-byte coalesced.
+constexpr int STT_TILE = NST3 * 32;  // words per tile of 32 pairs
+EDGE_HD long long stt_base(long long p) { return (p >> 5) * STT_TILE + (p & 31); }
+EDGE_HD long long stt_words(long long n) { return ((n / 2 + 31) / 32) * STT_TILE; }
+
+// FP32 stencil (NST3 arrays of n slots) -> the tile-major BF16 pair copy (n even; padding
+// pairs of the last tile are zero).  Same rounding as the linear BF16 copy.
+__global__ void k_stencil_tiled_bf16(long long n, const float* __restrict__ S, unsigned* __restrict__ St,
+                                     long long nw) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < nw; w += (long long)gridDim.x * blockDim.x) {
+    const long long tile = w / STT_TILE;
+    const int r = (int)(w - tile * STT_TILE), q = r >> 5;
+    const long long s = 2 * (tile * 32 + (r & 31));
+    unsigned v = 0u;
+    if (s < n) {
+      const float2 c = reinterpret_cast<const float2*>(S + (long long)q * n + s)[0];
+      v = (unsigned)__bfloat16_as_ushort(Conv<__nv_bfloat16>::from(c.x)) |
+          ((unsigned)__bfloat16_as_ushort(Conv<__nv_bfloat16>::from(c.y)) << 16);
+    }
+    St[w] = v;
+  }
+}
+
+// k_st3_apply2 on the tile-major BF16 copy: two consecutive z-slots per thread, the thread's
+// own coefficient pairs at constant offsets from one base, the transposed blocks of a lower
+// neighbour from one base per direction (two for dz = +-1, where the neighbour pair straddles
+// two stored pairs), and the three products of a block row on the packed FP32 pipe (both
+// slots of the pair in one instruction).  Same terms as k_st3_apply2 summed in the same order
+// (each block row: a v0, + b v1, + d v2, then added to the sum), with the packed instructions'
+// own rounding of each step.
+// The x += omega D^-1 (b - A x) sweep is held to 64 registers (8 blocks per SM instead of 6;
+// 4 bytes of spill).
+template <class Epi> struct StTiledMinBlocks {
+  static constexpr int value = 1;
+};
+template <typename T, typename TB, typename TD, typename TX, bool DOT, typename TV>
+struct StTiledMinBlocks<EpiJacobiAdd<T, TB, TD, TX, DOT, TV>> {
+  static constexpr int value = 8;
+};
+template <class Epi>
+__global__ void __launch_bounds__(128, StTiledMinBlocks<Epi>::value)
+k_st3_apply2t(const Geo g, const float* __restrict__ u, const unsigned* __restrict__ St, Epi epi, double* part,
+              unsigned* ticket, double* dot_dst) {
+  EDGE_PDL_ENTRY();
+  using T = float;
+  using T2 = float2;
+  const long long p = blockIdx.x * 128LL + threadIdx.x;  // slot pair
+  const long long s0 = 2 * p;
+  const long long n = g.n;
+  epi.init();
+  double dacc = 0.0;
+  if (s0 < n) {
+    const int k0 = (int)(s0 % g.pz), i = (int)((s0 / g.pz) % g.nx), j = (int)(s0 / g.plane);
+    const bool ok0 = k0 < g.nz, ok1 = k0 + 1 < g.nz;
+    const typename Epi::Pre pe0 = epi.pre(s0), pe1 = epi.pre(s0 + 1);
+    const unsigned* own = St + stt_base(p);
+    auto ld2 = [&](const T* a, long long s) { return reinterpret_cast<const T2*>(a + s)[0]; };
+    auto lo = [](unsigned w) { return __uint_as_float(w << 16); };
+    auto hi = [](unsigned w) { return __uint_as_float(w & 0xffff0000u); };
+    auto row = [](T2 a, T2 b, T2 d, const T2* v) {
+      return __ffma2_rn(d, v[2], __ffma2_rn(b, v[1], __fmul2_rn(a, v[0])));
+    };
+    T2 uc[3], Au[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) uc[c] = ld2(u + c * n, s0);
+    {
+      T2 cc[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) cc[q] = bf16x2_to_f2(__ldg(own + q * 32));
+      Au[0] = row(cc[0], cc[1], cc[2], uc);
+      Au[1] = row(cc[1], cc[3], cc[4], uc);
+      Au[2] = row(cc[2], cc[4], cc[5], uc);
+    }
+#pragma unroll
+    for (int nb = 14; nb < 27; ++nb) {
+      const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
+      const long long off = (long long)dy * g.plane + (long long)dx * g.pz + dz;
+      const int qb = 6 + (nb - 14) * 9;
+      if (i + dx >= 0 && i + dx < g.nx && j + dy >= 0 && j + dy < g.ny) {  // upper neighbour
+        const bool z0 = k0 + dz >= 0 && k0 + dz < g.nz, z1 = k0 + 1 + dz >= 0 && k0 + 1 + dz < g.nz;
+        const long long sn = s0 + off;
+        const long long sn1 = sn + 1 < n ? sn + 1 : n - 1;
+        T2 v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (dz == 0) {
+            v[c] = ld2(u + c * n, sn);
+          } else {
+            v[c].x = __ldg(u + c * n + sn);
+            v[c].y = __ldg(u + c * n + sn1);
+          }
+          v[c].x = z0 ? v[c].x : T(0);
+          v[c].y = z1 ? v[c].y : T(0);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          Au[c] = __fadd2_rn(Au[c], row(bf16x2_to_f2(__ldg(own + (qb + c * 3 + 0) * 32)),
+                                        bf16x2_to_f2(__ldg(own + (qb + c * 3 + 1) * 32)),
+                                        bf16x2_to_f2(__ldg(own + (qb + c * 3 + 2) * 32)), v));
+      }
+      if (i - dx >= 0 && i - dx < g.nx && j - dy >= 0 && j - dy < g.ny) {  // lower neighbour
+        const bool z0 = k0 - dz >= 0 && k0 - dz < g.nz, z1 = k0 + 1 - dz >= 0 && k0 + 1 - dz < g.nz;
+        const long long sm = s0 - off;  // >= -1 here; odd exactly when dz != 0
+        const long long sa = sm < 0 ? 0 : sm;
+        T2 v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if (dz == 0) {
+            v[c] = ld2(u + c * n, sm);
+          } else {
+            v[c].x = __ldg(u + c * n + sa);
+            v[c].y = __ldg(u + c * n + sm + 1);
+          }
+          v[c].x = z0 ? v[c].x : T(0);
+          v[c].y = z1 ? v[c].y : T(0);
+        }
+        if (dz == 0) {  // the neighbour pair is the stored pair sm / 2
+          const unsigned* lb = St + stt_base(sm >> 1);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            Au[c] = __fadd2_rn(Au[c], row(bf16x2_to_f2(__ldg(lb + (qb + 0 * 3 + c) * 32)),
+                                          bf16x2_to_f2(__ldg(lb + (qb + 1 * 3 + c) * 32)),
+                                          bf16x2_to_f2(__ldg(lb + (qb + 2 * 3 + c) * 32)), v));
+        } else {  // slot sm: high half of pair (sm - 1) / 2; slot sm + 1: low half of pair (sm + 1) / 2
+          const long long pa = (sm - 1) >> 1;
+          const unsigned* la = St + stt_base(pa < 0 ? 0 : pa);
+          const unsigned* lb = St + stt_base((sm + 1) >> 1);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const unsigned a0 = __ldg(la + (qb + 0 * 3 + c) * 32), a1 = __ldg(lb + (qb + 0 * 3 + c) * 32);
+            const unsigned b0 = __ldg(la + (qb + 1 * 3 + c) * 32), b1 = __ldg(lb + (qb + 1 * 3 + c) * 32);
+            const unsigned d0 = __ldg(la + (qb + 2 * 3 + c) * 32), d1 = __ldg(lb + (qb + 2 * 3 + c) * 32);
+            Au[c] = __fadd2_rn(Au[c], row(make_float2(hi(a0), lo(a1)), make_float2(hi(b0), lo(b1)),
+                                          make_float2(hi(d0), lo(d1)), v));
+          }
+        }
+      }
+    }
+    if (ok0) {
+      T o[3] = {uc[0].x, uc[1].x, uc[2].x}, A[3] = {Au[0].x, Au[1].x, Au[2].x};
+      epi.apply(s0, o, A, pe0, dacc);
+    }
+    if (ok1) {
+      T o[3] = {uc[0].y, uc[1].y, uc[2].y}, A[3] = {Au[0].y, Au[1].y, Au[2].y};
+      epi.apply(s0 + 1, o, A, pe1, dacc);
+    }
+  }
+  finish_dot(epi, dacc, part, ticket, dot_dst);
+}
+
 // Latency-oriented variant for small levels, where a sweep is a handful of dependent load
 // round trips rather than a bandwidth problem: four lanes per node share the 26 neighbour
 // terms (term t = 4m + lane; terms 0..12 are the stored upper blocks, 13..25 the transposed

@@ -153,6 +153,13 @@ int edge_set_graph(edge_problem* p, int enable);
 /* FP32 3-D coarse levels with at least min_slots slots use two nodes per thread (pair loads
  * of the centre and stored blocks; default 200000); min_slots < 0: one node per thread. */
 int edge_set_stencil_pair(edge_problem* p, long long min_slots);
+/* Mixed precision, 3-D: coarse levels (below the coarsest, above the four-lanes-per-node
+ * size) with at least min_slots slots keep a tile-major BF16 pair copy of their stencil,
+ * filled by every hierarchy set-up, and are applied from it two nodes per thread with
+ * constant-offset coefficient loads and packed FP32 products (k_st3_apply2t); min_slots < 0:
+ * off (k_st3_apply2 on the linear BF16 copy).  Default 200000.  Levels already allocated get
+ * their copy at this call. */
+int edge_set_stencil_tiled(edge_problem* p, long long min_slots);
 /* Mixed precision only: enable != 0 applies the coarse-level stencils (levels >= 1, below the
  * coarsest) from BF16 copies made after each Galerkin set-up (half the bytes of the largest
  * coarse kernel); the Jacobi diagonals and the Galerkin chain stay FP32.  Default 1 (at 12.8M

@@ -369,8 +369,9 @@ def test_packed_kernel_in_mixed_solve():
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_stencil_kernels_agree_in_solve(precision):
-    """The one-thread-per-node, two-nodes-per-thread and four-lanes-per-node coarse stencil
-    kernels give the same PCG run (same iteration count, solutions equal to rounding)."""
+    """The one-thread-per-node, two-nodes-per-thread, four-lanes-per-node and tile-major
+    coarse stencil kernels give the same PCG run (same iteration count, solutions equal to
+    rounding)."""
     import torch
     import edge_to_b200 as eb
     from edge_to_b200 import _lib
@@ -407,6 +408,15 @@ def test_stencil_kernels_agree_in_solve(precision):
         (xa, ia, ra), (xb, ib, rb) = bf
         assert abs(ia - ib) <= 1 and abs(ia - it0) <= 3 and ra < 1e-8 and rb < 1e-8
         assert rel(xb, xa) < 1e-7 and rel(xa, x0) < 1e-6
+        # tile-major BF16 pair copies with packed products (every coarse level here): the same
+        # terms in the same order as the pair kernel, rounded by the packed instructions
+        _lib.call("edge_set_stencil_tiled", k.handle, 0)
+        xt, rt = s.solve(torch.as_tensor(p.f, device="cuda"), use_last=False)
+        it_ = s.last_iters
+        _lib.call("edge_set_stencil_tiled", k.handle, 200000)
+        _lib.call("edge_set_stencil_pair", k.handle, 200000)
+        _lib.call("edge_set_stencil_quad", k.handle, 40000)
+        assert abs(it_ - ib) <= 1 and rt < 1e-8 and rel(xt.cpu().numpy(), xb) < 1e-7
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
