@@ -294,6 +294,9 @@ def run_ours(args, cfg_name):
     if args.no_kind_tune:
         from edge_to_b200 import _lib as _l
         _l.call("edge_set_kind_tune", opt.kernel.handle, 0)
+    if args.galerkin == "direct":
+        from edge_to_b200 import _lib as _l
+        _l.call("edge_set_galerkin_axis", opt.kernel.handle, 0)
     if args.stencil != "default":
         from edge_to_b200 import _lib as _l
         _l.call("edge_set_stencil_tiled", opt.kernel.handle, -1 if args.stencil == "linear" else 200000)
@@ -429,6 +432,7 @@ def run_ours(args, cfg_name):
                    "coarse_stencils": "fp32" if (args.coarse_fp32 or args.precision == "fp64") else "bf16",
                    "residual_recurrence": "fp64" if (args.residual64 or args.precision == "fp64") else "fp32",
                    "level_stencil_kernel": args.stencil,
+                   "galerkin_products": args.galerkin,
                    "programmatic_dependent_launch": args.pdl and not args.no_graph,
                    "fused_fine_launches": args.precision == "mixed" and not args.no_fuse,
                    "fused_xr_update": (args.precision == "mixed" and not args.no_fuse and args.fuse_xr
@@ -794,6 +798,8 @@ def main():
     ap.add_argument("--no-kind-tune", action="store_true",
                     help="mixed path: one fine tile for the three fused launch kinds (default: the autotuner may "
                          "give each kind its own)")
+    ap.add_argument("--galerkin", default="axis", choices=["axis", "direct"],
+                    help="3-D Galerkin products of levels >= 2: three one-axis passes (default) or one direct pass")
     ap.add_argument("--stencil", default="default", choices=["default", "linear", "tiled"],
                     help="mixed path, coarse levels of 200k slots and more: linear BF16 stencil copy (k_st3_apply2) "
                          "or tile-major copy (k_st3_apply2t)")

@@ -46,6 +46,7 @@ _SIGS = {
                                    ctypes.c_int, vp, vp, vp]),
     "edge_set_stencil_pair": (ctypes.c_int, [vp, ctypes.c_longlong]),
     "edge_set_stencil_tiled": (ctypes.c_int, [vp, ctypes.c_longlong]),
+    "edge_set_galerkin_axis": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_set_graph": (ctypes.c_int, [vp, ctypes.c_int]),
     "edge_mg_set_sweeps": (ctypes.c_int, [vp, c_int_p, ctypes.c_int]),
     "edge_mg_set_omega_carry": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -1028,6 +1028,55 @@ k_galerkin3_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __rest
   store_block(gc, Sc, sc, nb, V, valid);
 }
 
+// One axis of the Galerkin product: So = R_a Si R_a^T, with R_a the 1-D full weighting along
+// axis a (weight 1 at distance 0 and 1/2 at distance 1, divided by the coarse node's total: 2
+// inside, 1.5 at either end) and the identity along the other two axes.  The restriction of
+// k_galerkin3_st is the product of the three: its weights are 1/2^d by Manhattan distance d and
+// its totals 8 (3/4)^k with k = the node's end axes, the per-axis factors multiplied out, and
+// its fine index sets are per-axis intervals.  So three passes (x, y, z; FP64 intermediates)
+// give the same R A R^T with at most 7 fine (i, j) pairs per output (node, direction) instead
+// of up to 27 x 8; only the summation order differs.  One thread per (output slot, centre or
+// upper direction nb = 13 + blockIdx.y); padding slots store zeros.  AX: 0 = x, 1 = y, 2 = z.
+template <int AX, typename TI, typename TO>
+__global__ void __launch_bounds__(128)
+k_galerkin3_axis(const Geo gi, const Geo go, const TI* __restrict__ Si, TO* __restrict__ So) {
+  EDGE_PDL_ENTRY();
+  const long long so = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nb = 13 + blockIdx.y;
+  if (so >= go.n) return;
+  const int Kz = (int)(so % go.pz), Ix = (int)((so / go.pz) % go.nx), Jy = (int)(so / go.plane);
+  const int dz = nb % 3 - 1, dx = (nb / 3) % 3 - 1, dy = nb / 9 - 1;
+  const int I[3] = {Ix, Jy, Kz};
+  const int Jn[3] = {Ix + dx, Jy + dy, Kz + dz};
+  const int no[3] = {go.nx, go.ny, go.nz};
+  const int na = AX == 0 ? gi.nx : AX == 1 ? gi.ny : gi.nz;  // input nodes along the axis
+  bool valid = Kz < go.nz;
+  for (int d = 0; d < 3; ++d) valid = valid && Jn[d] >= 0 && Jn[d] < no[d];
+  double V[9];
+  for (int q = 0; q < 9; ++q) V[q] = 0.0;
+  if (valid) {
+    const int Ia = I[AX], Ja = Jn[AX];
+    for (int ia = max(2 * Ia - 1, 0); ia <= min(2 * Ia + 1, na - 1); ++ia) {
+      const double wi = ia == 2 * Ia ? 1.0 : 0.5;
+      int fi[3] = {I[0], I[1], I[2]};
+      fi[AX] = ia;
+      const long long si = gi.slot3(fi[0], fi[1], fi[2]);
+      const int jlo = max(max(2 * Ja - 1, ia - 1), 0), jhi = min(min(2 * Ja + 1, ia + 1), na - 1);
+      for (int ja = jlo; ja <= jhi; ++ja) {
+        const double w = wi * (ja == 2 * Ja ? 1.0 : 0.5);
+        int e[3] = {dx, dy, dz};  // the other axes keep the output direction
+        e[AX] = ja - ia;
+        const int fnb = (e[2] + 1) + 3 * (e[0] + 1) + 9 * (e[1] + 1);
+        for (int c = 0; c < 3; ++c)
+          for (int d = 0; d < 3; ++d) V[c * 3 + d] += w * st_get(gi, Si, si, fnb, c, d);
+      }
+    }
+    const double WI = is_bnd(Ia, no[AX]) ? 1.5 : 2.0, WJ = is_bnd(Ja, no[AX]) ? 1.5 : 2.0;
+    for (int q = 0; q < 9; ++q) V[q] = V[q] / WI / WJ;
+  }
+  store_block(go, So, so, nb, V, valid);
+}
+
 template <typename TS>
 __global__ void __launch_bounds__(128)
 k_galerkin2_st(const Geo gf, const Geo gc, const TS* __restrict__ Sf, TS* __restrict__ Sc) {

@@ -303,6 +303,10 @@ struct Prob {
   std::vector<Level> lv;
   int nd = 0;
   double *Adense = nullptr, *Ainv = nullptr, *Ut = nullptr;
+  // 3-D Galerkin products of the stencil levels as three one-axis passes (k_galerkin3_axis)
+  // through two FP64 intermediates sized for the level 1 -> 2 product; false: k_galerkin3_st
+  bool gal_axis = true;
+  double *gal_t1 = nullptr, *gal_t2 = nullptr;
   int* chol_status = nullptr;
   // PCG (level 0) vectors, FP64 slots
   double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr;
@@ -408,6 +412,18 @@ struct CatScope {
 // The 3-D fine level pads z to 8 nodes so that its BF16 rows (the Jacobi diagonal) are
 // 16-byte aligned TMA sources; coarser levels and 2-D pad to 4.
 static int fine_zalign(int dim, int level) { return (dim == 3 && level == 0) ? 8 : 4; }
+
+// Grids between the one-axis Galerkin passes from gf to gc: x coarsened (g1), then x and y (g2);
+// both keep the fine z padding.
+static void gal_axis_geos(const Geo& gf, const Geo& gc, Geo& g1, Geo& g2) {
+  g1 = gf;
+  g1.nx = gc.nx;
+  g1.plane = (long long)g1.nx * g1.pz;
+  g1.n = (long long)g1.ny * g1.plane;
+  g2 = g1;
+  g2.ny = gc.ny;
+  g2.n = (long long)g2.ny * g2.plane;
+}
 
 static Geo level_geo(const Prob& P, int l) {
   int ne[3] = {P.nel[0], P.nel[1], P.nel[2]};
@@ -1070,7 +1086,15 @@ static void mg_setup(Prob& P) {
     const Geo& gc = P.lv[l + 1].g;
     const int nnb = P.dim == 3 ? 14 : 5;
     dim3 grid(cdiv(gc.n, 128), nnb);
-    if (P.dim == 3)
+    if (P.dim == 3 && P.gal_axis && P.gal_t1) {
+      Geo g1, g2;
+      gal_axis_geos(gf, gc, g1, g2);
+      launch(P, k_galerkin3_axis<0, T, double>, dim3(cdiv(g1.n, 128), nnb), 128, 0, gf, g1, (const T*)P.lv[l].S,
+             P.gal_t1);
+      launch(P, k_galerkin3_axis<1, double, double>, dim3(cdiv(g2.n, 128), nnb), 128, 0, g1, g2,
+             (const double*)P.gal_t1, P.gal_t2);
+      launch(P, k_galerkin3_axis<2, double, T>, grid, 128, 0, g2, gc, (const double*)P.gal_t2, (T*)P.lv[l + 1].S);
+    } else if (P.dim == 3)
       launch(P, k_galerkin3_st<T>, grid, 128, 0, gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
     else
       launch(P, k_galerkin2_st<T>, grid, 128, 0, gf, gc, (const T*)P.lv[l].S, (T*)P.lv[l + 1].S);
@@ -1358,6 +1382,7 @@ static void vcycle(Prob& P, int l, const T* b, T* out, const TV* dotv, double* d
 // ------------------------------------------------------------------ allocation of the hierarchy
 static void mg_allocate(Prob& P) {
   const int L = P.n_level;
+  P.gal_t1 = P.gal_t2 = nullptr;
   const size_t vb = vbytes(P.prec);
   P.lv.clear();
   P.lv.resize(L + 1);
@@ -1403,6 +1428,12 @@ static void mg_allocate(Prob& P) {
   P.Adense = P.alloc<double>((size_t)P.nd * P.nd);
   P.Ainv = P.alloc<double>((size_t)P.nd * P.nd);
   P.Ut = P.alloc<double>((size_t)P.nd * P.nd);
+  if (P.dim == 3 && L >= 2) {  // the largest stencil product, level 1 -> 2
+    Geo g1, g2;
+    gal_axis_geos(P.lv[1].g, P.lv[2].g, g1, g2);
+    P.gal_t1 = P.alloc<double>((size_t)NST3 * g1.n);
+    P.gal_t2 = P.alloc<double>((size_t)NST3 * g2.n);
+  }
 }
 
 // ------------------------------------------------------------------ PCG
@@ -1723,7 +1754,7 @@ static std::vector<double> graph_key(const Prob& P, double tol, int maxiter, boo
                            P.min_omega, (double)P.cycle_w, (double)P.tile_variant, (double)P.blocks_per_sm,
                            (double)P.st_quad_max, (double)P.n_springs, (double)P.use_tma, (double)P.has_cons,
                            (double)P.st_bf16, (double)P.st_pair, (double)P.st_pair_min, (double)P.st_tile_min,
-                           (double)P.res32,
+                           (double)P.gal_axis, (double)P.res32,
                            (double)P.pdl, (double)P.fuse, (double)P.tail_l0, (double)P.omega_carry, (double)(P.omega_carry && P.omega_started),
                            (double)P.fuse_xr, (double)P.kind_variant[0], (double)P.kind_variant[1],
                            (double)P.kind_variant[2], (double)P.kind_bps[0], (double)P.kind_bps[1], (double)P.kind_bps[2]};
@@ -2370,6 +2401,13 @@ int edge_set_stencil_tiled(edge_problem* p, long long min_slots) {
   API_END
 }
 
+int edge_set_galerkin_axis(edge_problem* p, int enable) {
+  API_BEGIN
+  if (!p) fail(EDGE_EINVAL, "null handle");
+  p->P.gal_axis = enable != 0;
+  API_END
+}
+
 int edge_set_coarse_bf16(edge_problem* p, int enable) {
   API_BEGIN
   if (!p) fail(EDGE_EINVAL, "null handle");
@@ -2883,7 +2921,7 @@ int edge_mg_config(edge_problem* p, int n_level, int n_smooth, double omega, dou
         }
       }
     }
-    for (void* q : {(void*)P.Adense, (void*)P.Ainv, (void*)P.Ut}) {
+    for (void* q : {(void*)P.Adense, (void*)P.Ainv, (void*)P.Ut, (void*)P.gal_t1, (void*)P.gal_t2}) {
       if (!q) continue;
       auto it = std::find(P.allocs.begin(), P.allocs.end(), q);
       if (it != P.allocs.end()) {

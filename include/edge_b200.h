@@ -160,6 +160,11 @@ int edge_set_stencil_pair(edge_problem* p, long long min_slots);
  * off (k_st3_apply2 on the linear BF16 copy).  Default 200000.  Levels already allocated get
  * their copy at this call. */
 int edge_set_stencil_tiled(edge_problem* p, long long min_slots);
+/* 3-D: enable != 0 (default) forms the Galerkin operators of levels >= 2 (A_{l+1} = R A_l R^T)
+ * as three one-axis passes through FP64 intermediates, the restriction being the product of
+ * three 1-D full weightings; 0: one direct pass over the fine neighbourhoods.  Same operator,
+ * summed in another order. */
+int edge_set_galerkin_axis(edge_problem* p, int enable);
 /* Mixed precision only: enable != 0 applies the coarse-level stencils (levels >= 1, below the
  * coarsest) from BF16 copies made after each Galerkin set-up (half the bytes of the largest
  * coarse kernel); the Jacobi diagonals and the Galerkin chain stay FP32.  Default 1 (at 12.8M
