@@ -316,8 +316,8 @@ __global__ void k_stencil_tiled_bf16(long long n, const float* __restrict__ S, u
 // slots of the pair in one instruction).  Same terms as k_st3_apply2 summed in the same order
 // (each block row: a v0, + b v1, + d v2, then added to the sum), with the packed instructions'
 // own rounding of each step.
-// The x += omega D^-1 (b - A x) sweep is held to 64 registers (8 blocks per SM instead of 6;
-// 4 bytes of spill).
+// The x += omega D^-1 (b - A x) sweep is held to 64 registers (8 blocks per SM instead of 7
+// at its unbounded 71; 4 bytes of spill).
 template <class Epi> struct StTiledMinBlocks {
   static constexpr int value = 1;
 };
